@@ -1,0 +1,220 @@
+/*
+ * lym.h -- C ABI of the B200 (sm_100a) implementation of the TfLeonardYM
+ * Wilson-fermion / SU(N) gauge hot path.
+ *
+ * Conventions shared by every entry point
+ * ---------------------------------------
+ *  - Device buffers are plain CUDA device pointers in the reference's own
+ *    layouts (emanueleusai/TfLeonardYM):
+ *        spinor  complex128 (ns, N, V)       dirac.py:458-523
+ *        gauge   complex128 (nd, N, N, V)    lattice.py:7 (Configuration)
+ *        force / momenta  same as gauge      hmc.py:59-96, gauge_action.py:13-24
+ *    with the site index lexicographic, LAST coordinate fastest
+ *    (lattice.py:107-114).  complex128 = two interleaved doubles.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *    Work is enqueued on it; calls that return host scalars synchronise it.
+ *  - Every function returns an lym_status; lym_last_error() gives the text
+ *    of the last failure on the calling thread.
+ *  - The boundary condition is the reference's "factor on the last time
+ *    slice of the last direction's links" (boundary_conditions.py:10-46),
+ *    given as (bc_re, bc_im); (1, 0) is periodic, (-1, 0) antiperiodic.
+ *  - Nothing here allocates device memory except the *_create functions and
+ *    solver calls, which cache their workspaces in the object they belong to.
+ */
+#ifndef LYM_H
+#define LYM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum lym_status {
+  LYM_OK = 0,
+  LYM_ERR_BAD_ARG = 1,       /* null pointer, bad size or enum value               */
+  LYM_ERR_BAD_SHAPE = 2,     /* mirrors algebra_utils.py:6-7 RuntimeError           */
+  LYM_ERR_UNSUPPORTED = 3,   /* mirrors dirac.py:299-300 (nd without fermions), etc */
+  LYM_ERR_NOT_CONVERGED = 4, /* solver hit max steps; last iterate returned,
+                                as dirac_solver.py:52-53,109-110 do                */
+  LYM_ERR_CUDA = 5,          /* CUDA runtime error (text in lym_last_error)         */
+  LYM_ERR_OOM = 6,           /* device allocation failed                            */
+  LYM_ERR_REJECTED = 7,      /* serving admission refused (HBM budget)              */
+  LYM_ERR_TIMEOUT = 8        /* a bounded device wait ran out                       */
+} lym_status;
+
+typedef enum lym_precision {
+  LYM_PREC_F64 = 0,
+  LYM_PREC_F32 = 1,
+  LYM_PREC_F16 = 2, /* norm-scaled half spinors, FP32 arithmetic */
+  LYM_PREC_BF16 = 3 /* norm-scaled bfloat16 spinors, FP32 arithmetic */
+} lym_precision;
+
+/* ------------------------------------------------------------------ */
+/* library                                                             */
+/* ------------------------------------------------------------------ */
+int lym_version(void);
+const char* lym_last_error(void);
+const char* lym_status_string(int status);
+
+/* ------------------------------------------------------------------ */
+/* lattice runtime (host, no GPU needed)                               */
+/* ------------------------------------------------------------------ */
+
+/* Neighbour tables sup/sdn and coordinates, each int64 (nd, V), bit-exact
+ * with lattice.py:86-120 (mth_lookup_tables). */
+int lym_lookup_tables(int nd, const int64_t* dims, int64_t* sup, int64_t* sdn, int64_t* coords);
+
+/* complex128 (V,) field: factor where x_{nd-1} = L_{nd-1}-1, else 1
+ * (boundary_conditions.py:10-20, set_antiperiodic_field_in_t_direction). */
+int lym_antiperiodic_field(int nd, const int64_t* dims, double factor_re, double factor_im,
+                           double* field);
+
+/* ------------------------------------------------------------------ */
+/* lattice object on the current device                                */
+/* ------------------------------------------------------------------ */
+typedef struct lym_lattice lym_lattice;
+
+/* Uploads int32 neighbour tables (lattice.py:86-120) and, when every extent
+ * is even, the even-odd maps (builder-defined).  Replaces the per-process
+ * translate.set_translate(False, geometry, grid) binding (translate.py:9-36). */
+int lym_lattice_create(int nd, const int64_t* dims, lym_lattice** out);
+int lym_lattice_destroy(lym_lattice* lat);
+/* int64 device copies of sup/sdn (nd, V) for bit-exact checking. */
+int lym_lattice_tables_device(const lym_lattice* lat, int64_t* sup_dev, int64_t* sdn_dev, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* Wilson Dirac operator, reference layout, FP64                       */
+/* ------------------------------------------------------------------ */
+
+/* out = D in, or Q in = gamma_d D in when hermitian != 0, with
+ * D psi = psi + kappa sum_mu [U_mu(x)(1-g_mu)psi(x+mu) + U_mu(x-mu)^dag(1+g_mu)psi(x-mu)].
+ * Replaces DiracWilsonOperator.multiply_in_fundamental_representation /
+ * simple_multiply_in_fundamental_representation + apply_hermiticity
+ * (dirac.py:458-523, 649-662).  nd in {2, 4}; nd = 3 is builder-defined
+ * (Pauli gammas, no reference counterpart).  `in` and `out` must not alias. */
+int lym_wilson_apply(const lym_lattice* lat, int nc, double kappa, int hermitian,
+                     double bc_re, double bc_im, const void* gauge,
+                     const void* in, void* out, void* stream);
+
+/* Batched form: nvec spinors stored back to back (nvec, ns, N, V). */
+int lym_wilson_apply_batch(const lym_lattice* lat, int nc, double kappa, int hermitian,
+                           double bc_re, double bc_im, const void* gauge, int nvec,
+                           const void* in, void* out, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* vector algebra on complex128 arrays of n elements                   */
+/* ------------------------------------------------------------------ */
+
+/* result[0..1] (host) = sum conj(a) b  (algebra_utils.py:5-11 dot + lattice.py:375 global_sum).
+ * Synchronises `stream`. */
+int lym_cdot(int64_t n, const void* a, const void* b, double* result, void* stream);
+/* y = a*x + b*y with complex a, b (re, im pairs). */
+int lym_caxpby(int64_t n, const double* a, const void* x, const double* b, void* y, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* gauge objects for the solvers                                       */
+/* ------------------------------------------------------------------ */
+typedef struct lym_gauge lym_gauge;
+
+/* Converts a reference-layout gauge field (with the boundary factor) into
+ * the solver's even-odd layouts: FP64 18-real with the boundary factor
+ * folded in, plus the sloppy precisions in `prec_mask` (bit p = lym_precision
+ * p) with 12-real SU(3) / 4-real SU(2) reconstruction and the boundary factor
+ * applied at load time.  Replaces DiracWilsonOperator.set_gauge_configuration
+ * (dirac.py:351-378).  Needs every extent even.  The lattice must outlive it. */
+int lym_gauge_create(const lym_lattice* lat, int nc, const void* gauge, double bc_re, double bc_im,
+                     unsigned prec_mask, void* stream, lym_gauge** out);
+/* Refreshes the internal copies from a new reference-layout field (same lattice). */
+int lym_gauge_update(lym_gauge* g, const void* gauge, void* stream);
+int lym_gauge_destroy(lym_gauge* g);
+
+typedef struct lym_solver_params {
+  double tol;        /* target true relative residual |b - D x| / |b|          */
+  int max_iter;      /* iteration cap (counted in operator applications of M^dag M) */
+  int precision;     /* lym_precision of the inner (sloppy) iterations          */
+  double delta;      /* reliable-update trigger: sloppy |r| fell by this factor  */
+  int hermitian;     /* 1: system is Q x = b with Q = gamma_d D                  */
+  int chunk;         /* iterations per captured CUDA graph launch (0 = default)  */
+} lym_solver_params;
+
+typedef struct lym_solver_report {
+  int status;            /* lym_status of this right-hand side                  */
+  int iterations;        /* inner iterations                                     */
+  int reliable_updates;  /* FP64 residual recomputations                         */
+  double true_residual;  /* FP64 |b - D x| / |b| of the returned x               */
+} lym_solver_report;
+
+/* Solve D x_i = b_i (or Q x_i = b_i) for nrhs right-hand sides stored back to
+ * back in reference layout (nrhs, ns, N, V), by even-odd Schur preconditioning
+ * (M = 1 - kappa^2 H_eo H_oe, builder-defined: the reference has no even-odd)
+ * and CG on M^dag M with FP64 reliable updates.  The reference's own solvers
+ * (dirac_solver.py) reach the same x up to tolerance.  `reports` has nrhs
+ * entries.  Returns LYM_ERR_NOT_CONVERGED if any rhs missed tol. */
+int lym_wilson_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x,
+                     const lym_solver_params* params, lym_solver_report* reports, void* stream);
+
+/* Multishift CG on (Q^2 + sigma_k) x_k = b over the full lattice, FP64
+ * (nshift, ns, N, V) solutions.  Replaces multishift_solver.solve on a
+ * SquareOperator(DiracWilsonOperator) (dirac_solver.py:19-53) for positive
+ * shifts; stops when every shift's residual is below tol * |b|. */
+int lym_multishift_solve(lym_gauge* g, double kappa, int nshift, const double* shifts,
+                         const void* b, void* xs, double tol, int max_iter,
+                         int* iterations, void* stream);
+
+/* The reference's multishift MMMR itself (dirac_solver.py:19-53): base shift
+ * shifts[nshift-1], alpha = omega <p,r>/<p,p>, absolute stop |<r,r>| < precision.
+ * *steps receives the step index the reference prints. FP64, full lattice. */
+int lym_mmmr_solve(lym_gauge* g, double kappa, int nshift, const double* shifts,
+                   const void* b, void* xs, int max_steps, double precision, double omega,
+                   int* steps, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* gauge side (reference layout, FP64)                                 */
+/* ------------------------------------------------------------------ */
+
+/* force = Wilson gauge force -beta/(4N)(W^dag - W), traceless, W = U S^dag with
+ * S the staple sum over all planes (gauge_action.py:13-24,42-101).  When
+ * `momenta` is not NULL the force is not stored; instead momenta += eps*force
+ * (hmc.py:59-61 fused).  `force` may then be NULL. */
+int lym_gauge_force(const lym_lattice* lat, int nc, double beta, const void* gauge,
+                    void* force, void* momenta, double eps, void* stream);
+
+/* staples (nd, N, N, V) with direction `no_direction` excluded (-1: none)
+ * (staples.py:23-58, gauge_action.py:56-101). */
+int lym_staples(const lym_lattice* lat, int nc, const void* gauge, int no_direction,
+                void* staples, void* stream);
+
+/* out[0] (host) = sum_{x, mu<nu} Re Tr P_mu,nu(x); out[1] = Im (gauge_action.py:110-113
+ * summed as in measurements.py:22-43 and gauge_action.py:26-39).  Synchronises. */
+int lym_plaquette_sum(const lym_lattice* lat, int nc, const void* gauge, double* out, void* stream);
+
+/* out (host) = -Re sum Tr P^2 (hmc.py:170-176).  Synchronises. */
+int lym_momenta_energy(int nd, int nc, int64_t volume, const void* momenta, double* out, void* stream);
+
+/* momenta += eps * force (hmc.py:59-61); n = nd*N*N*V complex elements. */
+int lym_update_momenta(int64_t n, void* momenta, const void* force, double eps, void* stream);
+
+/* gauge <- expm(eps P) gauge per link (hmc.py:40-43), in place.  SU(2)/SU(3)
+ * closed forms; reunitarize != 0 projects the result back onto SU(N). */
+int lym_update_links(int nd, int nc, int64_t volume, void* gauge, const void* momenta,
+                     double eps, int reunitarize, void* stream);
+
+/* out = X (X^dag X)^{-1/2} / det^{1/N} per link (smearing.py:17-31). */
+int lym_unitary_projection(int nd, int nc, int64_t volume, const void* in, void* out, void* stream);
+
+/* force += scale * sum_i alpha_i [L(X_i, Y_i) + L(Y_i, X_i)] when symmetric != 0,
+ * else force += scale * sum_i alpha_i L(X_i, Y_i), with L the Lie derivative of
+ * dirac.py:525-565 (fundamental) and X, Y stored (nterms, ns, N, V).
+ * The fused form of n_flavor.force (fermion_action.py:64-93). */
+int lym_fermion_force(const lym_lattice* lat, int nc, double kappa, int hermitian,
+                      double bc_re, double bc_im, const void* gauge, int nterms,
+                      const double* alphas, const void* X, const void* Y, int symmetric,
+                      double scale, void* force, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LYM_H */

@@ -1,0 +1,292 @@
+"""Generate golden vectors by running the unmodified reference on CPU.
+
+Test infrastructure only.  Run in the build container (where the reference
+tree is mounted read-only at /root/reference):
+
+    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py --case d2  # one case
+
+Each case runs in its own subprocess because the reference binds its
+lookup tables at import time (``from translate import lookup_tables`` in
+boundary_conditions.py:3, hmc.py:2, staples.py:2, measurements.py:4), so one
+process can hold one geometry only.  The reference runs on the numpy-backed
+``tensorflow`` stand-in in ``tfshim/``; all randomness comes from that
+stand-in's seeded generator and is saved next to the outputs, so the oracle
+and the GPU path can be fed the identical inputs.
+
+Harness-side deviations from the shipped reference scripts (the reference
+files themselves are never modified):
+  * the boundary-condition provider takes one argument, as
+    dirac.py:369 calls it (tests.py:17-25 passes two and crashes);
+  * ``hmc.metropolis`` is replaced by the same rule (metropolis.py:11-18)
+    with a uniform drawn from a seeded generator on every call and saved;
+  * ``dirac_solver.print`` is captured to record solver iteration counts
+    (dirac_solver.py:49,102).
+"""
+import argparse
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE = "/root/reference"
+
+CASES = {
+    # BASELINE config-1 geometry: D=2 24x16 SU(2), kappa=-0.15, beta=3.0
+    "d2": dict(geometry=(24, 16), nc=2, kappa=-0.15, beta=3.0, seed=11,
+               hmc_steps=[4, 3], n_traj=10, shifts=[0.5, 0.1, 0.01]),
+    # 4D SU(3) on an asymmetric small lattice, kappa=0.13, beta=5.6
+    "d4": dict(geometry=(2, 4, 4, 6), nc=3, kappa=0.13, beta=5.6, seed=12,
+               hmc_steps=[2, 2], n_traj=1, shifts=[0.5, 0.1, 0.01]),
+    # extra (D, N) combinations: operator application only
+    "d4su2": dict(geometry=(4, 4, 2, 4), nc=2, kappa=0.12, beta=2.3, seed=13,
+                  apply_only=True),
+    "d2su3": dict(geometry=(6, 8), nc=3, kappa=0.11, beta=5.0, seed=14,
+                  apply_only=True),
+}
+
+TABLE_GEOMETRIES = [(2, 4, 6, 8), (3, 5, 2, 4), (4, 6, 8), (5, 7), (8, 8), (1, 4, 2, 2)]
+
+
+def _setup_reference(geometry):
+    sys.path.insert(0, REFERENCE)
+    sys.path.insert(0, os.path.join(HERE, "tfshim"))
+    import metropolis
+    metropolis.set_metropolis(False)
+    import translate
+    translate.set_translate(False, list(geometry), [1] * len(geometry))
+    import boundary_conditions
+    boundary_conditions.set_antiperiodic_field_in_t_direction(tuple(geometry))
+
+
+class _IterLog:
+    """Collects the iteration counts the reference solvers print."""
+
+    def __init__(self):
+        self.records = []
+
+    def __call__(self, *args, **_kw):
+        msg = " ".join(str(a) for a in args)
+        m = re.search(r"(MMMRMultishiftsolver|BiconjugateGradient): (convergence|failed to find convergence) after (\d+) steps", msg)
+        if m:
+            self.records.append((m.group(1), m.group(2) == "convergence", int(m.group(3))))
+
+    def take(self):
+        out, self.records = self.records, []
+        return out
+
+
+def run_tables():
+    out = {}
+    for geom in TABLE_GEOMETRIES:
+        code = (
+            "import sys, numpy as np\n"
+            f"sys.path.insert(0, {REFERENCE!r}); sys.path.insert(0, {os.path.join(HERE, 'tfshim')!r})\n"
+            "import lattice as lt\n"
+            f"t = lt.mth_lookup_tables({tuple(geom)!r})\n"
+            "import translate\n"
+            f"translate.set_translate(False, {list(geom)!r}, {[1] * len(geom)!r})\n"
+            "import boundary_conditions as bc\n"
+            f"bc.set_antiperiodic_field_in_t_direction({tuple(geom)!r})\n"
+            "np.savez(sys.argv[1], sup=np.asarray(t.sup), sdn=np.asarray(t.sdn),"
+            " coords=np.asarray(t.global_coordinates), bc=np.asarray(bc.antiperiodic_field_in_t_direction))\n"
+        )
+        tmp = os.path.join(HERE, "_tmp_tables.npz")
+        subprocess.run([sys.executable, "-c", code, tmp], check=True)
+        with np.load(tmp) as z:
+            key = "x".join(str(g) for g in geom)
+            for k in z.files:
+                out[f"{key}/{k}"] = z[k]
+        os.remove(tmp)
+    np.savez_compressed(os.path.join(HERE, "tables.npz"), **out)
+    print("wrote tables.npz", len(out), "arrays")
+
+
+def run_case(name):
+    spec = CASES[name]
+    geometry = spec["geometry"]
+    nd, nc = len(geometry), spec["nc"]
+    _setup_reference(geometry)
+    import tensorflow as tf
+    tf.set_seed(spec["seed"])
+    np.random.seed(spec["seed"])
+
+    import boundary_conditions
+    import dirac
+    import dirac_solver
+    import hmc
+    import gauge_action
+    import staples
+    import measurements
+    import fermion_action
+    import smearing
+    import algebra_utils
+
+    log = _IterLog()
+    dirac_solver.print = log
+
+    def bc_anti(x):
+        return boundary_conditions.apply_antiboundary_conditions_in_t_direction(x)
+
+    def bc_periodic(x):
+        return x
+
+    out = {}
+    kappa, beta = spec["kappa"], spec["beta"]
+    cfg = hmc.hotstart(list(geometry), nc, nd)
+    out["gauge"] = np.asarray(cfg.gauge_field)
+    ns = 2 if nd == 2 else 4
+    eta = hmc.generate_random_vector(nc, ns)
+    eta2 = hmc.generate_random_vector(nc, ns)
+    out["eta"], out["eta2"] = np.asarray(eta), np.asarray(eta2)
+
+    # dirac.py:458-523,649-662 -- all (hermitian, bc, mode) combinations
+    for herm in (False, True):
+        for bcname, prov in (("periodic", bc_periodic), ("anti", bc_anti)):
+            op = dirac.DiracWilsonOperator(cfg, kappa, herm, representation="fundamental",
+                                           boundary_condition_provider=prov)
+            out[f"apply/h{int(herm)}/{bcname}/projected"] = np.asarray(op.multiply_in_fundamental_representation(eta))
+            if herm and bcname == "anti":
+                out[f"apply/h{int(herm)}/{bcname}/simple"] = np.asarray(
+                    op.simple_multiply_in_fundamental_representation(eta))
+    out["dot/eta_eta2"] = np.asarray(algebra_utils.dot(eta, eta2))
+    out["plaquette"] = np.asarray(measurements.plaquette(cfg).value)
+
+    ym = gauge_action.yang_mills(cfg, beta)
+    out["gauge_force"] = np.asarray(ym.force())
+    out["gauge_energy"] = np.asarray(ym.energy())
+    st = gauge_action._get_staple_fields(cfg, no_direction=nd)
+    out["staples_all"] = np.asarray([np.sum([np.asarray(s) for s in elem], axis=0) for elem in st])
+    if nd > 3:
+        st3 = staples.get_staple_fields(cfg)  # default no_direction=3 (staples.py:23)
+        out["staples_no3"] = np.asarray([np.sum([np.asarray(s) for s in elem], axis=0) if elem else
+                                         np.zeros((nc, nc, cfg.gauge_field.shape[-1]), complex) for elem in st3])
+
+    mom = hmc.random_momenta(nc, nd)
+    out["momenta"] = np.asarray(mom)
+    out["momenta_energy"] = np.asarray(hmc.momenta_energy(mom))
+    out["update_link_field/eps"] = np.asarray(0.1)
+    out["update_link_field"] = np.asarray(hmc.update_link_field(cfg.gauge_field, mom, 0.1))
+    out["update_momenta"] = np.asarray(hmc.update_momenta(mom, out["gauge_force"], -0.05))
+    gauss = tf.complex(tf.random.normal(shape=(nd, nc, nc, cfg.gauge_field.shape[-1]), dtype=tf.float64),
+                       tf.random.normal(shape=(nd, nc, nc, cfg.gauge_field.shape[-1]), dtype=tf.float64))
+    out["unitary_in"] = np.asarray(gauss)
+    out["unitary_out"] = np.asarray(smearing.unitary_sqrt_projection(gauss))
+
+    Q = dirac.DiracWilsonOperator(cfg, kappa, True, representation="fundamental", boundary_condition_provider=bc_anti)
+    out["lie_derivative"] = np.asarray(Q.lie_derivative(eta, eta2))
+
+    if spec.get("apply_only"):
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print("wrote", name)
+        return
+
+    # dirac_solver.py:19-53 multishift MMMR on Q^2 (absolute |r|^2 stop), tests.py:96-106
+    Q2 = dirac.SquareOperator(Q)
+    shifts = spec["shifts"]
+    sols = dirac_solver.multishift_solver(2000, 1e-11).solve(Q2, eta, shifts)
+    out["mmmr/shifts"] = np.asarray(shifts)
+    out["mmmr/precision"] = np.asarray(1e-11)
+    out["mmmr/solutions"] = np.asarray([np.asarray(s) for s in sols])
+    rec = log.take()
+    out["mmmr/iterations"] = np.asarray([r[2] for r in rec])
+    # dirac_solver.py:61-110 BiCGStab on Q^2 + 0.01, tests.py:108-113
+    bic = dirac_solver.biconjugate_gradient(2000, 1e-11).solve(dirac.ShiftedOperator(Q2, shifts[-1]), eta)
+    out["bicgstab/solution"] = np.asarray(bic)
+    out["bicgstab/iterations"] = np.asarray([r[2] for r in log.take()])
+
+    # Nf=2 fundamental: fermion_action.py with R(Q^2) = (Q^2)^-1 and heatbath = Q
+    solver = dirac_solver.multishift_solver(5000, 1e-22)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(Q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [Q], solver, Q)
+    nf.set_gauge_configuration(cfg)
+    nf.initialize_pseudofermions([eta])
+    out["nf2/phi"] = np.asarray(nf.pseudofermions[0])
+    out["nf2/energy"] = np.asarray(nf.energy())
+    out["nf2/force"] = np.asarray(nf.force())
+    log.take()
+
+    # hmc.py:218-278 -- trajectories with harness-supplied momenta / eta / uniform
+    rng = np.random.default_rng(spec["seed"] + 1000)
+    state = {}
+
+    orig_random_momenta = hmc.random_momenta
+
+    def recording_momenta(ncol, ndim):
+        m = orig_random_momenta(ncol, ndim)
+        state.setdefault("momenta", []).append(np.asarray(m))
+        return m
+
+    def recording_metropolis(new_energy, old_energy):
+        u = rng.uniform()
+        state.setdefault("uniform", []).append(u)
+        if new_energy < old_energy:
+            return True
+        return bool(u < np.exp(-(new_energy - old_energy)))
+
+    hmc.random_momenta = recording_momenta
+    hmc.metropolis = recording_metropolis
+    actions = [nf, ym]
+
+    # one molecular-dynamics trajectory, hmc.py:133-162, outputs kept
+    md_mom = orig_random_momenta(nc, nd)
+    nf.set_gauge_configuration(cfg)
+    nf.initialize_pseudofermions([eta])
+    md_cfg, md_p = hmc.integrate_om(cfg, md_mom, actions, spec["hmc_steps"], 1.0)
+    out["md/momenta_in"] = np.asarray(md_mom)
+    out["md/cfg_out"] = np.asarray(md_cfg.gauge_field)
+    out["md/momenta_out"] = np.asarray(md_p)
+    out["md/iterations"] = np.asarray(sum(r[2] for r in log.take()))
+
+    traj = {"dH": [], "accepted": [], "plaquette": [], "iterations": [], "eta": []}
+    out["hmc/steps"] = np.asarray(spec["hmc_steps"])
+    cur = cfg
+    for _ in range(spec["n_traj"]):
+        e = hmc.generate_random_vector(nc, ns)
+        traj["eta"].append(np.asarray(e))
+        nf.set_gauge_configuration(cur)
+        nf.initialize_pseudofermions([e])
+        cur, minus_dh, acc = hmc.hybrid_mc(cur, actions, spec["hmc_steps"], 1.0)
+        traj["dH"].append(-float(np.real(minus_dh)))
+        traj["accepted"].append(bool(acc))
+        traj["plaquette"].append(float(measurements.plaquette(cur).value))
+        traj["iterations"].append(sum(r[2] for r in log.take()))
+    for k, v in traj.items():
+        out[f"hmc/{k}"] = np.asarray(v)
+    out["hmc/momenta"] = np.asarray(state["momenta"])
+    out["hmc/uniform"] = np.asarray(state["uniform"])
+    out["hmc/cfg_out"] = np.asarray(cur.gauge_field)
+
+    # hmc.py:249-278 reversibility on the final configuration
+    hmc.random_momenta = recording_momenta
+    nf.set_gauge_configuration(cur)
+    nf.initialize_pseudofermions([traj["eta"][0]])
+    state["momenta"] = []
+    out["hmc/reversibility_dH"] = np.asarray(hmc.reversibility_check(cur, actions, spec["hmc_steps"], 1.0))
+    out["hmc/reversibility_momenta"] = np.asarray(state["momenta"][0])
+    log.take()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print("wrote", name)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default=None)
+    ap.add_argument("--inproc", action="store_true")
+    args = ap.parse_args()
+    if args.case and args.inproc:
+        if args.case == "tables":
+            run_tables()
+        else:
+            run_case(args.case)
+        return
+    names = [args.case] if args.case else ["tables"] + list(CASES)
+    for n in names:
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc"], check=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,57 @@
+"""C-ABI checks that need no GPU: the library loads, exports every symbol the
+header declares, and its host-side table builders are bit-exact with the
+reference's lattice.py:86-120 / boundary_conditions.py:10-20 (golden tables)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from tests.conftest import ROOT, load_golden
+from tfleonardym_b200 import _lib
+
+HEADER = os.path.join(ROOT, "include", "lym.h")
+
+
+def header_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lym_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.lib()
+    syms = header_symbols()
+    assert len(syms) >= 25
+    for s in syms:
+        assert hasattr(lib, s), s
+    # and the ctypes signature table covers exactly the header
+    assert set(syms) == set(_lib.SIGNATURES)
+
+
+def test_version_and_status_strings():
+    lib = _lib.lib()
+    assert lib.lym_version() >= 10000
+    assert lib.lym_status_string(_lib.LYM_ERR_NOT_CONVERGED) == b"not converged"
+
+
+def test_host_tables_bit_exact():
+    z = load_golden("tables")
+    for key in sorted({k.split("/")[0] for k in z}):
+        geom = tuple(int(g) for g in key.split("x"))
+        sup, sdn, coords = _lib.host_lookup_tables(geom)
+        np.testing.assert_array_equal(sup, z[f"{key}/sup"])
+        np.testing.assert_array_equal(sdn, z[f"{key}/sdn"])
+        np.testing.assert_array_equal(coords, z[f"{key}/coords"])
+        np.testing.assert_array_equal(_lib.host_antiperiodic_field(geom), z[f"{key}/bc"])
+
+
+def test_bad_arguments_are_rejected():
+    lib = _lib.lib()
+    dims = _lib.dims_array((4, 4))
+    assert lib.lym_lookup_tables(0, dims, None, None, None) == _lib.LYM_ERR_BAD_ARG
+    assert lib.lym_lookup_tables(2, dims, None, None, None) == _lib.LYM_ERR_BAD_ARG
+    bad = _lib.dims_array((4, 0))
+    out = np.empty((2, 16), np.int64)
+    assert lib.lym_lookup_tables(2, bad, out.ctypes.data, None, None) == _lib.LYM_ERR_BAD_ARG
+    assert b"extent" in lib.lym_last_error()

@@ -1,0 +1,305 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's golden
+vectors and the pinned CPU oracle, on identical inputs.
+
+Tolerances: integer tables bit-exact; FP64 straight-line kernels 1e-13
+relative (summation order only); solver outputs against the tolerance they
+were solved to.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import lym_oracle as O
+from tests.conftest import GOLDEN_CASES, load_golden, relerr
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-13
+
+
+def cu(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def np_(t):
+    return t.detach().cpu().numpy()
+
+
+def make_cfg(gauge, geometry):
+    from tfleonardym_b200 import lattice as lt
+    nd, nc = gauge.shape[0], gauge.shape[1]
+    return lt.Configuration(cu(gauge), tuple(geometry), nc, nd)
+
+
+def make_op(g, spec, hermitian=True, anti=True):
+    from tfleonardym_b200 import boundary_conditions as bc
+    from tfleonardym_b200 import dirac
+    prov = bc.time_antiperiodic_provider(-1) if anti else bc.periodic_provider()
+    return dirac.DiracWilsonOperator(make_cfg(g["gauge"], spec["geometry"]), spec["kappa"], hermitian,
+                                     representation="fundamental", boundary_condition_provider=prov)
+
+
+def test_device_tables_bit_exact(cuda_device):
+    from tfleonardym_b200 import lattice as lt
+    z = load_golden("tables")
+    for key in sorted({k.split("/")[0] for k in z}):
+        geom = tuple(int(g) for g in key.split("x"))
+        sup, sdn = lt.get_lattice(geom).device_tables()
+        np.testing.assert_array_equal(np_(sup), z[f"{key}/sup"])
+        np.testing.assert_array_equal(np_(sdn), z[f"{key}/sdn"])
+
+
+@pytest.mark.parametrize("case", list(GOLDEN_CASES))
+def test_wilson_apply_vs_reference(cuda_device, case):
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    for herm in (0, 1):
+        for bcname in ("periodic", "anti"):
+            op = make_op(g, spec, bool(herm), bcname == "anti")
+            out = np_(op.apply(cu(g["eta"])))
+            assert relerr(out, g[f"apply/h{herm}/{bcname}/projected"]) < TOL, (herm, bcname)
+
+
+def test_wilson_apply_generic_provider(cuda_device):
+    """An arbitrary provider callable is applied to the tensor (dirac.py:368-370)."""
+    from tfleonardym_b200 import boundary_conditions as bc
+    from tfleonardym_b200 import dirac
+    g = load_golden("d2")
+    spec = GOLDEN_CASES["d2"]
+    bc.set_antiperiodic_field_in_t_direction(spec["geometry"])
+    op = dirac.DiracWilsonOperator(make_cfg(g["gauge"], spec["geometry"]), spec["kappa"], True,
+                                   representation="fundamental",
+                                   boundary_condition_provider=lambda x: bc.apply_antiboundary_conditions_in_t_direction(x))
+    assert relerr(np_(op.apply(cu(g["eta"]))), g["apply/h1/anti/projected"]) < TOL
+
+
+@pytest.mark.parametrize("geom,nc", [((4, 6, 4, 8), 3), ((8, 6), 2), ((6, 4, 2, 4), 2), ((10, 6), 3)])
+def test_wilson_apply_vs_oracle_random(cuda_device, geom, nc):
+    rng = np.random.default_rng(sum(geom) + nc)
+    nd = len(geom)
+    vol = int(np.prod(geom))
+    ns = 2 if nd == 2 else 4
+    u = O.unitary_sqrt_projection(rng.normal(size=(nd, nc, nc, vol)) + 1j * rng.normal(size=(nd, nc, nc, vol)))
+    psi = rng.normal(size=(3, ns, nc, vol)) + 1j * rng.normal(size=(3, ns, nc, vol))
+    spec = dict(geometry=geom, kappa=0.137)
+    op = make_op(dict(gauge=u), spec, True, True)
+    out = np_(op.apply(cu(psi)))  # batched over 3 vectors
+    tables = O.lookup_tables(geom)
+    ub = O.apply_time_bc(u, O.antiperiodic_field(geom))
+    for i in range(3):
+        assert relerr(out[i], O.wilson_apply(ub, psi[i], 0.137, True, tables)) < TOL
+
+
+def test_unsupported_dimension_raises(cuda_device):
+    from tfleonardym_b200 import dirac
+    g = np.zeros((3, 2, 2, 64), complex)
+    with pytest.raises(RuntimeError, match="not supported for fermions"):
+        dirac.DiracWilsonOperator(make_cfg(g, (4, 4, 4)), 0.1, True, representation="fundamental")
+
+
+def test_dot_and_shape_error(cuda_device):
+    from tfleonardym_b200 import algebra_utils
+    g = load_golden("d4")
+    d = algebra_utils.dot(cu(g["eta"]), cu(g["eta2"]))
+    assert abs(d - complex(g["dot/eta_eta2"])) < 1e-12 * abs(d)
+    with pytest.raises(RuntimeError, match="Incompatible"):
+        algebra_utils.dot(cu(g["eta"]), cu(g["eta"][:, :, :-1]))
+
+
+@pytest.mark.parametrize("case", list(GOLDEN_CASES))
+def test_gauge_side_vs_reference(cuda_device, case):
+    from tfleonardym_b200 import gauge_action, hmc, measurements, smearing, staples
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    cfg = make_cfg(g["gauge"], spec["geometry"])
+    nd = g["gauge"].shape[0]
+    ym = gauge_action.yang_mills(cfg, spec["beta"])
+    assert relerr(np_(ym.force()), g["gauge_force"]) < TOL
+    assert abs(ym.energy() - g["gauge_energy"]) < 1e-12 * abs(g["gauge_energy"])
+    assert abs(measurements.plaquette(cfg).value - g["plaquette"]) < 1e-14
+    assert relerr(np_(staples.get_staple_fields(cfg, no_direction=nd)), g["staples_all"]) < TOL
+    if "staples_no3" in g:
+        assert relerr(np_(staples.get_staple_fields(cfg)), g["staples_no3"]) < TOL
+    assert abs(hmc.momenta_energy(cu(g["momenta"])) - g["momenta_energy"]) < 1e-12 * abs(g["momenta_energy"])
+    assert relerr(np_(hmc.update_momenta(cu(g["momenta"]), cu(g["gauge_force"]), -0.05)), g["update_momenta"]) < TOL
+    assert relerr(np_(hmc.update_link_field(cu(g["gauge"]), cu(g["momenta"]), 0.1)), g["update_link_field"]) < 1e-13
+    assert relerr(np_(smearing.unitary_sqrt_projection(cu(g["unitary_in"]))), g["unitary_out"]) < 1e-12
+    # fused force + momentum update
+    p = cu(g["momenta"]).clone()
+    ym.force_into_momenta(p, -0.05)
+    assert relerr(np_(p), g["update_momenta"]) < TOL
+
+
+@pytest.mark.parametrize("case", list(GOLDEN_CASES))
+def test_lie_derivative_vs_reference(cuda_device, case):
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    op = make_op(g, spec)
+    assert relerr(np_(op.lie_derivative(cu(g["eta"]), cu(g["eta2"]))), g["lie_derivative"]) < TOL
+
+
+def test_link_update_large_and_small_steps(cuda_device):
+    """exp(eps P) U for eps from 1e-7 to 2 against scipy expm (the oracle)."""
+    from tfleonardym_b200 import hmc
+    g = load_golden("d4")
+    for eps in (1e-7, 1e-3, 0.3, 2.0):
+        out = np_(hmc.update_link_field(cu(g["gauge"]), cu(g["momenta"]), eps))
+        ref = O.update_link_field(g["gauge"], g["momenta"], eps)
+        assert relerr(out, ref) < 1e-13, eps
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_mmmr_vs_reference(cuda_device, case):
+    from tfleonardym_b200 import dirac, dirac_solver
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    op = make_op(g, spec)
+    solver = dirac_solver.multishift_solver(2000, float(g["mmmr/precision"]))
+    sols = solver.solve(dirac.SquareOperator(op), cu(g["eta"]), list(g["mmmr/shifts"]))
+    # same arithmetic as the reference: the printed step agrees (reduction order may move it by one)
+    assert abs(solver.last_steps - int(g["mmmr/iterations"][0])) <= 1
+    for s, ref in zip(sols, g["mmmr/solutions"]):
+        assert relerr(np_(s), ref) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_bicgstab_vs_reference(cuda_device, case):
+    from tfleonardym_b200 import dirac, dirac_solver
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    op = dirac.ShiftedOperator(dirac.SquareOperator(make_op(g, spec)), float(g["mmmr/shifts"][-1]))
+    solver = dirac_solver.biconjugate_gradient(2000, 1e-11)
+    x = solver.solve(op, cu(g["eta"]))
+    assert abs(solver.last_steps - int(g["bicgstab/iterations"][0])) <= 1
+    assert relerr(np_(x), g["bicgstab/solution"]) < 1e-8
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_multishift_cg(cuda_device, case):
+    from tfleonardym_b200 import dirac, dirac_solver
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    op = make_op(g, spec)
+    shifts = list(g["mmmr/shifts"])
+    xs = dirac_solver.multishift_cg(5000, 1e-12).solve(dirac.SquareOperator(op), cu(g["eta"]), shifts)
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    for x, s, ref in zip(xs, shifts, g["mmmr/solutions"]):
+        xn = np_(x)
+        res = np.linalg.norm(setup.Q2(xn) + s * xn - g["eta"]) / np.linalg.norm(g["eta"])
+        assert res < 1e-11, (s, res)
+        assert relerr(xn, ref) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])
+@pytest.mark.parametrize("case", ["d2", "d4", "d4su2", "d2su3"])
+def test_eo_cg_true_residual(cuda_device, case, precision):
+    """D x = b (and Q x = b) by even-odd CG: true residual recomputed by the oracle."""
+    from tfleonardym_b200 import dirac_solver
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    tables = O.lookup_tables(spec["geometry"])
+    ub = O.apply_time_bc(g["gauge"], O.antiperiodic_field(spec["geometry"]))
+    b = np.stack([g["eta"], g["eta2"]])
+    for herm in (False, True):
+        op = make_op(g, spec, herm, True)
+        solver = dirac_solver.conjugate_gradient(tol=1e-10, precision=precision)
+        x = np_(solver.solve(op, cu(b)))
+        for i in range(2):
+            res = np.linalg.norm(b[i] - O.wilson_apply(ub, x[i], spec["kappa"], herm, tables)) / np.linalg.norm(b[i])
+            assert res < 1e-10, (herm, i, res, solver.reports)
+            assert solver.reports[i]["true_residual"] < 1e-10
+
+
+def test_eo_cg_batch_equals_single(cuda_device):
+    """A right-hand side gives the same answer alone and inside a batch."""
+    from tfleonardym_b200 import dirac_solver
+    g = load_golden("d4")
+    spec = GOLDEN_CASES["d4"]
+    op = make_op(g, spec, True, True)
+    b = np.stack([g["eta"], g["eta2"], g["eta"] * 0.5 + 1j * g["eta2"]])
+    for precision in ("f64", "f16"):
+        solver = dirac_solver.conjugate_gradient(tol=1e-10, precision=precision)
+        xb = np_(solver.solve(op, cu(b)))
+        x1 = np_(solver.solve(op, cu(b[1])))
+        assert relerr(xb[1], x1) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_nf2_force_and_energy_vs_reference(cuda_device, case):
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_action
+    dirac_solver.VERBOSE = False
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    q = make_op(g, spec)
+    solver = dirac_solver.multishift_solver(5000, 1e-22)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    nf.initialize_pseudofermions([cu(g["eta"])])
+    assert relerr(np_(nf.pseudofermions[0]), g["nf2/phi"]) < TOL
+    assert abs(nf.energy() - g["nf2/energy"]) < 1e-9 * abs(g["nf2/energy"])
+    assert relerr(np_(nf.force()), g["nf2/force"]) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_md_trajectory_vs_reference(cuda_device, case):
+    """integrate_om (hmc.py:133-162) with the Nf=2 and gauge actions from the golden inputs."""
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_action, gauge_action, hmc
+    dirac_solver.VERBOSE = False
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    q = make_op(g, spec)
+    solver = dirac_solver.multishift_solver(5000, 1e-22)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    cfg = make_cfg(g["gauge"], spec["geometry"])
+    nf.set_gauge_configuration(cfg)
+    nf.initialize_pseudofermions([cu(g["eta"])])
+    ym = gauge_action.yang_mills(cfg, spec["beta"])
+    new_cfg, p = hmc.integrate_om(cfg, cu(g["md/momenta_in"]), [nf, ym], list(g["hmc/steps"]), 1.0)
+    assert relerr(np_(new_cfg.gauge_field), g["md/cfg_out"]) < 1e-9
+    assert relerr(np_(p), g["md/momenta_out"]) < 1e-9
+
+
+def test_hmc_chain_config1(cuda_device):
+    """BASELINE config 1 (D=2 24x16 SU(2), beta=3, kappa=-0.15, antiperiodic time,
+    Omelyan [4,3], t=1): 10 trajectories fed the reference's momenta, eta and
+    uniforms; dH, acceptance and plaquette per trajectory against the reference."""
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_action, gauge_action, hmc, measurements
+    dirac_solver.VERBOSE = False
+    g = load_golden("d2")
+    spec = GOLDEN_CASES["d2"]
+    q = make_op(g, spec)
+    solver = dirac_solver.multishift_solver(5000, 1e-22)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    cfg = make_cfg(g["gauge"], spec["geometry"])
+    ym = gauge_action.yang_mills(cfg, spec["beta"])
+    steps = list(g["hmc/steps"])
+    for k in range(len(g["hmc/dH"])):
+        nf.set_gauge_configuration(cfg)
+        nf.initialize_pseudofermions([cu(g["hmc/eta"][k])])
+        cfg, minus_dh, acc = hmc.hybrid_mc(cfg, [nf, ym], steps, 1.0, momenta=cu(g["hmc/momenta"][k]),
+                                           uniform=float(g["hmc/uniform"][k]))
+        assert abs(-minus_dh - g["hmc/dH"][k]) < 1e-7, k
+        assert acc == bool(g["hmc/accepted"][k])
+        assert abs(measurements.plaquette(cfg).value - g["hmc/plaquette"][k]) < 1e-10
+    assert relerr(np_(cfg.gauge_field), g["hmc/cfg_out"]) < 1e-8
+
+
+def test_reversibility(cuda_device):
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_action, gauge_action, hmc
+    dirac_solver.VERBOSE = False
+    g = load_golden("d2")
+    spec = GOLDEN_CASES["d2"]
+    q = make_op(g, spec)
+    solver = dirac_solver.multishift_solver(5000, 1e-24)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    cfg = make_cfg(g["hmc/cfg_out"], spec["geometry"])
+    nf.set_gauge_configuration(cfg)
+    nf.initialize_pseudofermions([cu(g["hmc/eta"][0])])
+    ym = gauge_action.yang_mills(cfg, spec["beta"])
+    dh = hmc.reversibility_check(cfg, [nf, ym], list(g["hmc/steps"]), 1.0,
+                                 momenta=cu(g["hmc/reversibility_momenta"]))
+    assert abs(dh) < 1e-9
+    assert abs(dh - g["hmc/reversibility_dH"]) < 1e-9

@@ -1,0 +1,132 @@
+"""Pin the CPU oracle to golden vectors produced by the unmodified reference.
+
+Every reference-restating function of ``oracle/lym_oracle.py`` is compared to
+the reference's own outputs on identical inputs (``tests/golden/*.npz``).
+Tolerances: 1e-13 relative for straight-line arithmetic (differences are
+summation order only); bit-exact for the integer tables.
+"""
+import numpy as np
+import pytest
+
+from oracle import lym_oracle as O
+from tests.conftest import GOLDEN_CASES, load_golden, relerr
+
+TOL = 1e-13
+
+
+def test_lookup_tables_bit_exact():
+    z = load_golden("tables")
+    geoms = sorted({k.split("/")[0] for k in z})
+    assert len(geoms) >= 5
+    for key in geoms:
+        geom = tuple(int(g) for g in key.split("x"))
+        sup, sdn, coords = O.lookup_tables(geom)
+        assert sup.dtype == np.int64
+        np.testing.assert_array_equal(sup, z[f"{key}/sup"])
+        np.testing.assert_array_equal(sdn, z[f"{key}/sdn"])
+        np.testing.assert_array_equal(coords, z[f"{key}/coords"])
+        np.testing.assert_array_equal(O.antiperiodic_field(geom), z[f"{key}/bc"])
+
+
+@pytest.mark.parametrize("case", list(GOLDEN_CASES))
+def test_wilson_apply(case):
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    tables = O.lookup_tables(spec["geometry"])
+    bcf = O.antiperiodic_field(spec["geometry"])
+    for herm in (0, 1):
+        for bcname in ("periodic", "anti"):
+            gauge = O.apply_time_bc(g["gauge"], bcf) if bcname == "anti" else g["gauge"]
+            out = O.wilson_apply(gauge, g["eta"], spec["kappa"], bool(herm), tables)
+            assert relerr(out, g[f"apply/h{herm}/{bcname}/projected"]) < TOL
+    # projected == simple in the reference itself (tests.py:51-59)
+    assert relerr(g["apply/h1/anti/simple"], g["apply/h1/anti/projected"]) < TOL
+
+
+@pytest.mark.parametrize("case", list(GOLDEN_CASES))
+def test_gauge_side(case):
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    geom = spec["geometry"]
+    tables = O.lookup_tables(geom)
+    u = g["gauge"]
+    assert relerr(O.dot(g["eta"], g["eta2"]), g["dot/eta_eta2"]) < TOL
+    assert abs(O.plaquette(u, tables) - g["plaquette"]) < 1e-14
+    assert relerr(O.staples(u, tables), g["staples_all"]) < TOL
+    if "staples_no3" in g:
+        assert relerr(O.staples(u, tables, no_direction=3), g["staples_no3"]) < TOL
+    assert relerr(O.gauge_force(u, spec["beta"], tables), g["gauge_force"]) < TOL
+    assert abs(O.gauge_energy(u, spec["beta"], tables) - g["gauge_energy"]) < 1e-12 * abs(g["gauge_energy"])
+    assert abs(O.momenta_energy(g["momenta"]) - g["momenta_energy"]) < 1e-12 * abs(g["momenta_energy"])
+    assert relerr(O.update_link_field(u, g["momenta"], 0.1), g["update_link_field"]) < 1e-13
+    assert relerr(O.update_momenta(g["momenta"], g["gauge_force"], -0.05), g["update_momenta"]) < TOL
+    assert relerr(O.unitary_sqrt_projection(g["unitary_in"]), g["unitary_out"]) < 1e-12
+    bcf = O.antiperiodic_field(geom)
+    ld = O.lie_derivative(O.apply_time_bc(u, bcf), g["eta"], g["eta2"], spec["kappa"], True, tables)
+    assert relerr(ld, g["lie_derivative"]) < TOL
+
+
+def test_momenta_structure():
+    """random_momenta output (hmc.py:69-96) is anti-Hermitian and traceless."""
+    g = load_golden("d4")
+    p = g["momenta"]
+    assert np.abs(p + np.conj(np.transpose(p, (0, 2, 1, 3)))).max() < 1e-15
+    assert np.abs(np.einsum("miic->mc", p)).max() < 1e-15
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_mmmr_and_bicgstab(case):
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    shifts = list(g["mmmr/shifts"])
+    sols, step, ok = O.mmmr_multishift(setup.Q2, g["eta"], shifts, 2000, float(g["mmmr/precision"]))
+    assert ok
+    # the reference prints `step`; identical arithmetic gives the identical count
+    assert step == int(g["mmmr/iterations"][0])
+    for s, ref in zip(sols, g["mmmr/solutions"]):
+        assert relerr(s, ref) < 1e-10
+    x, step_b, ok_b = O.bicgstab(lambda v: setup.Q2(v) + shifts[-1] * v, g["eta"], 2000, 1e-11)
+    assert ok_b and abs(step_b - int(g["bicgstab/iterations"][0])) <= 1
+    assert relerr(x, g["bicgstab/solution"]) < 1e-8
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_nf2_energy_force(case):
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    phi = setup.Q(g["eta"])
+    assert relerr(phi, g["nf2/phi"]) < TOL
+
+    def solve(a, b, shifts):
+        return O.mmmr_multishift(a, b, shifts, 5000, 1e-22)[0]
+
+    e = O.fermion_energy(setup, phi, [1.0], [0.0], solve)
+    assert abs(e - g["nf2/energy"]) < 1e-9 * abs(g["nf2/energy"])
+    f = O.fermion_force(setup, phi, [1.0], [0.0], solve)
+    assert relerr(f, g["nf2/force"]) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["d2", "d4"])
+def test_md_trajectory(case):
+    """integrate_om (hmc.py:133-162) with the Nf=2 and gauge forces."""
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    tables = setup.tables
+    phi = setup.Q(g["eta"])
+
+    def solve(a, b, shifts):
+        return O.mmmr_multishift(a, b, shifts, 5000, 1e-22)[0]
+
+    def f_ferm(u):
+        setup.set_gauge(u)
+        return O.fermion_force(setup, phi, [1.0], [0.0], solve)
+
+    def f_gauge(u):
+        return O.gauge_force(u, spec["beta"], tables)
+
+    u, p = O.integrate_om(g["gauge"], g["md/momenta_in"], [f_ferm, f_gauge], list(g["hmc/steps"]), 1.0)
+    assert relerr(u, g["md/cfg_out"]) < 1e-10
+    assert relerr(p, g["md/momenta_out"]) < 1e-10

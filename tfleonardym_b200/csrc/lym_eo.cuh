@@ -1,0 +1,299 @@
+// Even-odd (checkerboard) layouts and the hopping-term core for the solvers.
+//
+// Ordering (builder-defined; the reference has no even-odd preconditioning):
+// parity(x) = sum_i x_i mod 2; within a parity, sites keep the reference's
+// lexicographic order, so the checkerboard index is lex / 2 (all extents even).
+//
+// Spinor field of one parity, nrhs vectors:  unit[(rhs * nunits + u) * Vh + cb]
+//   FP64 : double2 units, 1 complex each
+//   FP32 : float4 units, 2 complex each
+//   FP16 / BF16 : uint4 units, 4 complex each, plus a float norm per site
+//          (values stored divided by the site's max |re|,|im|)
+// Gauge field: unit[((mu * 2 + parity) * nunits + u) * Vh + cb] holding
+//   U_mu(x) for x of that parity; full N x N, or compressed to the first
+//   N-1 rows (SU(3): 12 reals, third row = conj(row0 x row1); SU(2): 4 reals,
+//   row1 = (-conj(b), conj(a))).  FP64 and full links have the boundary
+//   factor folded in; compressed links get it at load time.
+#pragma once
+
+#include "lym_internal.cuh"
+
+namespace lym {
+
+enum { SP64 = 0, SP32 = 1, SP16 = 2, SPB16 = 3 };
+
+template <int SP> struct Prec;
+template <> struct Prec<SP64> { using real = double; using unit = double2; static constexpr int CPU = 1; };
+template <> struct Prec<SP32> { using real = float; using unit = float4; static constexpr int CPU = 2; };
+template <> struct Prec<SP16> { using real = float; using unit = uint4; static constexpr int CPU = 4; };
+template <> struct Prec<SPB16> { using real = float; using unit = uint4; static constexpr int CPU = 4; };
+
+constexpr int units_for(int ncomplex, int cpu) { return (ncomplex + cpu - 1) / cpu; }
+
+struct EoField {
+  void* data = nullptr;
+  float* norm = nullptr;
+  int nunits = 0;
+  int64_t Vh = 0;
+};
+
+// --- half / bfloat16 packing ------------------------------------------------
+template <int SP> LYM_D unsigned pack2(float a, float b);
+template <> LYM_D unsigned pack2<SP16>(float a, float b) {
+  __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<unsigned*>(&h);
+}
+template <> LYM_D unsigned pack2<SPB16>(float a, float b) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<unsigned*>(&h);
+}
+template <int SP> LYM_D cx<float> unpack2(unsigned w);
+template <> LYM_D cx<float> unpack2<SP16>(unsigned w) {
+  __half2 h = *reinterpret_cast<__half2*>(&w);
+  float2 f = __half22float2(h);
+  return {f.x, f.y};
+}
+template <> LYM_D cx<float> unpack2<SPB16>(unsigned w) {
+  __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&w);
+  float2 f = __bfloat1622float2(h);
+  return {f.x, f.y};
+}
+
+// --- spinor load / store ------------------------------------------------------
+template <int SP, int NCOMP>
+LYM_D void load_sp(const EoField& f, int rhs, int64_t cb, cx<typename Prec<SP>::real> (&v)[NCOMP]) {
+  using U = typename Prec<SP>::unit;
+  const U* base = reinterpret_cast<const U*>(f.data) + (int64_t)rhs * f.nunits * f.Vh + cb;
+  if constexpr (SP == SP64) {
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c) {
+      double2 t = __ldg(base + c * f.Vh);
+      v[c] = {t.x, t.y};
+    }
+  } else if constexpr (SP == SP32) {
+#pragma unroll
+    for (int u = 0; u < units_for(NCOMP, 2); ++u) {
+      float4 t = __ldg(base + u * f.Vh);
+      v[2 * u] = {t.x, t.y};
+      if (2 * u + 1 < NCOMP) v[2 * u + 1] = {t.z, t.w};
+    }
+  } else {
+    const float nrm = __ldg(f.norm + (int64_t)rhs * f.Vh + cb);
+#pragma unroll
+    for (int u = 0; u < units_for(NCOMP, 4); ++u) {
+      uint4 t = __ldg(base + u * f.Vh);
+      const unsigned w[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (4 * u + k < NCOMP) v[4 * u + k] = nrm * unpack2<SP>(w[k]);
+    }
+  }
+}
+
+template <int SP, int NCOMP>
+LYM_D void store_sp(const EoField& f, int rhs, int64_t cb, const cx<typename Prec<SP>::real> (&v)[NCOMP]) {
+  using U = typename Prec<SP>::unit;
+  U* base = reinterpret_cast<U*>(f.data) + (int64_t)rhs * f.nunits * f.Vh + cb;
+  if constexpr (SP == SP64) {
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c) base[c * f.Vh] = make_double2(v[c].re, v[c].im);
+  } else if constexpr (SP == SP32) {
+#pragma unroll
+    for (int u = 0; u < units_for(NCOMP, 2); ++u) {
+      cx<float> b = (2 * u + 1 < NCOMP) ? v[2 * u + 1] : cx<float>{0.f, 0.f};
+      base[u * f.Vh] = make_float4(v[2 * u].re, v[2 * u].im, b.re, b.im);
+    }
+  } else {
+    float m = 0.f;
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c) m = fmaxf(m, fmaxf(fabsf(v[c].re), fabsf(v[c].im)));
+    const float inv = m > 0.f ? 1.0f / m : 0.f;
+    f.norm[(int64_t)rhs * f.Vh + cb] = m;
+#pragma unroll
+    for (int u = 0; u < units_for(NCOMP, 4); ++u) {
+      unsigned w[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        cx<float> c = (4 * u + k < NCOMP) ? v[4 * u + k] : cx<float>{0.f, 0.f};
+        w[k] = pack2<SP>(c.re * inv, c.im * inv);
+      }
+      base[u * f.Vh] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+// --- gauge load -----------------------------------------------------------
+// GP: storage precision (SP64 double2, SP32 float4, SP16 uint2 of 2 half2)
+// COMP: compressed to N-1 rows
+template <int GP> struct GPrec;
+template <> struct GPrec<SP64> { using real = double; using unit = double2; static constexpr int CPU = 1; };
+template <> struct GPrec<SP32> { using real = float; using unit = float4; static constexpr int CPU = 2; };
+template <> struct GPrec<SP16> { using real = float; using unit = uint2; static constexpr int CPU = 2; };
+
+template <int NC, bool COMP> constexpr int link_complex() { return COMP ? (NC - 1) * NC : NC * NC; }
+
+template <int GP, int NC, bool COMP>
+LYM_D void load_link_eo(const void* g, int nunits, int64_t Vh, int mu, int par, int64_t cb,
+                        cx<typename GPrec<GP>::real> (&u)[NC][NC]) {
+  using R = typename GPrec<GP>::real;
+  using U = typename GPrec<GP>::unit;
+  constexpr int NCX = link_complex<NC, COMP>();
+  const U* base = reinterpret_cast<const U*>(g) + ((int64_t)(mu * 2 + par) * nunits) * Vh + cb;
+  cx<R> e[NCX];
+  if constexpr (GP == SP64) {
+#pragma unroll
+    for (int k = 0; k < NCX; ++k) {
+      double2 t = __ldg(base + k * Vh);
+      e[k] = {t.x, t.y};
+    }
+  } else if constexpr (GP == SP32) {
+#pragma unroll
+    for (int k = 0; k < units_for(NCX, 2); ++k) {
+      float4 t = __ldg(base + k * Vh);
+      e[2 * k] = {t.x, t.y};
+      if (2 * k + 1 < NCX) e[2 * k + 1] = {t.z, t.w};
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < units_for(NCX, 2); ++k) {
+      uint2 t = __ldg(base + k * Vh);
+      e[2 * k] = unpack2<SP16>(t.x);
+      if (2 * k + 1 < NCX) e[2 * k + 1] = unpack2<SP16>(t.y);
+    }
+  }
+  if constexpr (!COMP) {
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) u[i][j] = e[i * NC + j];
+  } else if constexpr (NC == 2) {
+    u[0][0] = e[0];
+    u[0][1] = e[1];
+    u[1][0] = -conj(e[1]);
+    u[1][1] = conj(e[0]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      u[0][j] = e[j];
+      u[1][j] = e[3 + j];
+    }
+    u[2][0] = conj(u[0][1] * u[1][2] - u[0][2] * u[1][1]);
+    u[2][1] = conj(u[0][2] * u[1][0] - u[0][0] * u[1][2]);
+    u[2][2] = conj(u[0][0] * u[1][1] - u[0][1] * u[1][0]);
+  }
+}
+
+// --- geometry of the checkerboard ------------------------------------------
+struct EoGeom {
+  int nd;
+  int dims[4];
+  int stride[4];  // lexicographic strides (last coordinate fastest)
+  int Lh;         // dims[nd-1] / 2
+  int64_t Vh;
+};
+
+// coordinates and lexicographic index of checkerboard site (cb, parity)
+template <int ND>
+LYM_D int64_t eo_coords(const EoGeom& g, int64_t cb, int par, int (&x)[ND]) {
+  const int Lt = g.dims[ND - 1];
+  int64_t row = cb / g.Lh;
+  const int th = (int)(cb - row * g.Lh);
+  int64_t r = row;
+  int sum = 0;
+#pragma unroll
+  for (int d = ND - 2; d >= 0; --d) {
+    x[d] = (int)(r % g.dims[d]);
+    r /= g.dims[d];
+    sum += x[d];
+  }
+  x[ND - 1] = 2 * th + ((par + sum) & 1);
+  return row * Lt + x[ND - 1];
+}
+
+template <int ND>
+LYM_D int64_t nb_fwd(const EoGeom& g, int64_t lex, const int (&x)[ND], int mu) {
+  return (x[mu] == g.dims[mu] - 1) ? lex - (int64_t)(g.dims[mu] - 1) * g.stride[mu] : lex + g.stride[mu];
+}
+template <int ND>
+LYM_D int64_t nb_bwd(const EoGeom& g, int64_t lex, const int (&x)[ND], int mu) {
+  return (x[mu] == 0) ? lex + (int64_t)(g.dims[mu] - 1) * g.stride[mu] : lex - g.stride[mu];
+}
+
+// --- hopping term -----------------------------------------------------------
+struct HopGauge {
+  const void* data;
+  int nunits;
+  double bcr, bci;  // boundary factor applied at load time (compressed links only)
+};
+
+// acc = sum_mu [U_mu(x)(1-g_mu) psi(x+mu) + U_mu(x-mu)^dag (1+g_mu) psi(x-mu)]
+// for x of parity `par`; psi is the opposite-parity field.  G5IN: psi is
+// replaced by gamma_d psi (lower spin components negated) on load.
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN>
+LYM_D void hop_site(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs, int64_t cb, int par,
+                    cx<typename Prec<SP>::real> (&acc)[Gamma<ND>::NS][NC]) {
+  using R = typename Prec<SP>::real;
+  using GR = typename GPrec<GP>::real;
+  constexpr int NS = Gamma<ND>::NS;
+  int x[ND];
+  const int64_t lex = eo_coords<ND>(g, cb, par, x);
+#pragma unroll
+  for (int a = 0; a < NS; ++a)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[a][c] = czero<R>();
+#pragma unroll
+  for (int mu = 0; mu < ND; ++mu) {
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      const bool fwd = dir == 0;
+      const int64_t nlex = fwd ? nb_fwd<ND>(g, lex, x, mu) : nb_bwd<ND>(g, lex, x, mu);
+      const int64_t ncb = nlex >> 1;
+      cx<GR> ug[NC][NC];
+      // forward link lives on x (parity par), backward link on x - mu (parity 1-par)
+      load_link_eo<GP, NC, COMP>(hg.data, hg.nunits, g.Vh, mu, fwd ? par : 1 - par, fwd ? cb : ncb, ug);
+      cx<R> u[NC][NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) u[i][j] = {(R)ug[i][j].re, (R)ug[i][j].im};
+      if (COMP && mu == ND - 1 && x[ND - 1] == (fwd ? g.dims[ND - 1] - 1 : 0)) {
+        const cx<R> bc{(R)hg.bcr, (R)hg.bci};
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+#pragma unroll
+          for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
+      }
+      cx<R> psi[NS * NC];
+      load_sp<SP, NS * NC>(in, rhs, ncb, psi);
+      if (G5IN) {
+#pragma unroll
+        for (int k = (NS / 2) * NC; k < NS * NC; ++k) psi[k] = -psi[k];
+      }
+      const R sgn = fwd ? R(1) : R(-1);
+#pragma unroll
+      for (int a = 0; a < NS / 2; ++a) {
+        const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+        cx<R> h[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) h[c] = psi[a * NC + c] - sgn * mul_phase(ph, psi[jb * NC + c]);
+        // lower row factor: -s conj(g_a)
+        const int lph = fwd ? phase_neg(phase_conj(ph)) : phase_conj(ph);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+          cx<R> t = czero<R>();
+          if (fwd) {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) t += u[i][j] * h[j];
+          } else {
+#pragma unroll
+            for (int j = 0; j < NC; ++j) t += cmul_cj(u[j][i], h[j]);
+          }
+          acc[a][i] += t;
+          acc[jb][i] += mul_phase(lph, t);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace lym

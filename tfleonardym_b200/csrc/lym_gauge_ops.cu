@@ -1,0 +1,580 @@
+// Gauge-side kernels in the reference layout (FP64): staples and gauge force
+// (fused with the momentum update), plaquette and momenta energy reductions,
+// the link update exp(eps P) U, polar reunitarisation and the fused per-link
+// fermion force.  One thread per link (site, direction); every neighbour link
+// is read straight from the gauge field through the reference's sup/sdn
+// tables -- no shifted copies are materialised (gauge_action.py:56-91 builds
+// five gathered copies per plane instead).
+#include "lym_internal.cuh"
+#include "lym_kernels.cuh"
+#include "lym_su.cuh"
+
+#include <mutex>
+
+namespace lym {
+
+// ---------------------------------------------------------------------------
+// staples: S_mu(x) = sum_{nu != mu} U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag
+//                               + U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu)
+// (gauge_action.py:56-101, staples.py:13-58)
+// ---------------------------------------------------------------------------
+template <int ND, int NC>
+LYM_D Mat<NC> staple_sum(const int32_t* __restrict__ tab, int64_t V, const double2* __restrict__ U, int mu,
+                         int64_t s, int no_dir) {
+  Mat<NC> S = mzero<NC>();
+#pragma unroll
+  for (int nu = 0; nu < ND; ++nu) {
+    if (nu == mu || nu == no_dir) continue;
+    const int64_t xmu = tab[mu * V + s];
+    const int64_t xnu = tab[nu * V + s];
+    const int64_t xmnu = tab[ND * V + nu * V + s];
+    const int64_t xmnu_pmu = tab[mu * V + xmnu];
+    Mat<NC> a = mul(load_link<NC>(U, nu, s, V), load_link<NC>(U, mu, xnu, V));
+    madd(S, mul_nd(a, load_link<NC>(U, nu, xmu, V)));
+    Mat<NC> b = mul_dn(load_link<NC>(U, nu, xmnu, V), load_link<NC>(U, mu, xmnu, V));
+    madd(S, mul(b, load_link<NC>(U, nu, xmnu_pmu, V)));
+  }
+  return S;
+}
+
+template <int ND, int NC>
+__global__ void __launch_bounds__(128) staples_kernel(const int32_t* __restrict__ tab, int64_t V,
+                                                      const double2* __restrict__ U, int no_dir,
+                                                      double2* __restrict__ out) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (s >= V) return;
+  Mat<NC> S = (mu == no_dir) ? mzero<NC>() : staple_sum<ND, NC>(tab, V, U, mu, s, no_dir);
+  store_link<NC>(out, mu, s, V, S);
+}
+
+// F = -beta/(4N) (W^dag - W) - trace/N, W = U S^dag (gauge_action.py:42-53).
+// With mom != null: mom += eps F instead of storing F (hmc.py:59-61).
+template <int ND, int NC>
+__global__ void __launch_bounds__(128) gauge_force_kernel(const int32_t* __restrict__ tab, int64_t V,
+                                                          const double2* __restrict__ U, double beta,
+                                                          double2* __restrict__ force, double2* __restrict__ mom,
+                                                          double eps) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (s >= V) return;
+  Mat<NC> S = staple_sum<ND, NC>(tab, V, U, mu, s, -1);
+  Mat<NC> W = mul_nd(load_link<NC>(U, mu, s, V), S);
+  const double c = -0.25 * beta / NC;
+  Mat<NC> F;
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) F.m[i][j] = c * (conj(W.m[j][i]) - W.m[i][j]);
+  cx<double> tr = trace(F);
+  tr = (1.0 / NC) * tr;
+#pragma unroll
+  for (int i = 0; i < NC; ++i) F.m[i][i] -= tr;
+  if (mom) {
+    Mat<NC> P = load_link<NC>(mom, mu, s, V);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) P.m[i][j] += eps * F.m[i][j];
+    store_link<NC>(mom, mu, s, V, P);
+  } else {
+    store_link<NC>(force, mu, s, V, F);
+  }
+}
+
+// sum_{x, mu<nu} Tr U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag (gauge_action.py:110-113)
+template <int ND, int NC>
+__global__ void __launch_bounds__(256) plaquette_kernel(const int32_t* __restrict__ tab, int64_t V,
+                                                        const double2* __restrict__ U, double* partials,
+                                                        unsigned* counter, double* result) {
+  __shared__ double sh[2 * 32];
+  double v[2] = {0.0, 0.0};
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < V; s += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int mu = 0; mu < ND; ++mu)
+#pragma unroll
+      for (int nu = mu + 1; nu < ND; ++nu) {
+        Mat<NC> a = mul(load_link<NC>(U, mu, s, V), load_link<NC>(U, nu, tab[mu * V + s], V));
+        Mat<NC> b = mul(load_link<NC>(U, nu, s, V), load_link<NC>(U, mu, tab[nu * V + s], V));
+        // Tr(a b^dag)
+        cx<double> t = czero<double>();
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+#pragma unroll
+          for (int k = 0; k < NC; ++k) t += a.m[i][k] * conj(b.m[i][k]);
+        v[0] += t.re;
+        v[1] += t.im;
+      }
+  }
+  if (grid_sum<2>(v, partials, counter, sh) && threadIdx.x == 0) {
+    result[0] = v[0];
+    result[1] = v[1];
+  }
+}
+
+// -Re sum Tr P^2 (hmc.py:170-176)
+template <int NC>
+__global__ void __launch_bounds__(256) momenta_energy_kernel(int64_t nlinks, int64_t V,
+                                                             const double2* __restrict__ P, double* partials,
+                                                             unsigned* counter, double* result) {
+  __shared__ double sh[32];
+  double v[1] = {0.0};
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < nlinks; l += (int64_t)gridDim.x * blockDim.x) {
+    const int mu = (int)(l / V);
+    const int64_t s = l - mu * V;
+    Mat<NC> p = load_link<NC>(P, mu, s, V);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) v[0] -= (p.m[i][j] * p.m[j][i]).re;
+  }
+  if (grid_sum<1>(v, partials, counter, sh) && threadIdx.x == 0) result[0] = v[0];
+}
+
+__global__ void axpy_real_kernel(int64_t n, double2* __restrict__ y, const double2* __restrict__ x, double a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double2 yv = y[i], xv = x[i];
+    y[i] = make_double2(yv.x + a * xv.x, yv.y + a * xv.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// exp of an anti-Hermitian matrix (the HMC momenta, hmc.py:69-96)
+// ---------------------------------------------------------------------------
+
+// sin(w)/w with its series near zero
+LYM_D double sinc(double w) {
+  if (fabs(w) < 0.05) {
+    double w2 = w * w;
+    return 1.0 - w2 / 6.0 * (1.0 - w2 / 20.0 * (1.0 - w2 / 42.0 * (1.0 - w2 / 72.0)));
+  }
+  return sin(w) / w;
+}
+
+// exp(X) for 2x2 X = t 1 + X0, X0 traceless: X0^2 = -det(X0) 1 (Cayley-Hamilton),
+// so exp(X0) = cos(a) 1 + sinc(a) X0 with a^2 = det(X0) (>= 0 for anti-Hermitian X0).
+LYM_D Mat<2> expm(const Mat<2>& X) {
+  cx<double> t = 0.5 * trace(X);
+  Mat<2> X0 = X;
+  X0.m[0][0] -= t;
+  X0.m[1][1] -= t;
+  double a2 = det(X0).re;
+  double a = sqrt(fmax(a2, 0.0));
+  double c = cos(a), sc = sinc(a);
+  Mat<2> R;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) R.m[i][j] = sc * X0.m[i][j];
+  R.m[0][0].re += c;
+  R.m[1][1].re += c;
+  // exp(t) with t = i phi for anti-Hermitian X (real part kept for generality)
+  double e = exp(t.re), sn, cs;
+  sincos(t.im, &sn, &cs);
+  return mscale(cx<double>{e * cs, e * sn}, R);
+}
+
+// exp(X) for 3x3 anti-Hermitian X: X = t 1 + i Q with Q Hermitian traceless,
+// exp(i Q) = f0 + f1 Q + f2 Q^2 with the closed-form coefficients of
+// Morningstar & Peardon, Phys. Rev. D 69 (2004) 054501, eqs. (23)-(34).
+LYM_D Mat<3> expm(const Mat<3>& X) {
+  cx<double> t = (1.0 / 3.0) * trace(X);
+  Mat<3> Q;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      cx<double> x = X.m[i][j];
+      if (i == j) x -= t;
+      Q.m[i][j] = {x.im, -x.re};  // -i x
+    }
+  Mat<3> Q2 = mul(Q, Q);
+  const double c1 = 0.5 * trace(Q2).re;
+  cx<double> f0, f1, f2;
+  if (c1 < 1e-12) {
+    // exp(iQ) = 1 + iQ - Q^2/2 + O(|Q|^3) with |Q| < 1e-6
+    f0 = {1.0, 0.0};
+    f1 = {0.0, 1.0};
+    f2 = {-0.5, 0.0};
+  } else {
+    double c0 = det(Q).re;
+    const bool neg = c0 < 0;
+    if (neg) c0 = -c0;
+    const double c0max = 2.0 * pow(c1 / 3.0, 1.5);
+    double ratio = c0 / c0max;
+    ratio = fmin(1.0, fmax(-1.0, ratio));
+    const double theta = acos(ratio);
+    double st3, ct3;
+    sincos(theta / 3.0, &st3, &ct3);
+    const double u = sqrt(c1 / 3.0) * ct3;
+    const double w = sqrt(c1) * st3;
+    const double u2 = u * u, w2 = w * w;
+    double s2u, c2u, su, cu;
+    sincos(2.0 * u, &s2u, &c2u);
+    sincos(u, &su, &cu);
+    const cx<double> e2iu{c2u, s2u}, emiu{cu, -su};
+    const double cw = cos(w), xi0 = sinc(w);
+    cx<double> h0 = (u2 - w2) * e2iu + emiu * cx<double>{8.0 * u2 * cw, 2.0 * u * (3.0 * u2 + w2) * xi0};
+    cx<double> h1 = (2.0 * u) * e2iu - emiu * cx<double>{2.0 * u * cw, -(3.0 * u2 - w2) * xi0};
+    cx<double> h2 = e2iu - emiu * cx<double>{cw, 3.0 * u * xi0};
+    const double d = 1.0 / (9.0 * u2 - w2);
+    f0 = d * h0;
+    f1 = d * h1;
+    f2 = d * h2;
+    if (neg) {  // f_j(-c0) = (-1)^j conj(f_j(c0))
+      f0 = conj(f0);
+      f1 = -conj(f1);
+      f2 = conj(f2);
+    }
+  }
+  Mat<3> R;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) R.m[i][j] = f1 * Q.m[i][j] + f2 * Q2.m[i][j];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) R.m[i][i] += f0;
+  double e = exp(t.re), sn, cs;
+  sincos(t.im, &sn, &cs);
+  return mscale(cx<double>{e * cs, e * sn}, R);
+}
+
+// Unitary polar factor by the scaled Newton iteration
+// U <- (g U + U^{-dag} / g) / 2, g = |det U|^{-1/N} (Higham, "Functions of
+// Matrices", sec. 8.6), then division by the principal det^{1/N}
+// (smearing.py:17-31 computes X (X^dag X)^{-1/2} / det^{1/N} via sqrtm).
+template <int NC>
+LYM_D Mat<NC> polar_su(const Mat<NC>& X) {
+  Mat<NC> Uk = X;
+  for (int it = 0; it < 40; ++it) {
+    cx<double> d = det(Uk);
+    double g = pow(sqrt(norm2(d)), -1.0 / NC);
+    Mat<NC> Z = mdag(inverse(Uk));
+    Mat<NC> Un;
+    double diff = 0.0;
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) {
+        Un.m[i][j] = 0.5 * (g * Uk.m[i][j] + (1.0 / g) * Z.m[i][j]);
+        diff += norm2(Un.m[i][j] - Uk.m[i][j]);
+      }
+    Uk = Un;
+    if (diff < 1e-30) break;
+  }
+  cx<double> r = principal_root(det(Uk), NC);
+  cx<double> ir = cdiv(cx<double>{1.0, 0.0}, r);
+  return mscale(ir, Uk);
+}
+
+template <int NC>
+__global__ void __launch_bounds__(128) update_links_kernel(int64_t nlinks, int64_t V, double2* __restrict__ U,
+                                                           const double2* __restrict__ P, double eps, int reunit) {
+  const int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (l >= nlinks) return;
+  const int mu = (int)(l / V);
+  const int64_t s = l - mu * V;
+  Mat<NC> p = load_link<NC>(P, mu, s, V);
+  Mat<NC> e = expm(mscale(cx<double>{eps, 0.0}, p));
+  Mat<NC> r = mul(e, load_link<NC>(U, mu, s, V));
+  if (reunit) r = polar_su<NC>(r);
+  store_link<NC>(U, mu, s, V, r);
+}
+
+template <int NC>
+__global__ void __launch_bounds__(128) unitary_projection_kernel(int64_t nlinks, int64_t V,
+                                                                 const double2* __restrict__ in,
+                                                                 double2* __restrict__ out) {
+  const int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (l >= nlinks) return;
+  const int mu = (int)(l / V);
+  const int64_t s = l - mu * V;
+  store_link<NC>(out, mu, s, V, polar_su<NC>(load_link<NC>(in, mu, s, V)));
+}
+
+// ---------------------------------------------------------------------------
+// fermion force (dirac.py:525-565, fermion_action.py:64-93)
+//
+// For link (mu, x), with V_m = U_mu(x) Y_m(x+mu) (colour matvec per spin row m):
+//   A = sum_m conj(X_m(x)) (x) (P+ V)_m ,  B = sum_m conj(V_m) (x) (P- X(x))_m
+//   L(X, Y)_{ut} = kappa/2 [A_{tu} - B_{tu} - delta_{ut} (Tr A - Tr B)/N]
+// which is the reference's sum over generators T^k_{ij} T^k_{ut} written with
+// the SU(N) completeness relation sum_k T^k_ij T^k_ut = (d_it d_ju - d_ij d_ut/N)/2.
+// P+- = (1 -+ gamma_mu), multiplied by gamma_d when hermitian.
+// ---------------------------------------------------------------------------
+constexpr int kMaxForceTerms = 64;
+struct ForceTerms {
+  double alpha[kMaxForceTerms];
+};
+
+// (1 - s gamma_mu) v, optionally times gamma_d, for the reference basis
+template <int ND, int NC, bool HERM>
+LYM_D void project_full(int mu, double sgn, const cx<double> (&v)[Gamma<ND>::NS][NC],
+                        cx<double> (&o)[Gamma<ND>::NS][NC]) {
+  constexpr int NS = Gamma<ND>::NS;
+#pragma unroll
+  for (int a = 0; a < NS / 2; ++a) {
+    const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      cx<double> up = v[a][c] - sgn * mul_phase(ph, v[jb][c]);
+      cx<double> lo = v[jb][c] - sgn * mul_phase(phase_conj(ph), v[a][c]);
+      o[a][c] = up;
+      o[jb][c] = HERM ? -lo : lo;
+    }
+  }
+}
+
+template <int ND, int NC, bool HERM>
+LYM_D void lie_term(int mu, const Mat<NC>& U, const cx<double> (&X)[Gamma<ND>::NS][NC],
+                    const cx<double> (&Ysup)[Gamma<ND>::NS][NC], Mat<NC>& A, Mat<NC>& B) {
+  constexpr int NS = Gamma<ND>::NS;
+  cx<double> Vv[NS][NC], PV[NS][NC], PX[NS][NC];
+#pragma unroll
+  for (int m = 0; m < NS; ++m)
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+      cx<double> t = czero<double>();
+#pragma unroll
+      for (int l = 0; l < NC; ++l) t += U.m[i][l] * Ysup[m][l];
+      Vv[m][i] = t;
+    }
+  project_full<ND, NC, HERM>(mu, 1.0, Vv, PV);
+  project_full<ND, NC, HERM>(mu, -1.0, X, PX);
+#pragma unroll
+  for (int m = 0; m < NS; ++m)
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) {
+        A.m[i][j] += cmul_cj(X[m][i], PV[m][j]);
+        B.m[i][j] += cmul_cj(Vv[m][i], PX[m][j]);
+      }
+}
+
+template <int ND, int NC, bool HERM>
+__global__ void __launch_bounds__(128) fermion_force_kernel(
+    const int32_t* __restrict__ tab, int64_t V, int Lt, double kappa, double bcr, double bci,
+    const double2* __restrict__ U, int nterms, ForceTerms terms, const double2* __restrict__ X,
+    const double2* __restrict__ Y, int symmetric, double scale, double2* __restrict__ force) {
+  constexpr int NS = Gamma<ND>::NS;
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (s >= V) return;
+  const int64_t y = tab[mu * V + s];
+  Mat<NC> u = load_link<NC>(U, mu, s, V);
+  if (mu == ND - 1 && (s % Lt) == Lt - 1) u = mscale(cx<double>{bcr, bci}, u);
+  Mat<NC> F = mzero<NC>();
+  const int64_t vec = (int64_t)NS * NC * V;
+  for (int k = 0; k < nterms; ++k) {
+    const double2* Xk = X + k * vec;
+    const double2* Yk = Y + k * vec;
+    cx<double> xs[NS][NC], ysup[NS][NC];
+#pragma unroll
+    for (int m = 0; m < NS; ++m)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        xs[m][c] = ld(Xk + (m * NC + c) * V + s);
+        ysup[m][c] = ld(Yk + (m * NC + c) * V + y);
+      }
+    Mat<NC> A = mzero<NC>(), B = mzero<NC>();
+    lie_term<ND, NC, HERM>(mu, u, xs, ysup, A, B);
+    if (symmetric) {
+#pragma unroll
+      for (int m = 0; m < NS; ++m)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          xs[m][c] = ld(Yk + (m * NC + c) * V + s);
+          ysup[m][c] = ld(Xk + (m * NC + c) * V + y);
+        }
+      lie_term<ND, NC, HERM>(mu, u, xs, ysup, A, B);
+    }
+    const double w = 0.5 * kappa * terms.alpha[k];
+    cx<double> tr = (1.0 / NC) * (trace(A) - trace(B));
+#pragma unroll
+    for (int uu = 0; uu < NC; ++uu)
+#pragma unroll
+      for (int tt = 0; tt < NC; ++tt) {
+        cx<double> v = A.m[tt][uu] - B.m[tt][uu];
+        if (uu == tt) v -= tr;
+        F.m[uu][tt] += w * v;
+      }
+  }
+  Mat<NC> out = load_link<NC>(force, mu, s, V);
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) out.m[i][j] += scale * F.m[i][j];
+  store_link<NC>(force, mu, s, V, out);
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+// ---------------------------------------------------------------------------
+#define LYM_DISPATCH_ND_NC(nd, nc, CALL)                                              \
+  do {                                                                                \
+    if ((nd) == 2 && (nc) == 2) { constexpr int ND = 2, NC = 2; CALL; }               \
+    else if ((nd) == 2 && (nc) == 3) { constexpr int ND = 2, NC = 3; CALL; }          \
+    else if ((nd) == 3 && (nc) == 2) { constexpr int ND = 3, NC = 2; CALL; }          \
+    else if ((nd) == 3 && (nc) == 3) { constexpr int ND = 3, NC = 3; CALL; }          \
+    else if ((nd) == 4 && (nc) == 2) { constexpr int ND = 4, NC = 2; CALL; }          \
+    else if ((nd) == 4 && (nc) == 3) { constexpr int ND = 4, NC = 3; CALL; }          \
+    else { set_error("unsupported (nd=%d, N=%d)", (nd), (nc)); return LYM_ERR_UNSUPPORTED; } \
+  } while (0)
+
+}  // namespace lym
+
+using namespace lym;
+
+extern "C" {
+
+int lym_staples(const lym_lattice* lat, int nc, const void* gauge, int no_direction, void* staples,
+                void* stream) {
+  LYM_REQUIRE(lat && gauge && staples, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(gauge != staples, LYM_ERR_BAD_ARG, "gauge and staples must not alias");
+  dim3 grid(grid_for(lat->V, 128), lat->nd);
+  cudaStream_t st = (cudaStream_t)stream;
+  LYM_DISPATCH_ND_NC(lat->nd, nc, (staples_kernel<ND, NC><<<grid, 128, 0, st>>>(
+                                      lat->d_tab, lat->V, (const double2*)gauge, no_direction, (double2*)staples)));
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+int lym_gauge_force(const lym_lattice* lat, int nc, double beta, const void* gauge, void* force, void* momenta,
+                    double eps, void* stream) {
+  LYM_REQUIRE(lat && gauge && (force || momenta), LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(gauge != force && gauge != momenta, LYM_ERR_BAD_ARG, "outputs must not alias the gauge field");
+  dim3 grid(grid_for(lat->V, 128), lat->nd);
+  cudaStream_t st = (cudaStream_t)stream;
+  LYM_DISPATCH_ND_NC(lat->nd, nc, (gauge_force_kernel<ND, NC><<<grid, 128, 0, st>>>(
+                                      lat->d_tab, lat->V, (const double2*)gauge, beta, (double2*)force,
+                                      (double2*)momenta, eps)));
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+int lym_plaquette_sum(const lym_lattice* lat, int nc, const void* gauge, double* out, void* stream) {
+  LYM_REQUIRE(lat && gauge && out, LYM_ERR_BAD_ARG, "null argument");
+  Scratch* s;
+  int rc = scratch_get(&s);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(host_reduce_mutex());
+  const int slot = 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned nb = reduction_blocks(lat->V, 256);
+  double* part = s->partials + (size_t)slot * Scratch::kMaxBlocks * Scratch::kMaxVals;
+  double* res = s->results + slot * Scratch::kMaxVals;
+  LYM_DISPATCH_ND_NC(lat->nd, nc, (plaquette_kernel<ND, NC><<<nb, 256, 0, st>>>(
+                                      lat->d_tab, lat->V, (const double2*)gauge, part, s->counters + slot, res)));
+  LYM_CHECK_LAUNCH();
+  LYM_CUDA(cudaMemcpyAsync(s->host + slot * Scratch::kMaxVals, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  LYM_CUDA(cudaStreamSynchronize(st));
+  out[0] = s->host[slot * Scratch::kMaxVals];
+  out[1] = s->host[slot * Scratch::kMaxVals + 1];
+  return LYM_OK;
+}
+
+int lym_momenta_energy(int nd, int nc, int64_t volume, const void* momenta, double* out, void* stream) {
+  LYM_REQUIRE(momenta && out && nd >= 1 && nd <= LYM_MAX_ND && volume >= 0, LYM_ERR_BAD_ARG, "bad argument");
+  LYM_REQUIRE(nc == 2 || nc == 3, LYM_ERR_UNSUPPORTED, "N must be 2 or 3");
+  Scratch* s;
+  int rc = scratch_get(&s);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(host_reduce_mutex());
+  const int slot = 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t nl = (int64_t)nd * volume;
+  unsigned nb = reduction_blocks(nl, 256);
+  double* part = s->partials + (size_t)slot * Scratch::kMaxBlocks * Scratch::kMaxVals;
+  double* res = s->results + slot * Scratch::kMaxVals;
+  if (nc == 2)
+    momenta_energy_kernel<2><<<nb, 256, 0, st>>>(nl, volume, (const double2*)momenta, part, s->counters + slot, res);
+  else
+    momenta_energy_kernel<3><<<nb, 256, 0, st>>>(nl, volume, (const double2*)momenta, part, s->counters + slot, res);
+  LYM_CHECK_LAUNCH();
+  LYM_CUDA(cudaMemcpyAsync(s->host + slot * Scratch::kMaxVals, res, sizeof(double), cudaMemcpyDeviceToHost, st));
+  LYM_CUDA(cudaStreamSynchronize(st));
+  out[0] = s->host[slot * Scratch::kMaxVals];
+  return LYM_OK;
+}
+
+int lym_update_momenta(int64_t n, void* momenta, const void* force, double eps, void* stream) {
+  LYM_REQUIRE(n >= 0 && momenta && force, LYM_ERR_BAD_ARG, "null argument");
+  if (n == 0) return LYM_OK;
+  axpy_real_kernel<<<reduction_blocks(n, 256) * 4, 256, 0, (cudaStream_t)stream>>>(n, (double2*)momenta,
+                                                                                     (const double2*)force, eps);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+int lym_update_links(int nd, int nc, int64_t volume, void* gauge, const void* momenta, double eps, int reunitarize,
+                     void* stream) {
+  LYM_REQUIRE(gauge && momenta && nd >= 1 && nd <= LYM_MAX_ND && volume >= 0, LYM_ERR_BAD_ARG, "bad argument");
+  if (volume == 0) return LYM_OK;
+  const int64_t nl = (int64_t)nd * volume;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nc == 2)
+    update_links_kernel<2><<<grid_for(nl, 128), 128, 0, st>>>(nl, volume, (double2*)gauge,
+                                                              (const double2*)momenta, eps, reunitarize);
+  else if (nc == 3)
+    update_links_kernel<3><<<grid_for(nl, 128), 128, 0, st>>>(nl, volume, (double2*)gauge,
+                                                              (const double2*)momenta, eps, reunitarize);
+  else {
+    set_error("N=%d not supported", nc);
+    return LYM_ERR_UNSUPPORTED;
+  }
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+int lym_unitary_projection(int nd, int nc, int64_t volume, const void* in, void* out, void* stream) {
+  LYM_REQUIRE(in && out && nd >= 1 && nd <= LYM_MAX_ND && volume >= 0, LYM_ERR_BAD_ARG, "bad argument");
+  if (volume == 0) return LYM_OK;
+  const int64_t nl = (int64_t)nd * volume;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nc == 2)
+    unitary_projection_kernel<2><<<grid_for(nl, 128), 128, 0, st>>>(nl, volume, (const double2*)in, (double2*)out);
+  else if (nc == 3)
+    unitary_projection_kernel<3><<<grid_for(nl, 128), 128, 0, st>>>(nl, volume, (const double2*)in, (double2*)out);
+  else {
+    set_error("N=%d not supported", nc);
+    return LYM_ERR_UNSUPPORTED;
+  }
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+int lym_fermion_force(const lym_lattice* lat, int nc, double kappa, int hermitian, double bc_re, double bc_im,
+                      const void* gauge, int nterms, const double* alphas, const void* X, const void* Y,
+                      int symmetric, double scale, void* force, void* stream) {
+  LYM_REQUIRE(lat && gauge && alphas && X && Y && force, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(nterms >= 1 && nterms <= kMaxForceTerms, LYM_ERR_BAD_ARG, "nterms must be in [1, %d]",
+              kMaxForceTerms);
+  if (lat->nd != 2 && lat->nd != 4) {
+    set_error("Number of dimensions %d not supported for fermions!", lat->nd);
+    return LYM_ERR_UNSUPPORTED;
+  }
+  ForceTerms t;
+  for (int i = 0; i < kMaxForceTerms; ++i) t.alpha[i] = i < nterms ? alphas[i] : 0.0;
+  dim3 grid(grid_for(lat->V, 128), lat->nd);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int Lt = lat->dims[lat->nd - 1];
+#define LYM_FF(ND_, NC_, H_)                                                                        \
+  fermion_force_kernel<ND_, NC_, H_><<<grid, 128, 0, st>>>(lat->d_tab, lat->V, Lt, kappa, bc_re, bc_im, \
+                                                           (const double2*)gauge, nterms, t,          \
+                                                           (const double2*)X, (const double2*)Y,      \
+                                                           symmetric, scale, (double2*)force)
+  if (lat->nd == 2 && nc == 2) { if (hermitian) LYM_FF(2, 2, true); else LYM_FF(2, 2, false); }
+  else if (lat->nd == 2 && nc == 3) { if (hermitian) LYM_FF(2, 3, true); else LYM_FF(2, 3, false); }
+  else if (lat->nd == 4 && nc == 2) { if (hermitian) LYM_FF(4, 2, true); else LYM_FF(4, 2, false); }
+  else if (lat->nd == 4 && nc == 3) { if (hermitian) LYM_FF(4, 3, true); else LYM_FF(4, 3, false); }
+  else {
+    set_error("N=%d not supported", nc);
+    return LYM_ERR_UNSUPPORTED;
+  }
+#undef LYM_FF
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1059 @@
+// Solvers: the lym_gauge object (even-odd packing of the links), the even-odd
+// preconditioned CG on M^dag M with FP64 reliable updates and sloppy inner
+// iterations in FP64 / FP32 / norm-scaled FP16 / BF16, the full-lattice
+// multishift CG, and the reference's MMMR (dirac_solver.py:19-53).
+//
+// Even-odd system (builder-defined; the reference has none): with
+// D = 1 + kappa H (the reference sign, dirac.py:400,521),
+//   b' = b_e - kappa H_eo b_o,  M = 1 - kappa^2 H_eo H_oe,  M x_e = b',
+//   x_o = b_o - kappa H_oe x_e,  and M^dag = gamma_d M gamma_d.
+// CG runs on M^dag M x_e = M^dag b'.  Iterations run in captured CUDA graphs
+// of `chunk` iterations; all CG scalars (alpha, beta, |r|^2) stay on the
+// device and are produced by the last block of each fused reduction.  A
+// right-hand side pauses itself on the device when its sloppy residual drops
+// below its pause target; the host then does the FP64 reliable update
+// (x += x_sloppy, q = b' - M x, r = M^dag q) for the paused ones and checks
+// the true residual |q| against tol |b|.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lym_eo.cuh"
+#include "lym_internal.cuh"
+#include "lym_kernels.cuh"
+
+namespace lym {
+
+struct CGState {
+  double rr;      // |r|^2 of the recursive (sloppy) residual
+  double alpha;
+  double beta;
+  double pause2;  // pause when rr < pause2
+  int active;     // iterate while 1
+  int iters;
+  int max_iter;
+  int pad;
+};
+
+// ---------------------------------------------------------------------------
+// geometry helpers
+// ---------------------------------------------------------------------------
+static EoGeom make_geom(const lym_lattice* lat) {
+  EoGeom g{};
+  g.nd = lat->nd;
+  int st = 1;
+  for (int d = lat->nd - 1; d >= 0; --d) {
+    g.dims[d] = lat->dims[d];
+    g.stride[d] = st;
+    st *= lat->dims[d];
+  }
+  for (int d = lat->nd; d < 4; ++d) {
+    g.dims[d] = 1;
+    g.stride[d] = 0;
+  }
+  g.Lh = lat->dims[lat->nd - 1] / 2;
+  g.Vh = lat->V / 2;
+  return g;
+}
+
+template <int ND>
+LYM_D void lex_coords(const EoGeom& g, int64_t lex, int (&x)[ND]) {
+  int64_t r = lex;
+#pragma unroll
+  for (int d = ND - 1; d >= 0; --d) {
+    x[d] = (int)(r % g.dims[d]);
+    r /= g.dims[d];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// gauge packing
+// ---------------------------------------------------------------------------
+template <int GP, int NC>
+LYM_D void store_link_eo(void* g, int nunits, int64_t Vh, int mu, int par, int64_t cb, bool comp,
+                         const cx<double> (&u)[NC][NC]) {
+  const int ncx = comp ? (NC - 1) * NC : NC * NC;
+  cx<double> e[NC * NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) e[i * NC + j] = u[i][j];
+  if constexpr (GP == SP64) {
+    double2* base = reinterpret_cast<double2*>(g) + ((int64_t)(mu * 2 + par) * nunits) * Vh + cb;
+    for (int k = 0; k < ncx; ++k) base[k * Vh] = make_double2(e[k].re, e[k].im);
+  } else if constexpr (GP == SP32) {
+    float4* base = reinterpret_cast<float4*>(g) + ((int64_t)(mu * 2 + par) * nunits) * Vh + cb;
+    for (int k = 0; k < nunits; ++k) {
+      cx<double> a = 2 * k < ncx ? e[2 * k] : cx<double>{0, 0};
+      cx<double> b = 2 * k + 1 < ncx ? e[2 * k + 1] : cx<double>{0, 0};
+      base[k * Vh] = make_float4((float)a.re, (float)a.im, (float)b.re, (float)b.im);
+    }
+  } else {
+    uint2* base = reinterpret_cast<uint2*>(g) + ((int64_t)(mu * 2 + par) * nunits) * Vh + cb;
+    for (int k = 0; k < nunits; ++k) {
+      cx<double> a = 2 * k < ncx ? e[2 * k] : cx<double>{0, 0};
+      cx<double> b = 2 * k + 1 < ncx ? e[2 * k + 1] : cx<double>{0, 0};
+      base[k * Vh] = make_uint2(pack2<SP16>((float)a.re, (float)a.im), pack2<SP16>((float)b.re, (float)b.im));
+    }
+  }
+}
+
+template <int ND, int NC>
+__global__ void pack_gauge_kernel(EoGeom g, int64_t V, const double2* __restrict__ ref, double bcr, double bci,
+                                  double2* g64, float4* g32, int n32, int comp32, uint2* g16, int n16, int comp16) {
+  const int64_t lex = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (lex >= V) return;
+  int x[ND];
+  lex_coords<ND>(g, lex, x);
+  int par = 0;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) par += x[d];
+  par &= 1;
+  const int64_t cb = lex >> 1;
+  cx<double> u[NC][NC], ub[NC][NC];
+  const bool edge = (mu == ND - 1) && (x[ND - 1] == g.dims[ND - 1] - 1);
+  const cx<double> bc{edge ? bcr : 1.0, edge ? bci : 0.0};
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) {
+      u[i][j] = ld(ref + ((int64_t)(mu * NC + i) * NC + j) * V + lex);
+      ub[i][j] = bc * u[i][j];
+    }
+  store_link_eo<SP64, NC>(g64, NC * NC, g.Vh, mu, par, cb, false, ub);
+  if (g32) store_link_eo<SP32, NC>(g32, n32, g.Vh, mu, par, cb, comp32, comp32 ? u : ub);
+  if (g16) store_link_eo<SP16, NC>(g16, n16, g.Vh, mu, par, cb, comp16, comp16 ? u : ub);
+}
+
+// sum over links of |U U^dag - 1|^2 + |det U - 1|^2
+template <int NC>
+__global__ void unitarity_kernel(int64_t nl, const double2* __restrict__ ref, int64_t V, double* partials,
+                                 unsigned* counter, double* result) {
+  __shared__ double sh[32];
+  double v[1] = {0.0};
+  for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < nl; l += (int64_t)gridDim.x * blockDim.x) {
+    const int mu = (int)(l / V);
+    const int64_t s = l - mu * V;
+    cx<double> u[NC][NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) u[i][j] = ld(ref + ((int64_t)(mu * NC + i) * NC + j) * V + s);
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) {
+        cx<double> t = czero<double>();
+#pragma unroll
+        for (int k = 0; k < NC; ++k) t += u[i][k] * conj(u[j][k]);
+        if (i == j) t.re -= 1.0;
+        v[0] += norm2(t);
+      }
+    cx<double> d;
+    if constexpr (NC == 2) d = u[0][0] * u[1][1] - u[0][1] * u[1][0];
+    else
+      d = u[0][0] * (u[1][1] * u[2][2] - u[1][2] * u[2][1]) - u[0][1] * (u[1][0] * u[2][2] - u[1][2] * u[2][0]) +
+          u[0][2] * (u[1][0] * u[2][1] - u[1][1] * u[2][0]);
+    d.re -= 1.0;
+    v[0] += norm2(d);
+  }
+  if (grid_sum<1>(v, partials, counter, sh) && threadIdx.x == 0) result[0] = v[0];
+}
+
+// ---------------------------------------------------------------------------
+// spinor conversions
+// ---------------------------------------------------------------------------
+// reference layout (nrhs, ns, N, V) -> FP64 even / odd fields; g5: multiply by gamma_d
+template <int ND, int NC>
+__global__ void ref_to_eo_kernel(EoGeom g, int64_t V, const double2* __restrict__ ref, EoField e, EoField o, int g5) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  const int64_t lex = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (lex >= V) return;
+  int x[ND];
+  lex_coords<ND>(g, lex, x);
+  int par = 0;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) par += x[d];
+  par &= 1;
+  cx<double> v[NCOMP];
+#pragma unroll
+  for (int c = 0; c < NCOMP; ++c) {
+    v[c] = ld(ref + ((int64_t)rhs * NCOMP + c) * V + lex);
+    if (g5 && c >= (NS / 2) * NC) v[c] = -v[c];
+  }
+  store_sp<SP64, NCOMP>(par ? o : e, rhs, lex >> 1, v);
+}
+
+template <int ND, int NC>
+__global__ void eo_to_ref_kernel(EoGeom g, int64_t V, EoField e, EoField o, double2* __restrict__ ref) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  const int64_t lex = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (lex >= V) return;
+  int x[ND];
+  lex_coords<ND>(g, lex, x);
+  int par = 0;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) par += x[d];
+  par &= 1;
+  cx<double> v[NCOMP];
+  load_sp<SP64, NCOMP>(par ? o : e, rhs, lex >> 1, v);
+#pragma unroll
+  for (int c = 0; c < NCOMP; ++c) st(ref + ((int64_t)rhs * NCOMP + c) * V + lex, v[c]);
+}
+
+// dst (precision SP) = src (FP64); optionally also dst2 = src
+template <int SP, int NCOMP>
+__global__ void convert_kernel(int64_t Vh, EoField src, EoField dst, EoField dst2, const CGState* st, int only_update,
+                               const int* upd) {
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (cb >= Vh) return;
+  if (only_update && !upd[rhs]) return;
+  cx<double> v[NCOMP];
+  load_sp<SP64, NCOMP>(src, rhs, cb, v);
+  cx<typename Prec<SP>::real> w[NCOMP];
+#pragma unroll
+  for (int c = 0; c < NCOMP; ++c) w[c] = {(typename Prec<SP>::real)v[c].re, (typename Prec<SP>::real)v[c].im};
+  store_sp<SP, NCOMP>(dst, rhs, cb, w);
+  if (dst2.data) store_sp<SP, NCOMP>(dst2, rhs, cb, w);
+}
+
+// x64 += xs; xs = 0  (for rhs with upd[rhs])
+template <int XP, int NCOMP>
+__global__ void accumulate_kernel(int64_t Vh, EoField xs, EoField x64, const int* upd) {
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (cb >= Vh || !upd[rhs]) return;
+  using R = typename Prec<XP>::real;
+  cx<R> a[NCOMP];
+  load_sp<XP, NCOMP>(xs, rhs, cb, a);
+  cx<double> b[NCOMP];
+  load_sp<SP64, NCOMP>(x64, rhs, cb, b);
+  cx<R> z[NCOMP];
+#pragma unroll
+  for (int c = 0; c < NCOMP; ++c) {
+    b[c] = b[c] + cx<double>{(double)a[c].re, (double)a[c].im};
+    z[c] = czero<R>();
+  }
+  store_sp<SP64, NCOMP>(x64, rhs, cb, b);
+  store_sp<XP, NCOMP>(xs, rhs, cb, z);
+}
+
+template <int NCOMP>
+__global__ void zero64_kernel(int64_t Vh, EoField f) {
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (cb >= Vh) return;
+  cx<double> z[NCOMP];
+#pragma unroll
+  for (int c = 0; c < NCOMP; ++c) z[c] = czero<double>();
+  store_sp<SP64, NCOMP>(f, blockIdx.y, cb, z);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 hop with a linear-combination epilogue (reliable updates, setup):
+//   out = z0 + a1 z1 + c * G5OUT(hop(G5IN(in)))  ; optional |out|^2 -> res[rhs]
+// ---------------------------------------------------------------------------
+template <int ND, int NC, bool G5IN, bool G5OUT>
+__global__ void __launch_bounds__(128) hop64_lincomb_kernel(EoGeom g, HopGauge hg, EoField in, int par, EoField out,
+                                                            EoField z0, EoField z1, double a1, double c,
+                                                            const int* upd, double* partials, unsigned* counters,
+                                                            double* res, int nblk) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  __shared__ double sh[32];
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (upd && !upd[rhs]) return;  // uniform per block
+  double nrm[1] = {0.0};
+  if (cb < g.Vh) {
+    cx<double> acc[NS][NC];
+    hop_site<ND, NC, SP64, SP64, false, G5IN>(g, hg, in, rhs, cb, par, acc);
+    cx<double> v[NCOMP], a[NCOMP];
+    if (z0.data) load_sp<SP64, NCOMP>(z0, rhs, cb, v);
+    else
+#pragma unroll
+      for (int k = 0; k < NCOMP; ++k) v[k] = czero<double>();
+    if (z1.data) {
+      load_sp<SP64, NCOMP>(z1, rhs, cb, a);
+#pragma unroll
+      for (int k = 0; k < NCOMP; ++k) v[k] += a1 * a[k];
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+      for (int cc = 0; cc < NC; ++cc) {
+        cx<double> h = (G5OUT && s >= NS / 2) ? -acc[s][cc] : acc[s][cc];
+        v[s * NC + cc] += c * h;
+        nrm[0] += norm2(v[s * NC + cc]);
+      }
+    store_sp<SP64, NCOMP>(out, rhs, cb, v);
+  }
+  if (res) {
+    if (grid_sum<1>(nrm, partials + (int64_t)rhs * nblk, counters + rhs, sh) && threadIdx.x == 0) res[rhs] = nrm[0];
+  }
+}
+
+// |f|^2 per rhs (FP64 field)
+template <int NCOMP>
+__global__ void __launch_bounds__(128) norm64_kernel(int64_t Vh, EoField f, double* partials, unsigned* counters,
+                                                     double* res, int nblk, int accumulate) {
+  __shared__ double sh[32];
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  double n[1] = {0.0};
+  if (cb < Vh) {
+    cx<double> v[NCOMP];
+    load_sp<SP64, NCOMP>(f, rhs, cb, v);
+#pragma unroll
+    for (int k = 0; k < NCOMP; ++k) n[0] += norm2(v[k]);
+  }
+  if (grid_sum<1>(n, partials + (int64_t)rhs * nblk, counters + rhs, sh) && threadIdx.x == 0)
+    res[rhs] = accumulate ? res[rhs] + n[0] : n[0];
+}
+
+// ---------------------------------------------------------------------------
+// sloppy CG iteration kernels (precision SP, links GP/COMP)
+// ---------------------------------------------------------------------------
+// s = H_oe G5IN(p)   (odd output)
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN>
+__global__ void __launch_bounds__(128) cg_hop_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
+                                                     const CGState* st) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (!st[rhs].active || cb >= g.Vh) return;
+  using R = typename Prec<SP>::real;
+  cx<R> acc[NS][NC];
+  hop_site<ND, NC, SP, GP, COMP, G5IN>(g, hg, in, rhs, cb, par, acc);
+  cx<R> v[NCOMP];
+#pragma unroll
+  for (int s = 0; s < NS; ++s)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) v[s * NC + c] = acc[s][c];
+  store_sp<SP, NCOMP>(out, rhs, cb, v);
+}
+
+// t = p - kappa^2 H_eo s ; alpha = rr / |t|^2
+template <int ND, int NC, int SP, int GP, bool COMP>
+__global__ void __launch_bounds__(128) cg_t_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t, double k2,
+                                                   CGState* st, double* partials, unsigned* counters, int nblk) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  __shared__ double sh[32];
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (!st[rhs].active) return;
+  using R = typename Prec<SP>::real;
+  double n[1] = {0.0};
+  if (cb < g.Vh) {
+    cx<R> acc[NS][NC];
+    hop_site<ND, NC, SP, GP, COMP, false>(g, hg, s, rhs, cb, 0, acc);
+    cx<R> v[NCOMP];
+    load_sp<SP, NCOMP>(p, rhs, cb, v);
+#pragma unroll
+    for (int a = 0; a < NS; ++a)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        cx<R>& w = v[a * NC + c];
+        w -= (R)k2 * acc[a][c];
+        n[0] += (double)w.re * w.re + (double)w.im * w.im;
+      }
+    store_sp<SP, NCOMP>(t, rhs, cb, v);
+  }
+  if (grid_sum<1>(n, partials + (int64_t)rhs * nblk, counters + rhs, sh) && threadIdx.x == 0) {
+    CGState& S = st[rhs];
+    if (n[0] > 0.0 && S.rr > 0.0) {
+      S.alpha = S.rr / n[0];
+    } else {
+      S.alpha = 0.0;
+      S.active = 0;  // p = 0: nothing left to do
+    }
+  }
+}
+
+// Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr
+template <int ND, int NC, int SP, int GP, bool COMP, int XP>
+__global__ void __launch_bounds__(128) cg_update_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
+                                                        EoField x, EoField r, double k2, CGState* st,
+                                                        double* partials, unsigned* counters, int nblk) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  __shared__ double sh[32];
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (!st[rhs].active) return;
+  using R = typename Prec<SP>::real;
+  using XR = typename Prec<XP>::real;
+  const double alpha = st[rhs].alpha;
+  double n[1] = {0.0};
+  if (cb < g.Vh) {
+    cx<R> acc[NS][NC];
+    hop_site<ND, NC, SP, GP, COMP, false>(g, hg, s, rhs, cb, 0, acc);
+    cx<R> tv[NCOMP], pv[NCOMP], rv[NCOMP];
+    cx<XR> xv[NCOMP];
+    load_sp<SP, NCOMP>(t, rhs, cb, tv);
+    load_sp<SP, NCOMP>(p, rhs, cb, pv);
+    load_sp<SP, NCOMP>(r, rhs, cb, rv);
+    load_sp<XP, NCOMP>(x, rhs, cb, xv);
+    const R a = (R)alpha;
+#pragma unroll
+    for (int sp = 0; sp < NS; ++sp)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int k = sp * NC + c;
+        cx<R> h = acc[sp][c];
+        if (sp >= NS / 2) h = -h;
+        cx<R> ap = tv[k] - (R)k2 * h;
+        rv[k] -= a * ap;
+        xv[k] += (XR)alpha * cx<XR>{(XR)pv[k].re, (XR)pv[k].im};
+        n[0] += (double)rv[k].re * rv[k].re + (double)rv[k].im * rv[k].im;
+      }
+    store_sp<SP, NCOMP>(r, rhs, cb, rv);
+    store_sp<XP, NCOMP>(x, rhs, cb, xv);
+  }
+  if (grid_sum<1>(n, partials + (int64_t)rhs * nblk, counters + rhs, sh) && threadIdx.x == 0) {
+    CGState& S = st[rhs];
+    S.beta = n[0] / S.rr;
+    S.rr = n[0];
+    S.iters += 1;
+    if (S.rr < S.pause2 || S.iters >= S.max_iter) S.active = 2;  // finish the p update, then stop
+  }
+}
+
+// p = r + beta p
+template <int SP, int NCOMP>
+__global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoField p, CGState* st) {
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  const int act = st[rhs].active;
+  if (!act) return;
+  if (cb < Vh) {
+    using R = typename Prec<SP>::real;
+    const R b = (R)st[rhs].beta;
+    cx<R> rv[NCOMP], pv[NCOMP];
+    load_sp<SP, NCOMP>(r, rhs, cb, rv);
+    load_sp<SP, NCOMP>(p, rhs, cb, pv);
+#pragma unroll
+    for (int k = 0; k < NCOMP; ++k) pv[k] = rv[k] + b * pv[k];
+    store_sp<SP, NCOMP>(p, rhs, cb, pv);
+  }
+}
+
+// turns the "stop after the p update" marker into a pause; one thread per rhs
+__global__ void cg_settle_kernel(int nrhs, CGState* st) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nrhs && st[r].active == 2) st[r].active = 0;
+}
+
+// ---------------------------------------------------------------------------
+// per-(ND, NC, SP, COMP) operation table
+// ---------------------------------------------------------------------------
+struct Work;
+struct CgOps {
+  void (*iterate)(Work&, cudaStream_t);                 // one sloppy CG iteration (5 launches)
+  void (*hop64)(Work&, int par, const EoField& in, const EoField& out, const EoField& z0, const EoField& z1,
+                double a1, double c, bool g5in, bool g5out, bool with_norm, cudaStream_t);
+  void (*to_eo)(Work&, const void* ref, int g5, cudaStream_t);
+  void (*from_eo)(Work&, void* ref, cudaStream_t);
+  void (*norm64)(Work&, const EoField& f, int accumulate, cudaStream_t);
+  void (*convert)(Work&, const EoField& src, const EoField& dst, const EoField& dst2, bool only_update, cudaStream_t);
+  void (*accumulate)(Work&, cudaStream_t);
+  void (*zero64)(Work&, const EoField& f, cudaStream_t);
+};
+
+}  // namespace lym
+
+struct lym_gauge {
+  const lym_lattice* lat = nullptr;
+  int nc = 0, nd = 0, ns = 0, ncomp = 0;
+  int64_t V = 0, Vh = 0;
+  double bcr = 1, bci = 0;
+  unsigned prec_mask = 0;
+  bool comp = false;  // sloppy links compressed (links are SU(N))
+  lym::EoGeom geom{};
+  double2* uref = nullptr;  // reference-layout FP64 copy (boundary factor NOT applied)
+  double2* u64 = nullptr;
+  float4* u32 = nullptr;
+  int n32 = 0;
+  uint2* u16 = nullptr;
+  int n16 = 0;
+  lym::Work* work = nullptr;
+};
+
+namespace lym {
+
+struct Work {
+  lym_gauge* g = nullptr;
+  int nrhs = 0, sp = 0, xp = 0;
+  int64_t Vh = 0;
+  int nblk = 0;
+  double kappa = 0;
+  // FP64 fields
+  EoField be, bo, bp, x64, xo, q, s64, r64;
+  // sloppy fields
+  EoField r, p, t, s, xs;
+  CGState* st = nullptr;
+  CGState* st_host = nullptr;
+  int* upd = nullptr;
+  int* upd_host = nullptr;
+  double* partials = nullptr;
+  unsigned* counters = nullptr;
+  double* res = nullptr;       // per rhs, several result slots
+  double* res_host = nullptr;
+  void* pool = nullptr;
+  size_t pool_bytes = 0;
+  HopGauge hg64, hgs;
+  CgOps ops{};
+  cudaGraphExec_t graph = nullptr;
+  int graph_chunk = 0;
+  double graph_kappa = 0;
+  cudaStream_t graph_stream = nullptr;
+  cudaStream_t stream = nullptr;  // solves run here (capturable even when the caller uses the legacy stream)
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+};
+
+template <int ND, int NC, int SP, bool COMP>
+struct Impl {
+  static constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  static constexpr int GP = SP == SP64 ? SP64 : (SP == SP32 ? SP32 : SP16);
+  static constexpr int XP = SP == SP64 ? SP64 : SP32;
+
+  static void iterate(Work& w, cudaStream_t st) {
+    const double k2 = w.kappa * w.kappa;
+    dim3 grid(w.nblk, w.nrhs);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, false><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, w.st);
+    cg_t_kernel<ND, NC, SP, GP, COMP><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st, w.partials,
+                                                            w.counters, w.nblk);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, true><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, w.st);
+    cg_update_kernel<ND, NC, SP, GP, COMP, XP><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.t, w.p, w.xs, w.r, k2,
+                                                                     w.st, w.partials, w.counters, w.nblk);
+    cg_p_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.r, w.p, w.st);
+    cg_settle_kernel<<<(w.nrhs + 63) / 64, 64, 0, st>>>(w.nrhs, w.st);
+  }
+
+  static void hop64(Work& w, int par, const EoField& in, const EoField& out, const EoField& z0, const EoField& z1,
+                    double a1, double c, bool g5in, bool g5out, bool with_norm, cudaStream_t st) {
+    dim3 grid(w.nblk, w.nrhs);
+    double* res = with_norm ? w.res : nullptr;
+#define LYM_H64(A, B)                                                                                     \
+  hop64_lincomb_kernel<ND, NC, A, B><<<grid, 128, 0, st>>>(w.g->geom, w.hg64, in, par, out, z0, z1, a1, c, \
+                                                           w.upd, w.partials, w.counters, res, w.nblk)
+    if (g5in && g5out) LYM_H64(true, true);
+    else if (g5in) LYM_H64(true, false);
+    else if (g5out) LYM_H64(false, true);
+    else LYM_H64(false, false);
+#undef LYM_H64
+  }
+
+  static void to_eo(Work& w, const void* ref, int g5, cudaStream_t st) {
+    dim3 grid(grid_for(w.g->V, 128), w.nrhs);
+    ref_to_eo_kernel<ND, NC><<<grid, 128, 0, st>>>(w.g->geom, w.g->V, (const double2*)ref, w.be, w.bo, g5);
+  }
+  static void from_eo(Work& w, void* ref, cudaStream_t st) {
+    dim3 grid(grid_for(w.g->V, 128), w.nrhs);
+    eo_to_ref_kernel<ND, NC><<<grid, 128, 0, st>>>(w.g->geom, w.g->V, w.x64, w.xo, (double2*)ref);
+  }
+  static void norm64(Work& w, const EoField& f, int accumulate, cudaStream_t st) {
+    dim3 grid(w.nblk, w.nrhs);
+    norm64_kernel<NCOMP><<<grid, 128, 0, st>>>(w.Vh, f, w.partials, w.counters, w.res, w.nblk, accumulate);
+  }
+  static void convert(Work& w, const EoField& src, const EoField& dst, const EoField& dst2, bool only_update,
+                      cudaStream_t st) {
+    dim3 grid(w.nblk, w.nrhs);
+    convert_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, src, dst, dst2, w.st, only_update, w.upd);
+  }
+  static void accumulate(Work& w, cudaStream_t st) {
+    if constexpr (SP != SP64) {
+      dim3 grid(w.nblk, w.nrhs);
+      accumulate_kernel<XP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.xs, w.x64, w.upd);
+    }
+  }
+  static void zero64(Work& w, const EoField& f, cudaStream_t st) {
+    dim3 grid(w.nblk, w.nrhs);
+    zero64_kernel<NCOMP><<<grid, 128, 0, st>>>(w.Vh, f);
+  }
+  static CgOps table() {
+    return CgOps{&iterate, &hop64, &to_eo, &from_eo, &norm64, &convert, &accumulate, &zero64};
+  }
+};
+
+template <int ND, int NC>
+static CgOps pick_sp(int sp, bool comp) {
+  switch (sp) {
+    case SP64: return Impl<ND, NC, SP64, false>::table();
+    case SP32: return comp ? Impl<ND, NC, SP32, true>::table() : Impl<ND, NC, SP32, false>::table();
+    case SP16: return comp ? Impl<ND, NC, SP16, true>::table() : Impl<ND, NC, SP16, false>::table();
+    default: return comp ? Impl<ND, NC, SPB16, true>::table() : Impl<ND, NC, SPB16, false>::table();
+  }
+}
+
+static bool pick_ops(int nd, int nc, int sp, bool comp, CgOps* out) {
+  if (nd == 2 && nc == 2) *out = pick_sp<2, 2>(sp, comp);
+  else if (nd == 2 && nc == 3) *out = pick_sp<2, 3>(sp, comp);
+  else if (nd == 4 && nc == 2) *out = pick_sp<4, 2>(sp, comp);
+  else if (nd == 4 && nc == 3) *out = pick_sp<4, 3>(sp, comp);
+  else return false;
+  return true;
+}
+
+static size_t field_bytes(int sp, int ncomp, int64_t Vh, int nrhs) {
+  const int cpu = sp == SP64 ? 1 : (sp == SP32 ? 2 : 4);
+  size_t b = (size_t)units_for(ncomp, cpu) * 16 * Vh * nrhs;
+  if (sp == SP16 || sp == SPB16) b += sizeof(float) * Vh * nrhs;
+  return (b + 255) & ~(size_t)255;
+}
+
+static EoField carve(char*& cur, int sp, int ncomp, int64_t Vh, int nrhs) {
+  EoField f;
+  const int cpu = sp == SP64 ? 1 : (sp == SP32 ? 2 : 4);
+  f.nunits = units_for(ncomp, cpu);
+  f.Vh = Vh;
+  f.data = cur;
+  size_t b = (size_t)f.nunits * 16 * Vh * nrhs;
+  if (sp == SP16 || sp == SPB16) {
+    f.norm = reinterpret_cast<float*>(cur + b);
+    b += sizeof(float) * Vh * nrhs;
+  }
+  cur += (b + 255) & ~(size_t)255;
+  return f;
+}
+
+static void free_work(Work* w) {
+  if (!w) return;
+  if (w->graph) cudaGraphExecDestroy(w->graph);
+  if (w->stream) cudaStreamSynchronize(w->stream);
+  if (w->pool) cudaFree(w->pool);
+  if (w->ev_in) cudaEventDestroy(w->ev_in);
+  if (w->ev_out) cudaEventDestroy(w->ev_out);
+  if (w->stream) cudaStreamDestroy(w->stream);
+  if (w->st_host) cudaFreeHost(w->st_host);
+  if (w->upd_host) cudaFreeHost(w->upd_host);
+  if (w->res_host) cudaFreeHost(w->res_host);
+  delete w;
+}
+
+static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
+  Work* w = g->work;
+  if (w && w->nrhs == nrhs && w->sp == sp) {
+    *out = w;
+    return LYM_OK;
+  }
+  free_work(w);
+  g->work = nullptr;
+  w = new Work();
+  w->g = g;
+  w->nrhs = nrhs;
+  w->sp = sp;
+  w->xp = sp == SP64 ? SP64 : SP32;
+  w->Vh = g->Vh;
+  w->nblk = (int)grid_for(g->Vh, 128);
+  if (!pick_ops(g->nd, g->nc, sp, g->comp && sp != SP64, &w->ops)) {
+    delete w;
+    set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
+    return LYM_ERR_UNSUPPORTED;
+  }
+  const int nc = g->ncomp;
+  size_t bytes = 8 * field_bytes(SP64, nc, g->Vh, nrhs);
+  bytes += 4 * field_bytes(sp, nc, g->Vh, nrhs);
+  if (sp != SP64) bytes += field_bytes(w->xp, nc, g->Vh, nrhs);
+  const size_t nres = 8;
+  bytes += ((sizeof(CGState) * nrhs + 255) & ~(size_t)255);
+  bytes += ((sizeof(int) * nrhs + 255) & ~(size_t)255);
+  bytes += ((sizeof(double) * (size_t)nrhs * w->nblk + 255) & ~(size_t)255);
+  bytes += ((sizeof(unsigned) * nrhs + 255) & ~(size_t)255);
+  bytes += ((sizeof(double) * nrhs * nres + 255) & ~(size_t)255);
+  if (cudaMalloc(&w->pool, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    delete w;
+    set_error("solver workspace of %zu bytes does not fit", bytes);
+    return LYM_ERR_OOM;
+  }
+  w->pool_bytes = bytes;
+  char* cur = (char*)w->pool;
+  w->be = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->bo = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->bp = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->x64 = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->xo = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->q = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->s64 = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->r64 = carve(cur, SP64, nc, g->Vh, nrhs);
+  w->r = carve(cur, sp, nc, g->Vh, nrhs);
+  w->p = carve(cur, sp, nc, g->Vh, nrhs);
+  w->t = carve(cur, sp, nc, g->Vh, nrhs);
+  w->s = carve(cur, sp, nc, g->Vh, nrhs);
+  w->xs = sp == SP64 ? w->x64 : carve(cur, w->xp, nc, g->Vh, nrhs);
+  w->st = reinterpret_cast<CGState*>(cur);
+  cur += (sizeof(CGState) * nrhs + 255) & ~(size_t)255;
+  w->upd = reinterpret_cast<int*>(cur);
+  cur += (sizeof(int) * nrhs + 255) & ~(size_t)255;
+  w->partials = reinterpret_cast<double*>(cur);
+  cur += (sizeof(double) * (size_t)nrhs * w->nblk + 255) & ~(size_t)255;
+  w->counters = reinterpret_cast<unsigned*>(cur);
+  cur += (sizeof(unsigned) * nrhs + 255) & ~(size_t)255;
+  w->res = reinterpret_cast<double*>(cur);
+  if (cudaMemset(w->counters, 0, sizeof(unsigned) * nrhs) != cudaSuccess ||
+      cudaMallocHost(&w->st_host, sizeof(CGState) * nrhs) != cudaSuccess ||
+      cudaMallocHost(&w->upd_host, sizeof(int) * nrhs) != cudaSuccess ||
+      cudaMallocHost(&w->res_host, sizeof(double) * nrhs * nres) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&w->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&w->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+    free_work(w);
+    set_error("solver workspace host buffers");
+    return LYM_ERR_OOM;
+  }
+  w->hg64 = HopGauge{g->u64, g->nc * g->nc, 1.0, 0.0};
+  if (sp == SP64) w->hgs = w->hg64;
+  else if (sp == SP32) w->hgs = HopGauge{g->u32, g->n32, g->bcr, g->bci};
+  else w->hgs = HopGauge{g->u16, g->n16, g->bcr, g->bci};
+  g->work = w;
+  *out = w;
+  return LYM_OK;
+}
+
+static int fetch_res(Work& w, int n, cudaStream_t st) {
+  LYM_CUDA(cudaMemcpyAsync(w.res_host, w.res, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  LYM_CUDA(cudaStreamSynchronize(st));
+  return LYM_OK;
+}
+
+// FP64 reliable update for the rhs flagged in upd_host (already copied to upd):
+// x += x_sloppy; q = b' - M x; r64 = M^dag q.  Leaves |q|^2 in res_host[0..nrhs)
+// and |r64|^2 in res_host[nrhs..2 nrhs).
+static int reliable_update(Work& w, cudaStream_t st) {
+  const double k = w.kappa, k2 = k * k;
+  EoField none;
+  w.ops.accumulate(w, st);
+  w.ops.hop64(w, 1, w.x64, w.s64, none, none, 0.0, 1.0, false, false, false, st);
+  w.ops.hop64(w, 0, w.s64, w.q, w.bp, w.x64, -1.0, k2, false, false, true, st);
+  LYM_CUDA(cudaMemcpyAsync(w.res_host, w.res, sizeof(double) * w.nrhs, cudaMemcpyDeviceToHost, st));
+  w.ops.hop64(w, 1, w.q, w.s64, none, none, 0.0, 1.0, true, false, false, st);
+  w.ops.hop64(w, 0, w.s64, w.r64, w.q, none, 0.0, -k2, false, true, true, st);
+  LYM_CUDA(cudaMemcpyAsync(w.res_host + w.nrhs, w.res, sizeof(double) * w.nrhs, cudaMemcpyDeviceToHost, st));
+  LYM_CHECK_LAUNCH();
+  LYM_CUDA(cudaStreamSynchronize(st));
+  return LYM_OK;
+}
+
+static int build_graph(Work& w, int chunk, cudaStream_t st) {
+  if (w.graph && w.graph_chunk == chunk && w.graph_kappa == w.kappa && w.graph_stream == st) return LYM_OK;
+  if (w.graph) {
+    cudaGraphExecDestroy(w.graph);
+    w.graph = nullptr;
+  }
+  cudaGraph_t graph;
+  LYM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < chunk; ++i) w.ops.iterate(w, st);
+  cudaError_t e = cudaStreamEndCapture(st, &graph);
+  if (e != cudaSuccess) {
+    set_error("graph capture: %s", cudaGetErrorString(e));
+    return LYM_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&w.graph, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    w.graph = nullptr;
+    set_error("graph instantiate: %s", cudaGetErrorString(e));
+    return LYM_ERR_CUDA;
+  }
+  w.graph_chunk = chunk;
+  w.graph_kappa = w.kappa;
+  w.graph_stream = st;
+  return LYM_OK;
+}
+
+static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void* b, void* x,
+                       const lym_solver_params* prm, lym_solver_report* rep, cudaStream_t st);
+
+static int cg_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x, const lym_solver_params* prm,
+                    lym_solver_report* rep, cudaStream_t caller) {
+  LYM_REQUIRE(g && b && x && prm && rep, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(nrhs >= 1 && nrhs <= 4096, LYM_ERR_BAD_ARG, "nrhs out of range");
+  LYM_REQUIRE(prm->tol > 0 && prm->max_iter > 0, LYM_ERR_BAD_ARG, "tol and max_iter must be positive");
+  LYM_REQUIRE(prm->precision >= 0 && prm->precision <= 3, LYM_ERR_BAD_ARG, "bad precision");
+  const int sp = prm->precision;
+  LYM_REQUIRE(sp == SP64 || (g->prec_mask >> sp) & 1u, LYM_ERR_BAD_ARG,
+              "precision %d was not enabled in lym_gauge_create", sp);
+  Work* wp;
+  int rc = get_work(g, nrhs, sp, &wp);
+  if (rc) return rc;
+  Work& w = *wp;
+  // order the solve after the caller's prior work, and the caller's later work after the solve
+  LYM_CUDA(cudaEventRecord(w.ev_in, caller));
+  LYM_CUDA(cudaStreamWaitEvent(w.stream, w.ev_in, 0));
+  rc = cg_solve_on(w, g, kappa, nrhs, b, x, prm, rep, w.stream);
+  cudaEventRecord(w.ev_out, w.stream);
+  cudaStreamWaitEvent(caller, w.ev_out, 0);
+  return rc;
+}
+
+static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void* b, void* x,
+                       const lym_solver_params* prm, lym_solver_report* rep, cudaStream_t st) {
+  int rc = LYM_OK;
+  const int sp = prm->precision;
+  w.kappa = kappa;
+  const double k = kappa;
+  const double delta = prm->delta > 0 && prm->delta < 1 ? prm->delta : 0.1;
+  const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 8;
+  EoField none;
+
+  // source: b (or gamma_d b for Q x = b) in even-odd form, |b|^2, b' = b_e - kappa H_eo b_o
+  w.ops.to_eo(w, b, prm->hermitian ? 1 : 0, st);
+  w.ops.norm64(w, w.be, 0, st);
+  w.ops.norm64(w, w.bo, 1, st);
+  LYM_CHECK_LAUNCH();
+  rc = fetch_res(w, nrhs, st);
+  if (rc) return rc;
+  std::vector<double> bnorm2(w.res_host, w.res_host + nrhs);
+  for (int i = 0; i < nrhs; ++i) w.upd_host[i] = 1;
+  LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+  w.ops.hop64(w, 0, w.bo, w.bp, w.be, none, 0.0, -k, false, false, false, st);
+  w.ops.zero64(w, w.x64, st);
+  if (sp != SP64) LYM_CUDA(cudaMemsetAsync(w.xs.data, 0, field_bytes(w.xp, g->ncomp, w.Vh, nrhs), st));
+  LYM_CHECK_LAUNCH();
+
+  std::vector<int> done(nrhs, 0), updates(nrhs, 0);
+  std::vector<double> target(nrhs, 0.0), tres(nrhs, 0.0);
+  auto plan_rhs = [&](int i, double q2, double r2) -> void {
+    CGState& S = w.st_host[i];
+    const double want = prm->tol * prm->tol * bnorm2[i];
+    tres[i] = bnorm2[i] > 0 ? std::sqrt(q2 / bnorm2[i]) : 0.0;
+    if (q2 <= want || r2 == 0.0) {
+      done[i] = 1;
+      S.active = 0;
+      return;
+    }
+    // pause target for the recursive residual of the normal equations:
+    // scale the present one by how far the true residual still has to fall
+    const double est = r2 * (want / q2) * 0.25;
+    target[i] = est;
+    S.rr = r2;
+    S.pause2 = sp == SP64 ? est : std::max(est, delta * delta * r2);
+    S.active = S.iters >= S.max_iter ? 0 : 1;
+  };
+  for (int i = 0; i < nrhs; ++i) {
+    CGState& S = w.st_host[i];
+    std::memset(&S, 0, sizeof(S));
+    S.max_iter = prm->max_iter;
+  }
+  // initial residual (x = 0): q = b', r64 = M^dag b'
+  rc = reliable_update(w, st);
+  if (rc) return rc;
+  for (int i = 0; i < nrhs; ++i) plan_rhs(i, w.res_host[i], w.res_host[nrhs + i]);
+  LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
+  w.ops.convert(w, w.r64, w.r, w.p, false, st);  // r = p = r64 in sloppy precision
+  LYM_CHECK_LAUNCH();
+  rc = build_graph(w, chunk, st);
+  if (rc) return rc;
+
+  while (true) {
+    bool any_active = false;
+    for (int i = 0; i < nrhs; ++i) any_active = any_active || (!done[i] && w.st_host[i].active);
+    if (!any_active) break;
+    // run chunks until every rhs paused, finished or hit max_iter
+    while (true) {
+      LYM_CUDA(cudaGraphLaunch(w.graph, st));
+      LYM_CUDA(cudaMemcpyAsync(w.st_host, w.st, sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
+      LYM_CUDA(cudaStreamSynchronize(st));
+      bool running = false;
+      for (int i = 0; i < nrhs; ++i) running = running || w.st_host[i].active;
+      if (!running) break;
+    }
+    // reliable update for every rhs that paused and is not done
+    bool any = false;
+    for (int i = 0; i < nrhs; ++i) {
+      w.upd_host[i] = (!done[i]) ? 1 : 0;
+      any = any || w.upd_host[i];
+    }
+    if (!any) break;
+    LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+    rc = reliable_update(w, st);
+    if (rc) return rc;
+    std::vector<double> q2(w.res_host, w.res_host + nrhs), r2(w.res_host + nrhs, w.res_host + 2 * nrhs);
+    for (int i = 0; i < nrhs; ++i) {
+      if (!w.upd_host[i]) continue;
+      updates[i] += 1;
+      plan_rhs(i, q2[i], r2[i]);
+    }
+    LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
+    // r = r64 (sloppy) for the updated rhs; p is kept
+    w.ops.convert(w, w.r64, w.r, none, true, st);
+    LYM_CHECK_LAUNCH();
+    bool left = false;
+    for (int i = 0; i < nrhs; ++i) left = left || (!done[i] && w.st_host[i].iters < prm->max_iter);
+    if (!left) break;
+  }
+  // x_o = b_o - kappa H_oe x_e, back to the reference layout
+  for (int i = 0; i < nrhs; ++i) w.upd_host[i] = 1;
+  LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+  w.ops.hop64(w, 1, w.x64, w.xo, w.bo, none, 0.0, -k, false, false, false, st);
+  w.ops.from_eo(w, x, st);
+  LYM_CHECK_LAUNCH();
+  LYM_CUDA(cudaStreamSynchronize(st));
+  int status = LYM_OK;
+  for (int i = 0; i < nrhs; ++i) {
+    rep[i].status = done[i] ? LYM_OK : LYM_ERR_NOT_CONVERGED;
+    rep[i].iterations = w.st_host[i].iters;
+    rep[i].reliable_updates = updates[i];
+    rep[i].true_residual = tres[i];
+    if (!done[i]) status = LYM_ERR_NOT_CONVERGED;
+  }
+  return status;
+}
+
+int gauge_view(const lym_gauge* g, GaugeView* v) {
+  LYM_REQUIRE(g && v, LYM_ERR_BAD_ARG, "null argument");
+  v->lat = g->lat;
+  v->nc = g->nc;
+  v->ncomp = g->ncomp;
+  v->V = g->V;
+  v->bcr = g->bcr;
+  v->bci = g->bci;
+  v->uref = g->uref;
+  return LYM_OK;
+}
+
+}  // namespace lym
+
+using namespace lym;
+
+// ---------------------------------------------------------------------------
+// gauge object
+// ---------------------------------------------------------------------------
+static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
+  const int64_t V = g->V;
+  LYM_CUDA(cudaMemcpyAsync(g->uref, gauge, sizeof(double2) * g->nd * g->nc * g->nc * V, cudaMemcpyDeviceToDevice, st));
+  // decide on link compression for the sloppy copies: links must be SU(N)
+  Scratch* s;
+  int rc = scratch_get(&s);
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lk(host_reduce_mutex());
+    const int slot = 1;
+    const int64_t nl = (int64_t)g->nd * V;
+    unsigned nb = reduction_blocks(nl, 256);
+    double* part = s->partials + (size_t)slot * Scratch::kMaxBlocks * Scratch::kMaxVals;
+    double* res = s->results + slot * Scratch::kMaxVals;
+    if (g->nc == 2)
+      unitarity_kernel<2><<<nb, 256, 0, st>>>(nl, (const double2*)gauge, V, part, s->counters + slot, res);
+    else
+      unitarity_kernel<3><<<nb, 256, 0, st>>>(nl, (const double2*)gauge, V, part, s->counters + slot, res);
+    LYM_CHECK_LAUNCH();
+    LYM_CUDA(cudaMemcpyAsync(s->host + slot * Scratch::kMaxVals, res, sizeof(double), cudaMemcpyDeviceToHost, st));
+    LYM_CUDA(cudaStreamSynchronize(st));
+    const double dev = s->host[slot * Scratch::kMaxVals] / (double)nl;
+    g->comp = dev < 1e-16;  // every link SU(N) to about 1e-8
+  }
+  const int nc = g->nc;
+  const int ncx = g->comp ? (nc - 1) * nc : nc * nc;
+  const int n32 = units_for(ncx, 2), n16 = units_for(ncx, 2);
+  if (g->u32 && g->n32 != n32) {
+    cudaFree(g->u32);
+    g->u32 = nullptr;
+  }
+  if (g->u16 && g->n16 != n16) {
+    cudaFree(g->u16);
+    g->u16 = nullptr;
+  }
+  const bool want32 = (g->prec_mask >> LYM_PREC_F32) & 1u;
+  const bool want16 = ((g->prec_mask >> LYM_PREC_F16) & 1u) || ((g->prec_mask >> LYM_PREC_BF16) & 1u);
+  if (want32 && !g->u32) {
+    if (cudaMalloc(&g->u32, sizeof(float4) * n32 * 2 * g->nd * g->Vh) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("FP32 links do not fit");
+      return LYM_ERR_OOM;
+    }
+  }
+  if (want16 && !g->u16) {
+    if (cudaMalloc(&g->u16, sizeof(uint2) * n16 * 2 * g->nd * g->Vh) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("FP16 links do not fit");
+      return LYM_ERR_OOM;
+    }
+  }
+  g->n32 = n32;
+  g->n16 = n16;
+  dim3 grid(grid_for(V, 128), g->nd);
+  const int c = g->comp ? 1 : 0;
+#define LYM_PACK(ND_, NC_)                                                                                        \
+  pack_gauge_kernel<ND_, NC_><<<grid, 128, 0, st>>>(g->geom, V, (const double2*)gauge, g->bcr, g->bci, g->u64, \
+                                                    g->u32, n32, c, g->u16, n16, c)
+  if (g->nd == 2 && nc == 2) LYM_PACK(2, 2);
+  else if (g->nd == 2 && nc == 3) LYM_PACK(2, 3);
+  else if (g->nd == 4 && nc == 2) LYM_PACK(4, 2);
+  else LYM_PACK(4, 3);
+#undef LYM_PACK
+  LYM_CHECK_LAUNCH();
+  if (g->work) {  // sloppy gauge pointers / compression may have changed
+    free_work(g->work);
+    g->work = nullptr;
+  }
+  return LYM_OK;
+}
+
+extern "C" {
+
+int lym_gauge_create(const lym_lattice* lat, int nc, const void* gauge, double bc_re, double bc_im,
+                     unsigned prec_mask, void* stream, lym_gauge** out) {
+  LYM_REQUIRE(lat && gauge && out, LYM_ERR_BAD_ARG, "null argument");
+  if (lat->nd != 2 && lat->nd != 4) {
+    set_error("Number of dimensions %d not supported for fermions!", lat->nd);
+    return LYM_ERR_UNSUPPORTED;
+  }
+  LYM_REQUIRE(nc == 2 || nc == 3, LYM_ERR_UNSUPPORTED, "N=%d not supported (2 or 3)", nc);
+  LYM_REQUIRE(lat->even, LYM_ERR_UNSUPPORTED, "even-odd ordering needs every extent even");
+  lym_gauge* g = new lym_gauge();
+  g->lat = lat;
+  g->nc = nc;
+  g->nd = lat->nd;
+  g->ns = lat->nd == 2 ? 2 : 4;
+  g->ncomp = g->ns * nc;
+  g->V = lat->V;
+  g->Vh = lat->V / 2;
+  g->bcr = bc_re;
+  g->bci = bc_im;
+  g->prec_mask = prec_mask;
+  g->geom = make_geom(lat);
+  const size_t nlink = (size_t)g->nd * nc * nc * g->V;
+  if (cudaMalloc(&g->uref, sizeof(double2) * nlink) != cudaSuccess ||
+      cudaMalloc(&g->u64, sizeof(double2) * nlink) != cudaSuccess) {
+    cudaGetLastError();
+    if (g->uref) cudaFree(g->uref);
+    delete g;
+    set_error("gauge copies do not fit");
+    return LYM_ERR_OOM;
+  }
+  int rc = pack_gauge(g, gauge, (cudaStream_t)stream);
+  if (rc) {
+    lym_gauge_destroy(g);
+    return rc;
+  }
+  *out = g;
+  return LYM_OK;
+}
+
+int lym_gauge_update(lym_gauge* g, const void* gauge, void* stream) {
+  LYM_REQUIRE(g && gauge, LYM_ERR_BAD_ARG, "null argument");
+  return pack_gauge(g, gauge, (cudaStream_t)stream);
+}
+
+int lym_gauge_destroy(lym_gauge* g) {
+  if (!g) return LYM_OK;
+  cudaDeviceSynchronize();
+  free_work(g->work);
+  if (g->uref) cudaFree(g->uref);
+  if (g->u64) cudaFree(g->u64);
+  if (g->u32) cudaFree(g->u32);
+  if (g->u16) cudaFree(g->u16);
+  delete g;
+  return LYM_OK;
+}
+
+int lym_wilson_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x, const lym_solver_params* params,
+                     lym_solver_report* reports, void* stream) {
+  return cg_solve(g, kappa, nrhs, b, x, params, reports, (cudaStream_t)stream);
+}
+
+}  // extern "C"

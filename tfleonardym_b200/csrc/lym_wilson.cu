@@ -1,0 +1,269 @@
+// Wilson Dirac operator in the reference layout (FP64, full lattice) and the
+// vector algebra the reference-compatible solvers need.
+//
+// One thread per (site, vector).  Each spinor component plane (ns, N, V) is
+// contiguous over sites, so every load of a complex128 is one coalesced
+// 16-byte access; neighbour indices come from the int32 copies of the
+// reference's own sup/sdn tables (lattice.py:86-120).
+#include <mutex>
+
+#include "lym_internal.cuh"
+#include "lym_kernels.cuh"
+
+namespace lym {
+
+// ---------------------------------------------------------------------------
+// library-owned reduction scratch, one per device
+// ---------------------------------------------------------------------------
+static std::mutex g_scratch_mu;
+static std::mutex g_host_reduce_mu;
+std::mutex& host_reduce_mutex() { return g_host_reduce_mu; }
+static Scratch g_scratch[64];
+static bool g_scratch_ok[64];
+
+int scratch_get(Scratch** out) {
+  int dev = 0;
+  LYM_CUDA(cudaGetDevice(&dev));
+  LYM_REQUIRE(dev >= 0 && dev < 64, LYM_ERR_BAD_ARG, "device index %d", dev);
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  Scratch& s = g_scratch[dev];
+  if (!g_scratch_ok[dev]) {
+    size_t np = (size_t)Scratch::kSlots * Scratch::kMaxBlocks * Scratch::kMaxVals;
+    if (cudaMalloc(&s.partials, np * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&s.counters, Scratch::kSlots * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&s.results, Scratch::kSlots * Scratch::kMaxVals * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&s.host, Scratch::kSlots * Scratch::kMaxVals * sizeof(double)) != cudaSuccess) {
+      set_error("scratch allocation failed");
+      return LYM_ERR_OOM;
+    }
+    LYM_CUDA(cudaMemset(s.counters, 0, Scratch::kSlots * sizeof(unsigned)));
+    LYM_CUDA(cudaDeviceSynchronize());
+    g_scratch_ok[dev] = true;
+  }
+  *out = &s;
+  return LYM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// full-lattice hop, reference layout
+// ---------------------------------------------------------------------------
+template <int ND, int NC, bool HERM>
+__global__ void __launch_bounds__(128) wilson_full_kernel(
+    const int32_t* __restrict__ tab, int V, int Lt, double kappa, double bcr, double bci,
+    const double2* __restrict__ U, const double2* __restrict__ in, double2* __restrict__ out) {
+  constexpr int NS = Gamma<ND>::NS;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  const size_t vec = (size_t)NS * NC * V;
+  const double2* psi = in + blockIdx.y * vec;
+  double2* res = out + blockIdx.y * vec;
+  const cx<double> bc{bcr, bci};
+
+  cx<double> acc[NS][NC];
+#pragma unroll
+  for (int a = 0; a < NS; ++a)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[a][c] = czero<double>();
+
+#pragma unroll
+  for (int mu = 0; mu < ND; ++mu) {
+    // forward: U_mu(x) (1 - g_mu) psi(x + mu)
+    {
+      const int y = tab[mu * V + s];
+      cx<double> u[NC][NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) u[i][j] = ld(U + ((size_t)(mu * NC + i) * NC + j) * V + s);
+      if (mu == ND - 1 && (s % Lt) == Lt - 1) {
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+#pragma unroll
+          for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
+      }
+#pragma unroll
+      for (int a = 0; a < NS / 2; ++a) {
+        const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+        cx<double> h[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+          h[c] = ld(psi + (size_t)(a * NC + c) * V + y) -
+                 mul_phase(ph, ld(psi + (size_t)(jb * NC + c) * V + y));
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+          cx<double> t = czero<double>();
+#pragma unroll
+          for (int j = 0; j < NC; ++j) t += u[i][j] * h[j];
+          acc[a][i] += t;
+          acc[jb][i] += mul_phase(phase_neg(phase_conj(ph)), t);
+        }
+      }
+    }
+    // backward: U_mu(x - mu)^dag (1 + g_mu) psi(x - mu)
+    {
+      const int y = tab[ND * V + mu * V + s];
+      cx<double> u[NC][NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) u[i][j] = ld(U + ((size_t)(mu * NC + i) * NC + j) * V + y);
+      if (mu == ND - 1 && (s % Lt) == 0) {
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+#pragma unroll
+          for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
+      }
+#pragma unroll
+      for (int a = 0; a < NS / 2; ++a) {
+        const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+        cx<double> h[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+          h[c] = ld(psi + (size_t)(a * NC + c) * V + y) +
+                 mul_phase(ph, ld(psi + (size_t)(jb * NC + c) * V + y));
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+          cx<double> t = czero<double>();
+#pragma unroll
+          for (int j = 0; j < NC; ++j) t += cmul_cj(u[j][i], h[j]);
+          acc[a][i] += t;
+          acc[jb][i] += mul_phase(phase_conj(ph), t);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < NS; ++a)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      cx<double> v = ld(psi + (size_t)(a * NC + c) * V + s) + kappa * acc[a][c];
+      if (HERM && a >= NS / 2) v = -v;
+      st(res + (size_t)(a * NC + c) * V + s, v);
+    }
+}
+
+template <int ND, int NC>
+static int launch_full(const lym_lattice* lat, double kappa, int herm, double bcr, double bci,
+                       const void* gauge, int nvec, const void* in, void* out, cudaStream_t st) {
+  dim3 grid(grid_for(lat->V, 128), nvec);
+  const int Lt = lat->dims[ND - 1];
+  if (herm)
+    wilson_full_kernel<ND, NC, true><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
+                                                          (const double2*)gauge, (const double2*)in,
+                                                          (double2*)out);
+  else
+    wilson_full_kernel<ND, NC, false><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
+                                                           (const double2*)gauge, (const double2*)in,
+                                                           (double2*)out);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+int wilson_full(const lym_lattice* lat, int nc, double kappa, int herm, double bcr, double bci,
+                const void* gauge, int nvec, const void* in, void* out, cudaStream_t st) {
+  LYM_REQUIRE(lat && gauge && in && out, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(in != out, LYM_ERR_BAD_ARG, "in and out must not alias");
+  LYM_REQUIRE(nvec >= 1 && nvec <= 65535, LYM_ERR_BAD_ARG, "nvec out of range");
+  if (lat->nd != 2 && lat->nd != 4) {
+    set_error("Number of dimensions %d not supported for fermions!", lat->nd);
+    return LYM_ERR_UNSUPPORTED;
+  }
+  LYM_REQUIRE(nc == 2 || nc == 3, LYM_ERR_UNSUPPORTED, "N=%d not supported (2 or 3)", nc);
+  if (lat->nd == 2 && nc == 2) return launch_full<2, 2>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);
+  if (lat->nd == 2 && nc == 3) return launch_full<2, 3>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);
+  if (lat->nd == 4 && nc == 2) return launch_full<4, 2>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);
+  return launch_full<4, 3>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);
+}
+
+// ---------------------------------------------------------------------------
+// vector algebra, complex128
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) cdot_kernel(int64_t n, const double2* __restrict__ a,
+                                                   const double2* __restrict__ b, double* partials,
+                                                   unsigned* counter, double* result) {
+  __shared__ double sh[2 * 32];
+  double v[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double2 x = a[i], y = b[i];
+    v[0] += x.x * y.x + x.y * y.y;
+    v[1] += x.x * y.y - x.y * y.x;
+  }
+  if (grid_sum<2>(v, partials, counter, sh) && threadIdx.x == 0) {
+    result[0] = v[0];
+    result[1] = v[1];
+  }
+}
+
+__global__ void caxpby_kernel(int64_t n, double ar, double ai, const double2* __restrict__ x, double br,
+                              double bi, double2* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double2 xv = x[i], yv = y[i];
+    y[i] = make_double2(ar * xv.x - ai * xv.y + br * yv.x - bi * yv.y,
+                        ar * xv.y + ai * xv.x + br * yv.y + bi * yv.x);
+  }
+}
+
+unsigned reduction_blocks(int64_t n, int block) {
+  int64_t b = (n + block - 1) / block;
+  if (b > Scratch::kMaxBlocks) b = Scratch::kMaxBlocks;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+int cdot_device(int64_t n, const void* a, const void* b, double* result_dev, int slot, cudaStream_t st) {
+  Scratch* s;
+  int rc = scratch_get(&s);
+  if (rc) return rc;
+  unsigned nb = reduction_blocks(n, 256);
+  cdot_kernel<<<nb, 256, 0, st>>>(n, (const double2*)a, (const double2*)b,
+                                   s->partials + (size_t)slot * Scratch::kMaxBlocks * Scratch::kMaxVals,
+                                   s->counters + slot, result_dev);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+}  // namespace lym
+
+using namespace lym;
+
+extern "C" {
+
+int lym_wilson_apply(const lym_lattice* lat, int nc, double kappa, int hermitian, double bc_re, double bc_im,
+                     const void* gauge, const void* in, void* out, void* stream) {
+  return wilson_full(lat, nc, kappa, hermitian, bc_re, bc_im, gauge, 1, in, out, (cudaStream_t)stream);
+}
+
+int lym_wilson_apply_batch(const lym_lattice* lat, int nc, double kappa, int hermitian, double bc_re,
+                           double bc_im, const void* gauge, int nvec, const void* in, void* out, void* stream) {
+  return wilson_full(lat, nc, kappa, hermitian, bc_re, bc_im, gauge, nvec, in, out, (cudaStream_t)stream);
+}
+
+int lym_cdot(int64_t n, const void* a, const void* b, double* result, void* stream) {
+  LYM_REQUIRE(n >= 0 && a && b && result, LYM_ERR_BAD_ARG, "null argument");
+  Scratch* s;
+  int rc = scratch_get(&s);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::lock_guard<std::mutex> lk(host_reduce_mutex());
+  const int slot = 1;
+  rc = cdot_device(n, a, b, s->results + slot * Scratch::kMaxVals, slot, st);
+  if (rc) return rc;
+  LYM_CUDA(cudaMemcpyAsync(s->host + slot * Scratch::kMaxVals, s->results + slot * Scratch::kMaxVals,
+                           2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  LYM_CUDA(cudaStreamSynchronize(st));
+  result[0] = s->host[slot * Scratch::kMaxVals];
+  result[1] = s->host[slot * Scratch::kMaxVals + 1];
+  return LYM_OK;
+}
+
+int lym_caxpby(int64_t n, const double* a, const void* x, const double* b, void* y, void* stream) {
+  LYM_REQUIRE(n >= 0 && a && b && x && y, LYM_ERR_BAD_ARG, "null argument");
+  if (n == 0) return LYM_OK;
+  unsigned nb = reduction_blocks(n, 256) * 4;
+  caxpby_kernel<<<nb, 256, 0, (cudaStream_t)stream>>>(n, a[0], a[1], (const double2*)x, b[0], b[1],
+                                                      (double2*)y);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+}  // extern "C"

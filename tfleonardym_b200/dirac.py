@@ -1,0 +1,221 @@
+"""Dirac operators (mirror of the reference's dirac.py on the GPU).
+
+``DiracWilsonOperator`` keeps the reference constructor and attributes
+(dirac.py:253-378).  ``apply`` runs the fused FP64 Wilson kernel
+(lym_wilson_apply, replacing dirac.py:458-523 + 649-662); ``lie_derivative``
+runs the fused per-link force kernel (lym_fermion_force, dirac.py:525-565).
+Only the fundamental representation exists here; the adjoint one raises.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _dev, _lib
+from . import boundary_conditions as bcs
+from . import lattice as lt
+
+
+class Operator:
+    def __init__(self, hermitian=False):
+        self.hermitian = hermitian
+
+
+class ShiftedOperator(Operator):
+    """(A + shift) (dirac.py:15-25)."""
+
+    def __init__(self, operator_to_shift: Operator, shift: float):
+        super().__init__(operator_to_shift.hermitian)
+        self.operator_to_shift = operator_to_shift
+        self.shift = shift
+
+    def set_gauge_configuration(self, cfg):
+        self.operator_to_shift.set_gauge_configuration(cfg)
+
+    def apply(self, vector):
+        return _dev.axpby(1.0, self.operator_to_shift.apply(vector), self.shift, vector)
+
+
+class SquareOperator(Operator):
+    """A A (dirac.py:28-37)."""
+
+    def __init__(self, operator_to_square: Operator):
+        super().__init__(operator_to_square.hermitian)
+        self.operator_to_square = operator_to_square
+
+    def set_gauge_configuration(self, cfg):
+        self.operator_to_square.set_gauge_configuration(cfg)
+
+    def apply(self, vector):
+        return self.operator_to_square.apply(self.operator_to_square.apply(vector))
+
+
+class RationalApproximation(Operator):
+    """shift + sum_i alpha_i (A + beta_i)^-1 (dirac.py:40-73)."""
+
+    def __init__(self, operator, alphas, betas, shift, solver):
+        super().__init__(operator.hermitian)
+        self.operator = operator
+        self.alphas = alphas
+        self.betas = betas
+        self.shift = shift
+        self.solver = solver
+
+    def set_gauge_configuration(self, cfg):
+        self.operator.set_gauge_configuration(cfg)
+
+    def apply(self, vector):
+        solutions = self.solver.solve(self.operator, vector, self.betas)
+        result = _dev.axpby(0.0, vector, self.shift, vector)
+        for solution, alpha in zip(solutions, self.alphas):
+            _dev.axpby_(alpha, solution, 1.0, result)
+        return result
+
+    def evaluate(self, x: float):
+        result = self.shift
+        for alpha, beta in zip(self.alphas, self.betas):
+            result += alpha / (x + beta)
+        return result
+
+    def test_inverter(self, vector):
+        """Residual |A x - v|^2 per pole (the reference prints them, dirac.py:69-73)."""
+        out = []
+        for solution, beta in zip(self.solver.solve(self.operator, vector, self.betas), self.betas):
+            v = _dev.axpby(1.0, self.operator.apply(solution), beta, solution)
+            d = _dev.axpby(1.0, v, -1.0, vector)
+            out.append(_dev.cdot(d, d))
+        return out
+
+
+class DiracWilsonOperator(Operator):
+    """Wilson operator D = 1 + kappa sum_mu [U(1-g_mu)T_+mu + U^dag(1+g_mu)T_-mu],
+    Q = gamma_d D when hermitian (dirac.py:253-662)."""
+
+    def __init__(self, cfg: lt.Configuration, kappa, hermitian=False, mode="projected",
+                 representation="adjoint", boundary_condition_provider=None):
+        super().__init__(hermitian)
+        self.kappa = kappa
+        self.mode = mode
+        self.representation = representation
+        if mode not in ("projected", "simple"):
+            raise RuntimeError(f"Unknown dirac multiplication mode {mode}")
+        if representation != "fundamental":
+            raise NotImplementedError("the adjoint representation is not built on the GPU path; "
+                                      "use representation='fundamental'")
+        self.boundary_condition_provider = boundary_condition_provider
+        self._solver_gauge = None
+        self._solver_gauge_key = None
+        self.set_gauge_configuration(cfg)
+        self.set_gamma_matrices()
+
+    # dirac.py:283-300: only D = 2 and 4 carry fermions
+    def set_gamma_matrices(self):
+        if self.number_of_dimensions == 2:
+            self.spinor_dimension = 2
+        elif self.number_of_dimensions == 4:
+            self.spinor_dimension = 4
+        else:
+            raise RuntimeError(f"Number of dimensions {self.number_of_dimensions} not supported for fermions!")
+
+    def set_gauge_configuration(self, cfg):
+        gauge = _dev.as_c128(cfg.gauge_field, "gauge_field")
+        self.number_of_dimensions = gauge.shape[0]
+        self.number_of_colors = gauge.shape[1]
+        self.volume = gauge.shape[-1]
+        self.cfg = cfg
+        self.original_cfg = cfg
+        factor, apply_tensor = bcs.provider_factor(self.boundary_condition_provider)
+        if apply_tensor:
+            gauge = _dev.as_c128(self.boundary_condition_provider(gauge))
+        self.bc = factor
+        self.fermion_gauge_field = gauge
+        geometry = tuple(cfg.geometry) if cfg.geometry is not None else None
+        if geometry is None or int(np.prod(geometry)) != self.volume:
+            raise RuntimeError("Configuration.geometry does not match the gauge field volume")
+        self.geometry = geometry
+        self.lattice = lt.get_lattice(geometry)
+        self._gauge_version = getattr(self, "_gauge_version", 0) + 1
+
+    # -- operator application ------------------------------------------------
+    def apply(self, input_vector):
+        v = _dev.as_c128(input_vector, "input_vector")
+        out = torch.empty_like(v)
+        nvec = 1
+        if v.dim() == 4:  # a batch (nvec, ns, N, V)
+            nvec = v.shape[0]
+        elif v.dim() != 3:
+            raise RuntimeError("spinor must be (ns, N, V) or (nvec, ns, N, V)")
+        _lib.check(_lib.lib().lym_wilson_apply_batch(
+            self.lattice.handle, self.number_of_colors, float(self.kappa), int(bool(self.hermitian)),
+            self.bc.real, self.bc.imag, _dev.ptr(self.fermion_gauge_field), nvec, _dev.ptr(v), _dev.ptr(out),
+            _dev.stream()), "lym_wilson_apply")
+        return out
+
+    multiply_in_fundamental_representation = apply
+    simple_multiply_in_fundamental_representation = apply
+
+    def apply_hermiticity(self, input_vector):
+        if not self.hermitian:
+            return input_vector.clone()
+        out = input_vector.clone()
+        out[input_vector.shape[0] // 2:] *= -1
+        return out
+
+    def lie_derivative(self, X, Y):
+        """kappa-weighted Lie derivative (nd, N, N, V) of dirac.py:525-565."""
+        force = torch.zeros((self.number_of_dimensions, self.number_of_colors, self.number_of_colors,
+                             self.volume), dtype=torch.complex128, device="cuda")
+        self.accumulate_force(force, [1.0], _dev.as_c128(X)[None], _dev.as_c128(Y)[None], symmetric=False)
+        return force
+
+    def accumulate_force(self, force, alphas, X, Y, symmetric=True, scale=1.0):
+        """force += scale * sum_i alpha_i [L(X_i, Y_i) (+ L(Y_i, X_i) if symmetric)];
+        X, Y stacked (nterms, ns, N, V).  Fused n_flavor.force (fermion_action.py:87-91)."""
+        X = _dev.as_c128(X)
+        Y = _dev.as_c128(Y)
+        n = X.shape[0]
+        al = (ctypes.c_double * n)(*[float(np.real(a)) for a in alphas])
+        _lib.check(_lib.lib().lym_fermion_force(
+            self.lattice.handle, self.number_of_colors, float(self.kappa), int(bool(self.hermitian)),
+            self.bc.real, self.bc.imag, _dev.ptr(self.fermion_gauge_field), n, al, _dev.ptr(X), _dev.ptr(Y),
+            int(bool(symmetric)), float(scale), _dev.ptr(force), _dev.stream()), "lym_fermion_force")
+        return force
+
+    # -- device gauge for the solvers -----------------------------------------
+    def solver_gauge(self, precisions=("f32", "f16", "bf16")):
+        """lym_gauge handle (even-odd links) for the current configuration."""
+        mask = 0
+        for p in precisions:
+            mask |= 1 << _lib.PREC[p]
+        key = (self._gauge_version, mask)
+        if self._solver_gauge is not None and self._solver_gauge_key == key:
+            return self._solver_gauge
+        if self._solver_gauge is not None and self._solver_gauge_key[1] == mask:
+            _lib.check(_lib.lib().lym_gauge_update(self._solver_gauge, _dev.ptr(self.fermion_gauge_field),
+                                                   _dev.stream()), "lym_gauge_update")
+        else:
+            self._free_solver_gauge()
+            h = ctypes.c_void_p()
+            _lib.check(_lib.lib().lym_gauge_create(self.lattice.handle, self.number_of_colors,
+                                                   _dev.ptr(self.fermion_gauge_field), self.bc.real, self.bc.imag,
+                                                   mask, _dev.stream(), ctypes.byref(h)), "lym_gauge_create")
+            self._solver_gauge = h
+        self._solver_gauge_key = key
+        self._gauge_ref = self.fermion_gauge_field  # keep the source alive while the handle is used
+        return self._solver_gauge
+
+    def _free_solver_gauge(self):
+        if self._solver_gauge is not None and _lib._lib is not None:
+            torch.cuda.synchronize()
+            _lib.lib().lym_gauge_destroy(self._solver_gauge)
+        self._solver_gauge = None
+
+    def __del__(self):
+        try:
+            self._free_solver_gauge()
+        except Exception:
+            pass
+
+
+def Propagator(*_a, **_k):  # noqa: N802 - reference name
+    raise NotImplementedError("Propagator is a measurement consumer outside the solve path")

@@ -1,0 +1,206 @@
+"""Krylov solvers (mirror of the reference's dirac_solver.py on the GPU).
+
+* ``multishift_solver`` -- the reference's multishift MMMR (dirac_solver.py:13-53):
+  same constructor, same ``solve(operator, source, shifts)`` returning a list,
+  absolute stop |<r,r>| < precision, negative leading shifts handed to
+  BiCGStab, "failed to converge" printed and the last iterate returned.  On a
+  ``SquareOperator(DiracWilsonOperator)`` the whole solve runs in lym_mmmr_solve;
+  on any other operator the loop calls ``operator.apply`` with lym vector kernels.
+* ``biconjugate_gradient`` -- BiCGStab of dirac_solver.py:56-110.
+* ``multishift_cg`` -- builder-defined drop-in for ``multishift_solver`` on
+  Q^2 + sigma (lym_multishift_solve); tolerance is relative, tol * |b|.
+* ``conjugate_gradient`` -- builder-defined even-odd CG for D x = b (or Q x = b)
+  with FP64 reliable updates and FP64 / FP32 / FP16 / BF16 inner iterations
+  (lym_wilson_solve).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _dev, _lib
+from .dirac import DiracWilsonOperator, ShiftedOperator, SquareOperator
+
+VERBOSE = True
+
+
+def _print(*args):
+    if VERBOSE:
+        print(*args)
+
+
+def _wilson_square(operator):
+    """The DiracWilsonOperator behind SquareOperator(Q) with hermitian Q, else None."""
+    if isinstance(operator, SquareOperator) and isinstance(operator.operator_to_square, DiracWilsonOperator):
+        q = operator.operator_to_square
+        if q.hermitian:
+            return q
+    return None
+
+
+class multishift_solver:  # noqa: N801 - reference name
+    def __init__(self, max_steps, precision, omega=0.95):
+        self.max_steps = max_steps
+        self.precision = precision
+        self.omega = omega
+        self.last_steps = None
+
+    def solve(self, operator, source, shifts: list):
+        source = _dev.as_c128(source, "source")
+        shifts = list(shifts)
+        solutions = [torch.zeros_like(source) for _ in shifts]
+        first = 0
+        while first < len(shifts) and shifts[first] < 0:  # dirac_solver.py:26-30
+            solver = biconjugate_gradient(self.max_steps, self.precision)
+            solutions[first] = solver.solve(ShiftedOperator(operator, shifts[first]), source)
+            first += 1
+        rest = shifts[first:]
+        if not rest:
+            return solutions
+        q = _wilson_square(operator)
+        if q is not None:
+            xs = torch.empty((len(rest),) + tuple(source.shape), dtype=torch.complex128, device=source.device)
+            steps = ctypes.c_int()
+            sh = (ctypes.c_double * len(rest))(*[float(s) for s in rest])
+            rc = _lib.lib().lym_mmmr_solve(q.solver_gauge(()), float(q.kappa), len(rest), sh, _dev.ptr(source),
+                                           _dev.ptr(xs), int(self.max_steps), float(self.precision),
+                                           float(self.omega), ctypes.byref(steps), _dev.stream())
+            self.last_steps = steps.value
+            if rc == _lib.LYM_ERR_NOT_CONVERGED:
+                _print(f"MMMRMultishiftsolver: failed to find convergence after {steps.value} steps")
+            else:
+                _lib.check(rc, "lym_mmmr_solve")
+                _print(f"MMMRMultishiftsolver: convergence after {steps.value} steps")
+            for i in range(len(rest)):
+                solutions[first + i] = xs[i]
+            return solutions
+        return self._generic(operator, source, rest, solutions, first)
+
+    def _generic(self, operator, source, shifts, solutions, first):
+        f = [1.0 for _ in shifts]
+        r = source.clone()
+        xs = [torch.zeros_like(source) for _ in shifts]
+        step = 0
+        for step in range(self.max_steps):
+            p = _dev.axpby(1.0, operator.apply(r), shifts[-1], r)
+            alpha = self.omega * _dev.cdot(p, r) / _dev.cdot(p, p)
+            _dev.axpby_(alpha, r, 1.0, xs[-1])
+            for i, s in enumerate(shifts[:-1]):
+                f[i] = f[i] / (1 + (s - shifts[-1]) * alpha)
+                _dev.axpby_(alpha * f[i], r, 1.0, xs[i])
+            _dev.axpby_(-alpha, p, 1.0, r)
+            if abs(_dev.cdot(r, r)) < self.precision:
+                self.last_steps = step
+                _print(f"MMMRMultishiftsolver: convergence after {step} steps")
+                break
+        else:
+            self.last_steps = step
+            _print(f"MMMRMultishiftsolver: failed to find convergence after {step} steps")
+        for i, x in enumerate(xs):
+            solutions[first + i] = x
+        return solutions
+
+
+class biconjugate_gradient:  # noqa: N801 - reference name
+    """BiCGStab of dirac_solver.py:61-110 (x0 = source or guess, r0 = x0 - A x0,
+    r_hat = x0 + A x0, absolute stop), with lym vector kernels."""
+
+    def __init__(self, max_steps, precision):
+        self.max_steps = max_steps
+        self.precision = precision
+        self.last_steps = None
+
+    def solve(self, operator, source, initial_guess=None):
+        source = _dev.as_c128(source)
+        x = (source if initial_guess is None else _dev.as_c128(initial_guess)).clone()
+        init = operator.apply(x)
+        r = _dev.axpby(1.0, x, -1.0, init)
+        rhat = _dev.axpby(1.0, x, 1.0, init)
+        alpha = omega = rho = 1.0
+        p = torch.zeros_like(source)
+        nu = torch.zeros_like(source)
+        step = 0
+        for step in range(self.max_steps):
+            rho_next = _dev.cdot(rhat, r)
+            beta = (rho_next / rho) * (alpha / omega)
+            p = _dev.axpby(1.0, r, beta, _dev.axpby(1.0, p, -omega, nu))
+            nu = operator.apply(p)
+            alpha = rho_next / _dev.cdot(rhat, nu)
+            s = _dev.axpby(1.0, r, -alpha, nu)
+            t = operator.apply(s)
+            omega = _dev.cdot(t, s) / _dev.cdot(t, t)
+            _dev.axpby_(alpha, p, 1.0, x)
+            _dev.axpby_(omega, s, 1.0, x)
+            r = _dev.axpby(1.0, s, -omega, t)
+            if abs(_dev.cdot(r, r)) < self.precision:
+                self.last_steps = step
+                _print(f"BiconjugateGradient: convergence after {step} steps")
+                return x
+            rho = rho_next
+        self.last_steps = step
+        _print(f"BiconjugateGradient: failed to find convergence after {step} steps")
+        return x
+
+
+class multishift_cg:  # noqa: N801 - named like the reference solvers
+    """Multishift CG on (Q^2 + sigma_k): same interface as multishift_solver;
+    stops when every shift's residual is below tol * |source|."""
+
+    def __init__(self, max_steps, tol):
+        self.max_steps = max_steps
+        self.tol = tol
+        self.last_steps = None
+
+    def solve(self, operator, source, shifts):
+        q = _wilson_square(operator)
+        if q is None:
+            raise TypeError("multishift_cg needs SquareOperator(DiracWilsonOperator(hermitian=True))")
+        source = _dev.as_c128(source)
+        xs = torch.empty((len(shifts),) + tuple(source.shape), dtype=torch.complex128, device=source.device)
+        it = ctypes.c_int()
+        sh = (ctypes.c_double * len(shifts))(*[float(s) for s in shifts])
+        rc = _lib.lib().lym_multishift_solve(q.solver_gauge(()), float(q.kappa), len(shifts), sh, _dev.ptr(source),
+                                             _dev.ptr(xs), float(self.tol), int(self.max_steps), ctypes.byref(it),
+                                             _dev.stream())
+        self.last_steps = it.value
+        if rc == _lib.LYM_ERR_NOT_CONVERGED:
+            _print(f"multishift CG: failed to find convergence after {it.value} steps")
+        else:
+            _lib.check(rc, "lym_multishift_solve")
+        return [xs[i] for i in range(len(shifts))]
+
+
+class conjugate_gradient:  # noqa: N801 - named like the reference solvers
+    """Even-odd CG for D x = b (Q x = b when the operator is hermitian) with FP64
+    reliable updates.  ``precision`` in {"f64", "f32", "f16", "bf16"} is the inner
+    precision; ``tol`` the target true relative residual |b - D x| / |b|."""
+
+    def __init__(self, max_steps=20000, tol=1e-10, precision="f64", delta=0.1, chunk=8):
+        self.max_steps = max_steps
+        self.tol = tol
+        self.precision = precision
+        self.delta = delta
+        self.chunk = chunk
+        self.reports = None
+
+    def solve(self, operator, source):
+        if not isinstance(operator, DiracWilsonOperator):
+            raise TypeError("conjugate_gradient solves with a DiracWilsonOperator")
+        b = _dev.as_c128(source)
+        batched = b.dim() == 4
+        bb = b if batched else b[None]
+        x = torch.empty_like(bb)
+        n = bb.shape[0]
+        prm = _lib.SolverParams(float(self.tol), int(self.max_steps), _lib.PREC[self.precision], float(self.delta),
+                                int(bool(operator.hermitian)), int(self.chunk))
+        reps = (_lib.SolverReport * n)()
+        precs = () if self.precision == "f64" else (self.precision,)
+        rc = _lib.lib().lym_wilson_solve(operator.solver_gauge(precs), float(operator.kappa), n, _dev.ptr(bb),
+                                         _dev.ptr(x), ctypes.byref(prm), reps, _dev.stream())
+        self.reports = [dict(status=r.status, iterations=r.iterations, reliable_updates=r.reliable_updates,
+                             true_residual=r.true_residual) for r in reps]
+        if rc == _lib.LYM_ERR_NOT_CONVERGED:
+            _print(f"conjugate_gradient: failed to find convergence ({self.reports})")
+        else:
+            _lib.check(rc, "lym_wilson_solve")
+        return x if batched else x[0]
