@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""Wilson-CG solves/s at 1e-10 true relative residual on one node.
+
+Workload (the reference's GPU-method configuration): D=4 SU(3) 16^4,
+kappa=0.13, links U = reunit(exp(i 0.25 H)) with H traceless Hermitian
+(complex entries of unit variance), antiperiodic time boundary for the
+fermions, sources unit complex Gaussian.  One step = one batched solve of
+``--nrhs`` right-hand sides D x_i = b_i by the even-odd CG with norm-scaled
+FP16 inner iterations and FP64 reliable updates, each answer verified by its
+FP64 true residual.  The plain FP64 even-odd CG, one solve at a time, is
+timed in the same run.  Inputs (nrhs x 12.6 MB of sources plus as much of
+solutions) are larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lym|reference]
+
+Multi-GPU: replicas only (independent solves per rank, no collective on the
+data path); the value is the whole-job solves/s.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GEOMETRY = (16, 16, 16, 16)
+NC = 3
+KAPPA = 0.13
+EPS = 0.25
+TOL = 1e-10
+METRIC = "Wilson-CG solves/s at 1e-10 true relative residual"
+ITER_FILE = os.path.join(ROOT, "profiles", "wilson_cg_16x16x16x16_iterations.txt")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dslash_eo_f16_16x16x16x16_traffic.txt")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lym", choices=["lym", "reference"])
+    ap.add_argument("--nrhs", type=int, default=16)
+    ap.add_argument("--precision", default="f16", choices=["f64", "f32", "f16", "bf16"])
+    ap.add_argument("--plain-solves", type=int, default=4)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def host_links(seed):
+    """H per link (nd, V, N, N): traceless Hermitian, complex entries of unit variance."""
+    rng = np.random.default_rng(seed)
+    nd, vol = len(GEOMETRY), int(np.prod(GEOMETRY))
+    a = rng.normal(size=(nd, vol, NC, NC)) + 1j * rng.normal(size=(nd, vol, NC, NC))
+    h = (a + np.conj(np.swapaxes(a, -1, -2))) / 2
+    tr = np.trace(h, axis1=-2, axis2=-1) / NC
+    h = h - tr[..., None, None] * np.eye(NC)
+    return h
+
+
+def host_sources(seed, n):
+    rng = np.random.default_rng(seed)
+    vol = int(np.prod(GEOMETRY))
+    return (rng.normal(size=(n, 4, NC, vol)) + 1j * rng.normal(size=(n, 4, NC, vol))) / np.sqrt(2)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle's even-odd CG on the same workload (bounded sample)
+# ---------------------------------------------------------------------------
+def oracle_cg_iteration_seconds(seconds, seed=2026):
+    """Time CG iterations of the oracle (oracle.lym_oracle.eo_solve's CGNR on the
+    16^4 even-odd system) for about ``seconds`` of CPU work; returns (s/iteration, n)."""
+    import scipy.linalg
+
+    from oracle import lym_oracle as O
+    h = host_links(seed)
+    u = scipy.linalg.expm(1j * EPS * h)  # (nd, V, N, N)
+    u = O.unitary_sqrt_projection(np.ascontiguousarray(np.transpose(u, (0, 2, 3, 1))))
+    setup = O.WilsonSetup(u, KAPPA, GEOMETRY, bc_factor=-1, hermitian=False)
+    b = host_sources(seed + 1, 1)[0]
+    par, cb, eo = O.parity_maps(GEOMETRY)
+    k = KAPPA
+
+    def h_eo(vo):
+        full = O.from_eo(np.zeros_like(vo), vo, eo)
+        return O.hopping(setup.gauge_bc, full, setup.tables)[..., eo[0]]
+
+    def h_oe(ve):
+        full = O.from_eo(ve, np.zeros_like(ve), eo)
+        return O.hopping(setup.gauge_bc, full, setup.tables)[..., eo[1]]
+
+    def m(ve):
+        return ve - k * k * h_eo(h_oe(ve))
+
+    def mdag(ve):
+        return O.gamma_d(m(O.gamma_d(ve)))
+
+    be, bo = O.to_eo(b, eo)
+    bp = be - k * h_eo(bo)
+    x = np.zeros_like(bp)
+    r = mdag(bp)
+    p = r.copy()
+    rr = np.real(O.dot(r, r))
+    t0 = time.perf_counter()
+    n = 0
+    while True:  # the loop body of oracle.lym_oracle.cg_normal
+        t = m(p)
+        alpha = rr / np.real(O.dot(t, t))
+        x = x + alpha * p
+        r = r - alpha * mdag(t)
+        rr_new = np.real(O.dot(r, r))
+        p = r + (rr_new / rr) * p
+        rr = rr_new
+        n += 1
+        if time.perf_counter() - t0 > seconds and n >= 2:
+            break
+    return (time.perf_counter() - t0) / n, n
+
+
+def read_iterations(default=80):
+    try:
+        for line in open(ITER_FILE):
+            if line.startswith("fp64_iterations="):
+                return int(line.split("=")[1])
+    except OSError:
+        pass
+    return default
+
+
+def read_traffic():
+    try:
+        for line in open(TRAFFIC_FILE):
+            if line.startswith("bytes_per_launch="):
+                return float(line.split("=")[1])
+    except OSError:
+        pass
+    return None
+
+
+def _ref_worker(args):
+    seconds, seed = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    return oracle_cg_iteration_seconds(seconds, seed)
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the oracle restatement of the reference's algorithm on
+    all host cores (one process per core, each on its own right-hand side)."""
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0))
+    procs = max(1, min(cores, 32))
+    iters = read_iterations()
+    per_step = []
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        for step in range(args.warmup + args.steps):
+            res = pool.map(_ref_worker, [(max(1.0, args.cpu_seconds / 4), 100 + i) for i in range(procs)])
+            if step >= args.warmup:
+                per_step.append(sum(1.0 / (s * iters) for s, _ in res))
+    value = statistics.mean(per_step)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic", "scaling": "weak", "vs_baseline": None,
+        "config": {"workload": "wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
+                   "links": "reunit(exp(i 0.25 H))", "bc": "antiperiodic time"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "port",
+                         "sample": f"{procs} processes x CG iterations of the oracle's even-odd CGNR on 16^4 "
+                                   f"(about {max(1.0, args.cpu_seconds / 4):.0f} s each per step), extrapolated "
+                                   f"with {iters} iterations per solve"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_lym(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from tfleonardym_b200 import _dev, _lib, boundary_conditions, dirac, dirac_solver, hmc
+    from tfleonardym_b200 import lattice as lt
+
+    dirac_solver.VERBOSE = False
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nd, vol = len(GEOMETRY), int(np.prod(GEOMETRY))
+    # links: exp(i eps H) via the link-update kernel from unit links, reunitarised
+    h = host_links(1234 + rank)
+    p = torch.from_numpy(np.ascontiguousarray(np.transpose(1j * h, (0, 2, 3, 1)))).to(dev)
+    ident = torch.zeros((nd, NC, NC, vol), dtype=torch.complex128, device=dev)
+    for i in range(NC):
+        ident[:, i, i] = 1
+    links = hmc.update_link_field(ident, p, EPS, reunitarize=True)
+    cfg = lt.Configuration(links, GEOMETRY, NC, nd)
+    op = dirac.DiracWilsonOperator(cfg, KAPPA, False, representation="fundamental",
+                                   boundary_condition_provider=boundary_conditions.time_antiperiodic_provider(-1))
+    B = args.nrhs
+    b_host = torch.from_numpy(host_sources(99 + rank, B)).pin_memory()
+    b_dev = b_host.to(dev)
+    x_host = torch.empty_like(b_host).pin_memory()
+    mixed = dirac_solver.conjugate_gradient(tol=TOL, precision=args.precision, chunk=8)
+    plain = dirac_solver.conjugate_gradient(tol=TOL, precision="f64", chunk=8)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def check(reports):
+        bad = [r for r in reports if r["status"] != 0 or r["true_residual"] > TOL]
+        if bad:
+            raise RuntimeError(f"solve missed the tolerance: {bad[:2]}")
+
+    # warm-up (also builds the graphs and workspaces)
+    for _ in range(max(args.warmup, 3)):
+        mixed.solve(op, b_dev)
+        check(mixed.reports)
+    plain.solve(op, b_dev[0])
+    check(plain.reports)
+    torch.cuda.synchronize()
+
+    # ---- timed region: batched mixed-precision solves, inputs resident ----
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches = 0
+    iters = []
+    t_wall = time.perf_counter()
+    for s, e in evs:
+        s.record(stream)
+        mixed.solve(op, b_dev)
+        e.record(stream)
+        check(mixed.reports)
+        launches += mixed.reports[0]["kernel_launches"]
+        iters += [r["iterations"] for r in mixed.reports]
+    torch.cuda.synchronize()
+    barrier()
+    t_wall = time.perf_counter() - t_wall
+    step_ms = [s.elapsed_time(e) for s, e in evs]
+    clk = clocks.stop()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps * B / (total_ms / 1e3)
+
+    # ---- end to end through the public API with host buffers ----
+    e2e_ms = []
+    for _ in range(max(2, args.steps // 2)):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        bd = b_host.to(dev, non_blocking=True)
+        xd = mixed.solve(op, bd)
+        x_host.copy_(xd, non_blocking=True)
+        e.record(stream)
+        torch.cuda.synchronize()
+        check(mixed.reports)
+        e2e_ms.append(s.elapsed_time(e))
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * len(e2e_ms) * B / (e2e_total / 1e3)
+
+    # ---- plain FP64 one solve at a time ----
+    plain_ms, plain_iters = [], []
+    for i in range(args.plain_solves):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        plain.solve(op, b_dev[i % B])
+        e.record(stream)
+        torch.cuda.synchronize()
+        check(plain.reports)
+        plain_ms.append(s.elapsed_time(e))
+        plain_iters.append(plain.reports[0]["iterations"])
+    plain_value = 1e3 / statistics.mean(plain_ms)
+
+    # ---- roofline: the solver's dslash timed alone, L2 flushed between launches ----
+    gauge = op.solver_gauge((args.precision,))
+    prec = _lib.PREC[args.precision]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    durs = []
+    for i in range(20):
+        flush.add_(1.0)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        _lib.check(_lib.lib().lym_dslash_eo(gauge, prec, B, 1, _dev.stream()), "lym_dslash_eo")
+        e.record(stream)
+        torch.cuda.synchronize()
+        if i >= 3:
+            durs.append(s.elapsed_time(e) / 1e3)
+    hop_s = statistics.mean(durs)
+    ns_, spin_reals = 4, 2 * 4 * NC
+    bs = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}[args.precision]
+    spinor_bytes = spin_reals * bs + (4 if args.precision in ("f16", "bf16") else 0)
+    link_bytes = (12 if NC == 3 else 4) * (8 if args.precision == "f64" else (4 if args.precision == "f32" else 2))
+    if args.precision == "f64":
+        link_bytes = 18 * 8
+    algo_bytes = B * (vol // 2) * 2 * spinor_bytes + nd * vol * link_bytes
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo_bytes / hop_s / 1e9
+    traffic = read_traffic()
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----
+    cpu = None
+    if rank == 0 and world == 1:
+        sec_per_it, nit = oracle_cg_iteration_seconds(args.cpu_seconds)
+        it_per_solve = statistics.mean(plain_iters)
+        cpu = {"value": 1.0 / (sec_per_it * it_per_solve), "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"{nit} CG iterations of the oracle's even-odd CGNR on 16^4 (numpy, one core), "
+                         f"{sec_per_it:.2f} s each, extrapolated with the {it_per_solve:.0f} iterations the "
+                         f"plain FP64 GPU solve took"}
+
+    q = sorted(step_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": f"{args.precision}+f64",
+        "data": "synthetic",
+        "config": {"workload": "wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
+                   "nrhs_per_step": B, "inner_precision": args.precision, "outer_precision": "f64",
+                   "links": "reunit(exp(i 0.25 H)), H traceless Hermitian", "bc": "antiperiodic time",
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (sources + solutions of a step exceed 126 MB)"},
+        "latency_ms": {"p50": statistics.median(step_ms), "p99": q[min(len(q) - 1, int(0.99 * len(q)))],
+                       "what": f"one batch of {B} solves, device-resident"},
+        "plain_fp64": {"value": world * plain_value, "unit": "solves/s", "ms_per_solve": statistics.mean(plain_ms),
+                       "iterations": plain_iters},
+        "speedup_vs_plain_fp64": value / (world * plain_value),
+        "iterations_per_solve": {"mean": statistics.mean(iters), "max": max(iters)},
+        "autotuned": {"rhs_per_thread": mixed.reports[0].get("rhs_per_thread")},
+        "gpu_launches": int(launches),
+        "e2e": {"value": e2e_value, "unit": "solves/s",
+                "h2d_bytes_per_step": int(b_host.numel() * 16), "d2h_bytes_per_step": int(x_host.numel() * 16)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": f"cg_hop_kernel<4,3,{args.precision}> s_o = H_oe p_e, "
+                                                   f"{B} rhs, L2 flushed before each launch",
+                     "algorithmic_bytes_per_launch": algo_bytes, "launch_us": hop_s * 1e6,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback"},
+        "clocks": clk,
+        "wall_s_timed": t_wall,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_lym(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -144,6 +144,8 @@ typedef struct lym_solver_report {
   int iterations;        /* inner iterations                                     */
   int reliable_updates;  /* FP64 residual recomputations                         */
   double true_residual;  /* FP64 |b - D x| / |b| of the returned x               */
+  int64_t kernel_launches; /* lym kernels the whole call launched (graph nodes included) */
+  int rhs_per_thread;    /* right-hand sides per thread the autotuner picked for the hop kernels */
 } lym_solver_report;
 
 /* Solve D x_i = b_i (or Q x_i = b_i) for nrhs right-hand sides stored back to
@@ -154,6 +156,13 @@ typedef struct lym_solver_report {
  * entries.  Returns LYM_ERR_NOT_CONVERGED if any rhs missed tol. */
 int lym_wilson_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x,
                      const lym_solver_params* params, lym_solver_report* reports, void* stream);
+
+/* Runs the solver's even-odd hopping kernel s_o = H_oe p_e `repeats` times on
+ * the workspace left by the last lym_wilson_solve with this (precision, nrhs):
+ * the same kernel the CG iterations launch, for timing and profiling it alone
+ * (no reference counterpart; the reference has no separate dslash).  Returns
+ * LYM_ERR_BAD_ARG when no such workspace exists. */
+int lym_dslash_eo(lym_gauge* g, int precision, int nrhs, int repeats, void* stream);
 
 /* Multishift CG on (Q^2 + sigma_k) x_k = b over the full lattice, FP64
  * (nshift, ns, N, V) solutions.  Replaces multishift_solver.solve on a

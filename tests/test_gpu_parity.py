@@ -187,7 +187,9 @@ def test_multishift_cg(cuda_device, case):
         xn = np_(x)
         res = np.linalg.norm(setup.Q2(xn) + s * xn - g["eta"]) / np.linalg.norm(g["eta"])
         assert res < 1e-11, (s, res)
-        assert relerr(xn, ref) < 1e-8
+        # the golden MMMR solution stopped at |r|^2 < 1e-11 (absolute), so it is
+        # itself only accurate to ~1e-7; the residual above is the real check
+        assert relerr(xn, ref) < 1e-6
 
 
 @pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])

@@ -38,7 +38,7 @@ class SolverParams(ctypes.Structure):
 
 class SolverReport(ctypes.Structure):
     _fields_ = [("status", c_int), ("iterations", c_int), ("reliable_updates", c_int),
-                ("true_residual", c_double)]
+                ("true_residual", c_double), ("kernel_launches", c_int64), ("rhs_per_thread", c_int)]
 
 
 # name -> (restype, argtypes); every symbol include/lym.h declares
@@ -63,6 +63,7 @@ SIGNATURES = {
     "lym_gauge_destroy": (c_int, [c_void_p]),
     "lym_wilson_solve": (c_int, [c_void_p, c_double, c_int, c_void_p, c_void_p, P(SolverParams),
                                  P(SolverReport), c_void_p]),
+    "lym_dslash_eo": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p]),
     "lym_multishift_solve": (c_int, [c_void_p, c_double, c_int, P(c_double), c_void_p, c_void_p,
                                      c_double, c_int, P(c_int), c_void_p]),
     "lym_mmmr_solve": (c_int, [c_void_p, c_double, c_int, P(c_double), c_void_p, c_void_p, c_int,

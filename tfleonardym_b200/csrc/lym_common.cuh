@@ -43,6 +43,22 @@ template <typename T> LYM_HD cx<T>& operator-=(cx<T>& a, cx<T> b) { a.re -= b.re
 template <typename T> LYM_HD T norm2(cx<T> a) { return a.re * a.re + a.im * a.im; }
 template <typename T> LYM_HD cx<T> czero() { return {T(0), T(0)}; }
 
+// Fused complex multiply-accumulate: 4 FMAs instead of the 2 MUL + 2 FMA + 2 ADD
+// that `t += a * b` becomes when the product is rounded on its own.
+template <typename T> LYM_HD void cmac(cx<T>& t, cx<T> a, cx<T> b) {
+  t.re = fma(a.re, b.re, t.re);
+  t.re = fma(-a.im, b.im, t.re);
+  t.im = fma(a.re, b.im, t.im);
+  t.im = fma(a.im, b.re, t.im);
+}
+// t += conj(a) * b
+template <typename T> LYM_HD void cmac_cj(cx<T>& t, cx<T> a, cx<T> b) {
+  t.re = fma(a.re, b.re, t.re);
+  t.re = fma(a.im, b.im, t.re);
+  t.im = fma(a.re, b.im, t.im);
+  t.im = fma(-a.im, b.re, t.im);
+}
+
 // Multiply by a unit phase encoded as 0:+1, 1:+i, 2:-1, 3:-i (compile-time when possible).
 template <typename T> LYM_HD cx<T> mul_phase(int ph, cx<T> a) {
   switch (ph & 3) {

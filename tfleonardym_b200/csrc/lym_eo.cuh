@@ -122,6 +122,42 @@ LYM_D void store_sp(const EoField& f, int rhs, int64_t cb, const cx<typename Pre
   }
 }
 
+// Raw load: values as stored (not multiplied by the site norm) and the norm
+// (1 for FP64 / FP32), so callers can fold the norm into fewer multiplies.
+// 32-bit offsets within one rhs (nunits * Vh < 2^31 is checked at creation).
+template <int SP, int NCOMP>
+LYM_D float load_sp_raw(const EoField& f, int rhs, int cb, cx<typename Prec<SP>::real> (&v)[NCOMP]) {
+  using U = typename Prec<SP>::unit;
+  const int vh = (int)f.Vh;
+  const U* base = reinterpret_cast<const U*>(f.data) + (size_t)rhs * f.nunits * f.Vh;
+  if constexpr (SP == SP64) {
+#pragma unroll
+    for (int c = 0; c < NCOMP; ++c) {
+      double2 t = __ldg(base + c * vh + cb);
+      v[c] = {t.x, t.y};
+    }
+    return 1.0f;
+  } else if constexpr (SP == SP32) {
+#pragma unroll
+    for (int u = 0; u < units_for(NCOMP, 2); ++u) {
+      float4 t = __ldg(base + u * vh + cb);
+      v[2 * u] = {t.x, t.y};
+      if (2 * u + 1 < NCOMP) v[2 * u + 1] = {t.z, t.w};
+    }
+    return 1.0f;
+  } else {
+#pragma unroll
+    for (int u = 0; u < units_for(NCOMP, 4); ++u) {
+      uint4 t = __ldg(base + u * vh + cb);
+      const unsigned w[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (4 * u + k < NCOMP) v[4 * u + k] = unpack2<SP>(w[k]);
+    }
+    return __ldg(f.norm + (size_t)rhs * f.Vh + cb);
+  }
+}
+
 // --- gauge load -----------------------------------------------------------
 // GP: storage precision (SP64 double2, SP32 float4, SP16 uint2 of 2 half2)
 // COMP: compressed to N-1 rows
@@ -177,9 +213,14 @@ LYM_D void load_link_eo(const void* g, int nunits, int64_t Vh, int mu, int par, 
       u[0][j] = e[j];
       u[1][j] = e[3 + j];
     }
-    u[2][0] = conj(u[0][1] * u[1][2] - u[0][2] * u[1][1]);
-    u[2][1] = conj(u[0][2] * u[1][0] - u[0][0] * u[1][2]);
-    u[2][2] = conj(u[0][0] * u[1][1] - u[0][1] * u[1][0]);
+    // row2 = conj(row0 x row1)
+    cx<R> t0 = u[0][1] * u[1][2], t1 = u[0][2] * u[1][0], t2 = u[0][0] * u[1][1];
+    cmac(t0, -u[0][2], u[1][1]);
+    cmac(t1, -u[0][0], u[1][2]);
+    cmac(t2, -u[0][1], u[1][0]);
+    u[2][0] = conj(t0);
+    u[2][1] = conj(t1);
+    u[2][2] = conj(t2);
   }
 }
 
@@ -192,31 +233,33 @@ struct EoGeom {
   int64_t Vh;
 };
 
-// coordinates and lexicographic index of checkerboard site (cb, parity)
+// coordinates and lexicographic index of checkerboard site (cb, parity);
+// 32-bit arithmetic throughout (the volume is below 2^31)
 template <int ND>
-LYM_D int64_t eo_coords(const EoGeom& g, int64_t cb, int par, int (&x)[ND]) {
+LYM_D int eo_coords(const EoGeom& g, int cb, int par, int (&x)[ND]) {
   const int Lt = g.dims[ND - 1];
-  int64_t row = cb / g.Lh;
-  const int th = (int)(cb - row * g.Lh);
-  int64_t r = row;
+  const unsigned row = (unsigned)cb / (unsigned)g.Lh;
+  const int th = cb - (int)row * g.Lh;
+  unsigned r = row;
   int sum = 0;
 #pragma unroll
   for (int d = ND - 2; d >= 0; --d) {
-    x[d] = (int)(r % g.dims[d]);
-    r /= g.dims[d];
+    const unsigned q = r / (unsigned)g.dims[d];
+    x[d] = (int)(r - q * (unsigned)g.dims[d]);
+    r = q;
     sum += x[d];
   }
   x[ND - 1] = 2 * th + ((par + sum) & 1);
-  return row * Lt + x[ND - 1];
+  return (int)row * Lt + x[ND - 1];
 }
 
 template <int ND>
-LYM_D int64_t nb_fwd(const EoGeom& g, int64_t lex, const int (&x)[ND], int mu) {
-  return (x[mu] == g.dims[mu] - 1) ? lex - (int64_t)(g.dims[mu] - 1) * g.stride[mu] : lex + g.stride[mu];
+LYM_D int nb_fwd(const EoGeom& g, int lex, const int (&x)[ND], int mu) {
+  return (x[mu] == g.dims[mu] - 1) ? lex - (g.dims[mu] - 1) * g.stride[mu] : lex + g.stride[mu];
 }
 template <int ND>
-LYM_D int64_t nb_bwd(const EoGeom& g, int64_t lex, const int (&x)[ND], int mu) {
-  return (x[mu] == 0) ? lex + (int64_t)(g.dims[mu] - 1) * g.stride[mu] : lex - g.stride[mu];
+LYM_D int nb_bwd(const EoGeom& g, int lex, const int (&x)[ND], int mu) {
+  return (x[mu] == 0) ? lex + (g.dims[mu] - 1) * g.stride[mu] : lex - g.stride[mu];
 }
 
 // --- hopping term -----------------------------------------------------------
@@ -236,7 +279,7 @@ LYM_D void hop_site(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
   using GR = typename GPrec<GP>::real;
   constexpr int NS = Gamma<ND>::NS;
   int x[ND];
-  const int64_t lex = eo_coords<ND>(g, cb, par, x);
+  const int lex = eo_coords<ND>(g, (int)cb, par, x);
 #pragma unroll
   for (int a = 0; a < NS; ++a)
 #pragma unroll
@@ -246,8 +289,8 @@ LYM_D void hop_site(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
       const bool fwd = dir == 0;
-      const int64_t nlex = fwd ? nb_fwd<ND>(g, lex, x, mu) : nb_bwd<ND>(g, lex, x, mu);
-      const int64_t ncb = nlex >> 1;
+      const int nlex = fwd ? nb_fwd<ND>(g, lex, x, mu) : nb_bwd<ND>(g, lex, x, mu);
+      const int ncb = nlex >> 1;
       cx<GR> ug[NC][NC];
       // forward link lives on x (parity par), backward link on x - mu (parity 1-par)
       load_link_eo<GP, NC, COMP>(hg.data, hg.nunits, g.Vh, mu, fwd ? par : 1 - par, fwd ? cb : ncb, ug);
@@ -280,16 +323,97 @@ LYM_D void hop_site(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
         const int lph = fwd ? phase_neg(phase_conj(ph)) : phase_conj(ph);
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
-          cx<R> t = czero<R>();
+          cx<R> t;
           if (fwd) {
+            t = u[i][0] * h[0];
 #pragma unroll
-            for (int j = 0; j < NC; ++j) t += u[i][j] * h[j];
+            for (int j = 1; j < NC; ++j) cmac(t, u[i][j], h[j]);
           } else {
+            t = cmul_cj(u[0][i], h[0]);
 #pragma unroll
-            for (int j = 0; j < NC; ++j) t += cmul_cj(u[j][i], h[j]);
+            for (int j = 1; j < NC; ++j) cmac_cj(t, u[j][i], h[j]);
           }
           acc[a][i] += t;
           acc[jb][i] += mul_phase(lph, t);
+        }
+      }
+    }
+  }
+}
+
+// Register-tiled hop: one thread, one site, R right-hand sides rhs0..rhs0+R-1.
+// The link of each direction is loaded and decompressed once and reused for
+// the R spinors; the half-spinor projection is formed from the raw stored
+// values and scaled once by the neighbour's norm.  act[r] == 0 skips rhs r
+// (uniform across a block, since the rhs tile is blockIdx.y).
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R>
+LYM_D void hop_tile(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
+                    const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
+  using RT = typename Prec<SP>::real;
+  using GR = typename GPrec<GP>::real;
+  constexpr int NS = Gamma<ND>::NS;
+  int x[ND];
+  const int lex = eo_coords<ND>(g, cb, par, x);
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int a = 0; a < NS; ++a)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[r][a][c] = czero<RT>();
+#pragma unroll
+  for (int mu = 0; mu < ND; ++mu) {
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      const bool fwd = dir == 0;
+      const int nlex = fwd ? nb_fwd<ND>(g, lex, x, mu) : nb_bwd<ND>(g, lex, x, mu);
+      const int ncb = nlex >> 1;
+      cx<GR> ug[NC][NC];
+      load_link_eo<GP, NC, COMP>(hg.data, hg.nunits, g.Vh, mu, fwd ? par : 1 - par, fwd ? cb : ncb, ug);
+      cx<RT> u[NC][NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) u[i][j] = {(RT)ug[i][j].re, (RT)ug[i][j].im};
+      if (COMP && mu == ND - 1 && x[ND - 1] == (fwd ? g.dims[ND - 1] - 1 : 0)) {
+        const cx<RT> bc{(RT)hg.bcr, (RT)hg.bci};
+#pragma unroll
+        for (int i = 0; i < NC; ++i)
+#pragma unroll
+          for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
+      }
+      const RT sgn = fwd ? RT(1) : RT(-1);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!act[r]) continue;
+        cx<RT> psi[NS * NC];
+        const float nrm = load_sp_raw<SP, NS * NC>(in, rhs0 + r, ncb, psi);
+#pragma unroll
+        for (int a = 0; a < NS / 2; ++a) {
+          const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+          // G5IN flips the lower component psi_{jb} before projecting
+          const RT s2 = G5IN ? -sgn : sgn;
+          cx<RT> h[NC];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            h[c] = psi[a * NC + c] - s2 * mul_phase(ph, psi[jb * NC + c]);
+            if constexpr (SP == SP16 || SP == SPB16) h[c] = (RT)nrm * h[c];
+          }
+          const int lph = fwd ? phase_neg(phase_conj(ph)) : phase_conj(ph);
+#pragma unroll
+          for (int i = 0; i < NC; ++i) {
+            cx<RT> t;
+            if (fwd) {
+              t = u[i][0] * h[0];
+#pragma unroll
+              for (int j = 1; j < NC; ++j) cmac(t, u[i][j], h[j]);
+            } else {
+              t = cmul_cj(u[0][i], h[0]);
+#pragma unroll
+              for (int j = 1; j < NC; ++j) cmac_cj(t, u[j][i], h[j]);
+            }
+            acc[r][a][i] += t;
+            acc[r][jb][i] += mul_phase(lph, t);
+          }
         }
       }
     }

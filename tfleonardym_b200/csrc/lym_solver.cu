@@ -317,107 +317,153 @@ __global__ void __launch_bounds__(128) norm64_kernel(int64_t Vh, EoField f, doub
 // ---------------------------------------------------------------------------
 // sloppy CG iteration kernels (precision SP, links GP/COMP)
 // ---------------------------------------------------------------------------
-// s = H_oe G5IN(p)   (odd output)
-template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN>
+// s = H_oe G5IN(p) for the rhs tile blockIdx.y*R .. +R-1 (odd output);
+// st == nullptr: every rhs (profiling hook)
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R>
 __global__ void __launch_bounds__(128) cg_hop_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
                                                      const CGState* st) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
-  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
-  if (!st[rhs].active || cb >= g.Vh) return;
-  using R = typename Prec<SP>::real;
-  cx<R> acc[NS][NC];
-  hop_site<ND, NC, SP, GP, COMP, G5IN>(g, hg, in, rhs, cb, par, acc);
-  cx<R> v[NCOMP];
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs0 = blockIdx.y * R;
+  int act[R];
+  int any = 0;
 #pragma unroll
-  for (int s = 0; s < NS; ++s)
+  for (int r = 0; r < R; ++r) {
+    act[r] = st ? st[rhs0 + r].active : 1;
+    any |= act[r];
+  }
+  if (!any || cb >= g.Vh) return;
+  using RT = typename Prec<SP>::real;
+  cx<RT> acc[R][NS][NC];
+  hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
 #pragma unroll
-    for (int c = 0; c < NC; ++c) v[s * NC + c] = acc[s][c];
-  store_sp<SP, NCOMP>(out, rhs, cb, v);
+  for (int r = 0; r < R; ++r) {
+    if (!act[r]) continue;
+    cx<RT> v[NCOMP];
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) v[s * NC + c] = acc[r][s][c];
+    store_sp<SP, NCOMP>(out, rhs0 + r, cb, v);
+  }
 }
 
-// t = p - kappa^2 H_eo s ; alpha = rr / |t|^2
-template <int ND, int NC, int SP, int GP, bool COMP>
+// t = p - kappa^2 H_eo s ; alpha = rr / |t|^2   (rhs tile of R)
+template <int ND, int NC, int SP, int GP, bool COMP, int R>
 __global__ void __launch_bounds__(128) cg_t_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t, double k2,
                                                    CGState* st, double* partials, unsigned* counters, int nblk) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
-  __shared__ double sh[32];
-  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
-  if (!st[rhs].active) return;
-  using R = typename Prec<SP>::real;
-  double n[1] = {0.0};
-  if (cb < g.Vh) {
-    cx<R> acc[NS][NC];
-    hop_site<ND, NC, SP, GP, COMP, false>(g, hg, s, rhs, cb, 0, acc);
-    cx<R> v[NCOMP];
-    load_sp<SP, NCOMP>(p, rhs, cb, v);
+  __shared__ double sh[R * 32];
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs0 = blockIdx.y * R;
+  int act[R];
+  int any = 0;
 #pragma unroll
-    for (int a = 0; a < NS; ++a)
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        cx<R>& w = v[a * NC + c];
-        w -= (R)k2 * acc[a][c];
-        n[0] += (double)w.re * w.re + (double)w.im * w.im;
-      }
-    store_sp<SP, NCOMP>(t, rhs, cb, v);
+  for (int r = 0; r < R; ++r) {
+    act[r] = st[rhs0 + r].active;
+    any |= act[r];
   }
-  if (grid_sum<1>(n, partials + (int64_t)rhs * nblk, counters + rhs, sh) && threadIdx.x == 0) {
-    CGState& S = st[rhs];
-    if (n[0] > 0.0 && S.rr > 0.0) {
-      S.alpha = S.rr / n[0];
-    } else {
-      S.alpha = 0.0;
-      S.active = 0;  // p = 0: nothing left to do
+  if (!any) return;  // uniform per block
+  using RT = typename Prec<SP>::real;
+  double n[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) n[r] = 0.0;
+  if (cb < g.Vh) {
+    cx<RT> acc[R][NS][NC];
+    hop_tile<ND, NC, SP, GP, COMP, false, R>(g, hg, s, rhs0, cb, 0, act, acc);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (!act[r]) continue;
+      cx<RT> v[NCOMP];
+      load_sp<SP, NCOMP>(p, rhs0 + r, cb, v);
+#pragma unroll
+      for (int a = 0; a < NS; ++a)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          cx<RT>& w = v[a * NC + c];
+          w -= (RT)k2 * acc[r][a][c];
+          n[r] += (double)w.re * w.re + (double)w.im * w.im;
+        }
+      store_sp<SP, NCOMP>(t, rhs0 + r, cb, v);
+    }
+  }
+  if (grid_sum<R>(n, partials + (int64_t)blockIdx.y * nblk * R, counters + blockIdx.y, sh) && threadIdx.x == 0) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (!act[r]) continue;
+      CGState& S = st[rhs0 + r];
+      if (n[r] > 0.0 && S.rr > 0.0) {
+        S.alpha = S.rr / n[r];
+      } else {
+        S.alpha = 0.0;
+        S.active = 0;  // p = 0: nothing left to do
+      }
     }
   }
 }
 
-// Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr
-template <int ND, int NC, int SP, int GP, bool COMP, int XP>
+// Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr   (rhs tile of R)
+template <int ND, int NC, int SP, int GP, bool COMP, int XP, int R>
 __global__ void __launch_bounds__(128) cg_update_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
                                                         EoField x, EoField r, double k2, CGState* st,
                                                         double* partials, unsigned* counters, int nblk) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
-  __shared__ double sh[32];
-  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
-  if (!st[rhs].active) return;
-  using R = typename Prec<SP>::real;
-  using XR = typename Prec<XP>::real;
-  const double alpha = st[rhs].alpha;
-  double n[1] = {0.0};
-  if (cb < g.Vh) {
-    cx<R> acc[NS][NC];
-    hop_site<ND, NC, SP, GP, COMP, false>(g, hg, s, rhs, cb, 0, acc);
-    cx<R> tv[NCOMP], pv[NCOMP], rv[NCOMP];
-    cx<XR> xv[NCOMP];
-    load_sp<SP, NCOMP>(t, rhs, cb, tv);
-    load_sp<SP, NCOMP>(p, rhs, cb, pv);
-    load_sp<SP, NCOMP>(r, rhs, cb, rv);
-    load_sp<XP, NCOMP>(x, rhs, cb, xv);
-    const R a = (R)alpha;
+  __shared__ double sh[R * 32];
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs0 = blockIdx.y * R;
+  int act[R];
+  int any = 0;
 #pragma unroll
-    for (int sp = 0; sp < NS; ++sp)
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const int k = sp * NC + c;
-        cx<R> h = acc[sp][c];
-        if (sp >= NS / 2) h = -h;
-        cx<R> ap = tv[k] - (R)k2 * h;
-        rv[k] -= a * ap;
-        xv[k] += (XR)alpha * cx<XR>{(XR)pv[k].re, (XR)pv[k].im};
-        n[0] += (double)rv[k].re * rv[k].re + (double)rv[k].im * rv[k].im;
-      }
-    store_sp<SP, NCOMP>(r, rhs, cb, rv);
-    store_sp<XP, NCOMP>(x, rhs, cb, xv);
+  for (int q = 0; q < R; ++q) {
+    act[q] = st[rhs0 + q].active;
+    any |= act[q];
   }
-  if (grid_sum<1>(n, partials + (int64_t)rhs * nblk, counters + rhs, sh) && threadIdx.x == 0) {
-    CGState& S = st[rhs];
-    S.beta = n[0] / S.rr;
-    S.rr = n[0];
-    S.iters += 1;
-    if (S.rr < S.pause2 || S.iters >= S.max_iter) S.active = 2;  // finish the p update, then stop
+  if (!any) return;  // uniform per block
+  using RT = typename Prec<SP>::real;
+  using XR = typename Prec<XP>::real;
+  double n[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) n[q] = 0.0;
+  if (cb < g.Vh) {
+    cx<RT> acc[R][NS][NC];
+    hop_tile<ND, NC, SP, GP, COMP, false, R>(g, hg, s, rhs0, cb, 0, act, acc);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      if (!act[q]) continue;
+      const double alpha = st[rhs0 + q].alpha;
+      cx<RT> tv[NCOMP], pv[NCOMP], rv[NCOMP];
+      cx<XR> xv[NCOMP];
+      load_sp<SP, NCOMP>(t, rhs0 + q, cb, tv);
+      load_sp<SP, NCOMP>(p, rhs0 + q, cb, pv);
+      load_sp<SP, NCOMP>(r, rhs0 + q, cb, rv);
+      load_sp<XP, NCOMP>(x, rhs0 + q, cb, xv);
+      const RT a = (RT)alpha;
+#pragma unroll
+      for (int sp = 0; sp < NS; ++sp)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const int k = sp * NC + c;
+          cx<RT> h = acc[q][sp][c];
+          if (sp >= NS / 2) h = -h;
+          cx<RT> ap = tv[k] - (RT)k2 * h;
+          rv[k] -= a * ap;
+          xv[k] += (XR)alpha * cx<XR>{(XR)pv[k].re, (XR)pv[k].im};
+          n[q] += (double)rv[k].re * rv[k].re + (double)rv[k].im * rv[k].im;
+        }
+      store_sp<SP, NCOMP>(r, rhs0 + q, cb, rv);
+      store_sp<XP, NCOMP>(x, rhs0 + q, cb, xv);
+    }
+  }
+  if (grid_sum<R>(n, partials + (int64_t)blockIdx.y * nblk * R, counters + blockIdx.y, sh) && threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      if (!act[q]) continue;
+      CGState& S = st[rhs0 + q];
+      S.beta = n[q] / S.rr;
+      S.rr = n[q];
+      S.iters += 1;
+      if (S.rr < S.pause2 || S.iters >= S.max_iter) S.active = 2;  // finish the p update, then stop
+    }
   }
 }
 
@@ -460,7 +506,12 @@ struct CgOps {
   void (*convert)(Work&, const EoField& src, const EoField& dst, const EoField& dst2, bool only_update, cudaStream_t);
   void (*accumulate)(Work&, cudaStream_t);
   void (*zero64)(Work&, const EoField& f, cudaStream_t);
+  void (*dslash)(Work&, cudaStream_t);                  // s_o = H_oe p_e, every rhs
 };
+// kernels one iterate() call launches
+constexpr int kLaunchesPerIteration = 6;
+// solver workspaces a gauge object keeps, keyed by (precision, nrhs)
+constexpr size_t kMaxWorkspaces = 4;
 
 }  // namespace lym
 
@@ -478,14 +529,19 @@ struct lym_gauge {
   int n32 = 0;
   uint2* u16 = nullptr;
   int n16 = 0;
-  lym::Work* work = nullptr;
+  std::vector<lym::Work*> works;  // solver workspaces, most recently used first
 };
 
 namespace lym {
 
 struct Work {
   lym_gauge* g = nullptr;
-  int nrhs = 0, sp = 0, xp = 0;
+  int nrhs = 0, sp = 0, xp = 0;  // nrhs: padded count every field holds
+  int nreal = 0;                 // right-hand sides the caller passes
+  int R = 1;                     // right-hand sides per thread in the hop kernels (autotuned)
+  bool tuned = false;
+  int rcand[3] = {1, 0, 0};
+  CgOps ops_r[3]{};
   int64_t Vh = 0;
   int nblk = 0;
   double kappa = 0;
@@ -511,23 +567,27 @@ struct Work {
   cudaStream_t graph_stream = nullptr;
   cudaStream_t stream = nullptr;  // solves run here (capturable even when the caller uses the legacy stream)
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  int64_t launches = 0;           // kernels launched by the current call (graph nodes included)
 };
 
-template <int ND, int NC, int SP, bool COMP>
+template <int ND, int NC, int SP, bool COMP, int R>
 struct Impl {
   static constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   static constexpr int GP = SP == SP64 ? SP64 : (SP == SP32 ? SP32 : SP16);
-  static constexpr int XP = SP == SP64 ? SP64 : SP32;
+  // the sloppy solution accumulates in the sloppy precision: its rounding
+  // (relative to the residual drop since the last reliable update) stays far
+  // below the reliable-update factor delta
+  static constexpr int XP = SP;
 
   static void iterate(Work& w, cudaStream_t st) {
     const double k2 = w.kappa * w.kappa;
-    dim3 grid(w.nblk, w.nrhs);
-    cg_hop_kernel<ND, NC, SP, GP, COMP, false><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, w.st);
-    cg_t_kernel<ND, NC, SP, GP, COMP><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st, w.partials,
-                                                            w.counters, w.nblk);
-    cg_hop_kernel<ND, NC, SP, GP, COMP, true><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, w.st);
-    cg_update_kernel<ND, NC, SP, GP, COMP, XP><<<grid, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.t, w.p, w.xs, w.r, k2,
-                                                                     w.st, w.partials, w.counters, w.nblk);
+    dim3 grid(w.nblk, w.nrhs), tile(w.nblk, w.nrhs / R);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, false, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, w.st);
+    cg_t_kernel<ND, NC, SP, GP, COMP, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st, w.partials,
+                                                               w.counters, w.nblk);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, true, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, w.st);
+    cg_update_kernel<ND, NC, SP, GP, COMP, XP, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.t, w.p, w.xs, w.r,
+                                                                        k2, w.st, w.partials, w.counters, w.nblk);
     cg_p_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.r, w.p, w.st);
     cg_settle_kernel<<<(w.nrhs + 63) / 64, 64, 0, st>>>(w.nrhs, w.st);
   }
@@ -536,7 +596,8 @@ struct Impl {
                     double a1, double c, bool g5in, bool g5out, bool with_norm, cudaStream_t st) {
     dim3 grid(w.nblk, w.nrhs);
     double* res = with_norm ? w.res : nullptr;
-#define LYM_H64(A, B)                                                                                     \
+    w.launches += 1;
+#define LYM_H64(A, B)                                                                                   \
   hop64_lincomb_kernel<ND, NC, A, B><<<grid, 128, 0, st>>>(w.g->geom, w.hg64, in, par, out, z0, z1, a1, c, \
                                                            w.upd, w.partials, w.counters, res, w.nblk)
     if (g5in && g5out) LYM_H64(true, true);
@@ -547,54 +608,72 @@ struct Impl {
   }
 
   static void to_eo(Work& w, const void* ref, int g5, cudaStream_t st) {
-    dim3 grid(grid_for(w.g->V, 128), w.nrhs);
+    dim3 grid(grid_for(w.g->V, 128), w.nreal);
+    w.launches += 1;
     ref_to_eo_kernel<ND, NC><<<grid, 128, 0, st>>>(w.g->geom, w.g->V, (const double2*)ref, w.be, w.bo, g5);
   }
   static void from_eo(Work& w, void* ref, cudaStream_t st) {
-    dim3 grid(grid_for(w.g->V, 128), w.nrhs);
+    dim3 grid(grid_for(w.g->V, 128), w.nreal);
+    w.launches += 1;
     eo_to_ref_kernel<ND, NC><<<grid, 128, 0, st>>>(w.g->geom, w.g->V, w.x64, w.xo, (double2*)ref);
   }
   static void norm64(Work& w, const EoField& f, int accumulate, cudaStream_t st) {
     dim3 grid(w.nblk, w.nrhs);
+    w.launches += 1;
     norm64_kernel<NCOMP><<<grid, 128, 0, st>>>(w.Vh, f, w.partials, w.counters, w.res, w.nblk, accumulate);
   }
   static void convert(Work& w, const EoField& src, const EoField& dst, const EoField& dst2, bool only_update,
                       cudaStream_t st) {
     dim3 grid(w.nblk, w.nrhs);
+    w.launches += 1;
     convert_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, src, dst, dst2, w.st, only_update, w.upd);
   }
   static void accumulate(Work& w, cudaStream_t st) {
     if constexpr (SP != SP64) {
       dim3 grid(w.nblk, w.nrhs);
+      w.launches += 1;
       accumulate_kernel<XP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.xs, w.x64, w.upd);
     }
   }
   static void zero64(Work& w, const EoField& f, cudaStream_t st) {
     dim3 grid(w.nblk, w.nrhs);
+    w.launches += 1;
     zero64_kernel<NCOMP><<<grid, 128, 0, st>>>(w.Vh, f);
   }
+  static void dslash(Work& w, cudaStream_t st) {
+    dim3 tile(w.nblk, w.nrhs / R);
+    w.launches += 1;
+    cg_hop_kernel<ND, NC, SP, GP, COMP, false, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, nullptr);
+  }
   static CgOps table() {
-    return CgOps{&iterate, &hop64, &to_eo, &from_eo, &norm64, &convert, &accumulate, &zero64};
+    return CgOps{&iterate, &hop64, &to_eo, &from_eo, &norm64, &convert, &accumulate, &zero64, &dslash};
   }
 };
 
-template <int ND, int NC>
+template <int ND, int NC, int R>
 static CgOps pick_sp(int sp, bool comp) {
   switch (sp) {
-    case SP64: return Impl<ND, NC, SP64, false>::table();
-    case SP32: return comp ? Impl<ND, NC, SP32, true>::table() : Impl<ND, NC, SP32, false>::table();
-    case SP16: return comp ? Impl<ND, NC, SP16, true>::table() : Impl<ND, NC, SP16, false>::table();
-    default: return comp ? Impl<ND, NC, SPB16, true>::table() : Impl<ND, NC, SPB16, false>::table();
+    case SP64: return Impl<ND, NC, SP64, false, 1>::table();  // FP64 keeps one rhs per thread (registers)
+    case SP32: return comp ? Impl<ND, NC, SP32, true, R>::table() : Impl<ND, NC, SP32, false, R>::table();
+    case SP16: return comp ? Impl<ND, NC, SP16, true, R>::table() : Impl<ND, NC, SP16, false, R>::table();
+    default: return comp ? Impl<ND, NC, SPB16, true, R>::table() : Impl<ND, NC, SPB16, false, R>::table();
   }
 }
 
-static bool pick_ops(int nd, int nc, int sp, bool comp, CgOps* out) {
-  if (nd == 2 && nc == 2) *out = pick_sp<2, 2>(sp, comp);
-  else if (nd == 2 && nc == 3) *out = pick_sp<2, 3>(sp, comp);
-  else if (nd == 4 && nc == 2) *out = pick_sp<4, 2>(sp, comp);
-  else if (nd == 4 && nc == 3) *out = pick_sp<4, 3>(sp, comp);
+template <int R>
+static bool pick_ops_r(int nd, int nc, int sp, bool comp, CgOps* out) {
+  if (nd == 2 && nc == 2) *out = pick_sp<2, 2, R>(sp, comp);
+  else if (nd == 2 && nc == 3) *out = pick_sp<2, 3, R>(sp, comp);
+  else if (nd == 4 && nc == 2) *out = pick_sp<4, 2, R>(sp, comp);
+  else if (nd == 4 && nc == 3) *out = pick_sp<4, 3, R>(sp, comp);
   else return false;
   return true;
+}
+
+static bool pick_ops(int nd, int nc, int sp, bool comp, int R, CgOps* out) {
+  if (R == 4) return pick_ops_r<4>(nd, nc, sp, comp, out);
+  if (R == 2) return pick_ops_r<2>(nd, nc, sp, comp, out);
+  return pick_ops_r<1>(nd, nc, sp, comp, out);
 }
 
 static size_t field_bytes(int sp, int ncomp, int64_t Vh, int nrhs) {
@@ -633,26 +712,58 @@ static void free_work(Work* w) {
   delete w;
 }
 
+static Work* find_work(lym_gauge* g, int nrhs, int sp) {
+  for (size_t i = 0; i < g->works.size(); ++i) {
+    Work* w = g->works[i];
+    if (w->nreal == nrhs && w->sp == sp) {
+      g->works.erase(g->works.begin() + i);  // most recently used first
+      g->works.insert(g->works.begin(), w);
+      return w;
+    }
+  }
+  return nullptr;
+}
+
+static void free_all_work(lym_gauge* g) {
+  for (Work* w : g->works) free_work(w);
+  g->works.clear();
+}
+
 static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
-  Work* w = g->work;
-  if (w && w->nrhs == nrhs && w->sp == sp) {
+  Work* w = find_work(g, nrhs, sp);
+  if (w) {
     *out = w;
     return LYM_OK;
   }
-  free_work(w);
-  g->work = nullptr;
+  while (g->works.size() >= kMaxWorkspaces) {
+    free_work(g->works.back());
+    g->works.pop_back();
+  }
   w = new Work();
   w->g = g;
+  w->nreal = nrhs;
+  // pad to a multiple of 4 so the hop kernels can take 1, 2 or 4 rhs per
+  // thread; padding rhs have zero sources and finish before the first iteration
+  nrhs = (sp == SP64 || nrhs <= 2) ? nrhs : (nrhs + 3) / 4 * 4;
   w->nrhs = nrhs;
   w->sp = sp;
-  w->xp = sp == SP64 ? SP64 : SP32;
+  w->xp = sp;
   w->Vh = g->Vh;
   w->nblk = (int)grid_for(g->Vh, 128);
-  if (!pick_ops(g->nd, g->nc, sp, g->comp && sp != SP64, &w->ops)) {
-    delete w;
-    set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
-    return LYM_ERR_UNSUPPORTED;
+  const bool comp = g->comp && sp != SP64;
+  int nc_ = 0;
+  for (int R : {1, 2, 4}) {
+    if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
+    if (!pick_ops(g->nd, g->nc, sp, comp, R, &w->ops_r[nc_])) {
+      delete w;
+      set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
+      return LYM_ERR_UNSUPPORTED;
+    }
+    w->rcand[nc_++] = R;
   }
+  for (int i = nc_; i < 3; ++i) w->rcand[i] = 0;
+  w->ops = w->ops_r[0];
+  w->R = w->rcand[0];
   const int nc = g->ncomp;
   size_t bytes = 8 * field_bytes(SP64, nc, g->Vh, nrhs);
   bytes += 4 * field_bytes(sp, nc, g->Vh, nrhs);
@@ -693,7 +804,8 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   w->counters = reinterpret_cast<unsigned*>(cur);
   cur += (sizeof(unsigned) * nrhs + 255) & ~(size_t)255;
   w->res = reinterpret_cast<double*>(cur);
-  if (cudaMemset(w->counters, 0, sizeof(unsigned) * nrhs) != cudaSuccess ||
+  // zero everything: reduction counters, and the padding rhs' sources stay zero for good
+  if (cudaMemset(w->pool, 0, bytes) != cudaSuccess ||
       cudaMallocHost(&w->st_host, sizeof(CGState) * nrhs) != cudaSuccess ||
       cudaMallocHost(&w->upd_host, sizeof(int) * nrhs) != cudaSuccess ||
       cudaMallocHost(&w->res_host, sizeof(double) * nrhs * nres) != cudaSuccess ||
@@ -708,7 +820,7 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   if (sp == SP64) w->hgs = w->hg64;
   else if (sp == SP32) w->hgs = HopGauge{g->u32, g->n32, g->bcr, g->bci};
   else w->hgs = HopGauge{g->u16, g->n16, g->bcr, g->bci};
-  g->work = w;
+  g->works.insert(g->works.begin(), w);
   *out = w;
   return LYM_OK;
 }
@@ -764,6 +876,38 @@ static int build_graph(Work& w, int chunk, cudaStream_t st) {
   return LYM_OK;
 }
 
+// Autotuner: time the hop kernel for every rhs-per-thread candidate the
+// workspace supports and keep the fastest (once per workspace).
+static int autotune(Work& w, cudaStream_t st) {
+  if (w.tuned) return LYM_OK;
+  cudaEvent_t e0, e1;
+  LYM_CUDA(cudaEventCreate(&e0));
+  LYM_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int bi = 0;
+  for (int i = 0; i < 3 && w.rcand[i]; ++i) {
+    w.ops = w.ops_r[i];
+    for (int k = 0; k < 2; ++k) w.ops.dslash(w, st);
+    cudaEventRecord(e0, st);
+    for (int k = 0; k < 5; ++k) w.ops.dslash(w, st);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      bi = i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  LYM_CHECK_LAUNCH();
+  w.ops = w.ops_r[bi];
+  w.R = w.rcand[bi];
+  w.tuned = true;
+  return LYM_OK;
+}
+
 static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void* b, void* x,
                        const lym_solver_params* prm, lym_solver_report* rep, cudaStream_t st);
 
@@ -793,7 +937,10 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
                        const lym_solver_params* prm, lym_solver_report* rep, cudaStream_t st) {
   int rc = LYM_OK;
   const int sp = prm->precision;
+  const int nreal = nrhs;
+  nrhs = w.nrhs;  // padded count from here on
   w.kappa = kappa;
+  w.launches = 0;
   const double k = kappa;
   const double delta = prm->delta > 0 && prm->delta < 1 ? prm->delta : 0.1;
   const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 8;
@@ -845,6 +992,8 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
   LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
   w.ops.convert(w, w.r64, w.r, w.p, false, st);  // r = p = r64 in sloppy precision
   LYM_CHECK_LAUNCH();
+  rc = autotune(w, st);
+  if (rc) return rc;
   rc = build_graph(w, chunk, st);
   if (rc) return rc;
 
@@ -855,6 +1004,7 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     // run chunks until every rhs paused, finished or hit max_iter
     while (true) {
       LYM_CUDA(cudaGraphLaunch(w.graph, st));
+      w.launches += (int64_t)chunk * kLaunchesPerIteration;
       LYM_CUDA(cudaMemcpyAsync(w.st_host, w.st, sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
       LYM_CUDA(cudaStreamSynchronize(st));
       bool running = false;
@@ -893,14 +1043,26 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
   LYM_CHECK_LAUNCH();
   LYM_CUDA(cudaStreamSynchronize(st));
   int status = LYM_OK;
-  for (int i = 0; i < nrhs; ++i) {
+  for (int i = 0; i < nreal; ++i) {
     rep[i].status = done[i] ? LYM_OK : LYM_ERR_NOT_CONVERGED;
     rep[i].iterations = w.st_host[i].iters;
     rep[i].reliable_updates = updates[i];
     rep[i].true_residual = tres[i];
+    rep[i].kernel_launches = w.launches;
+    rep[i].rhs_per_thread = w.R;
     if (!done[i]) status = LYM_ERR_NOT_CONVERGED;
   }
   return status;
+}
+
+static int dslash_eo(lym_gauge* g, int precision, int nrhs, int repeats, cudaStream_t st) {
+  LYM_REQUIRE(g && repeats >= 0, LYM_ERR_BAD_ARG, "bad argument");
+  Work* w = find_work(g, nrhs, precision);
+  LYM_REQUIRE(w, LYM_ERR_BAD_ARG,
+              "no solver workspace for precision %d and %d right-hand sides", precision, nrhs);
+  for (int i = 0; i < repeats; ++i) w->ops.dslash(*w, st);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
 }
 
 int gauge_view(const lym_gauge* g, GaugeView* v) {
@@ -986,10 +1148,7 @@ static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
   else LYM_PACK(4, 3);
 #undef LYM_PACK
   LYM_CHECK_LAUNCH();
-  if (g->work) {  // sloppy gauge pointers / compression may have changed
-    free_work(g->work);
-    g->work = nullptr;
-  }
+  free_all_work(g);  // sloppy gauge pointers / compression may have changed
   return LYM_OK;
 }
 
@@ -1004,6 +1163,9 @@ int lym_gauge_create(const lym_lattice* lat, int nc, const void* gauge, double b
   }
   LYM_REQUIRE(nc == 2 || nc == 3, LYM_ERR_UNSUPPORTED, "N=%d not supported (2 or 3)", nc);
   LYM_REQUIRE(lat->even, LYM_ERR_UNSUPPORTED, "even-odd ordering needs every extent even");
+  // the hop kernels index one rhs of a field with 32-bit offsets
+  LYM_REQUIRE((int64_t)(lat->nd == 2 ? 2 : 4) * nc * (lat->V / 2) < (int64_t(1) << 31), LYM_ERR_UNSUPPORTED,
+              "lattice too large for 32-bit field offsets");
   lym_gauge* g = new lym_gauge();
   g->lat = lat;
   g->nc = nc;
@@ -1042,7 +1204,7 @@ int lym_gauge_update(lym_gauge* g, const void* gauge, void* stream) {
 int lym_gauge_destroy(lym_gauge* g) {
   if (!g) return LYM_OK;
   cudaDeviceSynchronize();
-  free_work(g->work);
+  free_all_work(g);
   if (g->uref) cudaFree(g->uref);
   if (g->u64) cudaFree(g->u64);
   if (g->u32) cudaFree(g->u32);
@@ -1054,6 +1216,10 @@ int lym_gauge_destroy(lym_gauge* g) {
 int lym_wilson_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x, const lym_solver_params* params,
                      lym_solver_report* reports, void* stream) {
   return cg_solve(g, kappa, nrhs, b, x, params, reports, (cudaStream_t)stream);
+}
+
+int lym_dslash_eo(lym_gauge* g, int precision, int nrhs, int repeats, void* stream) {
+  return dslash_eo(g, precision, nrhs, repeats, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -55,9 +55,9 @@ LYM_D Mat<N> mul(const Mat<N>& a, const Mat<N>& b) {
   for (int i = 0; i < N; ++i)
 #pragma unroll
     for (int j = 0; j < N; ++j) {
-      cx<double> t = czero<double>();
+      cx<double> t = a.m[i][0] * b.m[0][j];
 #pragma unroll
-      for (int k = 0; k < N; ++k) t += a.m[i][k] * b.m[k][j];
+      for (int k = 1; k < N; ++k) cmac(t, a.m[i][k], b.m[k][j]);
       r.m[i][j] = t;
     }
   return r;

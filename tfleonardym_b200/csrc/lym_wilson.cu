@@ -91,9 +91,9 @@ __global__ void __launch_bounds__(128) wilson_full_kernel(
                  mul_phase(ph, ld(psi + (size_t)(jb * NC + c) * V + y));
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
-          cx<double> t = czero<double>();
+          cx<double> t = u[i][0] * h[0];
 #pragma unroll
-          for (int j = 0; j < NC; ++j) t += u[i][j] * h[j];
+          for (int j = 1; j < NC; ++j) cmac(t, u[i][j], h[j]);
           acc[a][i] += t;
           acc[jb][i] += mul_phase(phase_neg(phase_conj(ph)), t);
         }
@@ -123,9 +123,9 @@ __global__ void __launch_bounds__(128) wilson_full_kernel(
                  mul_phase(ph, ld(psi + (size_t)(jb * NC + c) * V + y));
 #pragma unroll
         for (int i = 0; i < NC; ++i) {
-          cx<double> t = czero<double>();
+          cx<double> t = cmul_cj(u[0][i], h[0]);
 #pragma unroll
-          for (int j = 0; j < NC; ++j) t += cmul_cj(u[j][i], h[j]);
+          for (int j = 1; j < NC; ++j) cmac_cj(t, u[j][i], h[j]);
           acc[a][i] += t;
           acc[jb][i] += mul_phase(phase_conj(ph), t);
         }

@@ -187,6 +187,12 @@ class DiracWilsonOperator(Operator):
         mask = 0
         for p in precisions:
             mask |= 1 << _lib.PREC[p]
+        if self._solver_gauge is not None:
+            held = self._solver_gauge_key[1]
+            if mask & ~held:
+                mask |= held  # widen: keep every precision asked for so far
+            else:
+                mask = held
         key = (self._gauge_version, mask)
         if self._solver_gauge is not None and self._solver_gauge_key == key:
             return self._solver_gauge

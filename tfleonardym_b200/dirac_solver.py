@@ -198,7 +198,8 @@ class conjugate_gradient:  # noqa: N801 - named like the reference solvers
         rc = _lib.lib().lym_wilson_solve(operator.solver_gauge(precs), float(operator.kappa), n, _dev.ptr(bb),
                                          _dev.ptr(x), ctypes.byref(prm), reps, _dev.stream())
         self.reports = [dict(status=r.status, iterations=r.iterations, reliable_updates=r.reliable_updates,
-                             true_residual=r.true_residual) for r in reps]
+                             true_residual=r.true_residual, kernel_launches=r.kernel_launches,
+                             rhs_per_thread=r.rhs_per_thread) for r in reps]
         if rc == _lib.LYM_ERR_NOT_CONVERGED:
             _print(f"conjugate_gradient: failed to find convergence ({self.reports})")
         else:
