@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--precision", default="f16", choices=["f64", "f32", "f16", "bf16"])
     ap.add_argument("--plain-solves", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update trigger of the mixed solver")
+    ap.add_argument("--chunk", type=int, default=8, help="CG iterations per captured graph launch")
     return ap.parse_args()
 
 
@@ -263,8 +265,9 @@ def run_lym(args, rank, world, local_rank):
     b_host = torch.from_numpy(host_sources(99 + rank, B)).pin_memory()
     b_dev = b_host.to(dev)
     x_host = torch.empty_like(b_host).pin_memory()
-    mixed = dirac_solver.conjugate_gradient(tol=TOL, precision=args.precision, chunk=8)
-    plain = dirac_solver.conjugate_gradient(tol=TOL, precision="f64", chunk=8)
+    mixed = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision=args.precision, chunk=args.chunk,
+                                            delta=args.delta)
+    plain = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision="f64", chunk=8)
     stream = torch.cuda.current_stream()
 
     def barrier():
@@ -291,7 +294,7 @@ def run_lym(args, rank, world, local_rank):
     torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     launches = 0
-    iters = []
+    iters, rupd = [], []
     t_wall = time.perf_counter()
     for s, e in evs:
         s.record(stream)
@@ -300,6 +303,7 @@ def run_lym(args, rank, world, local_rank):
         check(mixed.reports)
         launches += mixed.reports[0]["kernel_launches"]
         iters += [r["iterations"] for r in mixed.reports]
+        rupd += [r["reliable_updates"] for r in mixed.reports]
     torch.cuda.synchronize()
     barrier()
     t_wall = time.perf_counter() - t_wall
@@ -393,6 +397,7 @@ def run_lym(args, rank, world, local_rank):
         "data": "synthetic",
         "config": {"workload": "wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
                    "nrhs_per_step": B, "inner_precision": args.precision, "outer_precision": "f64",
+                   "reliable_update_delta": args.delta, "graph_chunk": args.chunk,
                    "links": "reunit(exp(i 0.25 H)), H traceless Hermitian", "bc": "antiperiodic time",
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (sources + solutions of a step exceed 126 MB)"},
@@ -401,7 +406,8 @@ def run_lym(args, rank, world, local_rank):
         "plain_fp64": {"value": world * plain_value, "unit": "solves/s", "ms_per_solve": statistics.mean(plain_ms),
                        "iterations": plain_iters},
         "speedup_vs_plain_fp64": value / (world * plain_value),
-        "iterations_per_solve": {"mean": statistics.mean(iters), "max": max(iters)},
+        "iterations_per_solve": {"mean": statistics.mean(iters), "max": max(iters),
+                                 "reliable_updates_mean": statistics.mean(rupd)},
         "autotuned": {"rhs_per_thread": mixed.reports[0].get("rhs_per_thread")},
         "gpu_launches": int(launches),
         "e2e": {"value": e2e_value, "unit": "solves/s",

@@ -33,7 +33,7 @@ struct CGState {
   int active;     // iterate while 1
   int iters;
   int max_iter;
-  int pad;
+  int pause_iter;  // pause at this iteration count at the latest (bounds the sloppy drift)
 };
 
 // ---------------------------------------------------------------------------
@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(128) norm64_kernel(int64_t Vh, EoField f, doub
 // ---------------------------------------------------------------------------
 // sloppy CG iteration kernels (precision SP, links GP/COMP)
 // ---------------------------------------------------------------------------
+
 // s = H_oe G5IN(p) for the rhs tile blockIdx.y*R .. +R-1 (odd output);
 // st == nullptr: every rhs (profiling hook)
 template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R>
@@ -462,9 +463,72 @@ __global__ void __launch_bounds__(128) cg_update_kernel(EoGeom g, HopGauge hg, E
       S.beta = n[q] / S.rr;
       S.rr = n[q];
       S.iters += 1;
-      if (S.rr < S.pause2 || S.iters >= S.max_iter) S.active = 2;  // finish the p update, then stop
+      if (S.rr < S.pause2 || S.iters >= S.max_iter || S.iters >= S.pause_iter)
+        S.active = 2;  // finish the p update, then stop
     }
   }
+}
+
+// Reliable-update residual in the sloppy precision: r = t - kappa^2 gamma_d H_eo s
+// (t = q converted, s = H_oe gamma_d t), i.e. r = M^dag q, for rhs with upd[rhs];
+// res[rhs] = |r|^2.
+template <int ND, int NC, int SP, int GP, bool COMP, int R>
+__global__ void __launch_bounds__(128) cg_rnew_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField r,
+                                                      double k2, const int* upd, double* partials,
+                                                      unsigned* counters, double* res, int nblk) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
+  __shared__ double sh[R * 32];
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs0 = blockIdx.y * R;
+  int act[R];
+  int any = 0;
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    act[q] = upd[rhs0 + q];
+    any |= act[q];
+  }
+  if (!any) return;  // uniform per block
+  using RT = typename Prec<SP>::real;
+  double n[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) n[q] = 0.0;
+  if (cb < g.Vh) {
+    cx<RT> acc[R][NS][NC];
+    hop_tile<ND, NC, SP, GP, COMP, false, R>(g, hg, s, rhs0, cb, 0, act, acc);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      if (!act[q]) continue;
+      cx<RT> v[NCOMP];
+      load_sp<SP, NCOMP>(t, rhs0 + q, cb, v);
+#pragma unroll
+      for (int sp = 0; sp < NS; ++sp)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          cx<RT> h = acc[q][sp][c];
+          if (sp >= NS / 2) h = -h;
+          cx<RT>& w = v[sp * NC + c];
+          w -= (RT)k2 * h;
+          n[q] += (double)w.re * w.re + (double)w.im * w.im;
+        }
+      store_sp<SP, NCOMP>(r, rhs0 + q, cb, v);
+    }
+  }
+  if (grid_sum<R>(n, partials + (int64_t)blockIdx.y * nblk * R, counters + blockIdx.y, sh) && threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      if (act[q]) res[rhs0 + q] = n[q];
+  }
+}
+
+// dst = src (same precision) for rhs with upd[rhs]
+template <int SP, int NCOMP>
+__global__ void __launch_bounds__(128) copy_sp_kernel(int64_t Vh, EoField src, EoField dst, const int* upd) {
+  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (cb >= Vh || !upd[rhs]) return;
+  cx<typename Prec<SP>::real> v[NCOMP];
+  load_sp<SP, NCOMP>(src, rhs, cb, v);
+  store_sp<SP, NCOMP>(dst, rhs, cb, v);
 }
 
 // p = r + beta p
@@ -507,6 +571,8 @@ struct CgOps {
   void (*accumulate)(Work&, cudaStream_t);
   void (*zero64)(Work&, const EoField& f, cudaStream_t);
   void (*dslash)(Work&, cudaStream_t);                  // s_o = H_oe p_e, every rhs
+  void (*rnew)(Work&, cudaStream_t);                    // r = M^dag t (sloppy), masked, |r|^2 -> res
+  void (*copy_rp)(Work&, cudaStream_t);                 // p = r, masked (restart)
 };
 // kernels one iterate() call launches
 constexpr int kLaunchesPerIteration = 6;
@@ -546,7 +612,7 @@ struct Work {
   int nblk = 0;
   double kappa = 0;
   // FP64 fields
-  EoField be, bo, bp, x64, xo, q, s64, r64;
+  EoField be, bo, bp, x64, xo, q, s64;
   // sloppy fields
   EoField r, p, t, s, xs;
   CGState* st = nullptr;
@@ -645,8 +711,22 @@ struct Impl {
     w.launches += 1;
     cg_hop_kernel<ND, NC, SP, GP, COMP, false, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, nullptr);
   }
+  static void rnew(Work& w, cudaStream_t st) {
+    const double k2 = w.kappa * w.kappa;
+    dim3 tile(w.nblk, w.nrhs / R);
+    w.launches += 2;
+    cg_hop_kernel<ND, NC, SP, GP, COMP, true, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, nullptr);
+    cg_rnew_kernel<ND, NC, SP, GP, COMP, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.t, w.r, k2, w.upd,
+                                                                  w.partials, w.counters, w.res, w.nblk);
+  }
+  static void copy_rp(Work& w, cudaStream_t st) {
+    dim3 grid(w.nblk, w.nrhs);
+    w.launches += 1;
+    copy_sp_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.r, w.p, w.upd);
+  }
   static CgOps table() {
-    return CgOps{&iterate, &hop64, &to_eo, &from_eo, &norm64, &convert, &accumulate, &zero64, &dslash};
+    return CgOps{&iterate, &hop64, &to_eo, &from_eo, &norm64, &convert, &accumulate, &zero64, &dslash, &rnew,
+                 &copy_rp};
   }
 };
 
@@ -765,7 +845,7 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   w->ops = w->ops_r[0];
   w->R = w->rcand[0];
   const int nc = g->ncomp;
-  size_t bytes = 8 * field_bytes(SP64, nc, g->Vh, nrhs);
+  size_t bytes = 7 * field_bytes(SP64, nc, g->Vh, nrhs);
   bytes += 4 * field_bytes(sp, nc, g->Vh, nrhs);
   if (sp != SP64) bytes += field_bytes(w->xp, nc, g->Vh, nrhs);
   const size_t nres = 8;
@@ -789,7 +869,6 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   w->xo = carve(cur, SP64, nc, g->Vh, nrhs);
   w->q = carve(cur, SP64, nc, g->Vh, nrhs);
   w->s64 = carve(cur, SP64, nc, g->Vh, nrhs);
-  w->r64 = carve(cur, SP64, nc, g->Vh, nrhs);
   w->r = carve(cur, sp, nc, g->Vh, nrhs);
   w->p = carve(cur, sp, nc, g->Vh, nrhs);
   w->t = carve(cur, sp, nc, g->Vh, nrhs);
@@ -831,9 +910,12 @@ static int fetch_res(Work& w, int n, cudaStream_t st) {
   return LYM_OK;
 }
 
-// FP64 reliable update for the rhs flagged in upd_host (already copied to upd):
-// x += x_sloppy; q = b' - M x; r64 = M^dag q.  Leaves |q|^2 in res_host[0..nrhs)
-// and |r64|^2 in res_host[nrhs..2 nrhs).
+// Reliable update for the rhs flagged in upd_host (already copied to upd):
+// x += x_sloppy and the true residual q = b' - M x in FP64 (the convergence
+// test); then the new recursion residual r = M^dag q in the sloppy precision
+// (it only has to be accurate relative to |q|).  Leaves |q|^2 in
+// res_host[0..nrhs) and |r|^2 in res_host[nrhs..2 nrhs).  t and s serve as
+// temporaries: the next iteration recomputes both before reading them.
 static int reliable_update(Work& w, cudaStream_t st) {
   const double k = w.kappa, k2 = k * k;
   EoField none;
@@ -841,8 +923,8 @@ static int reliable_update(Work& w, cudaStream_t st) {
   w.ops.hop64(w, 1, w.x64, w.s64, none, none, 0.0, 1.0, false, false, false, st);
   w.ops.hop64(w, 0, w.s64, w.q, w.bp, w.x64, -1.0, k2, false, false, true, st);
   LYM_CUDA(cudaMemcpyAsync(w.res_host, w.res, sizeof(double) * w.nrhs, cudaMemcpyDeviceToHost, st));
-  w.ops.hop64(w, 1, w.q, w.s64, none, none, 0.0, 1.0, true, false, false, st);
-  w.ops.hop64(w, 0, w.s64, w.r64, w.q, none, 0.0, -k2, false, true, true, st);
+  w.ops.convert(w, w.q, w.t, none, true, st);
+  w.ops.rnew(w, st);
   LYM_CUDA(cudaMemcpyAsync(w.res_host + w.nrhs, w.res, sizeof(double) * w.nrhs, cudaMemcpyDeviceToHost, st));
   LYM_CHECK_LAUNCH();
   LYM_CUDA(cudaStreamSynchronize(st));
@@ -961,12 +1043,18 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
   if (sp != SP64) LYM_CUDA(cudaMemsetAsync(w.xs.data, 0, field_bytes(w.xp, g->ncomp, w.Vh, nrhs), st));
   LYM_CHECK_LAUNCH();
 
-  std::vector<int> done(nrhs, 0), updates(nrhs, 0);
-  std::vector<double> target(nrhs, 0.0), tres(nrhs, 0.0);
+  std::vector<int> done(nrhs, 0), updates(nrhs, 0), restart(nrhs, 0);
+  std::vector<double> target(nrhs, 0.0), tres(nrhs, 0.0), prev_q2(nrhs, 0.0);
+  // sloppy runs get a reliable update at least this often, whatever the residual does
+  const int max_interval = sp == SP64 ? (1 << 30) : 50;
   auto plan_rhs = [&](int i, double q2, double r2) -> void {
     CGState& S = w.st_host[i];
     const double want = prm->tol * prm->tol * bnorm2[i];
     tres[i] = bnorm2[i] > 0 ? std::sqrt(q2 / bnorm2[i]) : 0.0;
+    // the true residual stalled since the last update: the sloppy recursion
+    // drifted, so restart the search direction from the true residual
+    restart[i] = (prev_q2[i] > 0.0 && q2 > 0.25 * prev_q2[i]) ? 1 : 0;
+    prev_q2[i] = q2;
     if (q2 <= want || r2 == 0.0) {
       done[i] = 1;
       S.active = 0;
@@ -978,6 +1066,7 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     target[i] = est;
     S.rr = r2;
     S.pause2 = sp == SP64 ? est : std::max(est, delta * delta * r2);
+    S.pause_iter = S.iters + max_interval;
     S.active = S.iters >= S.max_iter ? 0 : 1;
   };
   for (int i = 0; i < nrhs; ++i) {
@@ -985,12 +1074,12 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     std::memset(&S, 0, sizeof(S));
     S.max_iter = prm->max_iter;
   }
-  // initial residual (x = 0): q = b', r64 = M^dag b'
+  // initial residual (x = 0): q = b', r = M^dag b'
   rc = reliable_update(w, st);
   if (rc) return rc;
   for (int i = 0; i < nrhs; ++i) plan_rhs(i, w.res_host[i], w.res_host[nrhs + i]);
   LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
-  w.ops.convert(w, w.r64, w.r, w.p, false, st);  // r = p = r64 in sloppy precision
+  w.ops.copy_rp(w, st);  // p = r (upd is all ones here)
   LYM_CHECK_LAUNCH();
   rc = autotune(w, st);
   if (rc) return rc;
@@ -1028,8 +1117,16 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
       plan_rhs(i, q2[i], r2[i]);
     }
     LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
-    // r = r64 (sloppy) for the updated rhs; p is kept
-    w.ops.convert(w, w.r64, w.r, none, true, st);
+    // p is kept across an update, except where the true residual stalled
+    bool any_restart = false;
+    for (int i = 0; i < nrhs; ++i) {
+      w.upd_host[i] = (!done[i] && restart[i]) ? 1 : 0;
+      any_restart = any_restart || w.upd_host[i];
+    }
+    if (any_restart) {
+      LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * nrhs, cudaMemcpyHostToDevice, st));
+      w.ops.copy_rp(w, st);
+    }
     LYM_CHECK_LAUNCH();
     bool left = false;
     for (int i = 0; i < nrhs; ++i) left = left || (!done[i] && w.st_host[i].iters < prm->max_iter);
