@@ -113,6 +113,19 @@ int lym_cdot(int64_t n, const void* a, const void* b, double* result, void* stre
 /* y = a*x + b*y with complex a, b (re, im pairs). */
 int lym_caxpby(int64_t n, const double* a, const void* x, const double* b, void* y, void* stream);
 
+/* results[2i], results[2i+1] (host) = sum conj(a_i) b_i for nvec vector pairs of n
+ * complex128 elements each, stored back to back (nvec, n).  No counterpart in the
+ * reference: an entry point for callers that cannot allocate device memory, such as
+ * code running under a framework's pooling allocator (which owns the device heap and
+ * would not see a cudaMalloc) or under a fixed device-memory budget.  It allocates
+ * nothing: its reduction scratch is a static device array of about 263 KB that every
+ * GPU loading the library keeps until exit, which limits nvec to 64 (larger nvec
+ * returns LYM_ERR_BAD_ARG).  The first call on a device looks up the array's address;
+ * make that first call before any stream capture.  All calls share the array, so
+ * calls that overlap on the GPU (other streams, other host threads) race.
+ * Synchronises `stream`. */
+int lym_cdot_batch_noalloc(int nvec, int64_t n, const void* a, const void* b, double* results, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* gauge objects for the solvers                                       */
 /* ------------------------------------------------------------------ */

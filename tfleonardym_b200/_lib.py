@@ -57,6 +57,7 @@ SIGNATURES = {
                                        c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "lym_cdot": (c_int, [c_int64, c_void_p, c_void_p, P(c_double), c_void_p]),
     "lym_caxpby": (c_int, [c_int64, P(c_double), c_void_p, P(c_double), c_void_p, c_void_p]),
+    "lym_cdot_batch_noalloc": (c_int, [c_int, c_int64, c_void_p, c_void_p, P(c_double), c_void_p]),
     "lym_gauge_create": (c_int, [c_void_p, c_int, c_void_p, c_double, c_double, c_uint, c_void_p,
                                  P(c_void_p)]),
     "lym_gauge_update": (c_int, [c_void_p, c_void_p, c_void_p]),
