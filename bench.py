@@ -52,6 +52,7 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--delta", type=float, default=0.1, help="reliable-update trigger of the mixed solver")
     ap.add_argument("--chunk", type=int, default=8, help="CG iterations per captured graph launch")
+    ap.add_argument("--workers", type=int, default=2, help="solve-server worker streams")
     return ap.parse_args()
 
 
@@ -264,7 +265,6 @@ def run_lym(args, rank, world, local_rank):
     B = args.nrhs
     b_host = torch.from_numpy(host_sources(99 + rank, B)).pin_memory()
     b_dev = b_host.to(dev)
-    x_host = torch.empty_like(b_host).pin_memory()
     mixed = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision=args.precision, chunk=args.chunk,
                                             delta=args.delta)
     plain = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision="f64", chunk=8)
@@ -287,53 +287,94 @@ def run_lym(args, rank, world, local_rank):
     check(plain.reports)
     torch.cuda.synchronize()
 
-    # ---- timed region: batched mixed-precision solves, inputs resident ----
+    # ---- timed region: served mixed-precision solves ----
+    # a burst of steps x nrhs single-right-hand-side requests through the solve
+    # server (continuous batching, up to nrhs per batch); sources resident
+    from tfleonardym_b200 import serving
+    budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
+    srv = serving.SolveServer(budget, max_batch=B, workers=args.workers, device=local_rank)
+
+    x_host = torch.empty_like(b_host).pin_memory()
+
+    def served(nreq, src, rate=None):
+        futs = []
+        host = not src.is_cuda
+        for i in range(nreq):
+            if rate:
+                time.sleep(float(np.random.default_rng(i).exponential(1.0 / rate)))
+            futs.append(srv.submit(serving.SolveRequest("bench", GEOMETRY, NC, KAPPA, src[i % B], gauge=links,
+                                                        tol=TOL, precision=args.precision, bc=-1.0,
+                                                        max_iter=2000, out=x_host[i % B] if host else None)))
+        res = [f.result() for f in futs]
+        bad = [r for r in res if r.status != serving.OK]
+        if bad:
+            raise RuntimeError(f"served solve missed the tolerance: {bad[0].reports}")
+        return res
+
+    served(2 * B * args.workers, b_dev)  # warm the server: gauge copies, workspaces, graphs, autotuning
+    torch.cuda.synchronize()
     clocks = ClockSampler(local_rank)
     clocks.start()
     barrier()
     torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    launches = 0
-    iters, rupd = [], []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_wall = time.perf_counter()
-    for s, e in evs:
-        s.record(stream)
-        mixed.solve(op, b_dev)
-        e.record(stream)
-        check(mixed.reports)
-        launches += mixed.reports[0]["kernel_launches"]
-        iters += [r["iterations"] for r in mixed.reports]
-        rupd += [r["reliable_updates"] for r in mixed.reports]
+    ev0.record(stream)
+    res = served(args.steps * B, b_dev)
     torch.cuda.synchronize()
+    ev1.record(stream)
+    ev1.synchronize()
     barrier()
     t_wall = time.perf_counter() - t_wall
-    step_ms = [s.elapsed_time(e) for s, e in evs]
     clk = clocks.stop()
-    total_ms = sum(step_ms)
+    total_ms = ev0.elapsed_time(ev1)
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * args.steps * B / (total_ms / 1e3)
+    launches = sum(r.reports[0]["kernel_launches"] / r.batch_rhs for r in res)
+    iters = [m["iterations"] for r in res for m in r.reports]
+    rupd = [m["reliable_updates"] for r in res for m in r.reports]
+    batch_sizes = sorted({r.batch_rhs for r in res})
+    tuned = res[-1].reports[0].get("rhs_per_thread")
 
-    # ---- end to end through the public API with host buffers ----
-    e2e_ms = []
-    for _ in range(max(2, args.steps // 2)):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        bd = b_host.to(dev, non_blocking=True)
-        xd = mixed.solve(op, bd)
-        x_host.copy_(xd, non_blocking=True)
-        e.record(stream)
-        torch.cuda.synchronize()
-        check(mixed.reports)
-        e2e_ms.append(s.elapsed_time(e))
-    e2e_total = sum(e2e_ms)
+    # ---- latency: Poisson arrivals at half the saturated rate ----
+    rate = 0.5 * value / world
+    lat_res = served(4 * B, b_dev, rate=rate)
+    lat = sorted(1e3 * r.latency for r in lat_res)
+
+    # ---- end to end through the serving API with host buffers ----
+    torch.cuda.synchronize()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_e2e = max(2, args.steps // 2) * B
+    ev2.record(stream)
+    served(n_e2e, b_host)
+    torch.cuda.synchronize()
+    ev3.record(stream)
+    ev3.synchronize()
+    e2e_total = ev2.elapsed_time(ev3)
     if world > 1:
         t = torch.tensor([e2e_total], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = world * len(e2e_ms) * B / (e2e_total / 1e3)
+    e2e_value = world * n_e2e / (e2e_total / 1e3)
+    srv.close()
+
+    # ---- the same solves as direct batched calls (no server) ----
+    for _ in range(2):
+        mixed.solve(op, b_dev)
+    torch.cuda.synchronize()
+    direct_ms = []
+    for _ in range(max(2, args.steps // 2)):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        mixed.solve(op, b_dev)
+        e.record(stream)
+        torch.cuda.synchronize()
+        check(mixed.reports)
+        direct_ms.append(s.elapsed_time(e))
+    direct_value = B / (statistics.mean(direct_ms) / 1e3)
 
     # ---- plain FP64 one solve at a time ----
     plain_ms, plain_iters = [], []
@@ -389,29 +430,33 @@ def run_lym(args, rank, world, local_rank):
                          f"{sec_per_it:.2f} s each, extrapolated with the {it_per_solve:.0f} iterations the "
                          f"plain FP64 GPU solve took"}
 
-    q = sorted(step_ms)
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": f"{args.precision}+f64",
         "data": "synthetic",
-        "config": {"workload": "wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
-                   "nrhs_per_step": B, "inner_precision": args.precision, "outer_precision": "f64",
+        "config": {"workload": "served wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
+                   "step": f"{B} single-rhs requests", "max_batch_rhs": B, "server_workers": args.workers,
+                   "inner_precision": args.precision, "outer_precision": "f64",
                    "reliable_update_delta": args.delta, "graph_chunk": args.chunk,
                    "links": "reunit(exp(i 0.25 H)), H traceless Hermitian", "bc": "antiperiodic time",
                    "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (sources + solutions of a step exceed 126 MB)"},
-        "latency_ms": {"p50": statistics.median(step_ms), "p99": q[min(len(q) - 1, int(0.99 * len(q)))],
-                       "what": f"one batch of {B} solves, device-resident"},
+                   "l2": "inputs larger than L2 (the sources and solutions of the timed requests exceed 126 MB)"},
+        "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                       "what": f"request latency, Poisson arrivals at {rate:.0f} req/s (half the saturated rate)"},
+        "batch_rhs_seen": batch_sizes,
+        "direct_batched": {"value": world * direct_value, "unit": "solves/s",
+                           "what": f"lym_wilson_solve on {B} rhs per call, no server"},
         "plain_fp64": {"value": world * plain_value, "unit": "solves/s", "ms_per_solve": statistics.mean(plain_ms),
                        "iterations": plain_iters},
         "speedup_vs_plain_fp64": value / (world * plain_value),
         "iterations_per_solve": {"mean": statistics.mean(iters), "max": max(iters),
                                  "reliable_updates_mean": statistics.mean(rupd)},
-        "autotuned": {"rhs_per_thread": mixed.reports[0].get("rhs_per_thread")},
+        "autotuned": {"rhs_per_thread": tuned},
         "gpu_launches": int(launches),
         "e2e": {"value": e2e_value, "unit": "solves/s",
-                "h2d_bytes_per_step": int(b_host.numel() * 16), "d2h_bytes_per_step": int(x_host.numel() * 16)},
+                "h2d_bytes_per_step": int(b_host.numel() * 16), "d2h_bytes_per_step": int(b_host.numel() * 16),
+                "what": "the served path with pinned host sources; solutions come back to host memory"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": f"cg_hop_kernel<4,3,{args.precision}> s_o = H_oe p_e, "
                                                    f"{B} rhs, L2 flushed before each launch",

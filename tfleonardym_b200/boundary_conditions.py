@@ -53,6 +53,21 @@ def periodic_provider():
     return _tag(lambda x: x, 1.0)
 
 
+def factor_provider(factor):
+    """Provider for an arbitrary time-boundary factor (1 periodic, -1 antiperiodic),
+    applied by the kernels in registers."""
+    f = complex(factor)
+
+    def apply(x):
+        g = x.clone()
+        geom_last = _geometry[-1] if _geometry else None
+        if geom_last is None:
+            raise RuntimeError("set_antiperiodic_field_in_t_direction was not called")
+        g[-1][..., geom_last - 1::geom_last] *= f
+        return g
+    return _tag(apply, f)
+
+
 def provider_factor(provider):
     """(factor, needs_tensor_application) for a boundary_condition_provider."""
     if provider is None:

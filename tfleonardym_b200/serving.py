@@ -1,0 +1,311 @@
+"""Solve server: continuous batching of Wilson solve requests on one GPU.
+
+Requests of different geometry, N, kappa, tolerance and precision arrive at any
+time (``submit`` returns a future).  Each request is admitted by its HBM
+footprint against a byte budget: a request that could never fit is rejected
+(status REJECTED); one that fits but finds the budget in use waits in the
+queue and is admitted as earlier requests finish and free their bytes.
+Gauge fields stay resident in an LRU cache keyed by the caller's gauge key,
+so repeated requests on the same configuration skip the upload.
+
+Worker threads (one CUDA stream each) repeatedly take the oldest pending
+request and batch every other pending request that shares its gauge, kappa,
+tolerance, precision and operator form into one multi-right-hand-side solve
+(``lym_wilson_solve``), up to ``max_batch`` right-hand sides.  Requests that
+arrive while a batch runs join the next batch, and batches of different
+gauges run concurrently on different streams.  Every answer carries the FP64
+true residual the solver verified; a request whose residual misses its
+tolerance completes with status NOT_CONVERGED.
+
+Latency bookkeeping: ``submit`` time, admission time, start and end of the
+batch that served the request.
+"""
+import collections
+import concurrent.futures
+import itertools
+import threading
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+
+OK, NOT_CONVERGED, REJECTED = "ok", "not_converged", "rejected"
+
+
+class SolveRequest:
+    """One solve of D x = b (or Q x = b when ``hermitian``) on a gauge field.
+
+    ``gauge_key`` names the configuration for the resident cache; ``gauge``
+    (complex128 (nd, N, N, V) CUDA tensor or a zero-argument callable
+    producing it) is only used when the key is not cached.  ``b`` is one
+    spinor (ns, N, V) or several (k, ns, N, V) on the device.
+    """
+
+    _ids = itertools.count()
+
+    def __init__(self, gauge_key, geometry, nc, kappa, b, gauge=None, tol=1e-10, precision="f16",
+                 hermitian=False, bc=-1.0, max_iter=5000, out=None):
+        self.id = next(self._ids)
+        self.gauge_key = gauge_key
+        self.geometry = tuple(int(g) for g in geometry)
+        self.nc = int(nc)
+        self.kappa = float(kappa)
+        self.b = b
+        self.gauge = gauge
+        self.tol = float(tol)
+        self.precision = precision
+        self.hermitian = bool(hermitian)
+        self.bc = complex(bc)
+        self.max_iter = int(max_iter)
+        self.out = out  # optional tensor (e.g. pinned host memory) the solution is copied into
+        self.nrhs = 1 if b.dim() == 3 else int(b.shape[0])
+        self.t_submit = self.t_admit = self.t_start = self.t_end = None
+        self.future = concurrent.futures.Future()
+
+    def batch_key(self):
+        return (self.gauge_key, self.kappa, self.tol, self.precision, self.hermitian, self.bc)
+
+
+class SolveResult:
+    def __init__(self, request, x, status, reports):
+        self.request = request
+        self.x = x
+        self.status = status
+        self.reports = reports
+
+    @property
+    def latency(self):
+        r = self.request
+        return r.t_end - r.t_submit
+
+
+def footprint_bytes(geometry, nc, nrhs, precision="f16", with_gauge=True):
+    """Device bytes a request occupies: its sources and solutions, its share of
+    the solver workspace and (when not resident yet) the gauge copies."""
+    vol = int(np.prod(geometry))
+    nd = len(geometry)
+    ns = 2 if nd == 2 else 4
+    ncomp = ns * nc
+    spin = vol * ncomp * 16
+    sloppy = {"f64": 16, "f32": 8, "f16": 4 + 4 / ncomp, "bf16": 4 + 4 / ncomp}[precision]
+    per_rhs = 2 * spin + 7 * spin / 2 + 5 * (vol / 2) * ncomp * sloppy
+    gauge = 0
+    if with_gauge:
+        link = nd * nc * nc * vol * 16
+        gauge = 3 * link + (nd * vol * (nc - 1) * nc * 8 if precision != "f64" else 0)
+    return int(nrhs * per_rhs + gauge)
+
+
+class _Gauge:
+    """A resident configuration.  Each worker solves through its own Dirac
+    operator (and so its own lym_gauge and solver workspace), so batches on
+    the same configuration can run concurrently on different streams."""
+
+    def __init__(self, key, field, geometry, nc, bc, nbytes):
+        self.key = key
+        self.field = field
+        self.geometry = geometry
+        self.nc = nc
+        self.bc = bc
+        self.nbytes = nbytes
+        self.ops = {}
+        self.users = 0
+
+    def op_for(self, widx, kappa, hermitian):
+        from . import boundary_conditions, dirac
+        from . import lattice as lt
+        op = self.ops.get(widx)
+        if op is None:
+            cfg = lt.Configuration(self.field, self.geometry, self.nc, len(self.geometry))
+            op = dirac.DiracWilsonOperator(cfg, kappa, hermitian, representation="fundamental",
+                                           boundary_condition_provider=boundary_conditions.factor_provider(self.bc))
+            self.ops[widx] = op
+        op.kappa = kappa
+        op.hermitian = hermitian
+        return op
+
+
+class SolveServer:
+    def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8):
+        self.budget = int(hbm_budget_bytes)
+        self.max_batch = int(max_batch)
+        self.device = device  # CUDA device index; None: the caller's current device
+        self.cache_size = int(gauge_cache)
+        self._lock = threading.Condition()
+        self._pending = collections.deque()  # admitted, waiting for a worker
+        self._waiting = collections.deque()  # fits the budget in principle, waiting for bytes
+        self._in_use = 0
+        self._gauges = collections.OrderedDict()
+        self._closed = False
+        self.completed = []
+        if self.device is None and torch.cuda.is_available():
+            self.device = torch.cuda.current_device()
+        self._workers = [threading.Thread(target=self._run, args=(i,), daemon=True) for i in range(workers)]
+        for t in self._workers:
+            t.start()
+
+    # -- client side ----------------------------------------------------------
+    def submit(self, req: SolveRequest):
+        req.t_submit = time.perf_counter()
+        need = self._request_bytes(req)
+        if need > self.budget:
+            req.t_end = req.t_submit
+            req.future.set_result(SolveResult(req, None, REJECTED, []))
+            return req.future
+        with self._lock:
+            if self._closed:
+                raise RuntimeError("server closed")
+            req._bytes = need
+            if self._in_use + need <= self.budget and not self._waiting:
+                self._admit(req)
+            else:
+                self._waiting.append(req)
+            self._lock.notify_all()
+        return req.future
+
+    def close(self, wait=True):
+        with self._lock:
+            self._closed = True
+            self._lock.notify_all()
+        if wait:
+            for t in self._workers:
+                t.join()
+        self._gauges.clear()
+
+    def stats(self):
+        lat = [r.latency for r in self.completed if r.status != REJECTED]
+        if not lat:
+            return {}
+        return {"completed": len(lat), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                "p99_ms": 1e3 * float(np.percentile(lat, 99))}
+
+    # -- internals ------------------------------------------------------------
+    def _request_bytes(self, req):
+        resident = req.gauge_key in self._gauges
+        return footprint_bytes(req.geometry, req.nc, req.nrhs, req.precision, with_gauge=not resident)
+
+    def _admit(self, req):
+        self._in_use += req._bytes
+        req.t_admit = time.perf_counter()
+        self._pending.append(req)
+
+    def _release(self, reqs):
+        with self._lock:
+            for r in reqs:
+                self._in_use -= r._bytes
+            while self._waiting and self._in_use + self._waiting[0]._bytes <= self.budget:
+                self._admit(self._waiting.popleft())
+            self._lock.notify_all()
+
+    def _take_batch(self):
+        """Oldest pending request plus every compatible pending one, up to max_batch rhs."""
+        with self._lock:
+            while not self._pending and not (self._closed and not self._waiting):
+                self._lock.wait(timeout=0.05)
+            if not self._pending:
+                return None
+            first = self._pending.popleft()
+            key = first.batch_key()
+            batch, rhs = [first], first.nrhs
+            keep = collections.deque()
+            while self._pending:
+                r = self._pending.popleft()
+                if r.batch_key() == key and rhs + r.nrhs <= self.max_batch:
+                    batch.append(r)
+                    rhs += r.nrhs
+                else:
+                    keep.append(r)
+            self._pending = keep
+            return batch
+
+    def _gauge_for(self, req):
+        with self._lock:
+            g = self._gauges.get(req.gauge_key)
+            if g is not None:
+                self._gauges.move_to_end(req.gauge_key)
+                g.users += 1
+                return g
+        u = req.gauge() if callable(req.gauge) else req.gauge
+        if u is None:
+            raise ValueError(f"gauge {req.gauge_key!r} is not resident and no field was given")
+        if not u.is_cuda:
+            u = u.to(torch.device("cuda", self.device))
+        g = _Gauge(req.gauge_key, u, req.geometry, req.nc, req.bc,
+                   footprint_bytes(req.geometry, req.nc, 0, req.precision, True))
+        with self._lock:
+            old = self._gauges.get(req.gauge_key)
+            if old is not None:  # another worker loaded it meanwhile
+                old.users += 1
+                return old
+            self._gauges[req.gauge_key] = g
+            g.users += 1
+            while len(self._gauges) > self.cache_size:
+                k, victim = next(iter(self._gauges.items()))
+                if victim.users:
+                    break
+                self._gauges.pop(k)
+        return g
+
+    def _run(self, widx):
+        from . import dirac_solver
+        dirac_solver.VERBOSE = False
+        torch.cuda.set_device(self.device)
+        stream = torch.cuda.Stream(device=torch.device("cuda", self.device))
+        while True:
+            batch = self._take_batch()
+            if batch is None:
+                return
+            t0 = time.perf_counter()
+            for r in batch:
+                r.t_start = t0
+            try:
+                with torch.cuda.stream(stream):
+                    self._solve_batch(batch, widx)
+            except Exception as exc:  # noqa: BLE001 - delivered to every waiter
+                for r in batch:
+                    r.t_end = time.perf_counter()
+                    if not r.future.done():
+                        r.future.set_exception(exc)
+            finally:
+                self._release(batch)
+
+    def _solve_batch(self, batch, widx=0):
+        from . import dirac_solver
+        first = batch[0]
+        g = self._gauge_for(first)
+        dev = torch.device("cuda", self.device)
+        host = not first.b.is_cuda
+        try:
+            # host sources (the reference-facing path) cross here, on this worker's stream
+            b = torch.cat([(r.b if r.b.dim() == 4 else r.b[None]).to(dev, non_blocking=True) for r in batch])
+            solver = dirac_solver.conjugate_gradient(max_steps=max(r.max_iter for r in batch), tol=first.tol,
+                                                     precision=first.precision)
+            op = g.op_for(widx, first.kappa, first.hermitian)
+            x = solver.solve(op, b)
+            k = 0
+            for r in batch:  # caller-provided outputs (pinned host buffers on the host path)
+                if r.out is not None:
+                    r.out.copy_(x[k:k + r.nrhs] if r.b.dim() == 4 else x[k], non_blocking=True)
+                k += r.nrhs
+            if host and any(r.out is None for r in batch):
+                x = x.to("cpu", non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            reps = solver.reports
+        finally:
+            with self._lock:
+                g.users -= 1
+        t_end = time.perf_counter()
+        batch_rhs = sum(r.nrhs for r in batch)
+        k = 0
+        for r in batch:
+            mine = reps[k:k + r.nrhs]
+            xr = r.out if r.out is not None else (x[k:k + r.nrhs] if r.b.dim() == 4 else x[k])
+            k += r.nrhs
+            ok = all(m["status"] == 0 and m["true_residual"] <= r.tol for m in mine)
+            r.t_end = t_end
+            res = SolveResult(r, xr, OK if ok else NOT_CONVERGED, mine)
+            res.batch_rhs = batch_rhs
+            self.completed.append(res)
+            r.future.set_result(res)
