@@ -53,6 +53,10 @@ def parse_args():
     ap.add_argument("--delta", type=float, default=0.1, help="reliable-update trigger of the mixed solver")
     ap.add_argument("--chunk", type=int, default=8, help="CG iterations per captured graph launch")
     ap.add_argument("--workers", type=int, default=2, help="solve-server worker streams")
+    ap.add_argument("--rhs-per-thread", type=int, default=0, help="hop-kernel tile (0: autotune)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: one short solve, then 3 solver dslash launches inside the NVTX "
+                         "range 'dslash' (select them with ncu --nvtx --nvtx-include dslash/), no timing")
     return ap.parse_args()
 
 
@@ -266,13 +270,28 @@ def run_lym(args, rank, world, local_rank):
     b_host = torch.from_numpy(host_sources(99 + rank, B)).pin_memory()
     b_dev = b_host.to(dev)
     mixed = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision=args.precision, chunk=args.chunk,
-                                            delta=args.delta)
+                                            delta=args.delta, rhs_per_thread=args.rhs_per_thread)
     plain = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision="f64", chunk=8)
     stream = torch.cuda.current_stream()
 
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.profile:
+        short = dirac_solver.conjugate_gradient(max_steps=16, tol=TOL, precision=args.precision, chunk=8,
+                                                delta=args.delta, rhs_per_thread=max(1, args.rhs_per_thread))
+        short.solve(op, b_dev)  # builds the workspace; stops early on purpose
+        gauge = op.solver_gauge((args.precision,))
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("dslash")
+        _lib.check(_lib.lib().lym_dslash_eo(gauge, _lib.PREC[args.precision], B, 3, _dev.stream()), "lym_dslash_eo")
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        if rank == 0:
+            print(json.dumps({"profile": "dslash", "precision": args.precision, "nrhs": B,
+                              "rhs_per_thread": short.reports[0]["rhs_per_thread"]}), flush=True)
+        return 0
 
     def check(reports):
         bad = [r for r in reports if r["status"] != 0 or r["true_residual"] > TOL]
@@ -292,7 +311,9 @@ def run_lym(args, rank, world, local_rank):
     # server (continuous batching, up to nrhs per batch); sources resident
     from tfleonardym_b200 import serving
     budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
-    srv = serving.SolveServer(budget, max_batch=B, workers=args.workers, device=local_rank)
+    srv = serving.SolveServer(budget, max_batch=B, workers=args.workers, device=local_rank,
+                              solver_options=dict(delta=args.delta, chunk=args.chunk,
+                                                  rhs_per_thread=args.rhs_per_thread))
 
     x_host = torch.empty_like(b_host).pin_memory()
 

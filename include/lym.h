@@ -150,6 +150,8 @@ typedef struct lym_solver_params {
   double delta;      /* reliable-update trigger: sloppy |r| fell by this factor  */
   int hermitian;     /* 1: system is Q x = b with Q = gamma_d D                  */
   int chunk;         /* iterations per captured CUDA graph launch (0 = default)  */
+  int rhs_per_thread;/* at most this many right-hand sides per hop-kernel thread
+                        (1, 2 or 4; the largest available one is used); 0 = autotune */
 } lym_solver_params;
 
 typedef struct lym_solver_report {
@@ -159,6 +161,7 @@ typedef struct lym_solver_report {
   double true_residual;  /* FP64 |b - D x| / |b| of the returned x               */
   int64_t kernel_launches; /* lym kernels the whole call launched (graph nodes included) */
   int rhs_per_thread;    /* right-hand sides per thread the autotuner picked for the hop kernels */
+  int compressed_links;  /* 1: the hop kernels read the N-1-row sloppy links, 0: full links */
 } lym_solver_report;
 
 /* Solve D x_i = b_i (or Q x_i = b_i) for nrhs right-hand sides stored back to

@@ -212,6 +212,28 @@ def test_eo_cg_true_residual(cuda_device, case, precision):
             assert solver.reports[i]["true_residual"] < 1e-10
 
 
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_eo_cg_every_hop_tile(cuda_device, precision):
+    """Every hop-kernel variant (1, 2, 4 rhs per thread with full links, and the
+    autotuned pick, which may use compressed links) meets the true residual."""
+    from tfleonardym_b200 import dirac_solver
+    g = load_golden("d4")
+    spec = GOLDEN_CASES["d4"]
+    tables = O.lookup_tables(spec["geometry"])
+    ub = O.apply_time_bc(g["gauge"], O.antiperiodic_field(spec["geometry"]))
+    rng = np.random.default_rng(3)
+    b = rng.normal(size=(8,) + g["eta"].shape) + 1j * rng.normal(size=(8,) + g["eta"].shape)
+    op = make_op(g, spec, False, True)
+    for tile in (1, 2, 4, 0):
+        solver = dirac_solver.conjugate_gradient(tol=1e-10, precision=precision, rhs_per_thread=tile)
+        x = np_(solver.solve(op, cu(b)))
+        if tile:
+            assert solver.reports[0]["rhs_per_thread"] == tile and solver.reports[0]["compressed_links"] == 0
+        for i in range(8):
+            res = np.linalg.norm(b[i] - O.wilson_apply(ub, x[i], spec["kappa"], False, tables)) / np.linalg.norm(b[i])
+            assert res < 1e-10, (tile, i, res)
+
+
 def test_eo_cg_batch_equals_single(cuda_device):
     """A right-hand side gives the same answer alone and inside a batch."""
     from tfleonardym_b200 import dirac_solver

@@ -231,7 +231,13 @@ struct EoGeom {
   int stride[4];  // lexicographic strides (last coordinate fastest)
   int Lh;         // dims[nd-1] / 2
   int64_t Vh;
+  // Neighbour table of the checkerboard, nbr[(par * 2 nd + 2 mu + dir) * Vh + cb]:
+  // the checkerboard index of x +- mu (dir 0: +, 1: -) for x of parity par,
+  // with bit 31 set when the hop crosses the time boundary (mu = nd-1 and the
+  // link involved sits on the last time slice).  Built once per gauge object.
+  const int* nbr;
 };
+constexpr int kNbrBoundary = int(0x80000000u);
 
 // coordinates and lexicographic index of checkerboard site (cb, parity);
 // 32-bit arithmetic throughout (the volume is below 2^31)
@@ -352,8 +358,8 @@ LYM_D void hop_tile(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
   using RT = typename Prec<SP>::real;
   using GR = typename GPrec<GP>::real;
   constexpr int NS = Gamma<ND>::NS;
-  int x[ND];
-  const int lex = eo_coords<ND>(g, cb, par, x);
+  const int vh = (int)g.Vh;
+  const int* nb = g.nbr + par * 2 * ND * vh + cb;
 #pragma unroll
   for (int r = 0; r < R; ++r)
 #pragma unroll
@@ -365,8 +371,8 @@ LYM_D void hop_tile(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
       const bool fwd = dir == 0;
-      const int nlex = fwd ? nb_fwd<ND>(g, lex, x, mu) : nb_bwd<ND>(g, lex, x, mu);
-      const int ncb = nlex >> 1;
+      const int code = __ldg(nb + (2 * mu + dir) * vh);
+      const int ncb = code & 0x7fffffff;
       cx<GR> ug[NC][NC];
       load_link_eo<GP, NC, COMP>(hg.data, hg.nunits, g.Vh, mu, fwd ? par : 1 - par, fwd ? cb : ncb, ug);
       cx<RT> u[NC][NC];
@@ -374,7 +380,7 @@ LYM_D void hop_tile(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
       for (int i = 0; i < NC; ++i)
 #pragma unroll
         for (int j = 0; j < NC; ++j) u[i][j] = {(RT)ug[i][j].re, (RT)ug[i][j].im};
-      if (COMP && mu == ND - 1 && x[ND - 1] == (fwd ? g.dims[ND - 1] - 1 : 0)) {
+      if (COMP && mu == ND - 1 && (code & kNbrBoundary)) {
         const cx<RT> bc{(RT)hg.bcr, (RT)hg.bci};
 #pragma unroll
         for (int i = 0; i < NC; ++i)

@@ -99,9 +99,30 @@ LYM_D void store_link_eo(void* g, int nunits, int64_t Vh, int mu, int par, int64
   }
 }
 
+// Even-odd neighbour table (EoGeom::nbr): one thread per (cb, parity).
+template <int ND>
+__global__ void build_nbr_kernel(EoGeom g, int* __restrict__ nbr) {
+  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int par = blockIdx.y;
+  if (cb >= g.Vh) return;
+  int x[ND];
+  const int lex = eo_coords<ND>(g, cb, par, x);
+  const int vh = (int)g.Vh;
+#pragma unroll
+  for (int mu = 0; mu < ND; ++mu) {
+    const int up = nb_fwd<ND>(g, lex, x, mu) >> 1;
+    const int dn = nb_bwd<ND>(g, lex, x, mu) >> 1;
+    const bool tb = mu == ND - 1;
+    // forward hop: the link on x crosses when x_t = L-1; backward: the link on x-t when x_t = 0
+    nbr[(par * 2 * ND + 2 * mu) * vh + cb] = up | ((tb && x[ND - 1] == g.dims[ND - 1] - 1) ? kNbrBoundary : 0);
+    nbr[(par * 2 * ND + 2 * mu + 1) * vh + cb] = dn | ((tb && x[ND - 1] == 0) ? kNbrBoundary : 0);
+  }
+}
+
 template <int ND, int NC>
 __global__ void pack_gauge_kernel(EoGeom g, int64_t V, const double2* __restrict__ ref, double bcr, double bci,
-                                  double2* g64, float4* g32, int n32, int comp32, uint2* g16, int n16, int comp16) {
+                                  double2* g64, float4* g32, int n32, int comp32, uint2* g16, int n16, int comp16,
+                                  float4* g32f, int n32f, uint2* g16f, int n16f) {
   const int64_t lex = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int mu = blockIdx.y;
   if (lex >= V) return;
@@ -125,6 +146,8 @@ __global__ void pack_gauge_kernel(EoGeom g, int64_t V, const double2* __restrict
   store_link_eo<SP64, NC>(g64, NC * NC, g.Vh, mu, par, cb, false, ub);
   if (g32) store_link_eo<SP32, NC>(g32, n32, g.Vh, mu, par, cb, comp32, comp32 ? u : ub);
   if (g16) store_link_eo<SP16, NC>(g16, n16, g.Vh, mu, par, cb, comp16, comp16 ? u : ub);
+  if (g32f) store_link_eo<SP32, NC>(g32f, n32f, g.Vh, mu, par, cb, false, ub);
+  if (g16f) store_link_eo<SP16, NC>(g16f, n16f, g.Vh, mu, par, cb, false, ub);
 }
 
 // sum over links of |U U^dag - 1|^2 + |det U - 1|^2
@@ -591,10 +614,16 @@ struct lym_gauge {
   lym::EoGeom geom{};
   double2* uref = nullptr;  // reference-layout FP64 copy (boundary factor NOT applied)
   double2* u64 = nullptr;
-  float4* u32 = nullptr;
+  // sloppy links: compressed to N-1 rows (only when every link is SU(N)) and full N x N
+  float4* u32 = nullptr;   // compressed
   int n32 = 0;
-  uint2* u16 = nullptr;
+  uint2* u16 = nullptr;    // compressed
   int n16 = 0;
+  float4* u32f = nullptr;  // full, boundary factor folded in
+  int n32f = 0;
+  uint2* u16f = nullptr;   // full, boundary factor folded in
+  int n16f = 0;
+  int* nbr = nullptr;      // even-odd neighbour table (EoGeom::nbr)
   std::vector<lym::Work*> works;  // solver workspaces, most recently used first
 };
 
@@ -606,8 +635,12 @@ struct Work {
   int nreal = 0;                 // right-hand sides the caller passes
   int R = 1;                     // right-hand sides per thread in the hop kernels (autotuned)
   bool tuned = false;
-  int rcand[3] = {1, 0, 0};
-  CgOps ops_r[3]{};
+  int tuned_i = 0;
+  // hop-kernel candidates: right-hand sides per thread x compressed / full links
+  int ncand = 0, cur = 0;
+  int rcand[6] = {1, 0, 0, 0, 0, 0};
+  bool ccand[6] = {false, false, false, false, false, false};
+  CgOps ops_r[6]{};
   int64_t Vh = 0;
   int nblk = 0;
   double kappa = 0;
@@ -625,11 +658,12 @@ struct Work {
   double* res_host = nullptr;
   void* pool = nullptr;
   size_t pool_bytes = 0;
-  HopGauge hg64, hgs;
+  HopGauge hg64, hgs, hgs_c, hgs_f;  // hgs: the links of the selected candidate
   CgOps ops{};
   cudaGraphExec_t graph = nullptr;
   int graph_chunk = 0;
   double graph_kappa = 0;
+  int graph_cand = -1;
   cudaStream_t graph_stream = nullptr;
   cudaStream_t stream = nullptr;  // solves run here (capturable even when the caller uses the legacy stream)
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -830,18 +864,22 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   w->xp = sp;
   w->Vh = g->Vh;
   w->nblk = (int)grid_for(g->Vh, 128);
-  const bool comp = g->comp && sp != SP64;
   int nc_ = 0;
-  for (int R : {1, 2, 4}) {
-    if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
-    if (!pick_ops(g->nd, g->nc, sp, comp, R, &w->ops_r[nc_])) {
-      delete w;
-      set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
-      return LYM_ERR_UNSUPPORTED;
+  for (int comp = 0; comp < 2; ++comp) {
+    if (comp && !(g->comp && sp != SP64)) continue;  // compressed links need SU(N) links and a sloppy precision
+    for (int R : {1, 2, 4}) {
+      if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
+      if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, &w->ops_r[nc_])) {
+        delete w;
+        set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
+        return LYM_ERR_UNSUPPORTED;
+      }
+      w->rcand[nc_] = R;
+      w->ccand[nc_] = comp != 0;
+      ++nc_;
     }
-    w->rcand[nc_++] = R;
   }
-  for (int i = nc_; i < 3; ++i) w->rcand[i] = 0;
+  w->ncand = nc_;
   w->ops = w->ops_r[0];
   w->R = w->rcand[0];
   const int nc = g->ncomp;
@@ -896,9 +934,16 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
     return LYM_ERR_OOM;
   }
   w->hg64 = HopGauge{g->u64, g->nc * g->nc, 1.0, 0.0};
-  if (sp == SP64) w->hgs = w->hg64;
-  else if (sp == SP32) w->hgs = HopGauge{g->u32, g->n32, g->bcr, g->bci};
-  else w->hgs = HopGauge{g->u16, g->n16, g->bcr, g->bci};
+  if (sp == SP64) {
+    w->hgs_f = w->hgs_c = w->hg64;
+  } else if (sp == SP32) {
+    w->hgs_c = HopGauge{g->u32, g->n32, g->bcr, g->bci};
+    w->hgs_f = HopGauge{g->u32f, g->n32f, 1.0, 0.0};
+  } else {
+    w->hgs_c = HopGauge{g->u16, g->n16, g->bcr, g->bci};
+    w->hgs_f = HopGauge{g->u16f, g->n16f, 1.0, 0.0};
+  }
+  w->hgs = w->ccand[0] ? w->hgs_c : w->hgs_f;
   g->works.insert(g->works.begin(), w);
   *out = w;
   return LYM_OK;
@@ -932,7 +977,8 @@ static int reliable_update(Work& w, cudaStream_t st) {
 }
 
 static int build_graph(Work& w, int chunk, cudaStream_t st) {
-  if (w.graph && w.graph_chunk == chunk && w.graph_kappa == w.kappa && w.graph_stream == st) return LYM_OK;
+  if (w.graph && w.graph_chunk == chunk && w.graph_kappa == w.kappa && w.graph_stream == st && w.graph_cand == w.cur)
+    return LYM_OK;
   if (w.graph) {
     cudaGraphExecDestroy(w.graph);
     w.graph = nullptr;
@@ -953,22 +999,42 @@ static int build_graph(Work& w, int chunk, cudaStream_t st) {
     return LYM_ERR_CUDA;
   }
   w.graph_chunk = chunk;
+  w.graph_cand = w.cur;
   w.graph_kappa = w.kappa;
   w.graph_stream = st;
   return LYM_OK;
 }
 
-// Autotuner: time the hop kernel for every rhs-per-thread candidate the
-// workspace supports and keep the fastest (once per workspace).
-static int autotune(Work& w, cudaStream_t st) {
-  if (w.tuned) return LYM_OK;
+// Autotuner: time the hop kernel for every (right-hand sides per thread,
+// compressed or full links) candidate the workspace supports and keep the
+// fastest (once per workspace).  forced > 0: the caller fixed the tile; the
+// largest available one not above it is used, with full links.
+static void select_cand(Work& w, int i) {
+  w.cur = i;
+  w.ops = w.ops_r[i];
+  w.R = w.rcand[i];
+  w.hgs = w.ccand[i] ? w.hgs_c : w.hgs_f;
+}
+
+static int autotune(Work& w, cudaStream_t st, int forced) {
+  if (forced > 0) {
+    int pick = 0;
+    for (int i = 0; i < w.ncand; ++i)
+      if (w.rcand[i] <= forced && !w.ccand[i]) pick = i;
+    select_cand(w, pick);
+    return LYM_OK;
+  }
+  if (w.tuned) {
+    select_cand(w, w.tuned_i);
+    return LYM_OK;
+  }
   cudaEvent_t e0, e1;
   LYM_CUDA(cudaEventCreate(&e0));
   LYM_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int bi = 0;
-  for (int i = 0; i < 3 && w.rcand[i]; ++i) {
-    w.ops = w.ops_r[i];
+  for (int i = 0; i < w.ncand; ++i) {
+    select_cand(w, i);
     for (int k = 0; k < 2; ++k) w.ops.dslash(w, st);
     cudaEventRecord(e0, st);
     for (int k = 0; k < 5; ++k) w.ops.dslash(w, st);
@@ -984,9 +1050,9 @@ static int autotune(Work& w, cudaStream_t st) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   LYM_CHECK_LAUNCH();
-  w.ops = w.ops_r[bi];
-  w.R = w.rcand[bi];
+  select_cand(w, bi);
   w.tuned = true;
+  w.tuned_i = bi;
   return LYM_OK;
 }
 
@@ -1081,7 +1147,7 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
   LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
   w.ops.copy_rp(w, st);  // p = r (upd is all ones here)
   LYM_CHECK_LAUNCH();
-  rc = autotune(w, st);
+  rc = autotune(w, st, prm->rhs_per_thread);
   if (rc) return rc;
   rc = build_graph(w, chunk, st);
   if (rc) return rc;
@@ -1147,6 +1213,7 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     rep[i].true_residual = tres[i];
     rep[i].kernel_launches = w.launches;
     rep[i].rhs_per_thread = w.R;
+    rep[i].compressed_links = w.ccand[w.cur] ? 1 : 0;
     if (!done[i]) status = LYM_ERR_NOT_CONVERGED;
   }
   return status;
@@ -1206,39 +1273,50 @@ static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
     g->comp = dev < 1e-16;  // every link SU(N) to about 1e-8
   }
   const int nc = g->nc;
-  const int ncx = g->comp ? (nc - 1) * nc : nc * nc;
-  const int n32 = units_for(ncx, 2), n16 = units_for(ncx, 2);
-  if (g->u32 && g->n32 != n32) {
-    cudaFree(g->u32);
-    g->u32 = nullptr;
-  }
-  if (g->u16 && g->n16 != n16) {
-    cudaFree(g->u16);
-    g->u16 = nullptr;
-  }
   const bool want32 = (g->prec_mask >> LYM_PREC_F32) & 1u;
   const bool want16 = ((g->prec_mask >> LYM_PREC_F16) & 1u) || ((g->prec_mask >> LYM_PREC_BF16) & 1u);
-  if (want32 && !g->u32) {
-    if (cudaMalloc(&g->u32, sizeof(float4) * n32 * 2 * g->nd * g->Vh) != cudaSuccess) {
+  const int nxc = (nc - 1) * nc, nxf = nc * nc;
+  auto ensure = [&](void** p, size_t bytes, bool want) -> int {
+    if (!want) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+      return LYM_OK;
+    }
+    if (*p) return LYM_OK;  // sizes depend only on the lattice and N, fixed for this object
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
       cudaGetLastError();
-      set_error("FP32 links do not fit");
+      set_error("sloppy links do not fit");
       return LYM_ERR_OOM;
     }
-  }
-  if (want16 && !g->u16) {
-    if (cudaMalloc(&g->u16, sizeof(uint2) * n16 * 2 * g->nd * g->Vh) != cudaSuccess) {
+    return LYM_OK;
+  };
+  g->n32 = units_for(nxc, 2);
+  g->n16 = units_for(nxc, 2);
+  g->n32f = units_for(nxf, 2);
+  g->n16f = units_for(nxf, 2);
+  const size_t per = (size_t)2 * g->nd * g->Vh;
+  if ((rc = ensure((void**)&g->u32, sizeof(float4) * g->n32 * per, want32 && g->comp)) ||
+      (rc = ensure((void**)&g->u16, sizeof(uint2) * g->n16 * per, want16 && g->comp)) ||
+      (rc = ensure((void**)&g->u32f, sizeof(float4) * g->n32f * per, want32)) ||
+      (rc = ensure((void**)&g->u16f, sizeof(uint2) * g->n16f * per, want16)))
+    return rc;
+  if (!g->nbr) {
+    if (cudaMalloc(&g->nbr, sizeof(int) * 2 * g->nd * 2 * g->Vh) != cudaSuccess) {
       cudaGetLastError();
-      set_error("FP16 links do not fit");
+      set_error("neighbour table does not fit");
       return LYM_ERR_OOM;
     }
+    g->geom.nbr = g->nbr;
+    dim3 tg(grid_for(g->Vh, 128), 2);
+    if (g->nd == 2) build_nbr_kernel<2><<<tg, 128, 0, st>>>(g->geom, g->nbr);
+    else build_nbr_kernel<4><<<tg, 128, 0, st>>>(g->geom, g->nbr);
+    LYM_CHECK_LAUNCH();
   }
-  g->n32 = n32;
-  g->n16 = n16;
   dim3 grid(grid_for(V, 128), g->nd);
-  const int c = g->comp ? 1 : 0;
 #define LYM_PACK(ND_, NC_)                                                                                        \
   pack_gauge_kernel<ND_, NC_><<<grid, 128, 0, st>>>(g->geom, V, (const double2*)gauge, g->bcr, g->bci, g->u64, \
-                                                    g->u32, n32, c, g->u16, n16, c)
+                                                    g->u32, g->n32, 1, g->u16, g->n16, 1, g->u32f, g->n32f,     \
+                                                    g->u16f, g->n16f)
   if (g->nd == 2 && nc == 2) LYM_PACK(2, 2);
   else if (g->nd == 2 && nc == 3) LYM_PACK(2, 3);
   else if (g->nd == 4 && nc == 2) LYM_PACK(4, 2);
@@ -1306,6 +1384,9 @@ int lym_gauge_destroy(lym_gauge* g) {
   if (g->u64) cudaFree(g->u64);
   if (g->u32) cudaFree(g->u32);
   if (g->u16) cudaFree(g->u16);
+  if (g->u32f) cudaFree(g->u32f);
+  if (g->u16f) cudaFree(g->u16f);
+  if (g->nbr) cudaFree(g->nbr);
   delete g;
   return LYM_OK;
 }

@@ -128,7 +128,8 @@ class _Gauge:
 
 
 class SolveServer:
-    def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8):
+    def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None):
+        self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch)
         self.device = device  # CUDA device index; None: the caller's current device
@@ -281,7 +282,7 @@ class SolveServer:
             # host sources (the reference-facing path) cross here, on this worker's stream
             b = torch.cat([(r.b if r.b.dim() == 4 else r.b[None]).to(dev, non_blocking=True) for r in batch])
             solver = dirac_solver.conjugate_gradient(max_steps=max(r.max_iter for r in batch), tol=first.tol,
-                                                     precision=first.precision)
+                                                     precision=first.precision, **self.solver_options)
             op = g.op_for(widx, first.kappa, first.hermitian)
             x = solver.solve(op, b)
             k = 0
