@@ -50,10 +50,12 @@ def parse_args():
     ap.add_argument("--precision", default="f16", choices=["f64", "f32", "f16", "bf16"])
     ap.add_argument("--plain-solves", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--delta", type=float, default=0.1, help="reliable-update trigger of the mixed solver")
+    ap.add_argument("--delta", type=float, default=0.01, help="reliable-update trigger of the mixed solver")
     ap.add_argument("--chunk", type=int, default=8, help="CG iterations per captured graph launch")
     ap.add_argument("--workers", type=int, default=2, help="solve-server worker streams")
     ap.add_argument("--rhs-per-thread", type=int, default=0, help="hop-kernel tile (0: autotune)")
+    ap.add_argument("--dslash-sweep", action="store_true",
+                    help="dslash throughput sweep at 16^4 and 32^4 (one JSON line per case), no solve timing")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: one short solve, then 3 solver dslash launches inside the NVTX "
                          "range 'dslash' (select them with ncu --nvtx --nvtx-include dslash/), no timing")
@@ -341,8 +343,12 @@ def run_lym(args, rank, world, local_rank):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_wall = time.perf_counter()
     ev0.record(stream)
+    # process-wide NVTX start/end range (covers the server's worker threads):
+    # ncu --nvtx --nvtx-include timed selects the timed region's launches
+    nvtx_timed = torch.cuda.nvtx.range_start("timed")
     res = served(args.steps * B, b_dev)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_end(nvtx_timed)
     ev1.record(stream)
     ev1.synchronize()
     barrier()
@@ -493,11 +499,114 @@ def run_lym(args, rank, world, local_rank):
     return 0
 
 
+def run_dslash_sweep(args, local_rank):
+    """Dslash throughput against the HBM roofline at 16^4 and 32^4.
+
+    Cases: the reference-layout FP64 Wilson operator (lym_wilson_apply_batch) and
+    the solver's even-odd hop (lym_dslash_eo) in FP64 / FP32 / FP16 at 1 and 16
+    right-hand sides.  Each is timed with CUDA events over 20 launches, once with
+    a 256 MB write between launches (L2 flushed: DRAM-bound) and once back to back
+    (L2-warm).  Achieved = algorithmic bytes per launch / mean duration (bytes as
+    in the kernel table of the design notes: every field touched once per launch).
+    """
+    import torch
+
+    from tfleonardym_b200 import _dev, _lib, boundary_conditions, dirac, dirac_solver, hmc
+    from tfleonardym_b200 import lattice as lt
+    dirac_solver.VERBOSE = False
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def timed(fn, cold):
+        durs = []
+        for i in range(23):
+            if cold:
+                flush.add_(1.0)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            torch.cuda.synchronize()
+            if i >= 3:
+                durs.append(s.elapsed_time(e) / 1e3)
+        return statistics.mean(durs)
+
+    flops_site = 1320
+    for geom in ((16, 16, 16, 16), (32, 32, 32, 32)):
+        nd, vol = len(geom), int(np.prod(geom))
+        rng = np.random.default_rng(7)
+        a = rng.normal(size=(nd, vol, NC, NC)) + 1j * rng.normal(size=(nd, vol, NC, NC))
+        h = (a + np.conj(np.swapaxes(a, -1, -2))) / 2
+        h = h - (np.trace(h, axis1=-2, axis2=-1) / NC)[..., None, None] * np.eye(NC)
+        p = torch.from_numpy(np.ascontiguousarray(np.transpose(1j * h, (0, 2, 3, 1)))).to(dev)
+        del a, h
+        ident = torch.zeros((nd, NC, NC, vol), dtype=torch.complex128, device=dev)
+        for i in range(NC):
+            ident[:, i, i] = 1
+        links = hmc.update_link_field(ident, p, EPS, reunitarize=True)
+        del p, ident
+        op = dirac.DiracWilsonOperator(lt.Configuration(links, geom, NC, nd), KAPPA, False,
+                                       representation="fundamental",
+                                       boundary_condition_provider=boundary_conditions.time_antiperiodic_provider(-1))
+        ns = 4
+        spin = ns * NC * 16
+        # full-lattice FP64 operator: in + out spinors, every link once, the int32 sup/sdn tables
+        for nvec in (1, 4):
+            x = torch.randn((nvec, ns, NC, vol), dtype=torch.complex128, device=dev)
+            y = torch.empty_like(x)
+            algo = nvec * vol * 2 * spin + vol * nd * NC * NC * 16 + vol * 2 * nd * 4
+            for cold in (True, False):
+                t = timed(lambda: _lib.check(_lib.lib().lym_wilson_apply_batch(
+                    op.lattice.handle, NC, KAPPA, 0, -1.0, 0.0, _dev.ptr(op.fermion_gauge_field), nvec, _dev.ptr(x),
+                    _dev.ptr(y), _dev.stream()), "apply"), cold)
+                print(json.dumps({"dslash_sweep": "wilson_full_kernel f64 reference layout", "geometry": list(geom),
+                                  "nrhs": nvec, "l2": "flushed" if cold else "warm", "us": t * 1e6,
+                                  "algorithmic_bytes": algo, "gbs": algo / t / 1e9, "frac_hbm": algo / t / 1e9 / peak,
+                                  "gflops": nvec * vol * (flops_site + 4 * ns * NC) / t / 1e9}), flush=True)
+            del x, y
+        for prec, nrhs in (("f64", 1), ("f32", 1), ("f16", 1), ("f32", 16), ("f16", 16)):
+            b = torch.randn((nrhs, ns, NC, vol), dtype=torch.complex128, device=dev)
+            short = dirac_solver.conjugate_gradient(max_steps=4, tol=TOL, precision=prec)
+            short.solve(op, b)
+            rep = short.reports[0]
+            gauge = op.solver_gauge((prec,) if prec != "f64" else ())
+            bs = {"f64": 8, "f32": 4, "f16": 2}[prec]
+            sbytes = 2 * ns * NC * bs + (4 if prec == "f16" else 0)
+            if prec == "f64":
+                lbytes = 18 * 8
+            else:
+                lbytes = (12 if rep["compressed_links"] else 18) * bs
+            algo = nrhs * (vol // 2) * 2 * sbytes + nd * vol * lbytes
+            for cold in (True, False):
+                t = timed(lambda: _lib.check(_lib.lib().lym_dslash_eo(gauge, _lib.PREC[prec], nrhs, 1, _dev.stream()),
+                                             "dslash"), cold)
+                print(json.dumps({"dslash_sweep": f"cg_hop_kernel even-odd {prec}", "geometry": list(geom),
+                                  "nrhs": nrhs, "rhs_per_thread": rep["rhs_per_thread"],
+                                  "compressed_links": rep["compressed_links"], "l2": "flushed" if cold else "warm",
+                                  "us": t * 1e6, "algorithmic_bytes": algo, "gbs": algo / t / 1e9,
+                                  "frac_hbm": algo / t / 1e9 / peak,
+                                  "gflops": nrhs * (vol // 2) * flops_site / t / 1e9}), flush=True)
+            del b
+        del op, links
+        torch.cuda.empty_cache()
+    return 0
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.dslash_sweep:
+        return run_dslash_sweep(args, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if world > 1:

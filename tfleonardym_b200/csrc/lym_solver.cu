@@ -674,10 +674,10 @@ template <int ND, int NC, int SP, bool COMP, int R>
 struct Impl {
   static constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   static constexpr int GP = SP == SP64 ? SP64 : (SP == SP32 ? SP32 : SP16);
-  // the sloppy solution accumulates in the sloppy precision: its rounding
-  // (relative to the residual drop since the last reliable update) stays far
-  // below the reliable-update factor delta
-  static constexpr int XP = SP;
+  // the sloppy solution accumulates in FP32 for the half-precision modes (a
+  // norm-scaled half accumulator loses the small late corrections and forces
+  // frequent reliable updates) and in the sloppy precision otherwise
+  static constexpr int XP = (SP == SP16 || SP == SPB16) ? SP32 : SP;
 
   static void iterate(Work& w, cudaStream_t st) {
     const double k2 = w.kappa * w.kappa;
@@ -861,7 +861,7 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   nrhs = (sp == SP64 || nrhs <= 2) ? nrhs : (nrhs + 3) / 4 * 4;
   w->nrhs = nrhs;
   w->sp = sp;
-  w->xp = sp;
+  w->xp = (sp == SP16 || sp == SPB16) ? SP32 : sp;
   w->Vh = g->Vh;
   w->nblk = (int)grid_for(g->Vh, 128);
   int nc_ = 0;
@@ -1031,22 +1031,25 @@ static int autotune(Work& w, cudaStream_t st, int forced) {
   cudaEvent_t e0, e1;
   LYM_CUDA(cudaEventCreate(&e0));
   LYM_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int bi = 0;
-  for (int i = 0; i < w.ncand; ++i) {
-    select_cand(w, i);
-    for (int k = 0; k < 2; ++k) w.ops.dslash(w, st);
-    cudaEventRecord(e0, st);
-    for (int k = 0; k < 5; ++k) w.ops.dslash(w, st);
-    cudaEventRecord(e1, st);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best) {
-      best = ms;
-      bi = i;
+  // three interleaved rounds, best time per candidate: robust against a
+  // concurrent solve on another stream slowing one measurement down
+  float tbest[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+  for (int round = 0; round < 3; ++round) {
+    for (int i = 0; i < w.ncand; ++i) {
+      select_cand(w, i);
+      w.ops.dslash(w, st);
+      cudaEventRecord(e0, st);
+      for (int k = 0; k < 4; ++k) w.ops.dslash(w, st);
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      tbest[i] = std::min(tbest[i], ms);
     }
   }
+  int bi = 0;
+  for (int i = 1; i < w.ncand; ++i)
+    if (tbest[i] < tbest[bi]) bi = i;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   LYM_CHECK_LAUNCH();
