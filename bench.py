@@ -54,8 +54,13 @@ def parse_args():
     ap.add_argument("--chunk", type=int, default=8, help="CG iterations per captured graph launch")
     ap.add_argument("--workers", type=int, default=2, help="solve-server worker streams")
     ap.add_argument("--rhs-per-thread", type=int, default=0, help="hop-kernel tile (0: autotune)")
+    ap.add_argument("--compressed-links", type=int, default=0, help="with a forced tile: 1 = N-1-row links")
+    ap.add_argument("--mixed-fma", type=int, default=0,
+                    help="with a forced tile and f16: 1 = the mixed-precision hop (f16 x f16 + f32 FMAs)")
     ap.add_argument("--dslash-sweep", action="store_true",
                     help="dslash throughput sweep at 16^4 and 32^4 (one JSON line per case), no solve timing")
+    ap.add_argument("--sweep-tiles", action="store_true",
+                    help="with --dslash-sweep: also every forced hop tile at 16 right-hand sides")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: one short solve, then 3 solver dslash launches inside the NVTX "
                          "range 'dslash' (select them with ncu --nvtx --nvtx-include dslash/), no timing")
@@ -272,7 +277,9 @@ def run_lym(args, rank, world, local_rank):
     b_host = torch.from_numpy(host_sources(99 + rank, B)).pin_memory()
     b_dev = b_host.to(dev)
     mixed = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision=args.precision, chunk=args.chunk,
-                                            delta=args.delta, rhs_per_thread=args.rhs_per_thread)
+                                            delta=args.delta, rhs_per_thread=args.rhs_per_thread,
+                                            mixed_fma=args.mixed_fma,
+                                            compressed_links=args.compressed_links)
     plain = dirac_solver.conjugate_gradient(max_steps=2000, tol=TOL, precision="f64", chunk=8)
     stream = torch.cuda.current_stream()
 
@@ -282,7 +289,9 @@ def run_lym(args, rank, world, local_rank):
 
     if args.profile:
         short = dirac_solver.conjugate_gradient(max_steps=16, tol=TOL, precision=args.precision, chunk=8,
-                                                delta=args.delta, rhs_per_thread=max(1, args.rhs_per_thread))
+                                                delta=args.delta, rhs_per_thread=max(1, args.rhs_per_thread),
+                                                mixed_fma=args.mixed_fma,
+                                                compressed_links=args.compressed_links)
         short.solve(op, b_dev)  # builds the workspace; stops early on purpose
         gauge = op.solver_gauge((args.precision,))
         torch.cuda.synchronize()
@@ -292,7 +301,9 @@ def run_lym(args, rank, world, local_rank):
         torch.cuda.nvtx.range_pop()
         if rank == 0:
             print(json.dumps({"profile": "dslash", "precision": args.precision, "nrhs": B,
-                              "rhs_per_thread": short.reports[0]["rhs_per_thread"]}), flush=True)
+                              "rhs_per_thread": short.reports[0]["rhs_per_thread"],
+                              "mixed_fma": short.reports[0]["mixed_fma"],
+                              "compressed_links": short.reports[0]["compressed_links"]}), flush=True)
         return 0
 
     def check(reports):
@@ -315,7 +326,9 @@ def run_lym(args, rank, world, local_rank):
     budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
     srv = serving.SolveServer(budget, max_batch=B, workers=args.workers, device=local_rank,
                               solver_options=dict(delta=args.delta, chunk=args.chunk,
-                                                  rhs_per_thread=args.rhs_per_thread))
+                                                  rhs_per_thread=args.rhs_per_thread,
+                                                  mixed_fma=args.mixed_fma,
+                                                  compressed_links=args.compressed_links))
 
     x_host = torch.empty_like(b_host).pin_memory()
 
@@ -324,7 +337,9 @@ def run_lym(args, rank, world, local_rank):
         host = not src.is_cuda
         for i in range(nreq):
             if rate:
-                time.sleep(float(np.random.default_rng(i).exponential(1.0 / rate)))
+                # inter-arrival gaps capped at 50 ms: never binding at the measured
+                # rates (hundreds per second), it bounds the phase under a profiler
+                time.sleep(min(0.05, float(np.random.default_rng(i).exponential(1.0 / rate))))
             futs.append(srv.submit(serving.SolveRequest("bench", GEOMETRY, NC, KAPPA, src[i % B], gauge=links,
                                                         tol=TOL, precision=args.precision, bc=-1.0,
                                                         max_iter=2000, out=x_host[i % B] if host else None)))
@@ -364,7 +379,7 @@ def run_lym(args, rank, world, local_rank):
     iters = [m["iterations"] for r in res for m in r.reports]
     rupd = [m["reliable_updates"] for r in res for m in r.reports]
     batch_sizes = sorted({r.batch_rhs for r in res})
-    tuned = res[-1].reports[0].get("rhs_per_thread")
+    tuned = {k: res[-1].reports[0].get(k) for k in ("rhs_per_thread", "compressed_links", "mixed_fma")}
 
     # ---- latency: Poisson arrivals at half the saturated rate ----
     rate = 0.5 * value / world
@@ -479,7 +494,7 @@ def run_lym(args, rank, world, local_rank):
         "speedup_vs_plain_fp64": value / (world * plain_value),
         "iterations_per_solve": {"mean": statistics.mean(iters), "max": max(iters),
                                  "reliable_updates_mean": statistics.mean(rupd)},
-        "autotuned": {"rhs_per_thread": tuned},
+        "autotuned": tuned,
         "gpu_launches": int(launches),
         "e2e": {"value": e2e_value, "unit": "solves/s",
                 "h2d_bytes_per_step": int(b_host.numel() * 16), "d2h_bytes_per_step": int(b_host.numel() * 16),
@@ -572,28 +587,39 @@ def run_dslash_sweep(args, local_rank):
                                   "algorithmic_bytes": algo, "gbs": algo / t / 1e9, "frac_hbm": algo / t / 1e9 / peak,
                                   "gflops": nvec * vol * (flops_site + 4 * ns * NC) / t / 1e9}), flush=True)
             del x, y
+        # (rhs per thread, compressed links, mixed-precision FP16 hop); None: the autotuner's pick
+        forced = [None, (1, 0, 0), (1, 1, 0), (2, 0, 0), (4, 0, 0), (1, 0, 1), (2, 0, 1), (4, 0, 1)]
         for prec, nrhs in (("f64", 1), ("f32", 1), ("f16", 1), ("f32", 16), ("f16", 16)):
             b = torch.randn((nrhs, ns, NC, vol), dtype=torch.complex128, device=dev)
-            short = dirac_solver.conjugate_gradient(max_steps=4, tol=TOL, precision=prec)
-            short.solve(op, b)
-            rep = short.reports[0]
-            gauge = op.solver_gauge((prec,) if prec != "f64" else ())
-            bs = {"f64": 8, "f32": 4, "f16": 2}[prec]
-            sbytes = 2 * ns * NC * bs + (4 if prec == "f16" else 0)
-            if prec == "f64":
-                lbytes = 18 * 8
-            else:
-                lbytes = (12 if rep["compressed_links"] else 18) * bs
-            algo = nrhs * (vol // 2) * 2 * sbytes + nd * vol * lbytes
-            for cold in (True, False):
-                t = timed(lambda: _lib.check(_lib.lib().lym_dslash_eo(gauge, _lib.PREC[prec], nrhs, 1, _dev.stream()),
-                                             "dslash"), cold)
-                print(json.dumps({"dslash_sweep": f"cg_hop_kernel even-odd {prec}", "geometry": list(geom),
-                                  "nrhs": nrhs, "rhs_per_thread": rep["rhs_per_thread"],
-                                  "compressed_links": rep["compressed_links"], "l2": "flushed" if cold else "warm",
-                                  "us": t * 1e6, "algorithmic_bytes": algo, "gbs": algo / t / 1e9,
-                                  "frac_hbm": algo / t / 1e9 / peak,
-                                  "gflops": nrhs * (vol // 2) * flops_site / t / 1e9}), flush=True)
+            tiles = [None]
+            if nrhs == 16 and args.sweep_tiles:
+                tiles = [t for t in forced if t is None or prec == "f16" or not t[2]]
+            for tile in tiles:
+                kw = {} if tile is None else dict(rhs_per_thread=tile[0], compressed_links=tile[1],
+                                                  mixed_fma=tile[2])
+                short = dirac_solver.conjugate_gradient(max_steps=4, tol=TOL, precision=prec, **kw)
+                short.solve(op, b)
+                rep = short.reports[0]
+                gauge = op.solver_gauge((prec,) if prec != "f64" else ())
+                bs = {"f64": 8, "f32": 4, "f16": 2}[prec]
+                sbytes = 2 * ns * NC * bs + (4 if prec == "f16" else 0)
+                if prec == "f64":
+                    lbytes = 18 * 8
+                else:
+                    lbytes = (12 if rep["compressed_links"] else 18) * bs
+                algo = nrhs * (vol // 2) * 2 * sbytes + nd * vol * lbytes
+                for cold in (True, False):
+                    t = timed(lambda: _lib.check(_lib.lib().lym_dslash_eo(gauge, _lib.PREC[prec], nrhs, 1,
+                                                                          _dev.stream()), "dslash"), cold)
+                    print(json.dumps({"dslash_sweep": f"cg_hop_kernel even-odd {prec}", "geometry": list(geom),
+                                      "nrhs": nrhs, "tile": "autotuned" if tile is None else "forced",
+                                      "rhs_per_thread": rep["rhs_per_thread"],
+                                      "mixed_fma": rep["mixed_fma"],
+                                      "compressed_links": rep["compressed_links"],
+                                      "l2": "flushed" if cold else "warm",
+                                      "us": t * 1e6, "algorithmic_bytes": algo, "gbs": algo / t / 1e9,
+                                      "frac_hbm": algo / t / 1e9 / peak,
+                                      "gflops": nrhs * (vol // 2) * flops_site / t / 1e9}), flush=True)
             del b
         del op, links
         torch.cuda.empty_cache()

@@ -152,6 +152,10 @@ typedef struct lym_solver_params {
   int chunk;         /* iterations per captured CUDA graph launch (0 = default)  */
   int rhs_per_thread;/* at most this many right-hand sides per hop-kernel thread
                         (1, 2 or 4; the largest available one is used); 0 = autotune */
+  int compressed_links; /* with a forced tile (rhs_per_thread > 0): 1 = the N-1-row
+                        links (when the links are SU(N)), 0 = full links */
+  int mixed_fma;     /* with a forced tile and FP16: 1 = the mixed-precision hop (half
+                        spinor in FP16, U h through f16 x f16 + f32 FMAs), 0 = FP32 arithmetic */
 } lym_solver_params;
 
 typedef struct lym_solver_report {
@@ -162,6 +166,7 @@ typedef struct lym_solver_report {
   int64_t kernel_launches; /* lym kernels the whole call launched (graph nodes included) */
   int rhs_per_thread;    /* right-hand sides per thread the autotuner picked for the hop kernels */
   int compressed_links;  /* 1: the hop kernels read the N-1-row sloppy links, 0: full links */
+  int mixed_fma;         /* 1: the hop kernels ran the mixed-precision FP16 form */
 } lym_solver_report;
 
 /* Solve D x_i = b_i (or Q x_i = b_i) for nrhs right-hand sides stored back to

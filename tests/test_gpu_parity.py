@@ -234,6 +234,51 @@ def test_eo_cg_every_hop_tile(cuda_device, precision):
             assert res < 1e-10, (tile, i, res)
 
 
+def _smooth_links(geometry, nc, seed, spread=0.3):
+    """SU(N) links near unity: the polar projection of 1 + spread * Gaussian."""
+    rng = np.random.default_rng(seed)
+    nd, vol = len(geometry), int(np.prod(geometry))
+    a = rng.normal(size=(nd, vol, nc, nc)) + 1j * rng.normal(size=(nd, vol, nc, nc))
+    x = np.eye(nc) + spread * a
+    u = O.unitary_sqrt_projection(np.ascontiguousarray(np.transpose(x, (0, 2, 3, 1))))
+    return u
+
+
+@pytest.mark.parametrize("geometry,nc", [((4, 4, 4, 8), 3), ((2, 4, 4, 6), 3), ((4, 4, 4, 4), 2),
+                                         ((8, 6), 2), ((12, 4), 3)])
+def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
+    """The mixed-precision FP16 hop (half spinor in FP16, U h through
+    f16 x f16 + f32 FMAs) at 1, 2 and 4 rhs per thread meets the true residual
+    in about the iterations of the FP32-arithmetic FP16 hop."""
+    from tfleonardym_b200 import boundary_conditions as bcs
+    from tfleonardym_b200 import dirac, dirac_solver
+    from tfleonardym_b200 import lattice as lt
+    u = _smooth_links(geometry, nc, seed=sum(geometry) + nc)
+    kappa = 0.12
+    tables = O.lookup_tables(geometry)
+    ub = O.apply_time_bc(u, O.antiperiodic_field(geometry))
+    cfg = lt.Configuration(cu(u), tuple(geometry), nc, len(geometry))
+    op = dirac.DiracWilsonOperator(cfg, kappa, False, representation="fundamental",
+                                   boundary_condition_provider=bcs.time_antiperiodic_provider(-1))
+    rng = np.random.default_rng(5)
+    ns = 4 if len(geometry) == 4 else 2
+    b = rng.normal(size=(4, ns, nc, u.shape[-1])) + 1j * rng.normal(size=(4, ns, nc, u.shape[-1]))
+    ref = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=1)
+    ref.solve(op, cu(b))
+    assert ref.reports[0]["mixed_fma"] == 0
+    base = max(r["iterations"] for r in ref.reports)
+    for tile in (1, 2, 4):
+        mx = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=tile, mixed_fma=1)
+        x = np_(mx.solve(op, cu(b)))
+        rep = mx.reports[0]
+        assert rep["mixed_fma"] == 1 and rep["rhs_per_thread"] == tile and rep["compressed_links"] == 0, rep
+        for i in range(4):
+            res = np.linalg.norm(b[i] - O.wilson_apply(ub, x[i], kappa, False, tables)) / np.linalg.norm(b[i])
+            assert res < 1e-10, (tile, i, res)
+        its = max(r["iterations"] for r in mx.reports)
+        assert abs(its - base) <= max(3, base // 10), (tile, its, base)
+
+
 def test_eo_cg_batch_equals_single(cuda_device):
     """A right-hand side gives the same answer alone and inside a batch."""
     from tfleonardym_b200 import dirac_solver

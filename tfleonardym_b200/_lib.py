@@ -33,13 +33,14 @@ P = ctypes.POINTER
 
 class SolverParams(ctypes.Structure):
     _fields_ = [("tol", c_double), ("max_iter", c_int), ("precision", c_int),
-                ("delta", c_double), ("hermitian", c_int), ("chunk", c_int), ("rhs_per_thread", c_int)]
+                ("delta", c_double), ("hermitian", c_int), ("chunk", c_int), ("rhs_per_thread", c_int),
+                ("compressed_links", c_int), ("mixed_fma", c_int)]
 
 
 class SolverReport(ctypes.Structure):
     _fields_ = [("status", c_int), ("iterations", c_int), ("reliable_updates", c_int),
                 ("true_residual", c_double), ("kernel_launches", c_int64), ("rhs_per_thread", c_int),
-                ("compressed_links", c_int)]
+                ("compressed_links", c_int), ("mixed_fma", c_int)]
 
 
 # name -> (restype, argtypes); every symbol include/lym.h declares

@@ -426,4 +426,144 @@ LYM_D void hop_tile(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
   }
 }
 
+// raw spinor units of one site (values as stored) and its norm (1 for FP32)
+template <int SP, int NCOMP>
+LYM_D float load_sp_units(const EoField& f, int rhs, int cb,
+                          typename Prec<SP>::unit (&u)[units_for(NCOMP, Prec<SP>::CPU)]) {
+  using U = typename Prec<SP>::unit;
+  const int vh = (int)f.Vh;
+  const U* base = reinterpret_cast<const U*>(f.data) + (size_t)rhs * f.nunits * f.Vh;
+#pragma unroll
+  for (int k = 0; k < units_for(NCOMP, Prec<SP>::CPU); ++k) u[k] = __ldg(base + k * vh + cb);
+  if constexpr (SP == SP16 || SP == SPB16) return __ldg(f.norm + (size_t)rhs * f.Vh + cb);
+  return 1.0f;
+}
+
+// --- FP16 hop in mixed precision --------------------------------------------
+// For FP16 spinors and FP16 full links.  The half spinor h = psi_a + k psi_jb
+// (k = +-1, +-i) is formed in packed FP16 (one HADD2 / HFMA2 per complex, the
+// factors +-1 exact), and U h accumulates in FP32 through the sm_100 mixed-
+// precision FMA fma.rn.f32.f16 (f16 x f16 + f32; the product of two halves is
+// exact in FP32).  No value is converted to FP32 on its own, which takes the
+// conversions off the FMA-heavy pipe that bounds the FP32-arithmetic hop.  The
+// only extra rounding against hop_tile is h's to FP16 (2^-11 relative, the
+// storage precision).  The neighbour's norm scales the FP32 result.
+LYM_D float fma_hh(__half a, __half b, float c) {
+  float d;
+  asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(__half_as_ushort(a)), "h"(__half_as_ushort(b)), "f"(c));
+  return d;
+}
+LYM_D __half2 as_h2(unsigned w) { return *reinterpret_cast<__half2*>(&w); }
+
+// a + k b for the unit phase k (0:+1, 1:+i, 2:-1, 3:-i), (re, im) half2 pairs
+LYM_D __half2 proj_h2(__half2 a, __half2 b, int k) {
+  switch (k & 3) {
+    case 0: return __hadd2(a, b);
+    case 2: return __hsub2(a, b);
+    case 1: return __hfma2(__lowhigh2highlow(b), __halves2half2(__float2half_rn(-1.f), __float2half_rn(1.f)), a);
+    default: return __hfma2(__lowhigh2highlow(b), __halves2half2(__float2half_rn(1.f), __float2half_rn(-1.f)), a);
+  }
+}
+
+// acc += s k t for the unit phase k and the real scale s (ns = -s)
+LYM_D void acc_phase(cx<float>& acc, int k, float s, float ns, float tr, float ti) {
+  switch (k & 3) {
+    case 0: acc.re = fmaf(s, tr, acc.re); acc.im = fmaf(s, ti, acc.im); break;
+    case 1: acc.re = fmaf(ns, ti, acc.re); acc.im = fmaf(s, tr, acc.im); break;
+    case 2: acc.re = fmaf(ns, tr, acc.re); acc.im = fmaf(ns, ti, acc.im); break;
+    default: acc.re = fmaf(s, ti, acc.re); acc.im = fmaf(ns, tr, acc.im); break;
+  }
+}
+
+// Same result per site as hop_tile<ND, NC, SP16, SP16, false, G5IN, R> up to
+// the rounding of h; R right-hand sides share each link.
+template <int ND, int NC, bool G5IN, int R>
+LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
+                       const int (&act)[R], cx<float> (&acc)[R][Gamma<ND>::NS][NC]) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC, NU = units_for(NCOMP, 4);
+  constexpr int NCX = NC * NC, NLU = units_for(NCX, 2);
+  const int vh = (int)g.Vh;
+  const int* nb = g.nbr + par * 2 * ND * vh + cb;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int a = 0; a < NS; ++a)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[r][a][c] = czero<float>();
+  const __half2 conj_f = __halves2half2(__float2half_rn(1.f), __float2half_rn(-1.f));
+  const __half2 negre_f = __halves2half2(__float2half_rn(-1.f), __float2half_rn(1.f));
+#pragma unroll
+  for (int mu = 0; mu < ND; ++mu) {
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      const bool fwd = dir == 0;
+      const int code = __ldg(nb + (2 * mu + dir) * vh);
+      const int ncb = code & 0x7fffffff;
+      // full N x N link, boundary factor folded in; forward link on x (parity
+      // par), backward link on x - mu (parity 1-par)
+      const uint2* lp = reinterpret_cast<const uint2*>(hg.data) +
+                        (size_t)((mu * 2 + (fwd ? par : 1 - par)) * hg.nunits) * vh + (fwd ? cb : ncb);
+      __half2 u[NCX];
+#pragma unroll
+      for (int k = 0; k < NLU; ++k) {
+        const uint2 t = __ldg(lp + k * vh);
+        u[2 * k] = as_h2(t.x);
+        if (2 * k + 1 < NCX) u[2 * k + 1] = as_h2(t.y);
+      }
+      const bool s2pos = fwd != G5IN;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!act[r]) continue;
+        uint4 raw[NU];
+        const float nrm = load_sp_units<SP16, NCOMP>(in, rhs0 + r, ncb, raw);
+        const float nnrm = -nrm;
+        __half2 psi[NCOMP];
+#pragma unroll
+        for (int k = 0; k < NU; ++k) {
+          const unsigned w[4] = {raw[k].x, raw[k].y, raw[k].z, raw[k].w};
+#pragma unroll
+          for (int m = 0; m < 4; ++m)
+            if (4 * k + m < NCOMP) psi[4 * k + m] = as_h2(w[m]);
+        }
+#pragma unroll
+        for (int a = 0; a < NS / 2; ++a) {
+          const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+          // h = psi_a - s2 g_a psi_jb
+          const int kph = s2pos ? phase_neg(ph) : ph;
+          __half2 h[NC], hx[NC];  // hx: forward (re, -im), backward (-re, im)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            h[c] = proj_h2(psi[a * NC + c], psi[jb * NC + c], kph);
+            hx[c] = __hmul2(h[c], fwd ? conj_f : negre_f);
+          }
+          // lower row factor: -s conj(g_a)
+          const int lph = fwd ? phase_neg(phase_conj(ph)) : phase_conj(ph);
+#pragma unroll
+          for (int i = 0; i < NC; ++i) {
+            float tr = 0.f, ti = 0.f;
+#pragma unroll
+            for (int j = 0; j < NC; ++j) {
+              const __half2 uu = fwd ? u[i * NC + j] : u[j * NC + i];
+              const __half ure = __low2half(uu), uim = __high2half(uu);
+              if (fwd) {  // U h: (u.re h.re - u.im h.im, u.re h.im + u.im h.re)
+                tr = fma_hh(ure, __low2half(h[j]), tr);
+                tr = fma_hh(uim, __high2half(hx[j]), tr);
+                ti = fma_hh(ure, __high2half(h[j]), ti);
+                ti = fma_hh(uim, __low2half(h[j]), ti);
+              } else {  // U^dag h: (u.re h.re + u.im h.im, u.re h.im - u.im h.re)
+                tr = fma_hh(ure, __low2half(h[j]), tr);
+                tr = fma_hh(uim, __high2half(h[j]), tr);
+                ti = fma_hh(ure, __high2half(h[j]), ti);
+                ti = fma_hh(uim, __low2half(hx[j]), ti);
+              }
+            }
+            acc_phase(acc[r][a][i], 0, nrm, nnrm, tr, ti);
+            acc_phase(acc[r][jb][i], lph, nrm, nnrm, tr, ti);
+          }
+        }
+      }
+    }
+  }
+}
+
 }  // namespace lym

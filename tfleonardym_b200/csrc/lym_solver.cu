@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "lym_eo.cuh"
@@ -341,13 +343,27 @@ __global__ void __launch_bounds__(128) norm64_kernel(int64_t Vh, EoField f, doub
 // sloppy CG iteration kernels (precision SP, links GP/COMP)
 // ---------------------------------------------------------------------------
 
+// The hop of the CG kernels for R right-hand sides at one site: FP32
+// arithmetic (hop_tile), or for FP16 spinors with full links the mixed-
+// precision form (MX = 1, hop_tile_mx).
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
+LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
+                   const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
+  if constexpr (MX != 0) {
+    static_assert(SP == SP16 && GP == SP16 && !COMP, "the mixed-precision hop takes FP16 spinors and full links");
+    hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+  } else {
+    hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+  }
+}
+
 // s = H_oe G5IN(p) for the rhs tile blockIdx.y*R .. +R-1 (odd output);
 // st == nullptr: every rhs (profiling hook)
-template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R>
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
 __global__ void __launch_bounds__(128) cg_hop_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
                                                      const CGState* st) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
-  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int rhs0 = blockIdx.y * R;
   int act[R];
   int any = 0;
@@ -356,10 +372,10 @@ __global__ void __launch_bounds__(128) cg_hop_kernel(EoGeom g, HopGauge hg, EoFi
     act[r] = st ? st[rhs0 + r].active : 1;
     any |= act[r];
   }
-  if (!any || cb >= g.Vh) return;
+  if (!any || i >= g.Vh) return;
   using RT = typename Prec<SP>::real;
   cx<RT> acc[R][NS][NC];
-  hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+  hop_any<ND, NC, SP, GP, COMP, G5IN, R, MX>(g, hg, in, rhs0, i, par, act, acc);
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     if (!act[r]) continue;
@@ -368,17 +384,17 @@ __global__ void __launch_bounds__(128) cg_hop_kernel(EoGeom g, HopGauge hg, EoFi
     for (int s = 0; s < NS; ++s)
 #pragma unroll
       for (int c = 0; c < NC; ++c) v[s * NC + c] = acc[r][s][c];
-    store_sp<SP, NCOMP>(out, rhs0 + r, cb, v);
+    store_sp<SP, NCOMP>(out, rhs0 + r, i, v);
   }
 }
 
 // t = p - kappa^2 H_eo s ; alpha = rr / |t|^2   (rhs tile of R)
-template <int ND, int NC, int SP, int GP, bool COMP, int R>
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
 __global__ void __launch_bounds__(128) cg_t_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t, double k2,
                                                    CGState* st, double* partials, unsigned* counters, int nblk) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[R * 32];
-  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int rhs0 = blockIdx.y * R;
   int act[R];
   int any = 0;
@@ -392,11 +408,12 @@ __global__ void __launch_bounds__(128) cg_t_kernel(EoGeom g, HopGauge hg, EoFiel
   double n[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) n[r] = 0.0;
-  if (cb < g.Vh) {
+  if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    hop_tile<ND, NC, SP, GP, COMP, false, R>(g, hg, s, rhs0, cb, 0, act, acc);
+    hop_any<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, s, rhs0, i, 0, act, acc);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
+      const int q = r, cb = i;
       if (!act[r]) continue;
       cx<RT> v[NCOMP];
       load_sp<SP, NCOMP>(p, rhs0 + r, cb, v);
@@ -405,7 +422,7 @@ __global__ void __launch_bounds__(128) cg_t_kernel(EoGeom g, HopGauge hg, EoFiel
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           cx<RT>& w = v[a * NC + c];
-          w -= (RT)k2 * acc[r][a][c];
+          w -= (RT)k2 * acc[q][a][c];
           n[r] += (double)w.re * w.re + (double)w.im * w.im;
         }
       store_sp<SP, NCOMP>(t, rhs0 + r, cb, v);
@@ -427,13 +444,13 @@ __global__ void __launch_bounds__(128) cg_t_kernel(EoGeom g, HopGauge hg, EoFiel
 }
 
 // Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr   (rhs tile of R)
-template <int ND, int NC, int SP, int GP, bool COMP, int XP, int R>
+template <int ND, int NC, int SP, int GP, bool COMP, int XP, int R, int MX>
 __global__ void __launch_bounds__(128) cg_update_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
                                                         EoField x, EoField r, double k2, CGState* st,
                                                         double* partials, unsigned* counters, int nblk) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[R * 32];
-  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int rhs0 = blockIdx.y * R;
   int act[R];
   int any = 0;
@@ -448,11 +465,12 @@ __global__ void __launch_bounds__(128) cg_update_kernel(EoGeom g, HopGauge hg, E
   double n[R];
 #pragma unroll
   for (int q = 0; q < R; ++q) n[q] = 0.0;
-  if (cb < g.Vh) {
+  if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    hop_tile<ND, NC, SP, GP, COMP, false, R>(g, hg, s, rhs0, cb, 0, act, acc);
+    hop_any<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, s, rhs0, i, 0, act, acc);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
+      const int m = q, cb = i;
       if (!act[q]) continue;
       const double alpha = st[rhs0 + q].alpha;
       cx<RT> tv[NCOMP], pv[NCOMP], rv[NCOMP];
@@ -467,7 +485,7 @@ __global__ void __launch_bounds__(128) cg_update_kernel(EoGeom g, HopGauge hg, E
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           const int k = sp * NC + c;
-          cx<RT> h = acc[q][sp][c];
+          cx<RT> h = acc[m][sp][c];
           if (sp >= NS / 2) h = -h;
           cx<RT> ap = tv[k] - (RT)k2 * h;
           rv[k] -= a * ap;
@@ -495,13 +513,13 @@ __global__ void __launch_bounds__(128) cg_update_kernel(EoGeom g, HopGauge hg, E
 // Reliable-update residual in the sloppy precision: r = t - kappa^2 gamma_d H_eo s
 // (t = q converted, s = H_oe gamma_d t), i.e. r = M^dag q, for rhs with upd[rhs];
 // res[rhs] = |r|^2.
-template <int ND, int NC, int SP, int GP, bool COMP, int R>
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
 __global__ void __launch_bounds__(128) cg_rnew_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField r,
                                                       double k2, const int* upd, double* partials,
                                                       unsigned* counters, double* res, int nblk) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[R * 32];
-  const int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int rhs0 = blockIdx.y * R;
   int act[R];
   int any = 0;
@@ -515,11 +533,12 @@ __global__ void __launch_bounds__(128) cg_rnew_kernel(EoGeom g, HopGauge hg, EoF
   double n[R];
 #pragma unroll
   for (int q = 0; q < R; ++q) n[q] = 0.0;
-  if (cb < g.Vh) {
+  if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    hop_tile<ND, NC, SP, GP, COMP, false, R>(g, hg, s, rhs0, cb, 0, act, acc);
+    hop_any<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, s, rhs0, i, 0, act, acc);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
+      const int m = q, cb = i;
       if (!act[q]) continue;
       cx<RT> v[NCOMP];
       load_sp<SP, NCOMP>(t, rhs0 + q, cb, v);
@@ -527,7 +546,7 @@ __global__ void __launch_bounds__(128) cg_rnew_kernel(EoGeom g, HopGauge hg, EoF
       for (int sp = 0; sp < NS; ++sp)
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          cx<RT> h = acc[q][sp][c];
+          cx<RT> h = acc[m][sp][c];
           if (sp >= NS / 2) h = -h;
           cx<RT>& w = v[sp * NC + c];
           w -= (RT)k2 * h;
@@ -634,13 +653,17 @@ struct Work {
   int nrhs = 0, sp = 0, xp = 0;  // nrhs: padded count every field holds
   int nreal = 0;                 // right-hand sides the caller passes
   int R = 1;                     // right-hand sides per thread in the hop kernels (autotuned)
+  bool mx = false;               // the mixed-precision FP16 hop (hop_tile_mx)
   bool tuned = false;
   int tuned_i = 0;
   // hop-kernel candidates: right-hand sides per thread x compressed / full links
+  // (x FP32 / mixed-precision arithmetic for FP16)
+  static constexpr int kMaxCand = 10;
   int ncand = 0, cur = 0;
-  int rcand[6] = {1, 0, 0, 0, 0, 0};
-  bool ccand[6] = {false, false, false, false, false, false};
-  CgOps ops_r[6]{};
+  int rcand[kMaxCand] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  bool ccand[kMaxCand] = {};
+  bool mcand[kMaxCand] = {};
+  CgOps ops_r[kMaxCand]{};
   int64_t Vh = 0;
   int nblk = 0;
   double kappa = 0;
@@ -670,7 +693,7 @@ struct Work {
   int64_t launches = 0;           // kernels launched by the current call (graph nodes included)
 };
 
-template <int ND, int NC, int SP, bool COMP, int R>
+template <int ND, int NC, int SP, bool COMP, int R, int MX>
 struct Impl {
   static constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   static constexpr int GP = SP == SP64 ? SP64 : (SP == SP32 ? SP32 : SP16);
@@ -682,12 +705,12 @@ struct Impl {
   static void iterate(Work& w, cudaStream_t st) {
     const double k2 = w.kappa * w.kappa;
     dim3 grid(w.nblk, w.nrhs), tile(w.nblk, w.nrhs / R);
-    cg_hop_kernel<ND, NC, SP, GP, COMP, false, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, w.st);
-    cg_t_kernel<ND, NC, SP, GP, COMP, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st, w.partials,
-                                                               w.counters, w.nblk);
-    cg_hop_kernel<ND, NC, SP, GP, COMP, true, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, w.st);
-    cg_update_kernel<ND, NC, SP, GP, COMP, XP, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.t, w.p, w.xs, w.r,
-                                                                        k2, w.st, w.partials, w.counters, w.nblk);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, false, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, w.st);
+    cg_t_kernel<ND, NC, SP, GP, COMP, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st,
+                                                                   w.partials, w.counters, w.nblk);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, true, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, w.st);
+    cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX><<<tile, 128, 0, st>>>(
+        w.g->geom, w.hgs, w.s, w.t, w.p, w.xs, w.r, k2, w.st, w.partials, w.counters, w.nblk);
     cg_p_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.r, w.p, w.st);
     cg_settle_kernel<<<(w.nrhs + 63) / 64, 64, 0, st>>>(w.nrhs, w.st);
   }
@@ -743,15 +766,15 @@ struct Impl {
   static void dslash(Work& w, cudaStream_t st) {
     dim3 tile(w.nblk, w.nrhs / R);
     w.launches += 1;
-    cg_hop_kernel<ND, NC, SP, GP, COMP, false, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, nullptr);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, false, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, nullptr);
   }
   static void rnew(Work& w, cudaStream_t st) {
     const double k2 = w.kappa * w.kappa;
     dim3 tile(w.nblk, w.nrhs / R);
     w.launches += 2;
-    cg_hop_kernel<ND, NC, SP, GP, COMP, true, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, nullptr);
-    cg_rnew_kernel<ND, NC, SP, GP, COMP, R><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.t, w.r, k2, w.upd,
-                                                                  w.partials, w.counters, w.res, w.nblk);
+    cg_hop_kernel<ND, NC, SP, GP, COMP, true, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, nullptr);
+    cg_rnew_kernel<ND, NC, SP, GP, COMP, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.t, w.r, k2, w.upd,
+                                                                      w.partials, w.counters, w.res, w.nblk);
   }
   static void copy_rp(Work& w, cudaStream_t st) {
     dim3 grid(w.nblk, w.nrhs);
@@ -765,29 +788,32 @@ struct Impl {
 };
 
 template <int ND, int NC, int R>
-static CgOps pick_sp(int sp, bool comp) {
+static CgOps pick_sp(int sp, bool comp, bool mx) {
   switch (sp) {
-    case SP64: return Impl<ND, NC, SP64, false, 1>::table();  // FP64 keeps one rhs per thread (registers)
-    case SP32: return comp ? Impl<ND, NC, SP32, true, R>::table() : Impl<ND, NC, SP32, false, R>::table();
-    case SP16: return comp ? Impl<ND, NC, SP16, true, R>::table() : Impl<ND, NC, SP16, false, R>::table();
-    default: return comp ? Impl<ND, NC, SPB16, true, R>::table() : Impl<ND, NC, SPB16, false, R>::table();
+    case SP64: return Impl<ND, NC, SP64, false, 1, 0>::table();  // FP64 keeps one rhs per thread (registers)
+    case SP32: return comp ? Impl<ND, NC, SP32, true, R, 0>::table() : Impl<ND, NC, SP32, false, R, 0>::table();
+    case SP16:
+      if (mx) return Impl<ND, NC, SP16, false, R, 1>::table();
+      return comp ? Impl<ND, NC, SP16, true, R, 0>::table() : Impl<ND, NC, SP16, false, R, 0>::table();
+    default: return comp ? Impl<ND, NC, SPB16, true, R, 0>::table() : Impl<ND, NC, SPB16, false, R, 0>::table();
   }
 }
 
 template <int R>
-static bool pick_ops_r(int nd, int nc, int sp, bool comp, CgOps* out) {
-  if (nd == 2 && nc == 2) *out = pick_sp<2, 2, R>(sp, comp);
-  else if (nd == 2 && nc == 3) *out = pick_sp<2, 3, R>(sp, comp);
-  else if (nd == 4 && nc == 2) *out = pick_sp<4, 2, R>(sp, comp);
-  else if (nd == 4 && nc == 3) *out = pick_sp<4, 3, R>(sp, comp);
+static bool pick_ops_r(int nd, int nc, int sp, bool comp, bool mx, CgOps* out) {
+  if (nd == 2 && nc == 2) *out = pick_sp<2, 2, R>(sp, comp, mx);
+  else if (nd == 2 && nc == 3) *out = pick_sp<2, 3, R>(sp, comp, mx);
+  else if (nd == 4 && nc == 2) *out = pick_sp<4, 2, R>(sp, comp, mx);
+  else if (nd == 4 && nc == 3) *out = pick_sp<4, 3, R>(sp, comp, mx);
   else return false;
   return true;
 }
 
-static bool pick_ops(int nd, int nc, int sp, bool comp, int R, CgOps* out) {
-  if (R == 4) return pick_ops_r<4>(nd, nc, sp, comp, out);
-  if (R == 2) return pick_ops_r<2>(nd, nc, sp, comp, out);
-  return pick_ops_r<1>(nd, nc, sp, comp, out);
+// mx: the mixed-precision hop (FP16 spinors, full links)
+static bool pick_ops(int nd, int nc, int sp, bool comp, int R, bool mx, CgOps* out) {
+  if (R == 4) return pick_ops_r<4>(nd, nc, sp, comp, mx, out);
+  if (R == 2) return pick_ops_r<2>(nd, nc, sp, comp, mx, out);
+  return pick_ops_r<1>(nd, nc, sp, comp, mx, out);
 }
 
 static size_t field_bytes(int sp, int ncomp, int64_t Vh, int nrhs) {
@@ -867,21 +893,26 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   int nc_ = 0;
   for (int comp = 0; comp < 2; ++comp) {
     if (comp && !(g->comp && sp != SP64)) continue;  // compressed links need SU(N) links and a sloppy precision
-    for (int R : {1, 2, 4}) {
-      if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
-      if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, &w->ops_r[nc_])) {
-        delete w;
-        set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
-        return LYM_ERR_UNSUPPORTED;
+    for (int mx = 0; mx < 2; ++mx) {
+      if (mx && (sp != SP16 || comp)) continue;  // the mixed-precision hop: FP16 spinors, full links
+      for (int R : {1, 2, 4}) {
+        if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
+        if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, mx != 0, &w->ops_r[nc_])) {
+          delete w;
+          set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
+          return LYM_ERR_UNSUPPORTED;
+        }
+        w->rcand[nc_] = R;
+        w->ccand[nc_] = comp != 0;
+        w->mcand[nc_] = mx != 0;
+        ++nc_;
       }
-      w->rcand[nc_] = R;
-      w->ccand[nc_] = comp != 0;
-      ++nc_;
     }
   }
   w->ncand = nc_;
   w->ops = w->ops_r[0];
   w->R = w->rcand[0];
+  w->mx = w->mcand[0];
   const int nc = g->ncomp;
   size_t bytes = 7 * field_bytes(SP64, nc, g->Vh, nrhs);
   bytes += 4 * field_bytes(sp, nc, g->Vh, nrhs);
@@ -1006,21 +1037,50 @@ static int build_graph(Work& w, int chunk, cudaStream_t st) {
 }
 
 // Autotuner: time the hop kernel for every (right-hand sides per thread,
-// compressed or full links) candidate the workspace supports and keep the
-// fastest (once per workspace).  forced > 0: the caller fixed the tile; the
-// largest available one not above it is used, with full links.
+// compressed or full links, FP32 or mixed-precision FP16 arithmetic)
+// candidate the workspace supports and keep the fastest (once per workspace).
+// forced_rhs > 0: the largest rhs tile not above it, with compressed links
+// when forced_comp and the links allow it (else full links), and the mixed-
+// precision hop when forced_mx and the precision is FP16.
 static void select_cand(Work& w, int i) {
   w.cur = i;
   w.ops = w.ops_r[i];
   w.R = w.rcand[i];
+  w.mx = w.mcand[i];
   w.hgs = w.ccand[i] ? w.hgs_c : w.hgs_f;
 }
 
-static int autotune(Work& w, cudaStream_t st, int forced) {
-  if (forced > 0) {
+// Process-wide tuning results keyed by lattice shape, colours, sloppy
+// precision, right-hand sides and link compressibility: a workspace created
+// later for the same key (another gauge object of the same shape, such as a
+// solve-server worker's copy) takes the pick without timing again, and the
+// mutex keeps two tuning runs from timing each other's launches.
+struct TuneKey {
+  int v[9];
+  bool operator<(const TuneKey& o) const { return std::lexicographical_compare(v, v + 9, o.v, o.v + 9); }
+};
+struct TunePick {
+  int R;
+  bool comp, mx;
+};
+static std::mutex g_tune_mutex;
+static std::map<TuneKey, TunePick> g_tune_cache;
+
+static TuneKey tune_key(const Work& w) {
+  const EoGeom& g = w.g->geom;
+  return TuneKey{{g.nd, w.g->nc, g.dims[0], g.dims[1], g.dims[2], g.dims[3], w.sp, w.nrhs, w.g->comp ? 1 : 0}};
+}
+
+static int autotune(Work& w, cudaStream_t st, int forced_rhs, int forced_comp, int forced_mx) {
+  if (forced_rhs > 0) {
+    bool comp = false, mx = false;
+    for (int i = 0; i < w.ncand; ++i) {
+      comp = comp || (forced_comp && w.ccand[i]);
+      mx = mx || (forced_mx && w.mcand[i]);
+    }
     int pick = 0;
     for (int i = 0; i < w.ncand; ++i)
-      if (w.rcand[i] <= forced && !w.ccand[i]) pick = i;
+      if (w.ccand[i] == comp && w.mcand[i] == mx && w.rcand[i] <= forced_rhs) pick = i;
     select_cand(w, pick);
     return LYM_OK;
   }
@@ -1028,12 +1088,26 @@ static int autotune(Work& w, cudaStream_t st, int forced) {
     select_cand(w, w.tuned_i);
     return LYM_OK;
   }
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  const TuneKey key = tune_key(w);
+  auto hit = g_tune_cache.find(key);
+  if (hit != g_tune_cache.end()) {
+    for (int i = 0; i < w.ncand; ++i) {
+      if (w.rcand[i] == hit->second.R && w.ccand[i] == hit->second.comp && w.mcand[i] == hit->second.mx) {
+        select_cand(w, i);
+        w.tuned = true;
+        w.tuned_i = i;
+        return LYM_OK;
+      }
+    }
+  }
   cudaEvent_t e0, e1;
   LYM_CUDA(cudaEventCreate(&e0));
   LYM_CUDA(cudaEventCreate(&e1));
   // three interleaved rounds, best time per candidate: robust against a
   // concurrent solve on another stream slowing one measurement down
-  float tbest[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+  float tbest[Work::kMaxCand];
+  for (float& t : tbest) t = 1e30f;
   for (int round = 0; round < 3; ++round) {
     for (int i = 0; i < w.ncand; ++i) {
       select_cand(w, i);
@@ -1056,6 +1130,7 @@ static int autotune(Work& w, cudaStream_t st, int forced) {
   select_cand(w, bi);
   w.tuned = true;
   w.tuned_i = bi;
+  g_tune_cache[key] = TunePick{w.rcand[bi], w.ccand[bi], w.mcand[bi]};
   return LYM_OK;
 }
 
@@ -1150,7 +1225,7 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
   LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * nrhs, cudaMemcpyHostToDevice, st));
   w.ops.copy_rp(w, st);  // p = r (upd is all ones here)
   LYM_CHECK_LAUNCH();
-  rc = autotune(w, st, prm->rhs_per_thread);
+  rc = autotune(w, st, prm->rhs_per_thread, prm->compressed_links, prm->mixed_fma);
   if (rc) return rc;
   rc = build_graph(w, chunk, st);
   if (rc) return rc;
@@ -1217,6 +1292,7 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     rep[i].kernel_launches = w.launches;
     rep[i].rhs_per_thread = w.R;
     rep[i].compressed_links = w.ccand[w.cur] ? 1 : 0;
+    rep[i].mixed_fma = w.mx ? 1 : 0;
     if (!done[i]) status = LYM_ERR_NOT_CONVERGED;
   }
   return status;

@@ -175,13 +175,16 @@ class conjugate_gradient:  # noqa: N801 - named like the reference solvers
     reliable updates.  ``precision`` in {"f64", "f32", "f16", "bf16"} is the inner
     precision; ``tol`` the target true relative residual |b - D x| / |b|."""
 
-    def __init__(self, max_steps=20000, tol=1e-10, precision="f64", delta=0.1, chunk=8, rhs_per_thread=0):
+    def __init__(self, max_steps=20000, tol=1e-10, precision="f64", delta=0.1, chunk=8, rhs_per_thread=0,
+                 compressed_links=0, mixed_fma=0):
         self.max_steps = max_steps
         self.tol = tol
         self.precision = precision
         self.delta = delta
         self.chunk = chunk
         self.rhs_per_thread = rhs_per_thread  # 0: the library's autotuner picks the hop tile
+        self.compressed_links = compressed_links  # with a forced tile: 1 = N-1-row links
+        self.mixed_fma = mixed_fma  # with a forced tile and FP16: 1 = the mixed-precision hop
         self.reports = None
 
     def solve(self, operator, source):
@@ -193,14 +196,16 @@ class conjugate_gradient:  # noqa: N801 - named like the reference solvers
         x = torch.empty_like(bb)
         n = bb.shape[0]
         prm = _lib.SolverParams(float(self.tol), int(self.max_steps), _lib.PREC[self.precision], float(self.delta),
-                                int(bool(operator.hermitian)), int(self.chunk), int(self.rhs_per_thread))
+                                int(bool(operator.hermitian)), int(self.chunk), int(self.rhs_per_thread),
+                                int(self.compressed_links), int(self.mixed_fma))
         reps = (_lib.SolverReport * n)()
         precs = () if self.precision == "f64" else (self.precision,)
         rc = _lib.lib().lym_wilson_solve(operator.solver_gauge(precs), float(operator.kappa), n, _dev.ptr(bb),
                                          _dev.ptr(x), ctypes.byref(prm), reps, _dev.stream())
         self.reports = [dict(status=r.status, iterations=r.iterations, reliable_updates=r.reliable_updates,
                              true_residual=r.true_residual, kernel_launches=r.kernel_launches,
-                             rhs_per_thread=r.rhs_per_thread, compressed_links=r.compressed_links) for r in reps]
+                             rhs_per_thread=r.rhs_per_thread, compressed_links=r.compressed_links,
+                             mixed_fma=r.mixed_fma) for r in reps]
         if rc == _lib.LYM_ERR_NOT_CONVERGED:
             _print(f"conjugate_gradient: failed to find convergence ({self.reports})")
         else:
