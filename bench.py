@@ -33,6 +33,7 @@ sys.path.insert(0, ROOT)
 GEOMETRY = (16, 16, 16, 16)
 NC = 3
 KAPPA = 0.13
+BETA = 5.6
 EPS = 0.25
 TOL = 1e-10
 METRIC = "Wilson-CG solves/s at 1e-10 true relative residual"
@@ -59,6 +60,13 @@ def parse_args():
                     help="with a forced tile and f16: 1 = the mixed-precision hop (f16 x f16 + f32 FMAs)")
     ap.add_argument("--dslash-sweep", action="store_true",
                     help="dslash throughput sweep at 16^4 and 32^4 (one JSON line per case), no solve timing")
+    ap.add_argument("--hmc", action="store_true",
+                    help="HMC trajectories/hour on 16^4 SU(3) (beta 5.6, kappa 0.13, Nf=2 Wilson, Omelyan "
+                         "[10, 2], t = 1, even-odd CG at 1e-10): one JSON line, no solve timing")
+    ap.add_argument("--trajectories", type=int, default=5)
+    ap.add_argument("--hmc-inner", type=int, default=2, help="gauge steps per fermion step of the integrator")
+    ap.add_argument("--hmc-precision", default="f64", choices=["f64", "f32", "f16", "bf16"],
+                    help="inner precision of the HMC's CG solves (f64: the plain FP64 method)")
     ap.add_argument("--sweep-tiles", action="store_true",
                     help="with --dslash-sweep: also every forced hop tile at 16 right-hand sides")
     ap.add_argument("--profile", action="store_true",
@@ -449,9 +457,9 @@ def run_lym(args, rank, world, local_rank):
     ns_, spin_reals = 4, 2 * 4 * NC
     bs = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}[args.precision]
     spinor_bytes = spin_reals * bs + (4 if args.precision in ("f16", "bf16") else 0)
-    link_bytes = (12 if NC == 3 else 4) * (8 if args.precision == "f64" else (4 if args.precision == "f32" else 2))
-    if args.precision == "f64":
-        link_bytes = 18 * 8
+    # links as the tuned kernel reads them: N-1 rows (12 reals for SU(3)) or the full 18
+    comp = bool(mixed.reports[0]["compressed_links"])
+    link_bytes = ((12 if NC == 3 else 4) if comp else 2 * NC * NC) * bs
     algo_bytes = B * (vol // 2) * 2 * spinor_bytes + nd * vol * link_bytes
     peaks = {}
     try:
@@ -460,7 +468,8 @@ def run_lym(args, rank, world, local_rank):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = algo_bytes / hop_s / 1e9
-    traffic = read_traffic()
+    # ncu DRAM bytes of one launch of this kernel (FP16, 16 rhs, the tuned tile), captured once
+    traffic = read_traffic() if (args.precision == "f16" and B == 16 and mixed.reports[0]["mixed_fma"]) else None
 
     # ---- CPU baseline (rank 0, N = 1 only) ----
     cpu = None
@@ -500,8 +509,12 @@ def run_lym(args, rank, world, local_rank):
                 "h2d_bytes_per_step": int(b_host.numel() * 16), "d2h_bytes_per_step": int(b_host.numel() * 16),
                 "what": "the served path with pinned host sources; solutions come back to host memory"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": f"cg_hop_kernel<4,3,{args.precision}> s_o = H_oe p_e, "
-                                                   f"{B} rhs, L2 flushed before each launch",
+                     "traffic": traffic,
+                     "kernel": f"cg_hop_kernel 4D SU(3) {args.precision} s_o = H_oe p_e, {B} rhs, "
+                               f"{mixed.reports[0]['rhs_per_thread']} rhs per thread, "
+                               f"{'compressed' if comp else 'full'} links"
+                               f"{', mixed-precision FP16 hop' if mixed.reports[0]['mixed_fma'] else ''}, "
+                               f"L2 flushed before each launch",
                      "algorithmic_bytes_per_launch": algo_bytes, "launch_us": hop_s * 1e6,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback"},
         "clocks": clk,
@@ -626,6 +639,84 @@ def run_dslash_sweep(args, local_rank):
     return 0
 
 
+def run_hmc(args, rank, world, local_rank):
+    """HMC on 4D SU(3) 16^4: beta = 5.6, Nf = 2 Wilson fermions at kappa = 0.13
+    (pseudofermion phi = Q eta, Q = gamma_d D, antiperiodic time), links
+    reunit(exp(i 0.25 H)) to start, Gaussian su(3) momenta, Omelyan nested
+    integrator with 10 outer (fermion) steps and ``--hmc-inner`` (default 2)
+    inner (gauge) steps per outer step, trajectory length 1, force and energy solves (Q^2)^-1 phi by two
+    even-odd CG solves of Q at 1e-10 true relative residual.  One warm-up
+    trajectory, then ``--trajectories`` timed with CUDA events; the value is
+    trajectories per hour.  A reversibility check (forward then backward
+    trajectory) follows the timed ones."""
+    import torch
+
+    from tfleonardym_b200 import (boundary_conditions, dirac, dirac_solver, fermion_action, gauge_action, hmc,
+                                  measurements)
+    from tfleonardym_b200 import lattice as lt
+    dirac_solver.VERBOSE = False
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nd, vol = len(GEOMETRY), int(np.prod(GEOMETRY))
+    h = host_links(1234 + rank)
+    p = torch.from_numpy(np.ascontiguousarray(np.transpose(1j * h, (0, 2, 3, 1)))).to(dev)
+    ident = torch.zeros((nd, NC, NC, vol), dtype=torch.complex128, device=dev)
+    for i in range(NC):
+        ident[:, i, i] = 1
+    cfg = lt.Configuration(hmc.update_link_field(ident, p, EPS, reunitarize=True), GEOMETRY, NC, nd)
+    del p, ident
+    q = dirac.DiracWilsonOperator(cfg, KAPPA, True, representation="fundamental",
+                                  boundary_condition_provider=boundary_conditions.time_antiperiodic_provider(-1))
+    solver = dirac_solver.eo_square_solver(tol=TOL, precision=args.hmc_precision, delta=args.delta, chunk=args.chunk)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    ym = gauge_action.yang_mills(cfg, BETA)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(2026 + rank)
+    rng = np.random.default_rng(2026 + rank)
+    steps = [10, args.hmc_inner]
+    stream = torch.cuda.current_stream()
+    records = []
+    clocks = None
+    for k in range(1 + args.trajectories):
+        if k == 1:
+            clocks = ClockSampler(local_rank)
+            clocks.start()
+        eta = hmc.generate_random_vector(NC, 4, stddev=1 / np.sqrt(2), volume=vol, generator=gen)
+        momenta = hmc.random_momenta(NC, nd, vol, generator=gen)
+        it0 = solver.total_iterations
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        nf.set_gauge_configuration(cfg)
+        nf.initialize_pseudofermions([eta])
+        cfg, minus_dh, acc = hmc.hybrid_mc(cfg, [nf, ym], steps, 1.0, momenta=momenta, uniform=float(rng.uniform()))
+        e.record(stream)
+        torch.cuda.synchronize()
+        plaq = measurements.plaquette(cfg).value
+        records.append({"seconds": s.elapsed_time(e) / 1e3, "dH": -minus_dh, "accepted": bool(acc),
+                        "plaquette": plaq, "cg_iterations": solver.total_iterations - it0})
+    clk = clocks.stop()
+    timed = records[1:]
+    sec = statistics.mean(r["seconds"] for r in timed)
+    eta = hmc.generate_random_vector(NC, 4, stddev=1 / np.sqrt(2), volume=vol, generator=gen)
+    nf.set_gauge_configuration(cfg)
+    nf.initialize_pseudofermions([eta])
+    rev = hmc.reversibility_check(cfg, [nf, ym], steps, 1.0, momenta=hmc.random_momenta(NC, nd, vol, generator=gen))
+    line = {"metric": "HMC trajectories/hour", "value": world * 3600.0 / sec, "unit": "trajectories/hour",
+            "n_gpus": world, "trajectories": args.trajectories, "warmup": 1, "higher_is_better": True,
+            "seconds_per_trajectory": sec, "dtype": f"{args.hmc_precision}+f64" if args.hmc_precision != "f64"
+            else "f64", "data": "synthetic",
+            "config": {"workload": "hmc nf2 wilson 16^4 SU(3) beta=5.6 kappa=0.13", "geometry": list(GEOMETRY),
+                       "integrator": f"omelyan nested {steps}, t = 1", "solver": "even-odd CG on Q twice, tol 1e-10",
+                       "inner_precision": args.hmc_precision, "start": "reunit(exp(i 0.25 H))"},
+            "acceptance": statistics.mean(1.0 if r["accepted"] else 0.0 for r in timed),
+            "reversibility_dH": rev, "per_trajectory": records, "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -633,6 +724,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.dslash_sweep:
         return run_dslash_sweep(args, local_rank)
+    if args.hmc:
+        return run_hmc(args, rank, world, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if world > 1:

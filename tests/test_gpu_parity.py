@@ -309,6 +309,25 @@ def test_nf2_force_and_energy_vs_reference(cuda_device, case):
     assert relerr(np_(nf.force()), g["nf2/force"]) < 1e-9
 
 
+@pytest.mark.parametrize("case,precision", [("d2", "f64"), ("d4", "f64"), ("d4", "f16")])
+def test_nf2_force_with_eo_square_solver(cuda_device, case, precision):
+    """The even-odd square solver (two CG solves of Q for the zero shift) in
+    place of the reference's MMMR gives the reference's Nf=2 energy and force to
+    the accuracy of the solves."""
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_action
+    dirac_solver.VERBOSE = False
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    q = make_op(g, spec)
+    solver = dirac_solver.eo_square_solver(tol=1e-12, precision=precision)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    nf.initialize_pseudofermions([cu(g["eta"])])
+    assert abs(nf.energy() - g["nf2/energy"]) < 1e-9 * abs(g["nf2/energy"])
+    assert relerr(np_(nf.force()), g["nf2/force"]) < 1e-8
+    assert solver.total_iterations > 0
+
+
 @pytest.mark.parametrize("case", ["d2", "d4"])
 def test_md_trajectory_vs_reference(cuda_device, case):
     """integrate_om (hmc.py:133-162) with the Nf=2 and gauge actions from the golden inputs."""

@@ -441,7 +441,7 @@ LYM_D float load_sp_units(const EoField& f, int rhs, int cb,
 
 // --- FP16 hop in mixed precision --------------------------------------------
 // For FP16 spinors and FP16 full links.  The half spinor h = psi_a + k psi_jb
-// (k = +-1, +-i) is formed in packed FP16 (one HADD2 / HFMA2 per complex, the
+// (k = +-1, +-i) is formed in packed FP16 (one __hadd2 / __hfma2 per complex, the
 // factors +-1 exact), and U h accumulates in FP32 through the sm_100 mixed-
 // precision FMA fma.rn.f32.f16 (f16 x f16 + f32; the product of two halves is
 // exact in FP32).  No value is converted to FP32 on its own, which takes the

@@ -47,8 +47,10 @@ int scratch_get(Scratch** out) {
 // ---------------------------------------------------------------------------
 // full-lattice hop, reference layout
 // ---------------------------------------------------------------------------
+// One resident block per SM is declared enough, so ptxas keeps every
+// neighbour's loads in flight at once (memory-bound FP64 stencil).
 template <int ND, int NC, bool HERM>
-__global__ void __launch_bounds__(128) wilson_full_kernel(
+__global__ void __launch_bounds__(128, 1) wilson_full_kernel(
     const int32_t* __restrict__ tab, int V, int Lt, double kappa, double bcr, double bci,
     const double2* __restrict__ U, const double2* __restrict__ in, double2* __restrict__ out) {
   constexpr int NS = Gamma<ND>::NS;

@@ -12,6 +12,9 @@
 * ``conjugate_gradient`` -- builder-defined even-odd CG for D x = b (or Q x = b)
   with FP64 reliable updates and FP64 / FP32 / FP16 / BF16 inner iterations
   (lym_wilson_solve).
+* ``eo_square_solver`` -- builder-defined drop-in for ``multishift_solver`` on
+  SquareOperator(Q): shift 0 by two even-odd CG solves of Q, positive shifts by
+  ``multishift_cg``.
 """
 import ctypes
 
@@ -211,3 +214,49 @@ class conjugate_gradient:  # noqa: N801 - named like the reference solvers
         else:
             _lib.check(rc, "lym_wilson_solve")
         return x if batched else x[0]
+
+
+class eo_square_solver:  # noqa: N801 - named like the reference solvers
+    """(Q^2 + sigma_k) x_k = b for SquareOperator(DiracWilsonOperator(hermitian=True)),
+    with the interface of multishift_solver (dirac_solver.py:19), so that it plugs
+    into RationalApproximation and fermion_action.n_flavor.  sigma = 0: two
+    even-odd CG solves Q y = b, Q x = y (conjugate_gradient, relative true residual
+    ``tol`` each, inner ``precision``); sigma > 0: multishift_cg (relative
+    tolerance ``tol``).  ``last_iterations`` holds the CG iterations of the last call."""
+
+    def __init__(self, tol=1e-10, precision="f64", max_steps=20000, **cg_options):
+        self.tol = tol
+        self.precision = precision
+        self.max_steps = max_steps
+        self.cg_options = cg_options
+        self.last_iterations = 0
+        self.total_iterations = 0
+
+    def solve(self, operator, source, shifts):
+        q = _wilson_square(operator)
+        if q is None:
+            raise TypeError("eo_square_solver needs SquareOperator(DiracWilsonOperator(hermitian=True))")
+        shifts = [float(s) for s in shifts]
+        out = [None] * len(shifts)
+        self.last_iterations = 0
+        zero = [i for i, s in enumerate(shifts) if s == 0.0]
+        rest = [i for i, s in enumerate(shifts) if s != 0.0]
+        if zero:
+            cg = conjugate_gradient(max_steps=self.max_steps, tol=self.tol, precision=self.precision,
+                                    **self.cg_options)
+            y = cg.solve(q, source)
+            self.last_iterations += max(r["iterations"] for r in cg.reports)
+            x = cg.solve(q, y)
+            self.last_iterations += max(r["iterations"] for r in cg.reports)
+            for i in zero:
+                out[i] = x
+        if rest:
+            if any(shifts[i] < 0 for i in rest):
+                raise ValueError("eo_square_solver takes shifts >= 0")
+            ms = multishift_cg(self.max_steps, self.tol)
+            xs = ms.solve(operator, source, [shifts[i] for i in rest])
+            self.last_iterations += ms.last_steps
+            for k, i in enumerate(rest):
+                out[i] = xs[k]
+        self.total_iterations += self.last_iterations
+        return out
