@@ -154,8 +154,9 @@ typedef struct lym_solver_params {
                         (1, 2 or 4; the largest available one is used); 0 = autotune */
   int compressed_links; /* with a forced tile (rhs_per_thread > 0): 1 = the N-1-row
                         links (when the links are SU(N)), 0 = full links */
-  int mixed_fma;     /* with a forced tile and FP16: 1 = the mixed-precision hop (half
-                        spinor in FP16, U h through f16 x f16 + f32 FMAs), 0 = FP32 arithmetic */
+  int mixed_fma;     /* with a forced tile and FP16 (full links): 0 = FP32 arithmetic on
+                        converted values; 1 = half spinor in FP16, U h through f16 x f16 + f32
+                        FMAs */
 } lym_solver_params;
 
 typedef struct lym_solver_report {

@@ -349,8 +349,8 @@ __global__ void __launch_bounds__(128) norm64_kernel(int64_t Vh, EoField f, doub
 // that way.  Sloppy ones keep ptxas's default register target.
 //
 // The hop of the CG kernels for R right-hand sides at one site: FP32
-// arithmetic (hop_tile), or for FP16 spinors with full links the mixed-
-// precision form (MX = 1, hop_tile_mx).
+// arithmetic (MX = 0, hop_tile), or for FP16 spinors with full links the
+// mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx).
 template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
 LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
                    const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
@@ -658,7 +658,7 @@ struct Work {
   int nrhs = 0, sp = 0, xp = 0;  // nrhs: padded count every field holds
   int nreal = 0;                 // right-hand sides the caller passes
   int R = 1;                     // right-hand sides per thread in the hop kernels (autotuned)
-  bool mx = false;               // the mixed-precision FP16 hop (hop_tile_mx)
+  int mx = 0;                    // FP16 hop arithmetic: 0 FP32 (hop_tile), 1 mixed (hop_tile_mx)
   bool tuned = false;
   int tuned_i = 0;
   // hop-kernel candidates: right-hand sides per thread x compressed / full links
@@ -667,7 +667,7 @@ struct Work {
   int ncand = 0, cur = 0;
   int rcand[kMaxCand] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   bool ccand[kMaxCand] = {};
-  bool mcand[kMaxCand] = {};
+  int mcand[kMaxCand] = {};
   CgOps ops_r[kMaxCand]{};
   int64_t Vh = 0;
   int nblk = 0;
@@ -793,7 +793,7 @@ struct Impl {
 };
 
 template <int ND, int NC, int R>
-static CgOps pick_sp(int sp, bool comp, bool mx) {
+static CgOps pick_sp(int sp, bool comp, int mx) {
   switch (sp) {
     case SP64: return Impl<ND, NC, SP64, false, 1, 0>::table();  // FP64 keeps one rhs per thread (registers)
     case SP32: return comp ? Impl<ND, NC, SP32, true, R, 0>::table() : Impl<ND, NC, SP32, false, R, 0>::table();
@@ -805,7 +805,7 @@ static CgOps pick_sp(int sp, bool comp, bool mx) {
 }
 
 template <int R>
-static bool pick_ops_r(int nd, int nc, int sp, bool comp, bool mx, CgOps* out) {
+static bool pick_ops_r(int nd, int nc, int sp, bool comp, int mx, CgOps* out) {
   if (nd == 2 && nc == 2) *out = pick_sp<2, 2, R>(sp, comp, mx);
   else if (nd == 2 && nc == 3) *out = pick_sp<2, 3, R>(sp, comp, mx);
   else if (nd == 4 && nc == 2) *out = pick_sp<4, 2, R>(sp, comp, mx);
@@ -814,8 +814,8 @@ static bool pick_ops_r(int nd, int nc, int sp, bool comp, bool mx, CgOps* out) {
   return true;
 }
 
-// mx: the mixed-precision hop (FP16 spinors, full links)
-static bool pick_ops(int nd, int nc, int sp, bool comp, int R, bool mx, CgOps* out) {
+// mx: the mixed-precision hop (FP16 spinors, full links; f16 x f16 + f32 FMAs)
+static bool pick_ops(int nd, int nc, int sp, bool comp, int R, int mx, CgOps* out) {
   if (R == 4) return pick_ops_r<4>(nd, nc, sp, comp, mx, out);
   if (R == 2) return pick_ops_r<2>(nd, nc, sp, comp, mx, out);
   return pick_ops_r<1>(nd, nc, sp, comp, mx, out);
@@ -902,14 +902,14 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
       if (mx && (sp != SP16 || comp)) continue;  // the mixed-precision hop: FP16 spinors, full links
       for (int R : {1, 2, 4}) {
         if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
-        if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, mx != 0, &w->ops_r[nc_])) {
+        if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, mx, &w->ops_r[nc_])) {
           delete w;
           set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
           return LYM_ERR_UNSUPPORTED;
         }
         w->rcand[nc_] = R;
         w->ccand[nc_] = comp != 0;
-        w->mcand[nc_] = mx != 0;
+        w->mcand[nc_] = mx;
         ++nc_;
       }
     }
@@ -1066,7 +1066,8 @@ struct TuneKey {
 };
 struct TunePick {
   int R;
-  bool comp, mx;
+  bool comp;
+  int mx;
 };
 static std::mutex g_tune_mutex;
 static std::map<TuneKey, TunePick> g_tune_cache;
@@ -1078,10 +1079,11 @@ static TuneKey tune_key(const Work& w) {
 
 static int autotune(Work& w, cudaStream_t st, int forced_rhs, int forced_comp, int forced_mx) {
   if (forced_rhs > 0) {
-    bool comp = false, mx = false;
+    bool comp = false;
+    int mx = 0;
     for (int i = 0; i < w.ncand; ++i) {
       comp = comp || (forced_comp && w.ccand[i]);
-      mx = mx || (forced_mx && w.mcand[i]);
+      if (forced_mx && w.mcand[i] == forced_mx) mx = forced_mx;
     }
     int pick = 0;
     for (int i = 0; i < w.ncand; ++i)
@@ -1297,7 +1299,7 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     rep[i].kernel_launches = w.launches;
     rep[i].rhs_per_thread = w.R;
     rep[i].compressed_links = w.ccand[w.cur] ? 1 : 0;
-    rep[i].mixed_fma = w.mx ? 1 : 0;
+    rep[i].mixed_fma = w.mx;
     if (!done[i]) status = LYM_ERR_NOT_CONVERGED;
   }
   return status;
