@@ -244,6 +244,35 @@ int lym_fermion_force(const lym_lattice* lat, int nc, double kappa, int hermitia
                       const double* alphas, const void* X, const void* Y, int symmetric,
                       double scale, void* force, void* stream);
 
+/* ------------------------------------------------------------------ */
+/* adjoint representation (dirac.py:358-370, 380-456, 525-565)         */
+/* ------------------------------------------------------------------ */
+
+/* Adjoint Wilson operator on nvec matrix-valued spinors (nvec, ns, N, N, V): out =
+ * psi + kappa sum_mu [L_mu(x)(1-g_mu)psi(x+mu)U_mu(x)^dag + L_mu(x-mu)^dag(1+g_mu)
+ * psi(x-mu)U_mu(x-mu)], gamma_d applied when hermitian.  L = gauge_left with
+ * (bc_re, bc_im) on the last time slice of the last direction (the reference's cfg),
+ * U = gauge (its original_cfg); gauge_left may be gauge.  Replaces
+ * multiply_in_adjoint_representation / simple_multiply_in_adjoint_representation
+ * (same result). */
+int lym_wilson_apply_adjoint(const lym_lattice* lat, int nc, double kappa, int hermitian,
+                             double bc_re, double bc_im, const void* gauge_left, const void* gauge,
+                             int nvec, const void* in, void* out, void* stream);
+
+/* Adjoint links V_mu^{ab} = 2 Tr(T_a U_mu T_b U_mu^dag), (nd, N^2-1, N^2-1, V), times
+ * (bc_re, bc_im) on the last time slice of the last direction: the reference's
+ * fermion_gauge_field for representation "adjoint" (dirac.py:358-370). */
+int lym_adjoint_links(const lym_lattice* lat, int nc, double bc_re, double bc_im,
+                      const void* gauge, void* out, void* stream);
+
+/* force += scale * sum_i alpha_i [L(X_i, Y_i) (+ L(Y_i, X_i) if symmetric)] for matrix-valued
+ * X, Y (nterms, ns, N, N, V), L the adjoint branch of lie_derivative (dirac.py:525-565) with the
+ * adjoint links built in place from gauge and the boundary factor; nterms <= 32. */
+int lym_fermion_force_adjoint(const lym_lattice* lat, int nc, double kappa, int hermitian,
+                              double bc_re, double bc_im, const void* gauge, int nterms,
+                              const double* alphas, const void* X, const void* Y, int symmetric,
+                              double scale, void* force, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

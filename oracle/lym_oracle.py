@@ -293,6 +293,80 @@ def lie_derivative(gauge_bc, X, Y, kappa, hermitian, tables):
     return kappa * np.stack(out)
 
 
+# ---------------------------------------------------------------------------
+# Adjoint representation (dirac.py:358-364, 380-456, 525-565; lie_generators.py)
+# ---------------------------------------------------------------------------
+
+
+def adjoint_generators(nc):
+    """(T_adj^i)_{jk} = -2 Tr([T_i, T_j] T_k) (lie_generators.py:22-36)."""
+    T = generators(nc)
+    comm = np.einsum("iab,jbc->ijac", T, T) - np.einsum("jab,ibc->ijac", T, T)
+    return -2 * np.einsum("ijab,kba->ijk", comm, T)
+
+
+def adjoint_vector(psi):
+    """Matrix-valued adjoint spinor (ns, N, N, V) -> components (ns, N^2-1, V),
+    X_a = 2 Tr(T_a X) (dirac.py:531-532)."""
+    T = generators(psi.shape[1])
+    return 2 * np.einsum("ijk,mkjc->mic", T, psi)
+
+
+def adjoint_links(gauge, bc_field=None):
+    """V_mu^{ab} = 2 Tr(T_a U_mu T_b U_mu^dag) (dirac.py:358-364), then the
+    boundary field on the last direction when given (the provider of dirac.py:368-370)."""
+    T = generators(gauge.shape[1])
+    v = 2.0 * np.einsum("ijk,mklc,nlo,mjoc->minc", T, gauge, T, np.conj(gauge))
+    return apply_time_bc(v, bc_field) if bc_field is not None else v
+
+
+def adjoint_hopping(gauge_bc, gauge, psi, tables):
+    """sum_mu U_mu(x)(1-g_mu)psi(x+mu)U'_mu(x)^dag + U_mu(x-mu)^dag (1+g_mu)psi(x-mu) U'_mu(x-mu)
+    for matrix-valued spinors (ns, N, N, V): the left links carry the boundary
+    condition, the right ones (the original configuration) do not (dirac.py:380-403)."""
+    nd = gauge_bc.shape[0]
+    g, _ = gammas(nd)
+    ident = np.eye(g.shape[1])
+    out = np.zeros_like(psi)
+    for mu in range(nd):
+        fwd = translate(np.einsum("mn,njkc->mjkc", ident - g[mu], psi), tables, mu, +1)
+        out += np.einsum("ijc,mjkc,lkc->milc", gauge_bc[mu], fwd, np.conj(gauge[mu]))
+        bwd = translate(np.einsum("mn,njkc->mjkc", ident + g[mu], psi), tables, mu, -1)
+        ldn = translate(gauge_bc[mu], tables, mu, -1)
+        rdn = translate(gauge[mu], tables, mu, -1)
+        out += np.einsum("jic,mjkc,klc->milc", np.conj(ldn), bwd, rdn)
+    return out
+
+
+def wilson_apply_adjoint(gauge_bc, gauge, psi, kappa, hermitian, tables):
+    """Adjoint Wilson operator D psi = psi + kappa H psi (Q = gamma_d D when hermitian)."""
+    out = psi + kappa * adjoint_hopping(gauge_bc, gauge, psi, tables)
+    return gamma_d(out) if hermitian else out
+
+
+def lie_derivative_adjoint(vlinks, X, Y, kappa, hermitian, tables):
+    """dirac.py:525-565 for matrix-valued X, Y: per mu, kappa * sum_k T^k_{ut} [
+    Xv^dag P+ T_adj^k V_mu Yv(x+mu) - Yv(x+mu)^dag P- V_mu^dag T_adj^k Xv ] with the
+    adjoint components Xv, Yv and the adjoint links V (boundary condition applied)."""
+    nd, nc = vlinks.shape[0], X.shape[1]
+    g, gd = gammas(nd)
+    ident = np.eye(g.shape[1])
+    T = generators(nc)
+    TA = adjoint_generators(nc)
+    xv, yv = adjoint_vector(X), adjoint_vector(Y)
+    out = []
+    for mu in range(nd):
+        pp = ident - g[mu]
+        pm = ident + g[mu]
+        if hermitian:
+            pp, pm = gd @ pp, gd @ pm
+        ysup = translate(yv, tables, mu, +1)
+        d = np.einsum("mis,mn,kij,jls,nls,kut->uts", np.conj(xv), pp, TA, vlinks[mu], ysup, T)
+        d -= np.einsum("mis,mn,jis,kjl,nls,kut->uts", np.conj(ysup), pm, np.conj(vlinks[mu]), TA, xv, T)
+        out.append(d)
+    return kappa * np.stack(out)
+
+
 def update_link_field(links, momenta, eps):
     """U <- expm(eps P) U per link (hmc.py:40-43)."""
     ex = scipy.linalg.expm(np.transpose(eps * momenta, (0, 3, 1, 2)))  # (nd, V, N, N)

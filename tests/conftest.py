@@ -30,6 +30,13 @@ GOLDEN_CASES = {
     "d2su3": dict(geometry=(6, 8), nc=3, kappa=0.11, beta=5.0),
 }
 
+# adjoint-representation cases (tests/golden/make_golden.py ADJOINT_CASES)
+ADJOINT_CASES = {
+    "adj_d2su2": dict(geometry=(8, 6), nc=2, kappa=0.17),
+    "adj_d4su3": dict(geometry=(2, 4, 2, 4), nc=3, kappa=0.12),
+    "adj_d4su2": dict(geometry=(4, 2, 2, 4), nc=2, kappa=0.13),
+}
+
 
 def relerr(a, b):
     a = np.asarray(a)

@@ -48,6 +48,14 @@ CASES = {
                   apply_only=True),
 }
 
+# adjoint representation (dirac.py:380-456, 358-364, 525-565): operator, adjoint
+# links, lie derivative, and the Nf=2 energy/force through the reference's MMMR
+ADJOINT_CASES = {
+    "adj_d2su2": dict(geometry=(8, 6), nc=2, kappa=0.17, seed=21),
+    "adj_d4su3": dict(geometry=(2, 4, 2, 4), nc=3, kappa=0.12, seed=22),
+    "adj_d4su2": dict(geometry=(4, 2, 2, 4), nc=2, kappa=0.13, seed=23),
+}
+
 TABLE_GEOMETRIES = [(2, 4, 6, 8), (3, 5, 2, 4), (4, 6, 8), (5, 7), (8, 8), (1, 4, 2, 2)]
 
 
@@ -272,6 +280,62 @@ def run_case(name):
     print("wrote", name)
 
 
+def run_adjoint_case(name):
+    spec = ADJOINT_CASES[name]
+    geometry = spec["geometry"]
+    nd, nc = len(geometry), spec["nc"]
+    _setup_reference(geometry)
+    import tensorflow as tf
+    tf.set_seed(spec["seed"])
+    np.random.seed(spec["seed"])
+
+    import boundary_conditions
+    import dirac
+    import dirac_solver
+    import fermion_action
+    import hmc
+
+    log = _IterLog()
+    dirac_solver.print = log
+
+    def bc_anti(x):
+        return boundary_conditions.apply_antiboundary_conditions_in_t_direction(x)
+
+    def bc_periodic(x):
+        return x
+
+    out = {}
+    kappa = spec["kappa"]
+    cfg = hmc.hotstart(list(geometry), nc, nd)
+    out["gauge"] = np.asarray(cfg.gauge_field)
+    ns = 2 if nd == 2 else 4
+    eta = hmc.generate_random_vector(nc, ns, "adjoint")
+    eta2 = hmc.generate_random_vector(nc, ns, "adjoint")
+    out["eta"], out["eta2"] = np.asarray(eta), np.asarray(eta2)
+    for herm in (False, True):
+        for bcname, prov in (("periodic", bc_periodic), ("anti", bc_anti)):
+            op = dirac.DiracWilsonOperator(cfg, kappa, herm, representation="adjoint",
+                                           boundary_condition_provider=prov)
+            out[f"apply/h{int(herm)}/{bcname}/projected"] = np.asarray(op.multiply_in_adjoint_representation(eta))
+            out[f"apply/h{int(herm)}/{bcname}/simple"] = np.asarray(op.simple_multiply_in_adjoint_representation(eta))
+            if bcname == "anti":
+                out[f"lie_derivative/h{int(herm)}"] = np.asarray(op.lie_derivative(eta, eta2))
+    Q = dirac.DiracWilsonOperator(cfg, kappa, True, representation="adjoint", boundary_condition_provider=bc_anti)
+    out["fermion_gauge_field"] = np.asarray(Q.fermion_gauge_field)
+    # Nf=2 in the adjoint: phi = Q eta, S = <phi, (Q^2)^-1 phi>, F = the lie derivatives of the solution
+    solver = dirac_solver.multishift_solver(5000, 1e-22)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(Q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [Q], solver, Q)
+    nf.set_gauge_configuration(cfg)
+    nf.initialize_pseudofermions([eta])
+    out["nf2/phi"] = np.asarray(nf.pseudofermions[0])
+    out["nf2/energy"] = np.asarray(nf.energy())
+    out["nf2/force"] = np.asarray(nf.force())
+    log.take()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print("wrote", name)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default=None)
@@ -280,10 +344,12 @@ def main():
     if args.case and args.inproc:
         if args.case == "tables":
             run_tables()
+        elif args.case in ADJOINT_CASES:
+            run_adjoint_case(args.case)
         else:
             run_case(args.case)
         return
-    names = [args.case] if args.case else ["tables"] + list(CASES)
+    names = [args.case] if args.case else ["tables"] + list(CASES) + list(ADJOINT_CASES)
     for n in names:
         subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc"], check=True)
 

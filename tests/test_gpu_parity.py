@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from oracle import lym_oracle as O
-from tests.conftest import GOLDEN_CASES, load_golden, relerr
+from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, load_golden, relerr
 
 pytestmark = pytest.mark.gpu
 
@@ -391,3 +391,73 @@ def test_reversibility(cuda_device):
                                  momenta=cu(g["hmc/reversibility_momenta"]))
     assert abs(dh) < 1e-9
     assert abs(dh - g["hmc/reversibility_dH"]) < 1e-9
+
+
+# ---------------------------------------------------------------------------
+# adjoint representation (dirac.py:358-370, 380-456, 525-565)
+# ---------------------------------------------------------------------------
+def make_adj_op(g, spec, hermitian, anti=True, provider=None):
+    from tfleonardym_b200 import boundary_conditions as bc
+    from tfleonardym_b200 import dirac
+    prov = provider or (bc.time_antiperiodic_provider(-1) if anti else bc.periodic_provider())
+    return dirac.DiracWilsonOperator(make_cfg(g["gauge"], spec["geometry"]), spec["kappa"], hermitian,
+                                     representation="adjoint", boundary_condition_provider=prov)
+
+
+@pytest.mark.parametrize("case", list(ADJOINT_CASES))
+def test_adjoint_apply_links_force_vs_reference(cuda_device, case):
+    """Adjoint operator (both reference modes, all hermiticity / BC pairs, batched),
+    adjoint links and Lie derivative against the reference's outputs."""
+    g = load_golden(case)
+    spec = ADJOINT_CASES[case]
+    for herm in (0, 1):
+        for bcname in ("periodic", "anti"):
+            op = make_adj_op(g, spec, bool(herm), bcname == "anti")
+            ref = g[f"apply/h{herm}/{bcname}/projected"]
+            assert relerr(np_(op.multiply_in_adjoint_representation(cu(g["eta"]))), ref) < TOL, (herm, bcname)
+            assert relerr(np_(op.simple_multiply_in_adjoint_representation(cu(g["eta"]))),
+                          g[f"apply/h{herm}/{bcname}/simple"]) < TOL
+            both = np_(op.apply(cu(np.stack([g["eta"], g["eta2"]]))))
+            assert relerr(both[0], ref) < TOL
+            if bcname == "anti":
+                d = np_(op.lie_derivative(cu(g["eta"]), cu(g["eta2"])))
+                assert relerr(d, g[f"lie_derivative/h{herm}"]) < 1e-12, herm
+    q = make_adj_op(g, spec, True)
+    assert relerr(np_(q.fermion_gauge_field), g["fermion_gauge_field"]) < TOL
+
+
+def test_adjoint_generic_provider(cuda_device):
+    """An arbitrary provider callable multiplies the left links and the adjoint links."""
+    from tfleonardym_b200 import boundary_conditions as bc
+    g = load_golden("adj_d2su2")
+    spec = ADJOINT_CASES["adj_d2su2"]
+    bc.set_antiperiodic_field_in_t_direction(spec["geometry"])
+    op = make_adj_op(g, spec, True, provider=lambda x: bc.apply_antiboundary_conditions_in_t_direction(x))
+    assert relerr(np_(op.apply(cu(g["eta"]))), g["apply/h1/anti/projected"]) < TOL
+    assert relerr(np_(op.fermion_gauge_field), g["fermion_gauge_field"]) < TOL
+
+
+@pytest.mark.parametrize("case", list(ADJOINT_CASES))
+def test_adjoint_nf2_vs_reference(cuda_device, case):
+    """Nf=2 adjoint fermions through the reference's MMMR (generic operator path):
+    pseudofermion, energy and force against the reference's."""
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_action
+    dirac_solver.VERBOSE = False
+    g = load_golden(case)
+    spec = ADJOINT_CASES[case]
+    q = make_adj_op(g, spec, True)
+    solver = dirac_solver.multishift_solver(5000, 1e-22)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    nf.initialize_pseudofermions([cu(g["eta"])])
+    assert relerr(np_(nf.pseudofermions[0]), g["nf2/phi"]) < TOL
+    assert abs(nf.energy() - g["nf2/energy"]) < 1e-9 * abs(g["nf2/energy"])
+    assert relerr(np_(nf.force()), g["nf2/force"]) < 1e-8
+
+
+def test_adjoint_rejected_by_even_odd_solvers(cuda_device):
+    from tfleonardym_b200 import dirac_solver
+    g = load_golden("adj_d2su2")
+    q = make_adj_op(g, ADJOINT_CASES["adj_d2su2"], True)
+    with pytest.raises(TypeError):
+        dirac_solver.conjugate_gradient().solve(q, cu(g["eta"]))

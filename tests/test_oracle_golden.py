@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from oracle import lym_oracle as O
-from tests.conftest import GOLDEN_CASES, load_golden, relerr
+from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, load_golden, relerr
 
 TOL = 1e-13
 
@@ -130,3 +130,68 @@ def test_md_trajectory(case):
     u, p = O.integrate_om(g["gauge"], g["md/momenta_in"], [f_ferm, f_gauge], list(g["hmc/steps"]), 1.0)
     assert relerr(u, g["md/cfg_out"]) < 1e-10
     assert relerr(p, g["md/momenta_out"]) < 1e-10
+
+
+# ---------------------------------------------------------------------------
+# adjoint representation
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", list(ADJOINT_CASES))
+def test_adjoint_apply_links_and_lie_derivative(case):
+    """Adjoint Wilson operator (projected and simple forms, all hermiticity / BC
+    pairs), adjoint links and Lie derivative against the reference's outputs."""
+    g = load_golden(case)
+    spec = ADJOINT_CASES[case]
+    tables = O.lookup_tables(spec["geometry"])
+    bcf = O.antiperiodic_field(spec["geometry"])
+    u = g["gauge"]
+    for herm in (0, 1):
+        for bcname in ("periodic", "anti"):
+            ub = O.apply_time_bc(u, bcf) if bcname == "anti" else u
+            out = O.wilson_apply_adjoint(ub, u, g["eta"], spec["kappa"], bool(herm), tables)
+            assert relerr(out, g[f"apply/h{herm}/{bcname}/projected"]) < TOL, (herm, bcname)
+            assert relerr(out, g[f"apply/h{herm}/{bcname}/simple"]) < TOL, (herm, bcname)
+    v = O.adjoint_links(u, bcf)
+    assert relerr(v, g["fermion_gauge_field"]) < TOL
+    for herm in (0, 1):
+        d = O.lie_derivative_adjoint(v, g["eta"], g["eta2"], spec["kappa"], bool(herm), tables)
+        assert relerr(d, g[f"lie_derivative/h{herm}"]) < 1e-12, herm
+
+
+@pytest.mark.parametrize("case", list(ADJOINT_CASES))
+def test_adjoint_nf2_energy_force(case):
+    """Nf=2 in the adjoint: phi = Q eta, S = <phi, (Q^2)^-1 phi>, force from the
+    Lie derivatives of x = (Q^2)^-1 phi and Q x (fermion_action.py:64-93)."""
+    g = load_golden(case)
+    spec = ADJOINT_CASES[case]
+    geometry, kappa = spec["geometry"], spec["kappa"]
+    tables = O.lookup_tables(geometry)
+    bcf = O.antiperiodic_field(geometry)
+    u = g["gauge"]
+    ub = O.apply_time_bc(u, bcf)
+
+    def q(v):
+        return O.wilson_apply_adjoint(ub, u, v, kappa, True, tables)
+
+    phi = q(g["eta"])
+    assert relerr(phi, g["nf2/phi"]) < TOL
+    # (Q^2)^-1 phi by CG to full precision
+    x = np.zeros_like(phi)
+    r = phi.copy()
+    p = r.copy()
+    rr = np.vdot(r, r).real
+    for _ in range(2000):
+        ap = q(q(p))
+        a = rr / np.vdot(p, ap).real
+        x += a * p
+        r -= a * ap
+        rn = np.vdot(r, r).real
+        if rn < 1e-28 * np.vdot(phi, phi).real:
+            break
+        p = r + (rn / rr) * p
+        rr = rn
+    assert abs(np.vdot(phi, x).real - g["nf2/energy"]) < 1e-9 * abs(g["nf2/energy"])
+    v = O.adjoint_links(u, bcf)
+    y = q(x)
+    force = O.lie_derivative_adjoint(v, x, y, kappa, True, tables) + \
+        O.lie_derivative_adjoint(v, y, x, kappa, True, tables)
+    assert relerr(force, g["nf2/force"]) < 1e-8

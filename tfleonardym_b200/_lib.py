@@ -81,6 +81,12 @@ SIGNATURES = {
     "lym_unitary_projection": (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
     "lym_fermion_force": (c_int, [c_void_p, c_int, c_double, c_int, c_double, c_double, c_void_p, c_int,
                                   P(c_double), c_void_p, c_void_p, c_int, c_double, c_void_p, c_void_p]),
+    "lym_wilson_apply_adjoint": (c_int, [c_void_p, c_int, c_double, c_int, c_double, c_double, c_void_p,
+                                         c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "lym_adjoint_links": (c_int, [c_void_p, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p]),
+    "lym_fermion_force_adjoint": (c_int, [c_void_p, c_int, c_double, c_int, c_double, c_double, c_void_p, c_int,
+                                          P(c_double), c_void_p, c_void_p, c_int, c_double, c_void_p,
+                                          c_void_p]),
 }
 
 _lib = None

@@ -4,7 +4,10 @@
 (dirac.py:253-378).  ``apply`` runs the fused FP64 Wilson kernel
 (lym_wilson_apply, replacing dirac.py:458-523 + 649-662); ``lie_derivative``
 runs the fused per-link force kernel (lym_fermion_force, dirac.py:525-565).
-Only the fundamental representation exists here; the adjoint one raises.
+The adjoint representation (matrix-valued spinors (ns, N, N, V), dirac.py:358-370,
+380-456) runs lym_wilson_apply_adjoint and lym_fermion_force_adjoint; its
+``fermion_gauge_field`` (the adjoint links) is built on demand by lym_adjoint_links.
+The even-odd solvers take the fundamental representation only.
 """
 import ctypes
 
@@ -99,9 +102,8 @@ class DiracWilsonOperator(Operator):
         self.representation = representation
         if mode not in ("projected", "simple"):
             raise RuntimeError(f"Unknown dirac multiplication mode {mode}")
-        if representation != "fundamental":
-            raise NotImplementedError("the adjoint representation is not built on the GPU path; "
-                                      "use representation='fundamental'")
+        if representation not in ("fundamental", "adjoint"):
+            raise RuntimeError(f"Unknown representation {representation}")
         self.boundary_condition_provider = boundary_condition_provider
         self._solver_gauge = None
         self._solver_gauge_key = None
@@ -125,10 +127,15 @@ class DiracWilsonOperator(Operator):
         self.cfg = cfg
         self.original_cfg = cfg
         factor, apply_tensor = bcs.provider_factor(self.boundary_condition_provider)
+        self._generic_bc = apply_tensor
+        self._gauge_orig = gauge
         if apply_tensor:
             gauge = _dev.as_c128(self.boundary_condition_provider(gauge))
         self.bc = factor
-        self.fermion_gauge_field = gauge
+        self._gauge_left = gauge  # links with the boundary condition (the reference's cfg)
+        self._adjoint_links = None
+        if self.representation == "fundamental":
+            self.fermion_gauge_field = gauge
         geometry = tuple(cfg.geometry) if cfg.geometry is not None else None
         if geometry is None or int(np.prod(geometry)) != self.volume:
             raise RuntimeError("Configuration.geometry does not match the gauge field volume")
@@ -136,8 +143,33 @@ class DiracWilsonOperator(Operator):
         self.lattice = lt.get_lattice(geometry)
         self._gauge_version = getattr(self, "_gauge_version", 0) + 1
 
+    @property
+    def fermion_gauge_field(self):
+        """Fundamental: the links with the boundary condition.  Adjoint: the adjoint links
+        V^{ab} = 2 Tr(T_a U T_b U^dag) with the boundary condition (dirac.py:358-370)."""
+        if self.representation == "fundamental":
+            return self._fermion_gauge_field
+        if self._adjoint_links is None:
+            nc, nd = self.number_of_colors, self.number_of_dimensions
+            a = nc * nc - 1
+            v = torch.empty((nd, a, a, self.volume), dtype=torch.complex128, device=self._gauge_orig.device)
+            bc = 1.0 + 0j if self._generic_bc else self.bc
+            _lib.check(_lib.lib().lym_adjoint_links(self.lattice.handle, nc, bc.real, bc.imag,
+                                                    _dev.ptr(self._gauge_orig), _dev.ptr(v), _dev.stream()),
+                       "lym_adjoint_links")
+            if self._generic_bc:
+                v = _dev.as_c128(self.boundary_condition_provider(v))
+            self._adjoint_links = v
+        return self._adjoint_links
+
+    @fermion_gauge_field.setter
+    def fermion_gauge_field(self, value):
+        self._fermion_gauge_field = value
+
     # -- operator application ------------------------------------------------
     def apply(self, input_vector):
+        if self.representation == "adjoint":
+            return self._apply_adjoint(input_vector)
         v = _dev.as_c128(input_vector, "input_vector")
         out = torch.empty_like(v)
         nvec = 1
@@ -153,6 +185,23 @@ class DiracWilsonOperator(Operator):
 
     multiply_in_fundamental_representation = apply
     simple_multiply_in_fundamental_representation = apply
+    multiply_in_adjoint_representation = apply
+    simple_multiply_in_adjoint_representation = apply
+
+    def _apply_adjoint(self, input_vector):
+        v = _dev.as_c128(input_vector, "input_vector")
+        out = torch.empty_like(v)
+        nvec = 1
+        if v.dim() == 5:  # a batch (nvec, ns, N, N, V)
+            nvec = v.shape[0]
+        elif v.dim() != 4:
+            raise RuntimeError("adjoint spinor must be (ns, N, N, V) or (nvec, ns, N, N, V)")
+        bc = 1.0 + 0j if self._generic_bc else self.bc
+        _lib.check(_lib.lib().lym_wilson_apply_adjoint(
+            self.lattice.handle, self.number_of_colors, float(self.kappa), int(bool(self.hermitian)),
+            bc.real, bc.imag, _dev.ptr(self._gauge_left), _dev.ptr(self._gauge_orig), nvec, _dev.ptr(v),
+            _dev.ptr(out), _dev.stream()), "lym_wilson_apply_adjoint")
+        return out
 
     def apply_hermiticity(self, input_vector):
         if not self.hermitian:
@@ -162,7 +211,7 @@ class DiracWilsonOperator(Operator):
         return out
 
     def lie_derivative(self, X, Y):
-        """kappa-weighted Lie derivative (nd, N, N, V) of dirac.py:525-565."""
+        """kappa-weighted Lie derivative (nd, N, N, V) of dirac.py:525-565 (either representation)."""
         force = torch.zeros((self.number_of_dimensions, self.number_of_colors, self.number_of_colors,
                              self.volume), dtype=torch.complex128, device="cuda")
         self.accumulate_force(force, [1.0], _dev.as_c128(X)[None], _dev.as_c128(Y)[None], symmetric=False)
@@ -175,6 +224,15 @@ class DiracWilsonOperator(Operator):
         Y = _dev.as_c128(Y)
         n = X.shape[0]
         al = (ctypes.c_double * n)(*[float(np.real(a)) for a in alphas])
+        if self.representation == "adjoint":
+            if self._generic_bc:
+                raise NotImplementedError("the adjoint force takes a tagged boundary_condition_provider "
+                                          "(boundary_conditions.*_provider)")
+            _lib.check(_lib.lib().lym_fermion_force_adjoint(
+                self.lattice.handle, self.number_of_colors, float(self.kappa), int(bool(self.hermitian)),
+                self.bc.real, self.bc.imag, _dev.ptr(self._gauge_orig), n, al, _dev.ptr(X), _dev.ptr(Y),
+                int(bool(symmetric)), float(scale), _dev.ptr(force), _dev.stream()), "lym_fermion_force_adjoint")
+            return force
         _lib.check(_lib.lib().lym_fermion_force(
             self.lattice.handle, self.number_of_colors, float(self.kappa), int(bool(self.hermitian)),
             self.bc.real, self.bc.imag, _dev.ptr(self.fermion_gauge_field), n, al, _dev.ptr(X), _dev.ptr(Y),
@@ -184,6 +242,8 @@ class DiracWilsonOperator(Operator):
     # -- device gauge for the solvers -----------------------------------------
     def solver_gauge(self, precisions=("f32", "f16", "bf16")):
         """lym_gauge handle (even-odd links) for the current configuration."""
+        if self.representation != "fundamental":
+            raise TypeError("the even-odd solvers take the fundamental representation")
         mask = 0
         for p in precisions:
             mask |= 1 << _lib.PREC[p]

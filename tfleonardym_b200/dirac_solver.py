@@ -36,7 +36,7 @@ def _wilson_square(operator):
     """The DiracWilsonOperator behind SquareOperator(Q) with hermitian Q, else None."""
     if isinstance(operator, SquareOperator) and isinstance(operator.operator_to_square, DiracWilsonOperator):
         q = operator.operator_to_square
-        if q.hermitian:
+        if q.hermitian and q.representation == "fundamental":
             return q
     return None
 
@@ -191,8 +191,8 @@ class conjugate_gradient:  # noqa: N801 - named like the reference solvers
         self.reports = None
 
     def solve(self, operator, source):
-        if not isinstance(operator, DiracWilsonOperator):
-            raise TypeError("conjugate_gradient solves with a DiracWilsonOperator")
+        if not isinstance(operator, DiracWilsonOperator) or operator.representation != "fundamental":
+            raise TypeError("conjugate_gradient solves with a fundamental-representation DiracWilsonOperator")
         b = _dev.as_c128(source)
         batched = b.dim() == 4
         bb = b if batched else b[None]

@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 import torch
 
-from . import _dev, _lib
+from . import _dev, _lib, lie_generators
 from . import lattice as lt
 from . import smearing
 
@@ -108,12 +108,20 @@ def hotstart(geometry, nc=3, nd=4, generator=None):
 
 def generate_random_vector(nc=3, spinor_dimension=4, representation="fundamental", stddev=1, volume=None,
                            generator=None):
-    """Complex Gaussian spinor (hmc.py:196-210), fundamental representation."""
-    if representation != "fundamental":
-        raise NotImplementedError("the adjoint representation is not built on the GPU path")
+    """Complex Gaussian spinor (hmc.py:196-210): (ns, N, V) fundamental, or the
+    matrix-valued adjoint one sum_a v_a T^a, (ns, N, N, V)."""
+    if representation not in ("fundamental", "adjoint"):
+        raise RuntimeError(f"Unknown representation {representation}")
     if volume is None:
         from . import translate
         volume = translate.lookup_tables.local_volume
+    if representation == "adjoint":
+        ncomp = nc * nc - 1
+        shape = (spinor_dimension, ncomp, volume)
+        re = torch.randn(shape, dtype=torch.float64, device="cuda", generator=generator) * stddev
+        im = torch.randn(shape, dtype=torch.float64, device="cuda", generator=generator) * stddev
+        gens = torch.from_numpy(lie_generators.generators(nc, "fundamental")).to(re.device)
+        return torch.einsum("mic,ijk->mjkc", torch.complex(re, im), gens)
     shape = (spinor_dimension, nc, volume)
     re = torch.randn(shape, dtype=torch.float64, device="cuda", generator=generator) * stddev
     im = torch.randn(shape, dtype=torch.float64, device="cuda", generator=generator) * stddev
