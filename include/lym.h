@@ -273,6 +273,17 @@ int lym_fermion_force_adjoint(const lym_lattice* lat, int nc, double kappa, int 
                               const double* alphas, const void* X, const void* Y, int symmetric,
                               double scale, void* force, void* stream);
 
+/* ------------------------------------------------------------------ */
+/* fermion measurements (fermion_measurements.py:41-115)               */
+/* ------------------------------------------------------------------ */
+
+/* out (device, 2 * L doubles, L = the lattice extent in `direction`): out[2z], out[2z+1] =
+ * sum over nvec vectors and the sites with x_direction = z of sum_{spin,colour} conj(S) S
+ * (fundamental, vectors (ns, N, V)) or sum_{spin,c,d} conj(S_cd) S_dc (adjoint = 1, vectors
+ * (ns, N, N, V)): the slice sums of pion_correlator (fermion_measurements.py:76-90). */
+int lym_timeslice_sums(const lym_lattice* lat, int direction, int nvec, int ns, int nc, int adjoint,
+                       const void* in, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

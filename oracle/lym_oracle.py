@@ -367,6 +367,59 @@ def lie_derivative_adjoint(vlinks, X, Y, kappa, hermitian, tables):
     return kappa * np.stack(out)
 
 
+# ---------------------------------------------------------------------------
+# Fermion measurements (dirac.py:665-696, fermion_measurements.py:11-115)
+# ---------------------------------------------------------------------------
+
+
+def point_source(site, color, spin, volume, nc, ns, adjoint=False):
+    """Unit source at (spin, colour, site); in the adjoint the colour index is a
+    generator index and the source is the matrix T^color (fermion_measurements.py:27-38)."""
+    if not adjoint:
+        v = np.zeros((ns, nc, volume), dtype=np.complex128)
+        v[spin, color, site] = 1
+        return v
+    v = np.zeros((ns, nc, nc, volume), dtype=np.complex128)
+    v[spin, :, :, site] = generators(nc)[color]
+    return v
+
+
+def propagator(apply_q, source, tol=1e-26, max_iter=20000):
+    """gamma_d Q (Q^2)^-1 source = gamma_d Q^-1 source (dirac.py:670-682 for a Wilson
+    operator), with (Q^2)^-1 by CG to |r|^2 <= tol |b|^2."""
+    source = np.asarray(source, dtype=np.complex128)
+    x = np.zeros_like(source)
+    r = source.copy()
+    p = r.copy()
+    bb = np.vdot(source, source).real
+    rr = bb
+    for _ in range(max_iter):
+        ap = apply_q(apply_q(p))
+        a = rr / np.vdot(p, ap).real
+        x += a * p
+        r -= a * ap
+        rn = np.vdot(r, r).real
+        if rn <= tol * bb:
+            break
+        p = r + (rn / rr) * p
+        rr = rn
+    return gamma_d(apply_q(x))
+
+
+def pion_correlator(solutions, coords, direction, length, adjoint=False):
+    """sum over the solutions of sum_{spin,colour} conj(S) S per site, summed per
+    slice of `direction` (fermion_measurements.py:76-90; adjoint: conj(S_cd) S_dc)."""
+    corr = np.zeros(length, dtype=np.complex128)
+    for s in solutions:
+        if adjoint:
+            dot = np.einsum("icdm,idcm->m", np.conj(s), s)
+        else:
+            dot = np.einsum("icm,icm->m", np.conj(s), s)
+        for z in range(length):
+            corr[z] += dot[coords[direction] == z].sum()
+    return corr
+
+
 def update_link_field(links, momenta, eps):
     """U <- expm(eps P) U per link (hmc.py:40-43)."""
     ex = scipy.linalg.expm(np.transpose(eps * momenta, (0, 3, 1, 2)))  # (nd, V, N, N)

@@ -37,6 +37,13 @@ ADJOINT_CASES = {
     "adj_d4su2": dict(geometry=(4, 2, 2, 4), nc=2, kappa=0.13),
 }
 
+# fermion-measurement cases (tests/golden/make_golden.py MEASUREMENT_CASES)
+MEASUREMENT_CASES = {
+    "meas_d2": dict(geometry=(8, 6), nc=2, kappa=0.12, representation="fundamental"),
+    "meas_d4": dict(geometry=(2, 4, 2, 6), nc=3, kappa=0.11, representation="fundamental"),
+    "meas_adj": dict(geometry=(4, 6), nc=2, kappa=0.1, representation="adjoint"),
+}
+
 
 def relerr(a, b):
     a = np.asarray(a)

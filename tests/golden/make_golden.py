@@ -56,6 +56,15 @@ ADJOINT_CASES = {
     "adj_d4su2": dict(geometry=(4, 2, 2, 4), nc=2, kappa=0.13, seed=23),
 }
 
+# fermion measurements (fermion_measurements.py:41-115, dirac.py:665-696): pion
+# correlator from point sources, chiral condensate from recorded Z2 noise,
+# one propagator application
+MEASUREMENT_CASES = {
+    "meas_d2": dict(geometry=(8, 6), nc=2, kappa=0.12, seed=31, representation="fundamental"),
+    "meas_d4": dict(geometry=(2, 4, 2, 6), nc=3, kappa=0.11, seed=32, representation="fundamental"),
+    "meas_adj": dict(geometry=(4, 6), nc=2, kappa=0.1, seed=33, representation="adjoint"),
+}
+
 TABLE_GEOMETRIES = [(2, 4, 6, 8), (3, 5, 2, 4), (4, 6, 8), (5, 7), (8, 8), (1, 4, 2, 2)]
 
 
@@ -336,6 +345,55 @@ def run_adjoint_case(name):
     print("wrote", name)
 
 
+def run_measurement_case(name):
+    spec = MEASUREMENT_CASES[name]
+    geometry = spec["geometry"]
+    nd, nc, rep = len(geometry), spec["nc"], spec["representation"]
+    _setup_reference(geometry)
+    import tensorflow as tf
+    tf.set_seed(spec["seed"])
+    np.random.seed(spec["seed"])
+
+    import boundary_conditions
+    import dirac
+    import dirac_solver
+    import fermion_measurements
+    import hmc
+    import translate
+
+    log = _IterLog()
+    dirac_solver.print = log
+
+    def bc_anti(x):
+        return boundary_conditions.apply_antiboundary_conditions_in_t_direction(x)
+
+    out = {}
+    cfg = hmc.hotstart(list(geometry), nc, nd)
+    out["gauge"] = np.asarray(cfg.gauge_field)
+    Q = dirac.DiracWilsonOperator(cfg, spec["kappa"], True, representation=rep, boundary_condition_provider=bc_anti)
+    corr = fermion_measurements.pion_correlator(Q, nd - 1, translate.lookup_tables, lambda x: x)
+    out["pion_correlator"] = np.asarray(corr.value)
+    recorded = []
+    noise = fermion_measurements.generate_random_z2_noise
+
+    def recording_noise(*a, **k):
+        v = noise(*a, **k)
+        recorded.append(np.asarray(v))
+        return v
+
+    fermion_measurements.generate_random_z2_noise = recording_noise
+    cc = fermion_measurements.chiral_condensate(Q, num_estimators=3)
+    out["chiral_condensate"] = np.asarray(cc.value)
+    out["chiral_condensate/sources"] = np.stack(recorded)
+    prop = dirac.Propagator(Q, dirac_solver.biconjugate_gradient(5000, 1e-20))
+    src = fermion_measurements.generate_point_source(1, 0, 1, Q.volume, nc, Q.spinor_dimension, rep)
+    out["propagator/source"] = np.asarray(src)
+    out["propagator/out"] = np.asarray(prop.apply(src))
+    log.take()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print("wrote", name)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default=None)
@@ -346,10 +404,12 @@ def main():
             run_tables()
         elif args.case in ADJOINT_CASES:
             run_adjoint_case(args.case)
+        elif args.case in MEASUREMENT_CASES:
+            run_measurement_case(args.case)
         else:
             run_case(args.case)
         return
-    names = [args.case] if args.case else ["tables"] + list(CASES) + list(ADJOINT_CASES)
+    names = [args.case] if args.case else ["tables"] + list(CASES) + list(ADJOINT_CASES) + list(MEASUREMENT_CASES)
     for n in names:
         subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc"], check=True)
 

@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from oracle import lym_oracle as O
-from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, load_golden, relerr
+from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, MEASUREMENT_CASES, load_golden, relerr
 
 pytestmark = pytest.mark.gpu
 
@@ -461,3 +461,49 @@ def test_adjoint_rejected_by_even_odd_solvers(cuda_device):
     q = make_adj_op(g, ADJOINT_CASES["adj_d2su2"], True)
     with pytest.raises(TypeError):
         dirac_solver.conjugate_gradient().solve(q, cu(g["eta"]))
+
+
+# ---------------------------------------------------------------------------
+# fermion measurements (fermion_measurements.py:41-115, dirac.py:665-696)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", list(MEASUREMENT_CASES))
+def test_measurements_vs_reference(cuda_device, case):
+    """Propagator, pion correlator and chiral condensate (recorded Z2 sources)
+    against the reference: fundamental through the batched even-odd CG (default
+    inverter), adjoint through the reference's BiCGStab; the reference's own
+    BiCGStab tolerances bound the agreement."""
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_measurements
+    dirac_solver.VERBOSE = False
+    g = load_golden(case)
+    spec = MEASUREMENT_CASES[case]
+    from tfleonardym_b200 import boundary_conditions as bc
+    q = dirac.DiracWilsonOperator(make_cfg(g["gauge"], spec["geometry"]), spec["kappa"], True,
+                                  representation=spec["representation"],
+                                  boundary_condition_provider=bc.time_antiperiodic_provider(-1))
+    inv = dirac_solver.conjugate_gradient(tol=1e-12) if spec["representation"] == "fundamental" else \
+        dirac_solver.biconjugate_gradient(5000, 1e-24)
+    prop = dirac.Propagator(q, inv)
+    assert relerr(np_(prop.apply(cu(g["propagator/source"]))), g["propagator/out"]) < 1e-8
+    nd = len(spec["geometry"])
+    corr = fermion_measurements.pion_correlator(q, nd - 1, None, lambda x: x)
+    assert relerr(corr.value, g["pion_correlator"]) < 1e-5
+    cc = fermion_measurements.chiral_condensate(q, sources=cu(g["chiral_condensate/sources"]))
+    assert abs(cc.value - g["chiral_condensate"]) < 1e-4 * abs(g["chiral_condensate"])
+
+
+def test_pion_correlator_vs_oracle_exact(cuda_device):
+    """The batched-CG pion correlator against the oracle's exact-solve one (1e-9)."""
+    from tfleonardym_b200 import boundary_conditions as bc
+    from tfleonardym_b200 import dirac, fermion_measurements
+    g = load_golden("meas_d4")
+    spec = MEASUREMENT_CASES["meas_d4"]
+    geometry, kappa = spec["geometry"], spec["kappa"]
+    q = dirac.DiracWilsonOperator(make_cfg(g["gauge"], geometry), kappa, True, representation="fundamental",
+                                  boundary_condition_provider=bc.time_antiperiodic_provider(-1))
+    corr = fermion_measurements.pion_correlator(q, 1, None, None).value  # along x1 this time
+    tables = O.lookup_tables(geometry)
+    ub = O.apply_time_bc(g["gauge"], O.antiperiodic_field(geometry))
+    vol = int(np.prod(geometry))
+    sols = [O.propagator(lambda v: O.wilson_apply(ub, v, kappa, True, tables), O.point_source(0, c, s, vol, 3, 4))
+            for s in range(4) for c in range(3)]
+    assert relerr(corr, O.pion_correlator(sols, tables[2], 1, geometry[1])) < 1e-9

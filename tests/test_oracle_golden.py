@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from oracle import lym_oracle as O
-from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, load_golden, relerr
+from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, MEASUREMENT_CASES, load_golden, relerr
 
 TOL = 1e-13
 
@@ -195,3 +195,36 @@ def test_adjoint_nf2_energy_force(case):
     force = O.lie_derivative_adjoint(v, x, y, kappa, True, tables) + \
         O.lie_derivative_adjoint(v, y, x, kappa, True, tables)
     assert relerr(force, g["nf2/force"]) < 1e-8
+
+
+# ---------------------------------------------------------------------------
+# fermion measurements
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", list(MEASUREMENT_CASES))
+def test_measurements(case):
+    """Propagator, pion correlator (all ns x colour point sources at site 0) and the
+    chiral condensate on the recorded Z2 noise, against the reference (whose
+    BiCGStab stops at |r|^2 < 1e-13 for the correlator and 1e-10 for the condensate,
+    so those two agree to the solves' accuracy only)."""
+    g = load_golden(case)
+    spec = MEASUREMENT_CASES[case]
+    geometry, kappa = spec["geometry"], spec["kappa"]
+    adjoint = spec["representation"] == "adjoint"
+    tables = O.lookup_tables(geometry)
+    u = g["gauge"]
+    ub = O.apply_time_bc(u, O.antiperiodic_field(geometry))
+    nd, nc, vol = len(geometry), u.shape[1], u.shape[-1]
+    ns = 2 if nd == 2 else 4
+
+    def q(v):
+        if adjoint:
+            return O.wilson_apply_adjoint(ub, u, v, kappa, True, tables)
+        return O.wilson_apply(ub, v, kappa, True, tables)
+
+    assert relerr(O.propagator(q, g["propagator/source"]), g["propagator/out"]) < 1e-8
+    ncol = nc * nc - 1 if adjoint else nc
+    sols = [O.propagator(q, O.point_source(0, c, s, vol, nc, ns, adjoint)) for s in range(ns) for c in range(ncol)]
+    corr = O.pion_correlator(sols, tables[2], nd - 1, geometry[-1], adjoint)
+    assert relerr(corr, g["pion_correlator"]) < 1e-5
+    cc = np.mean([O.dot(src, O.propagator(q, src)) / vol for src in g["chiral_condensate/sources"]])
+    assert abs(cc - g["chiral_condensate"]) < 1e-4 * abs(g["chiral_condensate"])

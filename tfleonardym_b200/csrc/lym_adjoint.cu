@@ -408,3 +408,68 @@ int lym_fermion_force_adjoint(const lym_lattice* lat, int nc, double kappa, int 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// slice sums of the pion correlator (fermion_measurements.py:76-90)
+// ---------------------------------------------------------------------------
+namespace lym {
+
+// out[2z], out[2z+1] = sum over the vectors and the sites with x_dir = z of
+// sum_{spin,colour} conj(S) S (fundamental, (ns, N, V) per vector) or
+// sum_{spin,c,d} conj(S_cd) S_dc (adjoint, (ns, N, N, V)); one block per slice,
+// fixed-order block reduction (deterministic).
+__global__ void __launch_bounds__(256) timeslice_sums_kernel(int64_t V, int64_t stride, int L, int nvec, int ns,
+                                                             int nc, int adjoint, const double2* __restrict__ in,
+                                                             double* __restrict__ out) {
+  __shared__ double sh[2 * 32];
+  const int z = blockIdx.x;
+  const int64_t per = V / L;
+  const int ncomp = adjoint ? nc * nc : nc;
+  const int64_t vec = (int64_t)ns * ncomp * V;
+  double re = 0.0, im = 0.0;
+  for (int64_t j = threadIdx.x; j < per; j += blockDim.x) {
+    const int64_t x = (j / stride) * (L * stride) + (int64_t)z * stride + (j % stride);
+    for (int v = 0; v < nvec; ++v)
+      for (int s = 0; s < ns; ++s) {
+        const double2* base = in + v * vec + (int64_t)s * ncomp * V;
+        if (!adjoint) {
+          for (int c = 0; c < nc; ++c) {
+            const cx<double> a = ld(base + (int64_t)c * V + x);
+            re += a.re * a.re + a.im * a.im;
+          }
+        } else {
+          for (int c = 0; c < nc; ++c)
+            for (int d = 0; d < nc; ++d) {
+              const cx<double> a = ld(base + (int64_t)(c * nc + d) * V + x);
+              const cx<double> b = ld(base + (int64_t)(d * nc + c) * V + x);
+              const cx<double> t = cmul_cj(a, b);
+              re += t.re;
+              im += t.im;
+            }
+        }
+      }
+  }
+  double v2[2] = {re, im};
+  block_sum<2>(v2, sh);
+  if (threadIdx.x == 0) {
+    out[2 * z] = v2[0];
+    out[2 * z + 1] = v2[1];
+  }
+}
+
+}  // namespace lym
+
+extern "C" int lym_timeslice_sums(const lym_lattice* lat, int direction, int nvec, int ns, int nc, int adjoint,
+                                  const void* in, double* out, void* stream) {
+  using namespace lym;
+  LYM_REQUIRE(lat && in && out, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(direction >= 0 && direction < lat->nd, LYM_ERR_BAD_ARG, "direction %d out of range", direction);
+  LYM_REQUIRE(nvec >= 1 && ns >= 1 && nc >= 1, LYM_ERR_BAD_ARG, "bad sizes");
+  int64_t stride = 1;
+  for (int d = direction + 1; d < lat->nd; ++d) stride *= lat->dims[d];
+  const int L = lat->dims[direction];
+  timeslice_sums_kernel<<<L, 256, 0, (cudaStream_t)stream>>>(lat->V, stride, L, nvec, ns, nc, adjoint != 0,
+                                                            (const double2*)in, out);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}

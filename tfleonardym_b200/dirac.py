@@ -283,5 +283,41 @@ class DiracWilsonOperator(Operator):
             pass
 
 
-def Propagator(*_a, **_k):  # noqa: N802 - reference name
-    raise NotImplementedError("Propagator is a measurement consumer outside the solve path")
+class Propagator:
+    """gamma_d op^-1 source (dirac.py:665-696 for a Wilson operator: the reference
+    computes op (op^2)^-1 source with its inverter, then applies gamma_d).
+
+    With ``dirac_solver.conjugate_gradient`` as the inverter and a fundamental
+    DiracWilsonOperator, op x = source is solved directly by the even-odd CG, all
+    stacked sources (nsrc, ns, N, V) in one batched call; any other inverter
+    follows the reference's steps (inverter.solve(SquareOperator(op), source), then
+    op.apply) one source at a time."""
+
+    def __init__(self, operator, inverter):
+        self.operator = operator
+        self.inverter = inverter
+
+    def apply(self, source):
+        from . import dirac_solver
+        src = _dev.as_c128(source)
+        op = self.operator
+        fundamental = isinstance(op, DiracWilsonOperator) and op.representation == "fundamental"
+        if isinstance(self.inverter, dirac_solver.conjugate_gradient) and fundamental:
+            return self.apply_gammad(self.inverter.solve(op, src))
+        per = 4 if (isinstance(op, DiracWilsonOperator) and op.representation == "adjoint") else 3
+        if src.dim() == per + 1:  # a stack of sources, one reference-style solve each
+            return torch.stack([self.apply(src[i]) for i in range(src.shape[0])])
+        square_solution = self.inverter.solve(SquareOperator(op), src)
+        return self.apply_gammad(op.apply(square_solution))
+
+    def apply_gammad(self, input_vector):
+        """Negate the lower half of the spin components (dirac.py:684-696), of one vector
+        or of each vector of a stack."""
+        adjoint = isinstance(self.operator, DiracWilsonOperator) and self.operator.representation == "adjoint"
+        spin_axis = input_vector.dim() - (4 if adjoint else 3)
+        out = input_vector.clone()
+        ns = out.shape[spin_axis]
+        index = [slice(None)] * out.dim()
+        index[spin_axis] = slice(ns // 2, ns)
+        out[tuple(index)] *= -1
+        return out
