@@ -636,6 +636,29 @@ def run_dslash_sweep(args, local_rank):
             del b
         del op, links
         torch.cuda.empty_cache()
+    # on-disk gauge format: device decode of the XDR link section at 32^4 (read 48 B,
+    # write 144 B per link), beside the oracle's numpy decode of an 8^4 sample on one core
+    geom = (32, 32, 32, 32)
+    nd, vol = 4, 32 ** 4
+    rng = np.random.default_rng(5)
+    words_h = rng.normal(size=vol * nd * 12).astype(">f4")
+    words = torch.from_numpy(np.frombuffer(words_h.tobytes(), dtype=np.uint8).copy()).to(dev)
+    gauge = torch.empty((nd, 3, 3, vol), dtype=torch.complex128, device=dev)
+    algo = vol * nd * (48 + 144)
+    t = timed(lambda: _lib.check(_lib.lib().lym_decode_xdr_gauge(nd, 3, vol, _dev.ptr(words), _dev.ptr(gauge),
+                                                                 _dev.stream()), "xdr"), True)
+    from oracle import lym_oracle as O
+    small = 8 ** 4
+    raw_small = np.frombuffer(words_h[:small * nd * 12].tobytes() + bytes(4 * nd + 24), dtype=np.uint8)
+    t0 = time.perf_counter()
+    O.read_config_xdr(raw_small, (8, 8, 8, 8))
+    cpu_s = (time.perf_counter() - t0) * vol / small
+    print(json.dumps({"dslash_sweep": "xdr_su3_decode (lattice.read_config)", "geometry": list(geom), "nrhs": 0,
+                      "l2": "flushed", "us": t * 1e6, "algorithmic_bytes": algo, "gbs": algo / t / 1e9,
+                      "frac_hbm": algo / t / 1e9 / peak,
+                      "cpu_oracle_us_scaled": cpu_s * 1e6,
+                      "cpu_sample": "oracle numpy decode of an 8^4 sample on one core, scaled by volume"}),
+          flush=True)
     return 0
 
 

@@ -274,6 +274,17 @@ int lym_fermion_force_adjoint(const lym_lattice* lat, int nc, double kappa, int 
                               double scale, void* force, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* on-disk gauge format (lattice.py:10-70)                             */
+/* ------------------------------------------------------------------ */
+
+/* Decode the link section of the reference's XDR configuration file, already on the
+ * device: raw = volume x nd x 3 x 2 x 2 big-endian float32 words (the first two
+ * columns of conj(U), re/im, site slowest; 16-byte aligned) -> gauge (nd, 3, 3, V)
+ * complex128 with columns 0, 1 Gram-Schmidt normalised and column 2 = conj(col0 x col1),
+ * as read_config does.  nc must be 3. */
+int lym_decode_xdr_gauge(int nd, int nc, int64_t volume, const void* raw, void* gauge, void* stream);
+
+/* ------------------------------------------------------------------ */
 /* fermion measurements (fermion_measurements.py:41-115)               */
 /* ------------------------------------------------------------------ */
 

@@ -420,6 +420,42 @@ def pion_correlator(solutions, coords, direction, length, adjoint=False):
     return corr
 
 
+# ---------------------------------------------------------------------------
+# On-disk gauge format (lattice.py:10-70)
+# ---------------------------------------------------------------------------
+
+
+def read_config_xdr(raw, geometry, nc=3):
+    """Decode the reference's XDR configuration (lattice.py:10-70): V x nd x N x (N-1)
+    x 2 big-endian float32 (the first N-1 columns of conj(U), re/im, site slowest),
+    then nd int32 extents and 3 float64 parameters.  Columns 0 and 1 are
+    Gram-Schmidt normalised as the reference does and column 2 = conj(col0 x col1).
+    Returns (gauge (nd, N, N, V) complex128, extents, parameters)."""
+    raw = np.asarray(raw, dtype=np.uint8).tobytes()
+    nd, vol = len(geometry), int(np.prod(geometry))
+    n = vol * nd * nc * (nc - 1) * 2
+    words = np.frombuffer(raw, dtype=">f4", count=n).astype(np.float64).reshape(vol, nd, nc, nc - 1, 2)
+    loaded = words[..., 0] - 1j * words[..., 1]
+    out = np.empty((nd, nc, nc, vol), dtype=np.complex128)
+    for mu in range(nd):
+        c0 = loaded[:, mu, :, 0].T  # (row, V)
+        t = 1.0 / np.sqrt(np.abs(c0[0]) ** 2 + np.abs(c0[1]) ** 2 + np.abs(c0[2]) ** 2)
+        c0 = c0 * t
+        c1 = loaded[:, mu, :, 1].T
+        t = c1[0] * np.conj(c0[0]) + c1[1] * np.conj(c0[1]) + c1[2] * np.conj(c0[2])
+        c1 = c1 - t * c0
+        t = 1.0 / np.sqrt(np.abs(c1[0]) ** 2 + np.abs(c1[1]) ** 2 + np.abs(c1[2]) ** 2)
+        c1 = c1 * t
+        c2 = np.stack([np.conj(c0[1]) * np.conj(c1[2]) - np.conj(c0[2]) * np.conj(c1[1]),
+                       np.conj(c0[2]) * np.conj(c1[0]) - np.conj(c0[0]) * np.conj(c1[2]),
+                       np.conj(c0[0]) * np.conj(c1[1]) - np.conj(c0[1]) * np.conj(c1[0])])
+        out[mu] = np.stack([c0, c1, c2], axis=1)
+    off = 4 * n
+    dims = list(np.frombuffer(raw, dtype=">i4", count=nd, offset=off).astype(int))
+    params = list(np.frombuffer(raw, dtype=">f8", count=3, offset=off + 4 * nd).astype(float))
+    return out, dims, params
+
+
 def update_link_field(links, momenta, eps):
     """U <- expm(eps P) U per link (hmc.py:40-43)."""
     ex = scipy.linalg.expm(np.transpose(eps * momenta, (0, 3, 1, 2)))  # (nd, V, N, N)

@@ -21,7 +21,9 @@ files themselves are never modified):
   * ``hmc.metropolis`` is replaced by the same rule (metropolis.py:11-18)
     with a uniform drawn from a seeded generator on every call and saved;
   * ``dirac_solver.print`` is captured to record solver iteration counts
-    (dirac_solver.py:49,102).
+    (dirac_solver.py:49,102);
+  * ``lattice.Configuration`` gets a default for ``number_of_dimensions`` before
+    ``read_config`` runs, which builds it with three fields (lattice.py:69-70).
 """
 import argparse
 import os
@@ -63,6 +65,12 @@ MEASUREMENT_CASES = {
     "meas_d2": dict(geometry=(8, 6), nc=2, kappa=0.12, seed=31, representation="fundamental"),
     "meas_d4": dict(geometry=(2, 4, 2, 6), nc=3, kappa=0.11, seed=32, representation="fundamental"),
     "meas_adj": dict(geometry=(4, 6), nc=2, kappa=0.1, seed=33, representation="adjoint"),
+}
+
+# on-disk gauge format (lattice.py:10-70): an XDR file of two-column SU(3) links
+# (U* stored, float32) written here, read by the reference's read_config
+XDR_CASES = {
+    "xdr_su3": dict(geometry=(4, 2, 4, 6), seed=41),
 }
 
 TABLE_GEOMETRIES = [(2, 4, 6, 8), (3, 5, 2, 4), (4, 6, 8), (5, 7), (8, 8), (1, 4, 2, 2)]
@@ -394,6 +402,40 @@ def run_measurement_case(name):
     print("wrote", name)
 
 
+def run_xdr_case(name):
+    import xdrlib  # Python <= 3.12 (the reference's own reader uses it)
+    spec = XDR_CASES[name]
+    geometry = spec["geometry"]
+    nd, nc, vol = len(geometry), 3, int(np.prod(geometry))
+    rng = np.random.default_rng(spec["seed"])
+    # near-SU(3) links; the file holds conj(U)'s first two columns in float32
+    a = rng.normal(size=(vol, nd, nc, nc)) + 1j * rng.normal(size=(vol, nd, nc, nc))
+    q, _ = np.linalg.qr(a)
+    cols = np.conj(q[..., :2])  # (V, nd, row, col<2)
+    words = np.stack([cols.real, cols.imag], axis=-1).astype(np.float32).ravel()
+    pk = xdrlib.Packer()
+    pk.pack_farray(words.size, [float(w) for w in words], pk.pack_float)
+    for d in geometry:
+        pk.pack_int(int(d))
+    for prm in (5.6, 0.13, 1.0):
+        pk.pack_double(prm)
+    raw = pk.get_buffer()
+    path = os.path.join(HERE, f"_tmp_{name}.xdr")
+    with open(path, "wb") as f:
+        f.write(raw)
+    _setup_reference(geometry)
+    import lattice
+    # read_config builds Configuration without number_of_dimensions (lattice.py:69-70)
+    # and raises; a default for that field lets it finish (the file is not modified)
+    lattice.Configuration.__new__.__defaults__ = (None,)
+    cfg = lattice.read_config(path, list(geometry), 3)
+    os.remove(path)
+    out = {"raw": np.frombuffer(raw, dtype=np.uint8), "gauge": np.asarray(cfg.gauge_field),
+           "geometry": np.asarray(geometry)}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print("wrote", name)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default=None)
@@ -406,10 +448,13 @@ def main():
             run_adjoint_case(args.case)
         elif args.case in MEASUREMENT_CASES:
             run_measurement_case(args.case)
+        elif args.case in XDR_CASES:
+            run_xdr_case(args.case)
         else:
             run_case(args.case)
         return
-    names = [args.case] if args.case else ["tables"] + list(CASES) + list(ADJOINT_CASES) + list(MEASUREMENT_CASES)
+    names = [args.case] if args.case else (["tables"] + list(CASES) + list(ADJOINT_CASES) + list(MEASUREMENT_CASES)
+                                           + list(XDR_CASES))
     for n in names:
         subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc"], check=True)
 

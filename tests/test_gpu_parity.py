@@ -507,3 +507,45 @@ def test_pion_correlator_vs_oracle_exact(cuda_device):
     sols = [O.propagator(lambda v: O.wilson_apply(ub, v, kappa, True, tables), O.point_source(0, c, s, vol, 3, 4))
             for s in range(4) for c in range(3)]
     assert relerr(corr, O.pion_correlator(sols, tables[2], 1, geometry[1])) < 1e-9
+
+
+# ---------------------------------------------------------------------------
+# on-disk gauge format (lattice.py:10-70)
+# ---------------------------------------------------------------------------
+def test_read_config_vs_reference(cuda_device, tmp_path):
+    """read_config decodes the XDR file on the device to the reference's links."""
+    from tfleonardym_b200 import lattice as lt
+    g = load_golden("xdr_su3")
+    path = tmp_path / "cfg.xdr"
+    g["raw"].tofile(path)
+    geometry = tuple(int(d) for d in g["geometry"])
+    cfg = lt.read_config(str(path), geometry)
+    assert cfg.number_of_dimensions == len(geometry) and cfg.colors == 3
+    assert relerr(np_(cfg.gauge_field), g["gauge"]) < 1e-15
+
+
+def test_xdr_decode_round_trip_large(cuda_device):
+    """Size-independent property at 16^4: SU(3) links written in the XDR convention
+    (float32 conj columns) decode to SU(3) matrices within float32 of the originals,
+    and the oracle decodes the same bytes to the same links."""
+    from tfleonardym_b200 import _dev, _lib
+    geometry = (16, 16, 16, 16)
+    nd, vol = 4, 16 ** 4
+    rng = np.random.default_rng(9)
+    a = rng.normal(size=(vol, nd, 3, 3)) + 1j * rng.normal(size=(vol, nd, 3, 3))
+    q, _ = np.linalg.qr(a)
+    q = q / np.linalg.det(q)[..., None, None] ** (1 / 3)
+    cols = np.conj(q[..., :2])
+    raw = np.stack([cols.real, cols.imag], axis=-1).astype(">f4").tobytes()
+    words = torch.from_numpy(np.frombuffer(raw, dtype=np.uint8).copy()).cuda()
+    out = torch.empty((nd, 3, 3, vol), dtype=torch.complex128, device="cuda")
+    _lib.check(_lib.lib().lym_decode_xdr_gauge(nd, 3, vol, _dev.ptr(words), _dev.ptr(out), _dev.stream()))
+    u = np_(out)
+    ref = np.transpose(q, (1, 2, 3, 0))
+    assert np.abs(u - ref).max() < 1e-6
+    sample = u[:, :, :, :4096]
+    uu = np.einsum("mijc,mkjc->mikc", sample, np.conj(sample))
+    assert np.abs(uu - np.eye(3)[None, :, :, None]).max() < 1e-13
+    head = nd * 3 * 2 * 2 * 4 * 4096  # the first 4096 sites (site index slowest in the file)
+    o, _, _ = O.read_config_xdr(np.frombuffer(raw[:head] + bytes(4 * nd + 24), dtype=np.uint8), (8, 8, 8, 8))
+    assert relerr(sample, o) < 1e-15

@@ -228,3 +228,12 @@ def test_measurements(case):
     assert relerr(corr, g["pion_correlator"]) < 1e-5
     cc = np.mean([O.dot(src, O.propagator(q, src)) / vol for src in g["chiral_condensate/sources"]])
     assert abs(cc - g["chiral_condensate"]) < 1e-4 * abs(g["chiral_condensate"])
+
+
+def test_read_config_xdr():
+    """The XDR configuration reader (lattice.py:10-70) against the reference's output."""
+    g = load_golden("xdr_su3")
+    geometry = tuple(int(d) for d in g["geometry"])
+    gauge, dims, params = O.read_config_xdr(g["raw"], geometry)
+    assert relerr(gauge, g["gauge"]) < 1e-15
+    assert dims == list(geometry) and params == [5.6, 0.13, 1.0]

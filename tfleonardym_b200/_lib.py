@@ -84,6 +84,7 @@ SIGNATURES = {
     "lym_wilson_apply_adjoint": (c_int, [c_void_p, c_int, c_double, c_int, c_double, c_double, c_void_p,
                                          c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "lym_adjoint_links": (c_int, [c_void_p, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p]),
+    "lym_decode_xdr_gauge": (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
     "lym_timeslice_sums": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "lym_fermion_force_adjoint": (c_int, [c_void_p, c_int, c_double, c_int, c_double, c_double, c_void_p, c_int,
                                           P(c_double), c_void_p, c_void_p, c_int, c_double, c_void_p,

@@ -170,3 +170,73 @@ extern "C" int lym_lattice_tables_device(const lym_lattice* lat, int64_t* sup_de
   LYM_CHECK_LAUNCH();
   return LYM_OK;
 }
+
+// ---------------------------------------------------------------------------
+// on-disk gauge format (lattice.py:10-70): decode on the device
+// ---------------------------------------------------------------------------
+namespace lym {
+
+// One thread per (site, mu): 12 big-endian float32 words (the first two
+// columns of conj(U), re/im) -> U in the reference layout (nd, 3, 3, V).  Column
+// 0 is normalised, column 1 orthogonalised against it and normalised, column 2 =
+// conj(col0 x col1): the reference's steps in its order, FP64, |z|^2 as
+// hypot(re, im)^2 like the reference's abs(z)**2.
+__global__ void __launch_bounds__(128) xdr_su3_kernel(int nd, int64_t V, const unsigned* __restrict__ raw,
+                                                      double2* __restrict__ out) {
+  const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (x >= V) return;
+  // the link's 48-byte record as three 16-byte loads (records start 16-byte aligned)
+  const uint4* w4 = reinterpret_cast<const uint4*>(raw + (x * nd + mu) * 12);
+  unsigned w[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const uint4 t = __ldg(w4 + k);
+    w[4 * k] = t.x;
+    w[4 * k + 1] = t.y;
+    w[4 * k + 2] = t.z;
+    w[4 * k + 3] = t.w;
+  }
+  cx<double> c[3][2];  // c[row][col] of conj-stored values, conjugated back
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const float re = __uint_as_float(__byte_perm(w[2 * k], 0, 0x0123));
+    const float im = __uint_as_float(__byte_perm(w[2 * k + 1], 0, 0x0123));
+    c[k / 2][k % 2] = {(double)re, -(double)im};  // word order: row, column, re/im
+  }
+  auto a2 = [](cx<double> z) {
+    const double h = hypot(z.re, z.im);
+    return h * h;
+  };
+  cx<double> u[3][3];
+  double t = 1.0 / sqrt(a2(c[0][0]) + a2(c[1][0]) + a2(c[2][0]));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) u[i][0] = t * c[i][0];
+  cx<double> p = c[0][1] * conj(u[0][0]) + c[1][1] * conj(u[1][0]) + c[2][1] * conj(u[2][0]);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) u[i][1] = c[i][1] - p * u[i][0];
+  t = 1.0 / sqrt(a2(u[0][1]) + a2(u[1][1]) + a2(u[2][1]));
+#pragma unroll
+  for (int i = 0; i < 3; ++i) u[i][1] = t * u[i][1];
+  u[0][2] = conj(u[1][0]) * conj(u[2][1]) - conj(u[2][0]) * conj(u[1][1]);
+  u[1][2] = conj(u[2][0]) * conj(u[0][1]) - conj(u[0][0]) * conj(u[2][1]);
+  u[2][2] = conj(u[0][0]) * conj(u[1][1]) - conj(u[1][0]) * conj(u[0][1]);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) out[((int64_t)(mu * 3 + i) * 3 + j) * V + x] = make_double2(u[i][j].re, u[i][j].im);
+}
+
+}  // namespace lym
+
+extern "C" int lym_decode_xdr_gauge(int nd, int nc, int64_t volume, const void* raw, void* gauge, void* stream) {
+  using namespace lym;
+  LYM_REQUIRE(raw && gauge && nd >= 1 && nd <= LYM_MAX_ND && volume >= 0, LYM_ERR_BAD_ARG, "bad argument");
+  LYM_REQUIRE(nc == 3, LYM_ERR_UNSUPPORTED, "the XDR format holds SU(3) links (N=%d given)", nc);
+  LYM_REQUIRE(((uintptr_t)raw & 15) == 0, LYM_ERR_BAD_ARG, "raw words must be 16-byte aligned");
+  if (volume == 0) return LYM_OK;
+  dim3 grid(grid_for(volume, 128), nd);
+  xdr_su3_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(nd, volume, (const unsigned*)raw, (double2*)gauge);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}

@@ -18,6 +18,34 @@ from . import _dev, _lib
 Configuration = namedtuple("Configuration", ["gauge_field", "geometry", "colors", "number_of_dimensions"])
 Configuration.__new__.__defaults__ = (None,)
 
+def read_config(cfg_name, lattice_size, Nc=3):  # noqa: N803 - reference argument name
+    """Read the reference's XDR configuration file (lattice.py:10-70).
+
+    The link section (V x nd x 3 x 2 x 2 big-endian float32: the first two columns
+    of conj(U)) is copied to the device as bytes and decoded there by
+    lym_decode_xdr_gauge (Gram-Schmidt of the two columns, third column =
+    conj(col0 x col1)); the trailing extents and three parameters are printed as
+    the reference prints them.  The Configuration carries number_of_dimensions,
+    which the reference's omits (it raises there)."""
+    nd = len(lattice_size)
+    vol = int(np.prod(lattice_size))
+    if Nc != 3:
+        raise RuntimeError("the XDR configuration format holds SU(3) links")
+    raw = np.fromfile(cfg_name, dtype=np.uint8)
+    nbytes = vol * nd * Nc * (Nc - 1) * 2 * 4
+    trailer = 4 * nd + 8 * 3
+    if raw.size < nbytes + trailer:
+        raise RuntimeError(f"{cfg_name}: {raw.size} bytes, expected {nbytes + trailer} for {tuple(lattice_size)}")
+    words = torch.from_numpy(raw[:nbytes].copy()).to("cuda")
+    gauge = torch.empty((nd, Nc, Nc, vol), dtype=torch.complex128, device="cuda")
+    _lib.check(_lib.lib().lym_decode_xdr_gauge(nd, Nc, vol, _dev.ptr(words), _dev.ptr(gauge), _dev.stream()),
+               "lym_decode_xdr_gauge")
+    dims = [int(d) for d in np.frombuffer(raw.tobytes(), dtype=">i4", count=nd, offset=nbytes)]
+    params = [float(p) for p in np.frombuffer(raw.tobytes(), dtype=">f8", count=3, offset=nbytes + 4 * nd)]
+    print(cfg_name, dims, ", params", params)
+    return Configuration(gauge_field=gauge, geometry=tuple(lattice_size), colors=Nc, number_of_dimensions=nd)
+
+
 MthLookupTables = namedtuple("MthLookupTables", ["sup", "sdn", "global_coordinates", "global_volume",
                                                  "local_volume"])
 
