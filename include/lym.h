@@ -285,6 +285,24 @@ int lym_fermion_force_adjoint(const lym_lattice* lat, int nc, double kappa, int 
 int lym_decode_xdr_gauge(int nd, int nc, int64_t volume, const void* raw, void* gauge, void* stream);
 
 /* ------------------------------------------------------------------ */
+/* gauge observables (measurements.py:46-290)                          */
+/* ------------------------------------------------------------------ */
+
+/* Per starting site x, the ordered product of the links along a path of nsteps <= 256
+ * steps: +(mu+1) multiplies U_mu(y) and moves y to y + mu, -(mu+1) moves y to y - mu and
+ * multiplies U_mu(y)^dag.  trace = 1: out (V) complex128 = Tr of the product (plaquettes,
+ * 2x2 squares, Wilson loops, Polyakov loops); trace = 0: out (N, N, V) the product itself
+ * (wilson_lines_field). */
+int lym_path_product(const lym_lattice* lat, int nc, const void* gauge, int nsteps, const int* steps,
+                     int trace, void* out, void* stream);
+
+/* out (device, 2 L doubles, L = the extent of `direction`): out[2z], out[2z+1] = sum of the
+ * complex field (V) over the sites with x_direction = z and, when mask_direction >= 0,
+ * x_mask_direction = 0 (the zero-momentum projections of measurements.py:160-290). */
+int lym_slice_sums(const lym_lattice* lat, int direction, int mask_direction, const void* field,
+                   double* out, void* stream);
+
+/* ------------------------------------------------------------------ */
 /* fermion measurements (fermion_measurements.py:41-115)               */
 /* ------------------------------------------------------------------ */
 

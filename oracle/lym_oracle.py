@@ -456,6 +456,107 @@ def read_config_xdr(raw, geometry, nc=3):
     return out, dims, params
 
 
+# ---------------------------------------------------------------------------
+# Gauge observables and smearing (measurements.py:46-330, smearing.py:34-86)
+# ---------------------------------------------------------------------------
+
+
+def path_product(gauge, tables, steps):
+    """Per site x, the ordered link product along `steps` starting at x: +(mu+1)
+    multiplies U_mu(y) and moves y -> y + mu, -(mu+1) moves y -> y - mu and
+    multiplies U_mu(y)^dag.  Returns (N, N, V)."""
+    sup, sdn, _ = tables
+    nc, vol = gauge.shape[1], gauge.shape[-1]
+    y = np.arange(vol)
+    m = np.broadcast_to(np.eye(nc, dtype=np.complex128)[..., None], (nc, nc, vol)).copy()
+    for st in steps:
+        mu = abs(st) - 1
+        if st > 0:
+            m = np.einsum("ijc,jkc->ikc", m, gauge[mu][..., y])
+            y = sup[mu][y]
+        else:
+            y = sdn[mu][y]
+            m = np.einsum("ijc,kjc->ikc", m, np.conj(gauge[mu][..., y]))
+    return m
+
+
+def path_trace(gauge, tables, steps):
+    m = path_product(gauge, tables, steps)
+    return np.einsum("iic->c", m)
+
+
+def temporal_plaquette(gauge, tables):
+    """Re sum of the (mu, nd-1) plaquette traces / ((nd-1) N V) (measurements.py:46-66)."""
+    nd, nc, vol = gauge.shape[0], gauge.shape[1], gauge.shape[-1]
+    t = nd - 1
+    tot = sum(path_trace(gauge, tables, [mu + 1, t + 1, -(mu + 1), -(t + 1)]).sum() for mu in range(nd - 1))
+    return np.real(tot) / ((nd - 1) * nc * vol)
+
+
+def polyakov_loop_field(gauge, tables, geometry, direction):
+    """Trace of the product of the links around the compact `direction` (measurements.py:74-84)."""
+    return path_trace(gauge, tables, [direction + 1] * geometry[direction])
+
+
+def wilson_loops(gauge, tables, d_r, d_t, max_r, max_t):
+    """sum_x Tr(R-line T-line R-line^dag T-line^dag) / (N V) for r = 1..max_r,
+    t = 1..max_t, in that order (measurements.py:99-140)."""
+    nc, vol = gauge.shape[1], gauge.shape[-1]
+    out = []
+    for r in range(1, max_r + 1):
+        for t in range(1, max_t + 1):
+            steps = [d_r + 1] * r + [d_t + 1] * t + [-(d_r + 1)] * r + [-(d_t + 1)] * t
+            out.append(path_trace(gauge, tables, steps).sum() / (nc * vol))
+    return out
+
+
+def polyakov_operators(gauge, tables, geometry, correlator_direction=2, polyakov_direction=3):
+    """(meson zero-momentum projection per slice, Polyakov correlator, Polyakov loop)
+    (measurements.py:143-194; the meson pairs P(x) with P(x + e_1))."""
+    coords = tables[2]
+    p = polyakov_loop_field(gauge, tables, geometry, polyakov_direction)
+    meson = p * np.conj(translate(p, tables, 1, +1))
+    mz = [meson[(coords[correlator_direction] == z) & (coords[polyakov_direction] == 0)].mean()
+          for z in range(geometry[correlator_direction])]
+    corr = []
+    pdt = p
+    for _ in range(geometry[correlator_direction]):
+        corr.append((p * np.conj(pdt)).mean())
+        pdt = translate(pdt, tables, correlator_direction, +1)
+    return np.array(mz), np.array(corr), p.mean()
+
+
+def glueball_operators(gauge, tables, geometry, correlator_direction=2):
+    """Per-slice means of the summed 1x1 and 2x2 plaquette traces over the planes
+    that do not contain `correlator_direction` (measurements.py:197-290)."""
+    nd = gauge.shape[0]
+    coords = tables[2]
+    plaq = 0
+    square = 0
+    for mu in range(nd):
+        for nu in range(mu + 1, nd):
+            if correlator_direction in (mu, nu):
+                continue
+            a, b = mu + 1, nu + 1
+            plaq = plaq + path_trace(gauge, tables, [a, b, -a, -b])
+            square = square + path_trace(gauge, tables, [a, a, b, b, -a, -a, -b, -b])
+    length = geometry[correlator_direction]
+    pz = np.array([np.mean(plaq[coords[correlator_direction] == z]) for z in range(length)])
+    sz = np.array([np.mean(square[coords[correlator_direction] == z]) for z in range(length)])
+    return pz, sz
+
+
+def ape_smearing(gauge, tables, rho, no_smear_direction=3):
+    """P_SU(N)[(rho/6) S_mu + (1 - rho) U_mu], S the staples without the
+    no-smear direction; a direction without staples keeps rho U_mu + (1 - rho) U_mu
+    (smearing.py:34-51)."""
+    nd = gauge.shape[0]
+    nodir = no_smear_direction if 0 <= no_smear_direction < nd else None
+    st = staples(gauge, tables, nodir)
+    fat = np.array([(rho / 6) * st[mu] if mu != nodir else rho * gauge[mu] for mu in range(nd)])
+    return unitary_sqrt_projection(fat + (1 - rho) * gauge)
+
+
 def update_link_field(links, momenta, eps):
     """U <- expm(eps P) U per link (hmc.py:40-43)."""
     ex = scipy.linalg.expm(np.transpose(eps * momenta, (0, 3, 1, 2)))  # (nd, V, N, N)

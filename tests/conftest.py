@@ -37,6 +37,12 @@ ADJOINT_CASES = {
     "adj_d4su2": dict(geometry=(4, 2, 2, 4), nc=2, kappa=0.13),
 }
 
+# gauge-observable / smearing cases (tests/golden/make_golden.py OBSERVABLE_CASES)
+OBSERVABLE_CASES = {
+    "obs_su3": dict(geometry=(4, 4, 4, 6), nc=3),
+    "obs_su2": dict(geometry=(4, 6, 4, 4), nc=2),
+}
+
 # fermion-measurement cases (tests/golden/make_golden.py MEASUREMENT_CASES)
 MEASUREMENT_CASES = {
     "meas_d2": dict(geometry=(8, 6), nc=2, kappa=0.12, representation="fundamental"),

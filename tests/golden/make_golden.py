@@ -22,8 +22,9 @@ files themselves are never modified):
     with a uniform drawn from a seeded generator on every call and saved;
   * ``dirac_solver.print`` is captured to record solver iteration counts
     (dirac_solver.py:49,102);
-  * ``lattice.Configuration`` gets a default for ``number_of_dimensions`` before
-    ``read_config`` runs, which builds it with three fields (lattice.py:69-70).
+  * ``lattice.Configuration`` fills in ``number_of_dimensions`` from the gauge
+    field when a caller leaves it out: ``read_config`` (lattice.py:69-70) and
+    ``ape_smearing`` (smearing.py:49-51) build it with three fields and raise.
 """
 import argparse
 import os
@@ -73,7 +74,28 @@ XDR_CASES = {
     "xdr_su3": dict(geometry=(4, 2, 4, 6), seed=41),
 }
 
+# gauge observables and smearing (measurements.py:46-330, smearing.py:34-86)
+OBSERVABLE_CASES = {
+    "obs_su3": dict(geometry=(4, 4, 4, 6), nc=3, seed=51),
+    "obs_su2": dict(geometry=(4, 6, 4, 4), nc=2, seed=52),
+}
+
 TABLE_GEOMETRIES = [(2, 4, 6, 8), (3, 5, 2, 4), (4, 6, 8), (5, 7), (8, 8), (1, 4, 2, 2)]
+
+
+def _complete_configuration():
+    """lattice.Configuration with number_of_dimensions filled in from the gauge field
+    when a caller leaves it out (read_config, lattice.py:69-70; ape_smearing,
+    smearing.py:49-51 build it with three fields and raise)."""
+    import lattice
+    orig = lattice.Configuration
+
+    def configuration(gauge_field, geometry, colors, number_of_dimensions=None):
+        if number_of_dimensions is None:
+            number_of_dimensions = int(np.asarray(gauge_field).shape[0])
+        return orig(gauge_field, geometry, colors, number_of_dimensions)
+
+    lattice.Configuration = configuration
 
 
 def _setup_reference(geometry):
@@ -425,13 +447,48 @@ def run_xdr_case(name):
         f.write(raw)
     _setup_reference(geometry)
     import lattice
-    # read_config builds Configuration without number_of_dimensions (lattice.py:69-70)
-    # and raises; a default for that field lets it finish (the file is not modified)
-    lattice.Configuration.__new__.__defaults__ = (None,)
+    _complete_configuration()
     cfg = lattice.read_config(path, list(geometry), 3)
     os.remove(path)
     out = {"raw": np.frombuffer(raw, dtype=np.uint8), "gauge": np.asarray(cfg.gauge_field),
            "geometry": np.asarray(geometry)}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print("wrote", name)
+
+
+def run_observable_case(name):
+    spec = OBSERVABLE_CASES[name]
+    geometry = spec["geometry"]
+    nd, nc = len(geometry), spec["nc"]
+    _setup_reference(geometry)
+    import tensorflow as tf
+    tf.set_seed(spec["seed"])
+    np.random.seed(spec["seed"])
+    import hmc
+    import measurements
+    import smearing
+    _complete_configuration()
+
+    out = {}
+    cfg = hmc.hotstart(list(geometry), nc, nd)
+    # smooth the hot start a little so that loops are not pure noise
+    cfg = smearing.ape_smearing(cfg, 0.5, no_smear_direction=-1)
+    cfg = cfg._replace(geometry=list(geometry))
+    out["gauge"] = np.asarray(cfg.gauge_field)
+    out["temporal_plaquette"] = np.asarray(measurements.temporal_plaquette(cfg).value)
+    for m in measurements.polyakov_operators(cfg, 2, 3):
+        out[f"polyakov/{m.name}"] = np.asarray(m.value)
+    for m in measurements.glueball_operators(cfg, 2):
+        out[f"glueball/{m.name}"] = np.asarray(m.value)
+    for m in measurements.wilson_loops(cfg, 0, 3, 2, 3):
+        out[f"wilson/{m.name}"] = np.asarray(m.value)
+    out["polyakov_loop_field/1"] = np.asarray(measurements.polyakov_loop_field(cfg, 1))
+    sm = smearing.ape_smearing(cfg, 0.3, no_smear_direction=3)
+    out["ape/gauge"] = np.asarray(sm.gauge_field)
+    res = smearing.multi_smearing_operators(cfg, [lambda c: measurements.glueball_operators(c, 2)], smearing_levels=2,
+                                            rho=0.3, no_smear_direction=3, skip=1)
+    out["multi/values"] = np.stack([np.asarray(m.value) for m in res])
+    out["multi/levels"] = np.asarray([m.smearing_levels for m in res])
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
     print("wrote", name)
 
@@ -450,11 +507,13 @@ def main():
             run_measurement_case(args.case)
         elif args.case in XDR_CASES:
             run_xdr_case(args.case)
+        elif args.case in OBSERVABLE_CASES:
+            run_observable_case(args.case)
         else:
             run_case(args.case)
         return
     names = [args.case] if args.case else (["tables"] + list(CASES) + list(ADJOINT_CASES) + list(MEASUREMENT_CASES)
-                                           + list(XDR_CASES))
+                                           + list(XDR_CASES) + list(OBSERVABLE_CASES))
     for n in names:
         subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc"], check=True)
 

@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from oracle import lym_oracle as O
-from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, MEASUREMENT_CASES, load_golden, relerr
+from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, MEASUREMENT_CASES, OBSERVABLE_CASES, load_golden, relerr
 
 pytestmark = pytest.mark.gpu
 
@@ -549,3 +549,38 @@ def test_xdr_decode_round_trip_large(cuda_device):
     head = nd * 3 * 2 * 2 * 4 * 4096  # the first 4096 sites (site index slowest in the file)
     o, _, _ = O.read_config_xdr(np.frombuffer(raw[:head] + bytes(4 * nd + 24), dtype=np.uint8), (8, 8, 8, 8))
     assert relerr(sample, o) < 1e-15
+
+
+# ---------------------------------------------------------------------------
+# gauge observables and smearing (measurements.py:46-290, smearing.py:34-86)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", list(OBSERVABLE_CASES))
+def test_gauge_observables_vs_reference(cuda_device, case):
+    from tfleonardym_b200 import measurements as M
+    from tfleonardym_b200 import smearing
+    g = load_golden(case)
+    geometry = OBSERVABLE_CASES[case]["geometry"]
+    cfg = make_cfg(g["gauge"], geometry)
+    assert abs(M.temporal_plaquette(cfg).value - g["temporal_plaquette"]) < 1e-13
+    mz, corr, ploop = M.polyakov_operators(cfg, 2, 3)
+    assert relerr(mz.value, g["polyakov/meson_operator"]) < 1e-12
+    assert relerr(corr.value, g["polyakov/polyakov_correlator"]) < 1e-12
+    assert abs(ploop.value - g["polyakov/polyakov_loop"]) < 1e-13
+    assert relerr(np_(M.polyakov_loop_field(cfg, 1)), g["polyakov_loop_field/1"]) < 1e-13
+    pz, sz = M.glueball_operators(cfg, 2)
+    assert relerr(pz.value, g["glueball/zpp_operator"]) < 1e-12
+    assert relerr(sz.value, g["glueball/square_operator"]) < 1e-12
+    loops = M.wilson_loops(cfg, 0, 3, 2, 3)
+    assert [m.name for m in loops] == [f"wilson_loop_{r}_{t}" for r in (1, 2) for t in (1, 2, 3)]
+    for m in loops:
+        assert abs(m.value - g[f"wilson/{m.name}"]) < 1e-13, m.name
+    tables = O.lookup_tables(geometry)
+    lines = M.wilson_lines_field(cfg, 2, 2)
+    for k, line in enumerate(lines):
+        assert relerr(np_(line), O.path_product(g["gauge"], tables, [3] * (k + 1))) < 1e-14
+    sm = smearing.ape_smearing(cfg, 0.3, no_smear_direction=3)
+    assert relerr(np_(sm.gauge_field), g["ape/gauge"]) < 1e-13
+    res = smearing.multi_smearing_operators(cfg, [lambda c: M.glueball_operators(c, 2)], smearing_levels=2, rho=0.3,
+                                            no_smear_direction=3, skip=1)
+    assert relerr(np.stack([m.value for m in res]), g["multi/values"]) < 1e-12
+    assert [m.smearing_levels for m in res] == list(g["multi/levels"])

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from oracle import lym_oracle as O
-from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, MEASUREMENT_CASES, load_golden, relerr
+from tests.conftest import ADJOINT_CASES, GOLDEN_CASES, MEASUREMENT_CASES, OBSERVABLE_CASES, load_golden, relerr
 
 TOL = 1e-13
 
@@ -237,3 +237,35 @@ def test_read_config_xdr():
     gauge, dims, params = O.read_config_xdr(g["raw"], geometry)
     assert relerr(gauge, g["gauge"]) < 1e-15
     assert dims == list(geometry) and params == [5.6, 0.13, 1.0]
+
+
+# ---------------------------------------------------------------------------
+# gauge observables and smearing
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", list(OBSERVABLE_CASES))
+def test_gauge_observables_and_smearing(case):
+    g = load_golden(case)
+    geometry = OBSERVABLE_CASES[case]["geometry"]
+    tables = O.lookup_tables(geometry)
+    u = g["gauge"]
+    assert abs(O.temporal_plaquette(u, tables) - g["temporal_plaquette"]) < 1e-13
+    mz, corr, ploop = O.polyakov_operators(u, tables, geometry, 2, 3)
+    assert relerr(mz, g["polyakov/meson_operator"]) < 1e-12
+    assert relerr(corr, g["polyakov/polyakov_correlator"]) < 1e-12
+    assert abs(ploop - g["polyakov/polyakov_loop"]) < 1e-13
+    assert relerr(O.polyakov_loop_field(u, tables, geometry, 1), g["polyakov_loop_field/1"]) < 1e-13
+    pz, sz = O.glueball_operators(u, tables, geometry, 2)
+    assert relerr(pz, g["glueball/zpp_operator"]) < 1e-12
+    assert relerr(sz, g["glueball/square_operator"]) < 1e-12
+    loops = O.wilson_loops(u, tables, 0, 3, 2, 3)
+    ref = [g[f"wilson/wilson_loop_{r}_{t}"] for r in range(1, 3) for t in range(1, 4)]
+    assert relerr(np.array(loops), np.array(ref)) < 1e-12
+    assert relerr(O.ape_smearing(u, tables, 0.3, 3), g["ape/gauge"]) < 1e-13
+    # multi_smearing_operators: unsmeared glueball operators, then after each smearing step
+    vals, v = [], u
+    vals.extend(O.glueball_operators(v, tables, geometry, 2))
+    for _ in range(2):
+        v = O.ape_smearing(v, tables, 0.3, 3)
+        vals.extend(O.glueball_operators(v, tables, geometry, 2))
+    assert relerr(np.stack(vals), g["multi/values"]) < 1e-12
+    assert list(g["multi/levels"]) == [0, 0, 0, 0, 1, 1]

@@ -85,6 +85,8 @@ SIGNATURES = {
                                          c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "lym_adjoint_links": (c_int, [c_void_p, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p]),
     "lym_decode_xdr_gauge": (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
+    "lym_path_product": (c_int, [c_void_p, c_int, c_void_p, c_int, P(c_int), c_int, c_void_p, c_void_p]),
+    "lym_slice_sums": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "lym_timeslice_sums": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p]),
     "lym_fermion_force_adjoint": (c_int, [c_void_p, c_int, c_double, c_int, c_double, c_double, c_void_p, c_int,
                                           P(c_double), c_void_p, c_void_p, c_int, c_double, c_void_p,

@@ -578,3 +578,118 @@ int lym_fermion_force(const lym_lattice* lat, int nc, double kappa, int hermitia
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// gauge observables (measurements.py:46-290): link products along paths, slice sums
+// ---------------------------------------------------------------------------
+namespace lym {
+
+constexpr int kMaxPathSteps = 256;
+struct PathSteps {
+  signed char step[kMaxPathSteps];  // +(mu+1): U_mu(y), y += mu;  -(mu+1): y -= mu, U_mu(y)^dag
+};
+
+// One thread per starting site: M = product of the links along the path; writes
+// Tr M (trace = 1, out (V) complex) or M (out (N, N, V)).
+template <int NC>
+__global__ void __launch_bounds__(128) path_kernel(const int32_t* __restrict__ tab, int nd, int64_t V,
+                                                   const double2* __restrict__ U, int nsteps, PathSteps path,
+                                                   int want_trace, double2* __restrict__ out) {
+  const int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (x >= V) return;
+  Mat<NC> m = mident<NC>();
+  int64_t y = x;
+  for (int k = 0; k < nsteps; ++k) {
+    const int s = path.step[k];
+    const int mu = (s > 0 ? s : -s) - 1;
+    if (s > 0) {
+      m = mul(m, load_link<NC>(U, mu, y, V));
+      y = tab[mu * V + y];
+    } else {
+      y = tab[(nd + mu) * V + y];
+      m = mul_nd(m, load_link<NC>(U, mu, y, V));
+    }
+  }
+  if (want_trace) {
+    st(out + x, trace(m));
+  } else {
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) st(out + ((int64_t)i * NC + j) * V + x, m.m[i][j]);
+  }
+}
+
+// out[2z], out[2z+1] = sum of f(x) over the sites with x_dir = z (and, when
+// mask_len > 0, x_mask = 0); x_d = (x / stride_d) mod L_d for the lexicographic
+// index with the last coordinate fastest.  One block per slice, fixed-order
+// reduction (deterministic).
+__global__ void __launch_bounds__(256) slice_sum_kernel(int64_t V, int64_t stride, int L, int64_t mask_stride,
+                                                        int mask_len, const double2* __restrict__ f,
+                                                        double* __restrict__ out) {
+  __shared__ double sh[2 * 32];
+  const int z = blockIdx.x;
+  double re = 0.0, im = 0.0;
+  for (int64_t x = threadIdx.x; x < V; x += blockDim.x) {
+    if ((x / stride) % L != z) continue;
+    if (mask_len > 0 && (x / mask_stride) % mask_len != 0) continue;
+    const double2 v = f[x];
+    re += v.x;
+    im += v.y;
+  }
+  double v2[2] = {re, im};
+  block_sum<2>(v2, sh);
+  if (threadIdx.x == 0) {
+    out[2 * z] = v2[0];
+    out[2 * z + 1] = v2[1];
+  }
+}
+
+}  // namespace lym
+
+extern "C" int lym_path_product(const lym_lattice* lat, int nc, const void* gauge, int nsteps, const int* steps,
+                                int trace, void* out, void* stream) {
+  using namespace lym;
+  LYM_REQUIRE(lat && gauge && out && (steps || nsteps == 0), LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(nsteps >= 0 && nsteps <= kMaxPathSteps, LYM_ERR_BAD_ARG, "at most %d steps", kMaxPathSteps);
+  PathSteps p{};
+  for (int k = 0; k < nsteps; ++k) {
+    const int s = steps[k];
+    LYM_REQUIRE(s != 0 && (s > 0 ? s : -s) <= lat->nd, LYM_ERR_BAD_ARG, "step %d out of range", s);
+    p.step[k] = (signed char)s;
+  }
+  dim3 grid(grid_for(lat->V, 128));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nc == 2)
+    path_kernel<2><<<grid, 128, 0, st>>>(lat->d_tab, lat->nd, lat->V, (const double2*)gauge, nsteps, p, trace != 0,
+                                         (double2*)out);
+  else if (nc == 3)
+    path_kernel<3><<<grid, 128, 0, st>>>(lat->d_tab, lat->nd, lat->V, (const double2*)gauge, nsteps, p, trace != 0,
+                                         (double2*)out);
+  else {
+    set_error("N=%d not supported", nc);
+    return LYM_ERR_UNSUPPORTED;
+  }
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+extern "C" int lym_slice_sums(const lym_lattice* lat, int direction, int mask_direction, const void* field,
+                              double* out, void* stream) {
+  using namespace lym;
+  LYM_REQUIRE(lat && field && out, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(direction >= 0 && direction < lat->nd && mask_direction < lat->nd, LYM_ERR_BAD_ARG,
+              "direction out of range");
+  auto stride_of = [&](int d) {
+    int64_t s = 1;
+    for (int e = d + 1; e < lat->nd; ++e) s *= lat->dims[e];
+    return s;
+  };
+  const int L = lat->dims[direction];
+  const int mask_len = mask_direction >= 0 ? lat->dims[mask_direction] : 0;
+  slice_sum_kernel<<<L, 256, 0, (cudaStream_t)stream>>>(lat->V, stride_of(direction), L,
+                                                        mask_direction >= 0 ? stride_of(mask_direction) : 1,
+                                                        mask_len, (const double2*)field, out);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
