@@ -67,6 +67,13 @@ def parse_args():
     ap.add_argument("--hmc-inner", type=int, default=2, help="gauge steps per fermion step of the integrator")
     ap.add_argument("--hmc-precision", default="f64", choices=["f64", "f32", "f16", "bf16"],
                     help="inner precision of the HMC's CG solves (f64: the plain FP64 method)")
+    ap.add_argument("--serve-sweep", action="store_true",
+                    help="serving under an open-loop Poisson stream of mixed requests (D, N, geometry, kappa, "
+                         "rhs count, shifts, tolerance, gauge reuse), one JSON line per rate, then the same "
+                         "requests as plain FP64 one-at-a-time solves")
+    ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
+    ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per rate")
+    ap.add_argument("--serve-max-requests", type=int, default=600)
     ap.add_argument("--sweep-tiles", action="store_true",
                     help="with --dslash-sweep: also every forced hop tile at 16 right-hand sides")
     ap.add_argument("--profile", action="store_true",
@@ -662,6 +669,133 @@ def run_dslash_sweep(args, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# serving under a mixed open-loop request stream
+# ---------------------------------------------------------------------------
+def _device_links(geometry, nc, eps, seed, dev):
+    """reunit(exp(i eps H)) links with H traceless Hermitian from the request seed, on the device."""
+    import torch
+
+    from tfleonardym_b200 import hmc
+    nd, vol = len(geometry), int(np.prod(geometry))
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed))
+    a = torch.complex(torch.randn((nd, nc, nc, vol), generator=g, device=dev, dtype=torch.float64),
+                      torch.randn((nd, nc, nc, vol), generator=g, device=dev, dtype=torch.float64))
+    h = (a + torch.conj(a.transpose(1, 2))) / 2
+    tr = torch.diagonal(h, dim1=1, dim2=2).sum(-1) / nc  # (nd, vol)
+    for i in range(nc):
+        h[:, i, i] -= tr
+    ident = torch.zeros_like(h)
+    for i in range(nc):
+        ident[:, i, i] = 1
+    return hmc.update_link_field(ident, 1j * h, eps, reunitarize=True)
+
+
+def _request_specs(rng, n, max_bytes=2 << 30):
+    """Mixed requests: D in {2, 4}, N in {2, 3}, extents log-uniform between 8 and 24
+    (space) / 48 (time) in 4D and between 8 and 816 in 2D (even), footprint <= 2 GB;
+    kappa in [0.10, 0.14]; 1-16 rhs or (half of the requests) one rhs with 12 shifts
+    log-spaced in [1e-4, 1]; tol log-uniform in [1e-12, 1e-8]; eps in [0.1, 0.4];
+    30% reuse one of the last 8 gauge fields."""
+    from tfleonardym_b200 import serving
+    specs, recent = [], []
+    for i in range(n):
+        if recent and rng.uniform() < 0.3:
+            key, geom, nc, eps, seed = recent[int(rng.integers(len(recent)))]
+        else:
+            while True:
+                nd = int(rng.choice([2, 4]))
+                nc = int(rng.choice([2, 3]))
+                if nd == 4:
+                    geom = tuple(2 * int(round(np.exp(rng.uniform(np.log(8), np.log(hi))) / 2))
+                                 for hi in (24, 24, 24, 48))
+                else:
+                    geom = tuple(2 * int(round(np.exp(rng.uniform(np.log(8), np.log(816))) / 2)) for _ in range(2))
+                if serving.footprint_bytes(geom, nc, 16, "f16") <= max_bytes:
+                    break
+            eps, seed = float(rng.uniform(0.1, 0.4)), int(rng.integers(1 << 30))
+            key = f"cfg{seed}"
+            recent = (recent + [(key, geom, nc, eps, seed)])[-8:]
+        shifted = rng.uniform() < 0.5
+        specs.append(dict(key=key, geometry=geom, nc=nc, eps=eps, seed=seed, kappa=float(rng.uniform(0.10, 0.14)),
+                          nrhs=1 if shifted else int(rng.integers(1, 17)),
+                          shifts=list(np.logspace(-4, 0, 12)) if shifted else None,
+                          tol=float(10 ** rng.uniform(-12, -8)), src_seed=int(rng.integers(1 << 30))))
+    return specs
+
+
+def _serve(specs, times, precision, workers, max_batch, dev, budget):
+    import torch
+
+    from tfleonardym_b200 import serving
+    srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=dev.index)
+    futs = []
+    t0 = time.perf_counter()
+    for sp, t in zip(specs, times):
+        delay = t0 + t - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        nd, vol = len(sp["geometry"]), int(np.prod(sp["geometry"]))
+        ns = 2 if nd == 2 else 4
+        g = torch.Generator(device=dev)
+        g.manual_seed(sp["src_seed"])
+        shape = (sp["nrhs"], ns, sp["nc"], vol) if sp["shifts"] is None else (ns, sp["nc"], vol)
+        b = torch.complex(torch.randn(shape, generator=g, device=dev, dtype=torch.float64),
+                          torch.randn(shape, generator=g, device=dev, dtype=torch.float64)) / np.sqrt(2)
+        gauge = (lambda s=sp: _device_links(s["geometry"], s["nc"], s["eps"], s["seed"], dev))
+        futs.append(srv.submit(serving.SolveRequest(sp["key"], sp["geometry"], sp["nc"], sp["kappa"], b, gauge=gauge,
+                                                    tol=sp["tol"], precision=precision, bc=-1.0, max_iter=4000,
+                                                    shifts=sp["shifts"])))
+    res = [f.result() for f in futs]
+    wall = time.perf_counter() - t0
+    srv.close()
+    ok = [r for r in res if r.status == serving.OK]
+    lat = sorted(1e3 * r.latency for r in res if r.status != serving.REJECTED)
+    return {"requests": len(res), "ok": len(ok), "not_converged": sum(r.status == serving.NOT_CONVERGED for r in res),
+            "rejected": sum(r.status == serving.REJECTED for r in res),
+            "solves": int(sum(r.request.solves for r in ok)), "wall_s": wall,
+            "solves_per_s": sum(r.request.solves for r in ok) / wall,
+            "p50_ms": lat[len(lat) // 2] if lat else None,
+            "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))] if lat else None,
+            "max_true_residual_over_tol": max((m["true_residual"] / r.request.tol for r in res
+                                               if r.status != serving.REJECTED for m in r.reports), default=None)}
+
+
+def run_serve_sweep(args, local_rank):
+    """Open-loop Poisson streams of mixed solve requests through the solve server at
+    each rate of --serve-rates (arrivals over --serve-seconds, at most
+    --serve-max-requests), inner precision FP16 for unshifted requests (shifted ones
+    run the FP64 multishift CG), every answer checked by its FP64 true residual.
+    Then the lowest rate's requests again as plain FP64 one-at-a-time solves (one
+    worker, batches of one)."""
+    import torch
+
+    from tfleonardym_b200 import dirac_solver
+    dirac_solver.VERBOSE = False
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    warm = _request_specs(np.random.default_rng(1), 24)
+    _serve(warm, [0.0] * len(warm), "f16", args.workers, args.nrhs, dev, budget)  # compile-free warm-up of the path
+    first = None
+    for rate in rates:
+        rng = np.random.default_rng(int(rate) + 7)
+        times = np.cumsum(rng.exponential(1.0 / rate, size=args.serve_max_requests))
+        times = times[times < args.serve_seconds]
+        specs = _request_specs(rng, len(times))
+        if first is None:
+            first = (specs, times)
+        r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget)
+        print(json.dumps({"serve_sweep": "mixed", "rate_per_s": rate, "workers": args.workers,
+                          "max_batch_rhs": args.nrhs, **r}), flush=True)
+    specs, times = first
+    r = _serve(specs, times, "f64", 1, 1, dev, budget)
+    print(json.dumps({"serve_sweep": "plain_fp64_one_at_a_time", "rate_per_s": rates[0], **r}), flush=True)
+    return 0
+
+
 def run_hmc(args, rank, world, local_rank):
     """HMC on 4D SU(3) 16^4: beta = 5.6, Nf = 2 Wilson fermions at kappa = 0.13
     (pseudofermion phi = Q eta, Q = gamma_d D, antiperiodic time), links
@@ -749,6 +883,8 @@ def main():
         return run_dslash_sweep(args, local_rank)
     if args.hmc:
         return run_hmc(args, rank, world, local_rank)
+    if args.serve_sweep:
+        return run_serve_sweep(args, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if world > 1:

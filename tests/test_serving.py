@@ -101,7 +101,8 @@ def test_workers_overlap_when_budget_allows():
 @pytest.mark.gpu
 def test_same_answer_alone_and_in_the_mix(cuda_device):
     """Each request's solution alone equals its solution inside a mixed stream
-    (different geometry, N, kappa, precision), within the solve tolerance."""
+    (different geometry, N, kappa, precision, shifted and unshifted requests),
+    within the solve tolerance, and every answer meets its FP64 true residual."""
     from oracle import lym_oracle as O
     from tfleonardym_b200 import boundary_conditions
     rng = np.random.default_rng(77)
@@ -114,12 +115,15 @@ def test_same_answer_alone_and_in_the_mix(cuda_device):
         ns = 2 if nd == 2 else 4
         for k in range(3):
             b = torch.from_numpy(rng.normal(size=(ns, nc, vol)) + 1j * rng.normal(size=(ns, nc, vol))).cuda()
-            reqs.append((gi, geom, nc, kappa, b, "f16" if k % 2 == 0 else "f32"))
+            reqs.append((gi, geom, nc, kappa, b, "f16" if k % 2 == 0 else "f32", None))
+        if gi in (0, 2):  # a shifted request: (Q^2 + sigma) x = b for three shifts
+            reqs.append((gi, geom, nc, kappa, b, "f64", [0.0, 0.05, 0.5]))
     boundary_conditions.set_antiperiodic_field_in_t_direction((4, 4, 4, 8))
 
     def make(r):
-        gi, geom, nc, kappa, b, prec = r
-        return serving.SolveRequest(f"g{gi}", geom, nc, kappa, b, gauge=gauges[gi], tol=1e-10, precision=prec)
+        gi, geom, nc, kappa, b, prec, shifts = r
+        return serving.SolveRequest(f"g{gi}", geom, nc, kappa, b, gauge=gauges[gi], tol=1e-10, precision=prec,
+                                    shifts=shifts)
 
     alone = []
     srv = serving.SolveServer(hbm_budget_bytes=8 << 30, workers=1)
@@ -130,9 +134,12 @@ def test_same_answer_alone_and_in_the_mix(cuda_device):
     futs = [srv.submit(make(r)) for r in reqs]
     mixed = [f.result(timeout=300) for f in futs]
     srv.close()
-    for a, m in zip(alone, mixed):
+    for r, a, m in zip(reqs, alone, mixed):
         assert a.status == serving.OK and m.status == serving.OK
+        assert all(rep["true_residual"] <= 1e-10 for rep in m.reports)
         xa, xm = a.x.cpu().numpy(), m.x.cpu().numpy()
         assert np.linalg.norm(xa - xm) / np.linalg.norm(xa) < 1e-8
+        if r[6] is not None:
+            assert xm.shape[0] == len(r[6]) and m.request.solves == len(r[6])
     st = srv.stats()
     assert st["completed"] == len(reqs) and st["p99_ms"] >= st["p50_ms"]

@@ -19,6 +19,8 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include "lym_eo.cuh"
@@ -620,6 +622,7 @@ struct CgOps {
   void (*dslash)(Work&, cudaStream_t);                  // s_o = H_oe p_e, every rhs
   void (*rnew)(Work&, cudaStream_t);                    // r = M^dag t (sloppy), masked, |r|^2 -> res
   void (*copy_rp)(Work&, cudaStream_t);                 // p = r, masked (restart)
+  void (*preload)();                                    // load the iteration kernels before a capture
 };
 // kernels one iterate() call launches
 constexpr int kLaunchesPerIteration = 6;
@@ -689,6 +692,9 @@ struct Work {
   HopGauge hg64, hgs, hgs_c, hgs_f;  // hgs: the links of the selected candidate
   CgOps ops{};
   cudaGraphExec_t graph = nullptr;
+  cudaGraph_t rec = nullptr;          // graph being recorded by build_graph (explicit kernel nodes)
+  cudaGraphNode_t rec_last = nullptr;  // its last node (each launch depends on the previous one)
+  cudaError_t rec_err = cudaSuccess;
   int graph_chunk = 0;
   double graph_kappa = 0;
   int graph_cand = -1;
@@ -697,6 +703,36 @@ struct Work {
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   int64_t launches = 0;           // kernels launched by the current call (graph nodes included)
 };
+
+// Launch a kernel, or, while build_graph records (w.rec set), append it to the
+// graph as a kernel node after the previous one.  Recording builds the graph
+// with explicit nodes instead of stream capture, so nothing is ever capturing:
+// another thread's first launch of a lazily loaded kernel (a library or a torch
+// kernel) cannot collide with a capture in progress.
+template <typename... KArgs, typename... Args>
+static void launch(Work& w, cudaStream_t st, void (*kernel)(KArgs...), dim3 grid, dim3 block, Args&&... args) {
+  if (!w.rec) {
+    kernel<<<grid, block, 0, st>>>(std::forward<Args>(args)...);
+    return;
+  }
+  std::tuple<KArgs...> vals(std::forward<Args>(args)...);
+  void* ptrs[sizeof...(KArgs)];
+  std::apply([&](auto&... v) {
+    int i = 0;
+    ((ptrs[i++] = (void*)&v), ...);
+  }, vals);
+  cudaKernelNodeParams p{};
+  p.func = (void*)kernel;
+  p.gridDim = grid;
+  p.blockDim = block;
+  p.sharedMemBytes = 0;
+  p.kernelParams = ptrs;
+  cudaGraphNode_t node = nullptr;
+  const cudaError_t e = cudaGraphAddKernelNode(&node, w.rec, w.rec_last ? &w.rec_last : nullptr,
+                                               w.rec_last ? 1 : 0, &p);
+  if (e != cudaSuccess && w.rec_err == cudaSuccess) w.rec_err = e;
+  if (e == cudaSuccess) w.rec_last = node;
+}
 
 template <int ND, int NC, int SP, bool COMP, int R, int MX>
 struct Impl {
@@ -710,14 +746,17 @@ struct Impl {
   static void iterate(Work& w, cudaStream_t st) {
     const double k2 = w.kappa * w.kappa;
     dim3 grid(w.nblk, w.nrhs), tile(w.nblk, w.nrhs / R);
-    cg_hop_kernel<ND, NC, SP, GP, COMP, false, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.p, w.s, 1, w.st);
-    cg_t_kernel<ND, NC, SP, GP, COMP, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st,
-                                                                   w.partials, w.counters, w.nblk);
-    cg_hop_kernel<ND, NC, SP, GP, COMP, true, R, MX><<<tile, 128, 0, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, w.st);
-    cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX><<<tile, 128, 0, st>>>(
-        w.g->geom, w.hgs, w.s, w.t, w.p, w.xs, w.r, k2, w.st, w.partials, w.counters, w.nblk);
-    cg_p_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.r, w.p, w.st);
-    cg_settle_kernel<<<(w.nrhs + 63) / 64, 64, 0, st>>>(w.nrhs, w.st);
+    const CGState* cst = w.st;
+    launch(w, st, cg_hop_kernel<ND, NC, SP, GP, COMP, false, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.p, w.s, 1,
+           cst);
+    launch(w, st, cg_t_kernel<ND, NC, SP, GP, COMP, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.s, w.p, w.t, k2,
+           w.st, w.partials, w.counters, w.nblk);
+    launch(w, st, cg_hop_kernel<ND, NC, SP, GP, COMP, true, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.t, w.s, 1,
+           cst);
+    launch(w, st, cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.s, w.t,
+           w.p, w.xs, w.r, k2, w.st, w.partials, w.counters, w.nblk);
+    launch(w, st, cg_p_kernel<SP, NCOMP>, grid, dim3(128), w.Vh, w.r, w.p, w.st);
+    launch(w, st, cg_settle_kernel, dim3((w.nrhs + 63) / 64), dim3(64), w.nrhs, w.st);
   }
 
   static void hop64(Work& w, int par, const EoField& in, const EoField& out, const EoField& z0, const EoField& z1,
@@ -786,9 +825,21 @@ struct Impl {
     w.launches += 1;
     copy_sp_kernel<SP, NCOMP><<<grid, 128, 0, st>>>(w.Vh, w.r, w.p, w.upd);
   }
+  // Loads every kernel iterate() launches (with lazily loaded modules a kernel's
+  // code is loaded at its first use) before build_graph records them.
+  static void preload() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, cg_hop_kernel<ND, NC, SP, GP, COMP, false, R, MX>);
+    cudaFuncGetAttributes(&a, cg_hop_kernel<ND, NC, SP, GP, COMP, true, R, MX>);
+    cudaFuncGetAttributes(&a, cg_t_kernel<ND, NC, SP, GP, COMP, R, MX>);
+    cudaFuncGetAttributes(&a, cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX>);
+    cudaFuncGetAttributes(&a, cg_p_kernel<SP, NCOMP>);
+    cudaFuncGetAttributes(&a, cg_settle_kernel);
+  }
+
   static CgOps table() {
     return CgOps{&iterate, &hop64, &to_eo, &from_eo, &norm64, &convert, &accumulate, &zero64, &dslash, &rnew,
-                 &copy_rp};
+                 &copy_rp, &preload};
   }
 };
 
@@ -1019,20 +1070,31 @@ static int build_graph(Work& w, int chunk, cudaStream_t st) {
     cudaGraphExecDestroy(w.graph);
     w.graph = nullptr;
   }
-  cudaGraph_t graph;
-  LYM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < chunk; ++i) w.ops.iterate(w, st);
-  cudaError_t e = cudaStreamEndCapture(st, &graph);
-  if (e != cudaSuccess) {
-    set_error("graph capture: %s", cudaGetErrorString(e));
-    return LYM_ERR_CUDA;
+  w.ops.preload();
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaGraphCreate(&graph, 0);
+  if (e == cudaSuccess) {
+    w.rec = graph;
+    w.rec_last = nullptr;
+    w.rec_err = cudaSuccess;
+    for (int i = 0; i < chunk; ++i) w.ops.iterate(w, st);
+    w.rec = nullptr;
+    e = w.rec_err;
   }
-  e = cudaGraphInstantiate(&w.graph, graph, 0);
-  cudaGraphDestroy(graph);
+  if (e == cudaSuccess) {
+    e = cudaGraphInstantiate(&w.graph, graph, 0);
+    if (e != cudaSuccess) w.graph = nullptr;
+  }
+  if (graph) cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
-    w.graph = nullptr;
-    set_error("graph instantiate: %s", cudaGetErrorString(e));
-    return LYM_ERR_CUDA;
+    // a graph that could not be built leaves nothing launched; the solve runs
+    // the same kernels as plain launches instead (w.graph stays null)
+    cudaGetLastError();
+    w.graph_chunk = chunk;
+    w.graph_cand = w.cur;
+    w.graph_kappa = w.kappa;
+    w.graph_stream = st;
+    return LYM_OK;
   }
   w.graph_chunk = chunk;
   w.graph_cand = w.cur;
@@ -1243,7 +1305,12 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     if (!any_active) break;
     // run chunks until every rhs paused, finished or hit max_iter
     while (true) {
-      LYM_CUDA(cudaGraphLaunch(w.graph, st));
+      if (w.graph) {
+        LYM_CUDA(cudaGraphLaunch(w.graph, st));
+      } else {
+        for (int i = 0; i < chunk; ++i) w.ops.iterate(w, st);
+        LYM_CHECK_LAUNCH();
+      }
       w.launches += (int64_t)chunk * kLaunchesPerIteration;
       LYM_CUDA(cudaMemcpyAsync(w.st_host, w.st, sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
       LYM_CUDA(cudaStreamSynchronize(st));

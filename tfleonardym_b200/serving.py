@@ -1,7 +1,7 @@
 """Solve server: continuous batching of Wilson solve requests on one GPU.
 
-Requests of different geometry, N, kappa, tolerance and precision arrive at any
-time (``submit`` returns a future).  Each request is admitted by its HBM
+Requests of different geometry, N, kappa, tolerance, precision and shift count
+arrive at any time (``submit`` returns a future).  Each request is admitted by its HBM
 footprint against a byte budget: a request that could never fit is rejected
 (status REJECTED); one that fits but finds the budget in use waits in the
 queue and is admitted as earlier requests finish and free their bytes.
@@ -13,9 +13,11 @@ request and batch every other pending request that shares its gauge, kappa,
 tolerance, precision and operator form into one multi-right-hand-side solve
 (``lym_wilson_solve``), up to ``max_batch`` right-hand sides.  Requests that
 arrive while a batch runs join the next batch, and batches of different
-gauges run concurrently on different streams.  Every answer carries the FP64
-true residual the solver verified; a request whose residual misses its
-tolerance completes with status NOT_CONVERGED.
+gauges run concurrently on different streams.  A request with ``shifts``
+solves (Q^2 + sigma_k) x_k = b for all its shifts in one multishift CG
+(lym_multishift_solve, FP64) and is served on its own.  Every answer carries
+the FP64 true residual (recomputed here for the shifted systems); a request
+whose residual misses its tolerance completes with status NOT_CONVERGED.
 
 Latency bookkeeping: ``submit`` time, admission time, start and end of the
 batch that served the request.
@@ -35,18 +37,20 @@ OK, NOT_CONVERGED, REJECTED = "ok", "not_converged", "rejected"
 
 
 class SolveRequest:
-    """One solve of D x = b (or Q x = b when ``hermitian``) on a gauge field.
+    """One solve of D x = b (or Q x = b when ``hermitian``) on a gauge field, or,
+    with ``shifts``, of (Q^2 + sigma_k) x_k = b for every shift (Q = gamma_d D).
 
     ``gauge_key`` names the configuration for the resident cache; ``gauge``
     (complex128 (nd, N, N, V) CUDA tensor or a zero-argument callable
     producing it) is only used when the key is not cached.  ``b`` is one
-    spinor (ns, N, V) or several (k, ns, N, V) on the device.
+    spinor (ns, N, V) or several (k, ns, N, V) on the device (one spinor for a
+    shifted request; its solution is (nshift, ns, N, V)).
     """
 
     _ids = itertools.count()
 
     def __init__(self, gauge_key, geometry, nc, kappa, b, gauge=None, tol=1e-10, precision="f16",
-                 hermitian=False, bc=-1.0, max_iter=5000, out=None):
+                 hermitian=False, bc=-1.0, max_iter=5000, out=None, shifts=None):
         self.id = next(self._ids)
         self.gauge_key = gauge_key
         self.geometry = tuple(int(g) for g in geometry)
@@ -61,10 +65,23 @@ class SolveRequest:
         self.max_iter = int(max_iter)
         self.out = out  # optional tensor (e.g. pinned host memory) the solution is copied into
         self.nrhs = 1 if b.dim() == 3 else int(b.shape[0])
+        self.shifts = None if shifts is None else [float(s) for s in shifts]
+        if self.shifts is not None:
+            if self.nrhs != 1 or any(s < 0 for s in self.shifts):
+                raise ValueError("a shifted request takes one source and shifts >= 0")
+            self.hermitian = True
+            self.precision = "f64"
         self.t_submit = self.t_admit = self.t_start = self.t_end = None
         self.future = concurrent.futures.Future()
 
+    @property
+    def solves(self):
+        """Linear systems the request solves (right-hand sides x shifts)."""
+        return self.nrhs * (len(self.shifts) if self.shifts is not None else 1)
+
     def batch_key(self):
+        if self.shifts is not None:
+            return ("multishift", self.id)  # served on its own
         return (self.gauge_key, self.kappa, self.tol, self.precision, self.hermitian, self.bc)
 
 
@@ -81,14 +98,19 @@ class SolveResult:
         return r.t_end - r.t_submit
 
 
-def footprint_bytes(geometry, nc, nrhs, precision="f16", with_gauge=True):
+def footprint_bytes(geometry, nc, nrhs, precision="f16", with_gauge=True, nshift=0):
     """Device bytes a request occupies: its sources and solutions, its share of
-    the solver workspace and (when not resident yet) the gauge copies."""
+    the solver workspace and (when not resident yet) the gauge copies.  A
+    shifted request holds nshift solutions and search vectors plus a few
+    full-lattice FP64 work vectors."""
     vol = int(np.prod(geometry))
     nd = len(geometry)
     ns = 2 if nd == 2 else 4
     ncomp = ns * nc
     spin = vol * ncomp * 16
+    if nshift:
+        link = nd * nc * nc * vol * 16
+        return int((2 * nshift + 6) * spin + (3 * link if with_gauge else 0))
     sloppy = {"f64": 16, "f32": 8, "f16": 4 + 4 / ncomp, "bf16": 4 + 4 / ncomp}[precision]
     per_rhs = 2 * spin + 7 * spin / 2 + 5 * (vol / 2) * ncomp * sloppy
     gauge = 0
@@ -185,7 +207,8 @@ class SolveServer:
     # -- internals ------------------------------------------------------------
     def _request_bytes(self, req):
         resident = req.gauge_key in self._gauges
-        return footprint_bytes(req.geometry, req.nc, req.nrhs, req.precision, with_gauge=not resident)
+        return footprint_bytes(req.geometry, req.nc, req.nrhs, req.precision, with_gauge=not resident,
+                               nshift=len(req.shifts) if req.shifts is not None else 0)
 
     def _admit(self, req):
         self._in_use += req._bytes
@@ -272,10 +295,43 @@ class SolveServer:
             finally:
                 self._release(batch)
 
+    def _solve_shifted(self, req, g, widx):
+        """(Q^2 + sigma_k) x_k = b by multishift CG, then each true residual in FP64."""
+        from . import _dev, dirac, dirac_solver
+        dev = torch.device("cuda", self.device)
+        b = (req.b if req.b.dim() == 3 else req.b[0]).to(dev, non_blocking=True)
+        op = g.op_for(widx, req.kappa, True)
+        ms = dirac_solver.multishift_cg(req.max_iter, req.tol)
+        xs = ms.solve(dirac.SquareOperator(op), b, req.shifts)
+        bn = float(np.sqrt(abs(_dev.cdot(b, b))))
+        reports = []
+        for s, x in zip(req.shifts, xs):
+            r = _dev.axpby(1.0, b, -1.0, _dev.axpby(1.0, op.apply(op.apply(x)), s, x))
+            res = float(np.sqrt(abs(_dev.cdot(r, r)))) / bn
+            reports.append(dict(status=0, iterations=ms.last_steps, true_residual=res, shift=s))
+        x = torch.stack(xs)
+        if req.out is not None:
+            req.out.copy_(x, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return x, reports
+
     def _solve_batch(self, batch, widx=0):
         from . import dirac_solver
         first = batch[0]
         g = self._gauge_for(first)
+        if first.shifts is not None:
+            try:
+                x, reps = self._solve_shifted(first, g, widx)
+            finally:
+                with self._lock:
+                    g.users -= 1
+            first.t_end = time.perf_counter()
+            ok = all(m["true_residual"] <= first.tol for m in reps)
+            res = SolveResult(first, first.out if first.out is not None else x, OK if ok else NOT_CONVERGED, reps)
+            res.batch_rhs = 1
+            self.completed.append(res)
+            first.future.set_result(res)
+            return
         dev = torch.device("cuda", self.device)
         host = not first.b.is_cuda
         try:
