@@ -44,7 +44,7 @@ TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dslash_eo_f16_16x16x16x16_traffic
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lym", choices=["lym", "reference"])
     ap.add_argument("--nrhs", type=int, default=16)
@@ -71,6 +71,10 @@ def parse_args():
                     help="serving under an open-loop Poisson stream of mixed requests (D, N, geometry, kappa, "
                          "rhs count, shifts, tolerance, gauge reuse), one JSON line per rate, then the same "
                          "requests as plain FP64 one-at-a-time solves")
+    ap.add_argument("--batch-lattices", action="store_true",
+                    help="64 independent lattices of uneven geometry, 4 rhs each, solved together through the "
+                         "solve server (FP32 inner / FP64 outer, 1e-10), plus one gauge HMC step per lattice; "
+                         "one JSON line")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per rate")
     ap.add_argument("--serve-max-requests", type=int, default=600)
@@ -796,6 +800,99 @@ def run_serve_sweep(args, local_rank):
     return 0
 
 
+def run_batch_lattices(args, local_rank):
+    """64 independent lattices -- 2D SU(2) from 8^2 to 64^2 and 4D SU(3) from 8^4 to
+    12^3 x 24 (the even-odd solver has no D = 3, so the 3D SU(2) third of the mix
+    is 2D SU(2) here), kappa in [0.10, 0.14], links reunit(exp(i eps H)) with eps in
+    [0.1, 0.4] -- with 4 unit complex Gaussian rhs each (256 solves), submitted
+    together to the solve server (4 workers, one CUDA stream each) with FP32 inner
+    and FP64 outer iterations to true relative residual 1e-10.  Then the same 256
+    solves as plain FP64 one-at-a-time solves, and one gauge HMC step per lattice
+    (staples and force fused into the momentum update, then the link update).
+    Device time of each phase by CUDA events around it (the server's streams are
+    joined by a device synchronise)."""
+    import torch
+
+    from tfleonardym_b200 import dirac_solver, gauge_action, hmc, serving
+    from tfleonardym_b200 import lattice as lt
+    dirac_solver.VERBOSE = False
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    rng = np.random.default_rng(44)
+    lattices = []
+    for i in range(64):
+        if i % 2 == 0:
+            n = int(2 * round(np.exp(rng.uniform(np.log(8), np.log(64))) / 2))
+            m = int(2 * round(np.exp(rng.uniform(np.log(8), np.log(64))) / 2))
+            geom, nc = (n, m), 2
+        else:
+            geom = tuple(int(rng.choice([8, 10, 12])) for _ in range(3)) + (int(rng.choice([8, 12, 16, 20, 24])),)
+            nc = 3
+        lattices.append(dict(geometry=geom, nc=nc, kappa=float(rng.uniform(0.10, 0.14)),
+                             eps=float(rng.uniform(0.1, 0.4)), seed=int(rng.integers(1 << 30))))
+    gauges = [_device_links(l["geometry"], l["nc"], l["eps"], l["seed"], dev) for l in lattices]
+    sources = []
+    for l in lattices:
+        nd, vol = len(l["geometry"]), int(np.prod(l["geometry"]))
+        ns = 2 if nd == 2 else 4
+        g = torch.Generator(device=dev)
+        g.manual_seed(l["seed"] + 1)
+        sources.append(torch.complex(torch.randn((4, ns, l["nc"], vol), generator=g, device=dev, dtype=torch.float64),
+                                     torch.randn((4, ns, l["nc"], vol), generator=g, device=dev, dtype=torch.float64))
+                       / np.sqrt(2))
+    budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
+
+    def solve_all(precision, workers, max_batch):
+        srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=local_rank)
+        futs = []
+        for k, l in enumerate(lattices):
+            reqs = [sources[k]] if max_batch >= 4 else [sources[k][j] for j in range(4)]
+            for b in reqs:
+                futs.append(srv.submit(serving.SolveRequest(f"lat{k}", l["geometry"], l["nc"], l["kappa"], b,
+                                                            gauge=gauges[k], tol=1e-10, precision=precision,
+                                                            bc=-1.0, max_iter=4000)))
+        res = [f.result() for f in futs]
+        srv.close()
+        return res
+
+    solve_all("f32", 4, 16)  # warm-up: workspaces, autotuning, graphs
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = solve_all("f32", 4, 16)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ok = sum(r.status == serving.OK for r in res)
+    worst = max(m["true_residual"] for r in res for m in r.reports)
+    solve_all("f64", 1, 1)  # warm-up of the plain path
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = solve_all("f64", 1, 1)
+    torch.cuda.synchronize()
+    plain_wall = time.perf_counter() - t0
+    # one gauge HMC step per lattice: P += eps F (fused), U <- exp(eps P) U
+    stream = torch.cuda.current_stream()
+    cfgs = [lt.Configuration(g, l["geometry"], l["nc"], len(l["geometry"])) for g, l in zip(gauges, lattices)]
+    moms = [hmc.random_momenta(l["nc"], len(l["geometry"]), int(np.prod(l["geometry"]))) for l in lattices]
+    acts = [gauge_action.yang_mills(c, 5.6 if l["nc"] == 3 else 2.3) for c, l in zip(cfgs, lattices)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for rep in range(2):
+        e0.record(stream)
+        for c, p, a in zip(cfgs, moms, acts):
+            p2 = hmc._apply_force(a, p, -0.05)
+            hmc.update_link_field(c.gauge_field, p2, 0.05)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    print(json.dumps({"batch_lattices": "64 uneven lattices x 4 rhs", "solves": 256, "ok": ok,
+                      "worst_true_residual": worst, "wall_s": wall, "solves_per_s": 256 / wall,
+                      "plain_fp64_one_at_a_time": {"ok": sum(r.status == serving.OK for r in plain),
+                                                   "wall_s": plain_wall, "solves_per_s": 256 / plain_wall},
+                      "gauge_hmc_step_all_lattices_ms": e0.elapsed_time(e1),
+                      "config": {"lattices": "32 x 2D SU(2) 8^2..64^2 + 32 x 4D SU(3) 8^4..12^3x24",
+                                 "inner_precision": "f32", "outer_precision": "f64", "tol": 1e-10,
+                                 "server_workers": 4, "max_batch_rhs": 16}}), flush=True)
+    return 0
+
+
 def run_hmc(args, rank, world, local_rank):
     """HMC on 4D SU(3) 16^4: beta = 5.6, Nf = 2 Wilson fermions at kappa = 0.13
     (pseudofermion phi = Q eta, Q = gamma_d D, antiperiodic time), links
@@ -885,6 +982,8 @@ def main():
         return run_hmc(args, rank, world, local_rank)
     if args.serve_sweep:
         return run_serve_sweep(args, local_rank)
+    if args.batch_lattices:
+        return run_batch_lattices(args, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if world > 1:

@@ -580,13 +580,16 @@ __global__ void __launch_bounds__(128) copy_sp_kernel(int64_t Vh, EoField src, E
   store_sp<SP, NCOMP>(dst, rhs, cb, v);
 }
 
-// p = r + beta p
+// p = r + beta p; the last block of each rhs to finish then turns the "stop
+// after the p update" marker (active == 2) into a pause.  Every block of the rhs
+// read `active` before it counted itself, so the last one may change it.
 template <int SP, int NCOMP>
-__global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoField p, CGState* st) {
+__global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoField p, CGState* st,
+                                                   unsigned* counters) {
   const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int rhs = blockIdx.y;
   const int act = st[rhs].active;
-  if (!act) return;
+  if (!act) return;  // uniform per rhs
   if (cb < Vh) {
     using R = typename Prec<SP>::real;
     const R b = (R)st[rhs].beta;
@@ -597,12 +600,14 @@ __global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoFiel
     for (int k = 0; k < NCOMP; ++k) pv[k] = rv[k] + b * pv[k];
     store_sp<SP, NCOMP>(p, rhs, cb, pv);
   }
-}
-
-// turns the "stop after the p update" marker into a pause; one thread per rhs
-__global__ void cg_settle_kernel(int nrhs, CGState* st) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < nrhs && st[r].active == 2) st[r].active = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(counters + rhs, 1u) == gridDim.x - 1) {
+      if (act == 2) st[rhs].active = 0;
+      counters[rhs] = 0u;  // ready for the next use of this slot
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -625,7 +630,7 @@ struct CgOps {
   void (*preload)();                                    // load the iteration kernels before a capture
 };
 // kernels one iterate() call launches
-constexpr int kLaunchesPerIteration = 6;
+constexpr int kLaunchesPerIteration = 5;
 // solver workspaces a gauge object keeps, keyed by (precision, nrhs)
 constexpr size_t kMaxWorkspaces = 4;
 
@@ -755,8 +760,7 @@ struct Impl {
            cst);
     launch(w, st, cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.s, w.t,
            w.p, w.xs, w.r, k2, w.st, w.partials, w.counters, w.nblk);
-    launch(w, st, cg_p_kernel<SP, NCOMP>, grid, dim3(128), w.Vh, w.r, w.p, w.st);
-    launch(w, st, cg_settle_kernel, dim3((w.nrhs + 63) / 64), dim3(64), w.nrhs, w.st);
+    launch(w, st, cg_p_kernel<SP, NCOMP>, grid, dim3(128), w.Vh, w.r, w.p, w.st, w.counters);
   }
 
   static void hop64(Work& w, int par, const EoField& in, const EoField& out, const EoField& z0, const EoField& z1,
@@ -834,7 +838,6 @@ struct Impl {
     cudaFuncGetAttributes(&a, cg_t_kernel<ND, NC, SP, GP, COMP, R, MX>);
     cudaFuncGetAttributes(&a, cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX>);
     cudaFuncGetAttributes(&a, cg_p_kernel<SP, NCOMP>);
-    cudaFuncGetAttributes(&a, cg_settle_kernel);
   }
 
   static CgOps table() {

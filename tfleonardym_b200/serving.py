@@ -223,14 +223,28 @@ class SolveServer:
                 self._admit(self._waiting.popleft())
             self._lock.notify_all()
 
-    def _take_batch(self):
-        """Oldest pending request plus every compatible pending one, up to max_batch rhs."""
+    # how far past the oldest pending request a worker looks for one whose gauge it
+    # already serves (its operator, solver workspace and CUDA graphs exist)
+    AFFINITY_LOOKAHEAD = 8
+
+    def _take_batch(self, widx=None):
+        """Oldest pending request -- or, within the next AFFINITY_LOOKAHEAD, the oldest
+        whose gauge this worker already holds -- plus every compatible pending one,
+        up to max_batch rhs."""
         with self._lock:
             while not self._pending and not (self._closed and not self._waiting):
                 self._lock.wait(timeout=0.05)
             if not self._pending:
                 return None
-            first = self._pending.popleft()
+            pick = 0
+            if widx is not None:
+                for k, r in enumerate(itertools.islice(self._pending, self.AFFINITY_LOOKAHEAD)):
+                    g = self._gauges.get(r.gauge_key)
+                    if g is not None and widx in g.ops:
+                        pick = k
+                        break
+            first = self._pending[pick]
+            del self._pending[pick]
             key = first.batch_key()
             batch, rhs = [first], first.nrhs
             keep = collections.deque()
@@ -278,7 +292,7 @@ class SolveServer:
         torch.cuda.set_device(self.device)
         stream = torch.cuda.Stream(device=torch.device("cuda", self.device))
         while True:
-            batch = self._take_batch()
+            batch = self._take_batch(widx)
             if batch is None:
                 return
             t0 = time.perf_counter()
