@@ -229,6 +229,18 @@ def read_traffic():
     return None
 
 
+def workload_config(args, world):
+    """The workload both arms report (the reference arm solves the same systems with
+    the oracle port of the reference's algorithm on the host cores)."""
+    return {"workload": "served wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
+            "step": f"{args.nrhs} single-rhs requests", "max_batch_rhs": args.nrhs, "server_workers": args.workers,
+            "inner_precision": args.precision, "outer_precision": "f64",
+            "reliable_update_delta": args.delta, "graph_chunk": args.chunk,
+            "links": "reunit(exp(i 0.25 H)), H traceless Hermitian", "bc": "antiperiodic time",
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (the sources and solutions of the timed requests exceed 126 MB)"}
+
+
 def _ref_worker(args):
     seconds, seed = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
@@ -256,8 +268,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
         "data": "synthetic", "scaling": "weak", "vs_baseline": None,
-        "config": {"workload": "wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
-                   "links": "reunit(exp(i 0.25 H))", "bc": "antiperiodic time"},
+        "config": workload_config(args, world),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "port",
                          "sample": f"{procs} processes x CG iterations of the oracle's even-odd CGNR on 16^4 "
                                    f"(about {max(1.0, args.cpu_seconds / 4):.0f} s each per step), extrapolated "
@@ -497,13 +508,7 @@ def run_lym(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": f"{args.precision}+f64",
         "data": "synthetic",
-        "config": {"workload": "served wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
-                   "step": f"{B} single-rhs requests", "max_batch_rhs": B, "server_workers": args.workers,
-                   "inner_precision": args.precision, "outer_precision": "f64",
-                   "reliable_update_delta": args.delta, "graph_chunk": args.chunk,
-                   "links": "reunit(exp(i 0.25 H)), H traceless Hermitian", "bc": "antiperiodic time",
-                   "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (the sources and solutions of the timed requests exceed 126 MB)"},
+        "config": workload_config(args, world),
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                        "what": f"request latency, Poisson arrivals at {rate:.0f} req/s (half the saturated rate)"},
         "batch_rhs_seen": batch_sizes,
