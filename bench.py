@@ -229,6 +229,22 @@ def read_traffic():
     return None
 
 
+def max_over_ranks(ms, world, device):
+    """The slowest rank's time (every rank takes the same collective step)."""
+    if world == 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, units_per_rank, max_ms):
+    """Whole-job rate of `world` independent replicas: all units over the slowest rank's time."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
 def workload_config(args, world):
     """The workload both arms report (the reference arm solves the same systems with
     the oracle port of the reference's algorithm on the host cores)."""
@@ -399,12 +415,8 @@ def run_lym(args, rank, world, local_rank):
     barrier()
     t_wall = time.perf_counter() - t_wall
     clk = clocks.stop()
-    total_ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps * B / (total_ms / 1e3)
+    total_ms = max_over_ranks(ev0.elapsed_time(ev1), world, dev)
+    value = replica_throughput(world, args.steps * B, total_ms)
     launches = sum(r.reports[0]["kernel_launches"] / r.batch_rhs for r in res)
     iters = [m["iterations"] for r in res for m in r.reports]
     rupd = [m["reliable_updates"] for r in res for m in r.reports]
@@ -425,12 +437,8 @@ def run_lym(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ev3.record(stream)
     ev3.synchronize()
-    e2e_total = ev2.elapsed_time(ev3)
-    if world > 1:
-        t = torch.tensor([e2e_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * n_e2e / (e2e_total / 1e3)
+    e2e_total = max_over_ranks(ev2.elapsed_time(ev3), world, dev)
+    e2e_value = replica_throughput(world, n_e2e, e2e_total)
     srv.close()
 
     # ---- the same solves as direct batched calls (no server) ----
