@@ -54,6 +54,7 @@ def parse_args():
     ap.add_argument("--delta", type=float, default=0.01, help="reliable-update trigger of the mixed solver")
     ap.add_argument("--chunk", type=int, default=8, help="CG iterations per captured graph launch")
     ap.add_argument("--workers", type=int, default=2, help="solve-server worker streams")
+    ap.add_argument("--max-batch", type=int, default=0, help="solve-server batch limit in rhs (0: --nrhs)")
     ap.add_argument("--rhs-per-thread", type=int, default=0, help="hop-kernel tile (0: autotune)")
     ap.add_argument("--compressed-links", type=int, default=0, help="with a forced tile: 1 = N-1-row links")
     ap.add_argument("--mixed-fma", type=int, default=0,
@@ -249,7 +250,8 @@ def workload_config(args, world):
     """The workload both arms report (the reference arm solves the same systems with
     the oracle port of the reference's algorithm on the host cores)."""
     return {"workload": "served wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
-            "step": f"{args.nrhs} single-rhs requests", "max_batch_rhs": args.nrhs, "server_workers": args.workers,
+            "step": f"{args.nrhs} single-rhs requests", "max_batch_rhs": args.max_batch or args.nrhs,
+            "server_workers": args.workers,
             "inner_precision": args.precision, "outer_precision": "f64",
             "reliable_update_delta": args.delta, "graph_chunk": args.chunk,
             "links": "reunit(exp(i 0.25 H)), H traceless Hermitian", "bc": "antiperiodic time",
@@ -370,7 +372,7 @@ def run_lym(args, rank, world, local_rank):
     # server (continuous batching, up to nrhs per batch); sources resident
     from tfleonardym_b200 import serving
     budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
-    srv = serving.SolveServer(budget, max_batch=B, workers=args.workers, device=local_rank,
+    srv = serving.SolveServer(budget, max_batch=args.max_batch or B, workers=args.workers, device=local_rank,
                               solver_options=dict(delta=args.delta, chunk=args.chunk,
                                                   rhs_per_thread=args.rhs_per_thread,
                                                   mixed_fma=args.mixed_fma,
