@@ -76,6 +76,10 @@ def parse_args():
                     help="64 independent lattices of uneven geometry, 4 rhs each, solved together through the "
                          "solve server (FP32 inner / FP64 outer, 1e-10), plus one gauge HMC step per lattice; "
                          "one JSON line")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="24^3x48 SU(3), eps 0.3, kappa 0.12 and 0.13, 8 rhs: the even-odd CG with FP64 / FP32 / "
+                         "FP16 / BF16 inner iterations against the FP64 solution, and the FP64 multishift CG on "
+                         "Q^2 + sigma_k with the reference's 17-pole rational approximation; one JSON line per case")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per rate")
     ap.add_argument("--serve-max-requests", type=int, default=600)
@@ -908,6 +912,89 @@ def run_batch_lattices(args, local_rank):
     return 0
 
 
+# shifts of the reference's metropolis rational approximation: the second half of
+# metropolis_rational_approximation_coefficients (approximations.py:127-139), which the
+# reference's driver passes as the betas of RationalApproximation (TfLeonardYMNDim.py:326-332)
+REFERENCE_17_POLES = [708.456969133708774250236839, 20.5545836704482543092111935, 5.16460586130848066092696251,
+                      1.77335742461795338089518681, 0.663483773139054161068555408, 0.251260388600611110026798526,
+                      0.0933210176761593454438480966, 0.0334329670158591978976640839,
+                      0.0114225244703120473204264627, 0.00368309198965533868820332893,
+                      0.00110757598877812519195949185, 0.000305911192767903423411472490,
+                      0.0000759625965715284538520399041, 0.0000164241384694373051997536552,
+                      0.00000293320679744054879906466158, 0.000000390128040236098295575734048,
+                      0.0000000269253347571438797470449799]
+
+
+def run_precision_study(args, local_rank):
+    """BASELINE config 3 as far as it is built: on 24^3 x 48 SU(3) (links
+    reunit(exp(i 0.3 H)), antiperiodic time) at kappa 0.12 and 0.13, 8 unit complex
+    Gaussian rhs: (a) the even-odd CG to true relative residual 1e-10 with FP64, FP32,
+    FP16 and BF16 inner iterations (FP64 reliable updates), each solution's relative
+    difference to the FP64 one; (b) the FP64 multishift CG on Q^2 + sigma_k (Q = gamma_d D)
+    for the 17 shifts of the reference's metropolis rational approximation, per-shift
+    FP64 true residual.  The mixed-precision multishift of the configuration is not
+    built (shifted systems run in FP64 only)."""
+    import torch
+
+    from tfleonardym_b200 import boundary_conditions, dirac, dirac_solver
+    from tfleonardym_b200 import lattice as lt
+    dirac_solver.VERBOSE = False
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    geom = (24, 24, 24, 48)
+    nd, vol = 4, int(np.prod(geom))
+    links = _device_links(geom, NC, 0.3, 2026, dev)
+    cfg = lt.Configuration(links, geom, NC, nd)
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    b = torch.complex(torch.randn((8, 4, NC, vol), generator=g, device=dev, dtype=torch.float64),
+                      torch.randn((8, 4, NC, vol), generator=g, device=dev, dtype=torch.float64)) / np.sqrt(2)
+    stream = torch.cuda.current_stream()
+    prov = boundary_conditions.time_antiperiodic_provider(-1)
+    for kappa in (0.12, 0.13):
+        op = dirac.DiracWilsonOperator(cfg, kappa, False, representation="fundamental",
+                                       boundary_condition_provider=prov)
+        ref = None
+        for prec in ("f64", "f32", "f16", "bf16"):
+            solver = dirac_solver.conjugate_gradient(max_steps=20000, tol=1e-10, precision=prec, delta=0.01)
+            solver.solve(op, b)  # warm-up: workspace, autotuning, graphs
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            x = solver.solve(op, b)
+            e.record(stream)
+            torch.cuda.synchronize()
+            if ref is None:
+                ref = x.clone()
+            diff = [float(torch.linalg.vector_norm(x[i] - ref[i]) / torch.linalg.vector_norm(ref[i]))
+                    for i in range(8)]
+            print(json.dumps({"precision_study": "even-odd CG", "geometry": list(geom), "kappa": kappa,
+                              "inner_precision": prec, "rhs": 8, "ms": s.elapsed_time(e),
+                              "iterations": [r["iterations"] for r in solver.reports],
+                              "reliable_updates": [r["reliable_updates"] for r in solver.reports],
+                              "true_residual_max": max(r["true_residual"] for r in solver.reports),
+                              "rel_diff_to_fp64_max": max(diff)}), flush=True)
+        q = dirac.DiracWilsonOperator(cfg, kappa, True, representation="fundamental", boundary_condition_provider=prov)
+        ms_cg = dirac_solver.multishift_cg(20000, 1e-10)
+        sq = dirac.SquareOperator(q)
+        ms_cg.solve(sq, b[0], REFERENCE_17_POLES)  # warm-up
+        res, times, iters = [], [], []
+        for i in range(2):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            xs = ms_cg.solve(sq, b[i], REFERENCE_17_POLES)
+            e.record(stream)
+            torch.cuda.synchronize()
+            times.append(s.elapsed_time(e))
+            iters.append(ms_cg.last_steps)
+            bn = float(torch.linalg.vector_norm(b[i]))
+            res.append([float(torch.linalg.vector_norm(b[i] - (q.apply(q.apply(x)) + sg * x))) / bn
+                        for sg, x in zip(REFERENCE_17_POLES, xs)])
+        print(json.dumps({"precision_study": "multishift CG FP64, 17 reference shifts", "geometry": list(geom),
+                          "kappa": kappa, "rhs": 2, "ms_per_rhs": statistics.mean(times), "iterations": iters,
+                          "true_residual_per_shift_max": [max(r[k] for r in res) for k in range(17)]}), flush=True)
+    return 0
+
+
 def run_hmc(args, rank, world, local_rank):
     """HMC on 4D SU(3) 16^4: beta = 5.6, Nf = 2 Wilson fermions at kappa = 0.13
     (pseudofermion phi = Q eta, Q = gamma_d D, antiperiodic time), links
@@ -999,6 +1086,8 @@ def main():
         return run_serve_sweep(args, local_rank)
     if args.batch_lattices:
         return run_batch_lattices(args, local_rank)
+    if args.precision_study:
+        return run_precision_study(args, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if world > 1:
