@@ -52,7 +52,7 @@ def parse_args():
     ap.add_argument("--plain-solves", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--delta", type=float, default=0.01, help="reliable-update trigger of the mixed solver")
-    ap.add_argument("--chunk", type=int, default=8, help="CG iterations per captured graph launch")
+    ap.add_argument("--chunk", type=int, default=8, help="CG iterations per CUDA graph launch")
     ap.add_argument("--workers", type=int, default=2, help="solve-server worker streams")
     ap.add_argument("--max-batch", type=int, default=0, help="solve-server batch limit in rhs (0: --nrhs)")
     ap.add_argument("--rhs-per-thread", type=int, default=0, help="hop-kernel tile (0: autotune)")

@@ -149,7 +149,7 @@ typedef struct lym_solver_params {
   int precision;     /* lym_precision of the inner (sloppy) iterations          */
   double delta;      /* reliable-update trigger: sloppy |r| fell by this factor  */
   int hermitian;     /* 1: system is Q x = b with Q = gamma_d D                  */
-  int chunk;         /* iterations per captured CUDA graph launch (0 = default)  */
+  int chunk;         /* iterations per CUDA graph launch (0 = default)           */
   int rhs_per_thread;/* at most this many right-hand sides per hop-kernel thread
                         (1, 2 or 4; the largest available one is used); 0 = autotune */
   int compressed_links; /* with a forced tile (rhs_per_thread > 0): 1 = the N-1-row

@@ -7,7 +7,7 @@
 // D = 1 + kappa H (the reference sign, dirac.py:400,521),
 //   b' = b_e - kappa H_eo b_o,  M = 1 - kappa^2 H_eo H_oe,  M x_e = b',
 //   x_o = b_o - kappa H_oe x_e,  and M^dag = gamma_d M gamma_d.
-// CG runs on M^dag M x_e = M^dag b'.  Iterations run in captured CUDA graphs
+// CG runs on M^dag M x_e = M^dag b'.  Iterations run in CUDA graphs (built
 // of `chunk` iterations; all CG scalars (alpha, beta, |r|^2) stay on the
 // device and are produced by the last block of each fused reduction.  A
 // right-hand side pauses itself on the device when its sloppy residual drops
@@ -627,7 +627,7 @@ struct CgOps {
   void (*dslash)(Work&, cudaStream_t);                  // s_o = H_oe p_e, every rhs
   void (*rnew)(Work&, cudaStream_t);                    // r = M^dag t (sloppy), masked, |r|^2 -> res
   void (*copy_rp)(Work&, cudaStream_t);                 // p = r, masked (restart)
-  void (*preload)();                                    // load the iteration kernels before a capture
+  void (*preload)();                                    // load the iteration kernels before a graph is built
 };
 // kernels one iterate() call launches
 constexpr int kLaunchesPerIteration = 5;
@@ -704,7 +704,7 @@ struct Work {
   double graph_kappa = 0;
   int graph_cand = -1;
   cudaStream_t graph_stream = nullptr;
-  cudaStream_t stream = nullptr;  // solves run here (capturable even when the caller uses the legacy stream)
+  cudaStream_t stream = nullptr;  // solves run here (non-blocking, fenced to the caller's stream by events)
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   int64_t launches = 0;           // kernels launched by the current call (graph nodes included)
 };
