@@ -8,7 +8,7 @@
 //   b' = b_e - kappa H_eo b_o,  M = 1 - kappa^2 H_eo H_oe,  M x_e = b',
 //   x_o = b_o - kappa H_oe x_e,  and M^dag = gamma_d M gamma_d.
 // CG runs on M^dag M x_e = M^dag b'.  Iterations run in CUDA graphs (built
-// of `chunk` iterations; all CG scalars (alpha, beta, |r|^2) stay on the
+// from kernel nodes) of `chunk` iterations; all CG scalars (alpha, beta, |r|^2) stay on the
 // device and are produced by the last block of each fused reduction.  A
 // right-hand side pauses itself on the device when its sloppy residual drops
 // below its pause target; the host then does the FP64 reliable update
