@@ -932,8 +932,10 @@ def run_precision_study(args, local_rank):
     FP16 and BF16 inner iterations (FP64 reliable updates), each solution's relative
     difference to the FP64 one; (b) the FP64 multishift CG on Q^2 + sigma_k (Q = gamma_d D)
     for the 17 shifts of the reference's metropolis rational approximation, per-shift
-    FP64 true residual.  The mixed-precision multishift of the configuration is not
-    built (shifted systems run in FP64 only)."""
+    FP64 true residual; (c) the even-odd multishift CG on the same 17 shifts, all 8 rhs in
+    one call, inner iterations in FP64, FP32, FP16 and BF16 with FP64 reliable updates,
+    each (rhs, shift) verified by its FP64 true residual, and each shift's largest
+    relative difference to the FP64 solutions."""
     import torch
 
     from tfleonardym_b200 import boundary_conditions, dirac, dirac_solver
@@ -992,6 +994,39 @@ def run_precision_study(args, local_rank):
         print(json.dumps({"precision_study": "multishift CG FP64, 17 reference shifts", "geometry": list(geom),
                           "kappa": kappa, "rhs": 2, "ms_per_rhs": statistics.mean(times), "iterations": iters,
                           "true_residual_per_shift_max": [max(r[k] for r in res) for k in range(17)]}), flush=True)
+        # the even-odd multishift, all 8 sources in one call, inner precision swept;
+        # errors per shift against its FP64 solutions
+        ref_ms = None
+        for prec in ("f64", "f32", "f16", "bf16"):
+            ms = dirac_solver.multishift_cg(20000, 1e-10, precision=prec, delta=0.01)
+            ms.solve(sq, b, REFERENCE_17_POLES)  # warm-up: workspaces, graphs
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            xs = ms.solve(sq, b, REFERENCE_17_POLES)
+            e.record(stream)
+            torch.cuda.synchronize()
+            xs = torch.stack(xs, 1)  # (rhs, shift, ...)
+            if ref_ms is None:
+                ref_ms = xs.clone()
+            nsh = len(REFERENCE_17_POLES)
+            reps = ms.reports
+            diff = [max(float(torch.linalg.vector_norm(xs[i, k] - ref_ms[i, k]) /
+                              torch.linalg.vector_norm(ref_ms[i, k])) for i in range(8)) for k in range(nsh)]
+            # independent FP64 check of source 0 through the reference-layout operator
+            bn = float(torch.linalg.vector_norm(b[0]))
+            chk = [float(torch.linalg.vector_norm(b[0] - (q.apply(q.apply(xs[0, k])) + sg * xs[0, k]))) / bn
+                   for k, sg in enumerate(REFERENCE_17_POLES)]
+            print(json.dumps({"precision_study": "even-odd multishift CG, 17 reference shifts", "geometry": list(geom),
+                              "kappa": kappa, "inner_precision": prec, "rhs": 8, "ms": s.elapsed_time(e),
+                              "ms_per_rhs": s.elapsed_time(e) / 8,
+                              "iterations_per_shift_max": [max(reps[i * nsh + k]["iterations"] for i in range(8))
+                                                           for k in range(nsh)],
+                              "reliable_updates_max": max(r["reliable_updates"] for r in reps),
+                              "true_residual_per_shift_max": [max(reps[i * nsh + k]["true_residual"]
+                                                                  for i in range(8)) for k in range(nsh)],
+                              "rhs0_reference_layout_residual_max": max(chk),
+                              "rel_diff_to_fp64_per_shift_max": diff,
+                              "status_ok": all(r["status"] == 0 for r in reps)}), flush=True)
     return 0
 
 

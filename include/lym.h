@@ -194,6 +194,21 @@ int lym_multishift_solve(lym_gauge* g, double kappa, int nshift, const double* s
                          const void* b, void* xs, double tol, int max_iter,
                          int* iterations, void* stream);
 
+/* Multishift CG on (Q^2 + sigma_k) x_{i,k} = b_i for nrhs right-hand sides b_i
+ * (reference layout (nrhs, ns, N, V)) and nshift >= 0 shifts at once, with the
+ * inner iterations in params->precision (FP64, FP32, norm-scaled FP16 / BF16)
+ * and FP64 reliable updates; every (i, k) is verified by its FP64 true residual
+ * and refined by a CG of its own if it is above params->tol |b_i|.  xs receives
+ * (nrhs, nshift, ns, N, V); reports has nrhs * nshift entries (i * nshift + k).
+ * Replaces multishift_solver.solve on a SquareOperator(DiracWilsonOperator)
+ * (dirac_solver.py:19-53) for positive shifts, several sources per call;
+ * builder-defined algorithm (even-odd layout, Jegerlehner's recurrences).
+ * params->hermitian, compressed_links and mixed_fma are not used;
+ * rhs_per_thread = 1 forces one group per hop-kernel thread. */
+int lym_multishift_solve_eo(lym_gauge* g, double kappa, int nrhs, int nshift, const double* shifts,
+                            const void* b, void* xs, const lym_solver_params* params,
+                            lym_solver_report* reports, void* stream);
+
 /* The reference's multishift MMMR itself (dirac_solver.py:19-53): base shift
  * shifts[nshift-1], alpha = omega <p,r>/<p,p>, absolute stop |<r,r>| < precision.
  * *steps receives the step index the reference prints. FP64, full lattice. */

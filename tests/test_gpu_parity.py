@@ -194,6 +194,58 @@ def test_multishift_cg(cuda_device, case):
 
 @pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])
 @pytest.mark.parametrize("case", ["d2", "d4", "d4su2", "d2su3"])
+def test_multishift_eo(cuda_device, case, precision):
+    """Even-odd multishift CG, two sources, shifts out of order (0 included):
+    every (source, shift) meets 1e-10 by the oracle's Q^2 and agrees with the
+    full-lattice FP64 multishift CG."""
+    from tfleonardym_b200 import dirac, dirac_solver
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    op = make_op(g, spec)
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    shifts = [0.5, 0.0, 2.0, 0.01]
+    b = np.stack([g["eta"], g["eta2"]])
+    ms = dirac_solver.multishift_cg(5000, 1e-10, precision=precision, delta=0.01)
+    xs = ms.solve(dirac.SquareOperator(op), cu(b), shifts)
+    full = [dirac_solver.multishift_cg(5000, 1e-12).solve(dirac.SquareOperator(op), cu(b[i]), shifts)
+            for i in range(2)]
+    for k, s in enumerate(shifts):
+        x = np_(xs[k])
+        assert x.shape == b.shape
+        for i in range(2):
+            rep = ms.reports[i * len(shifts) + k]
+            res = np.linalg.norm(setup.Q2(x[i]) + s * x[i] - b[i]) / np.linalg.norm(b[i])
+            assert res < 1e-10, (precision, i, s, res, rep)
+            assert rep["status"] == 0 and rep["true_residual"] < 1e-10, rep
+            assert relerr(x[i], np_(full[i][k])) < 1e-7, (i, s)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+@pytest.mark.parametrize("tile", [0, 1])
+def test_multishift_eo_padded_groups(cuda_device, precision, tile):
+    """Five sources (four per hop thread, three padding groups, or one per
+    thread), 17 shifts from 1e-4 to 300 (a rational approximation's spread):
+    true residual 1e-10 each."""
+    from tfleonardym_b200 import dirac, dirac_solver
+    g = load_golden("d4")
+    spec = GOLDEN_CASES["d4"]
+    op = make_op(g, spec)
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    shifts = list(np.geomspace(1e-4, 300.0, 17))
+    rng = np.random.default_rng(11)
+    b = (rng.normal(size=(5,) + g["eta"].shape) + 1j * rng.normal(size=(5,) + g["eta"].shape)) / np.sqrt(2)
+    ms = dirac_solver.multishift_cg(5000, 1e-10, precision=precision, delta=0.01, rhs_per_thread=tile)
+    xs = ms.solve(dirac.SquareOperator(op), cu(b), shifts)
+    assert ms.reports[0]["rhs_per_thread"] == (1 if tile == 1 else 4)
+    for k, s in enumerate(shifts):
+        x = np_(xs[k])
+        for i in range(5):
+            res = np.linalg.norm(setup.Q2(x[i]) + s * x[i] - b[i]) / np.linalg.norm(b[i])
+            assert res < 1e-10, (i, s, res, ms.reports[i * len(shifts) + k])
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])
+@pytest.mark.parametrize("case", ["d2", "d4", "d4su2", "d2su3"])
 def test_eo_cg_true_residual(cuda_device, case, precision):
     """D x = b (and Q x = b) by even-odd CG: true residual recomputed by the oracle."""
     from tfleonardym_b200 import dirac_solver

@@ -69,6 +69,8 @@ SIGNATURES = {
     "lym_dslash_eo": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p]),
     "lym_multishift_solve": (c_int, [c_void_p, c_double, c_int, P(c_double), c_void_p, c_void_p,
                                      c_double, c_int, P(c_int), c_void_p]),
+    "lym_multishift_solve_eo": (c_int, [c_void_p, c_double, c_int, c_int, P(c_double), c_void_p, c_void_p,
+                                        P(SolverParams), P(SolverReport), c_void_p]),
     "lym_mmmr_solve": (c_int, [c_void_p, c_double, c_int, P(c_double), c_void_p, c_void_p, c_int,
                                c_double, c_double, P(c_int), c_void_p]),
     "lym_gauge_force": (c_int, [c_void_p, c_int, c_double, c_void_p, c_void_p, c_void_p, c_double,

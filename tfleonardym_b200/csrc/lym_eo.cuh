@@ -259,6 +259,17 @@ LYM_D int eo_coords(const EoGeom& g, int cb, int par, int (&x)[ND]) {
   return (int)row * Lt + x[ND - 1];
 }
 
+// coordinates of lexicographic site lex (last coordinate fastest)
+template <int ND>
+LYM_D void lex_coords(const EoGeom& g, int64_t lex, int (&x)[ND]) {
+  int64_t r = lex;
+#pragma unroll
+  for (int d = ND - 1; d >= 0; --d) {
+    x[d] = (int)(r % g.dims[d]);
+    r /= g.dims[d];
+  }
+}
+
 template <int ND>
 LYM_D int nb_fwd(const EoGeom& g, int lex, const int (&x)[ND], int mu) {
   return (x[mu] == g.dims[mu] - 1) ? lex - (g.dims[mu] - 1) * g.stride[mu] : lex + g.stride[mu];

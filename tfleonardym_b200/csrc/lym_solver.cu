@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "lym_eo.cuh"
+#include "lym_gauge_obj.cuh"
 #include "lym_internal.cuh"
 #include "lym_kernels.cuh"
 
@@ -59,16 +60,6 @@ static EoGeom make_geom(const lym_lattice* lat) {
   g.Lh = lat->dims[lat->nd - 1] / 2;
   g.Vh = lat->V / 2;
   return g;
-}
-
-template <int ND>
-LYM_D void lex_coords(const EoGeom& g, int64_t lex, int (&x)[ND]) {
-  int64_t r = lex;
-#pragma unroll
-  for (int d = ND - 1; d >= 0; --d) {
-    x[d] = (int)(r % g.dims[d]);
-    r /= g.dims[d];
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -634,33 +625,6 @@ constexpr int kLaunchesPerIteration = 5;
 // solver workspaces a gauge object keeps, keyed by (precision, nrhs)
 constexpr size_t kMaxWorkspaces = 4;
 
-}  // namespace lym
-
-struct lym_gauge {
-  const lym_lattice* lat = nullptr;
-  int nc = 0, nd = 0, ns = 0, ncomp = 0;
-  int64_t V = 0, Vh = 0;
-  double bcr = 1, bci = 0;
-  unsigned prec_mask = 0;
-  bool comp = false;  // sloppy links compressed (links are SU(N))
-  lym::EoGeom geom{};
-  double2* uref = nullptr;  // reference-layout FP64 copy (boundary factor NOT applied)
-  double2* u64 = nullptr;
-  // sloppy links: compressed to N-1 rows (only when every link is SU(N)) and full N x N
-  float4* u32 = nullptr;   // compressed
-  int n32 = 0;
-  uint2* u16 = nullptr;    // compressed
-  int n16 = 0;
-  float4* u32f = nullptr;  // full, boundary factor folded in
-  int n32f = 0;
-  uint2* u16f = nullptr;   // full, boundary factor folded in
-  int n16f = 0;
-  int* nbr = nullptr;      // even-odd neighbour table (EoGeom::nbr)
-  std::vector<lym::Work*> works;  // solver workspaces, most recently used first
-};
-
-namespace lym {
-
 struct Work {
   lym_gauge* g = nullptr;
   int nrhs = 0, sp = 0, xp = 0;  // nrhs: padded count every field holds
@@ -697,9 +661,7 @@ struct Work {
   HopGauge hg64, hgs, hgs_c, hgs_f;  // hgs: the links of the selected candidate
   CgOps ops{};
   cudaGraphExec_t graph = nullptr;
-  cudaGraph_t rec = nullptr;          // graph being recorded by build_graph (explicit kernel nodes)
-  cudaGraphNode_t rec_last = nullptr;  // its last node (each launch depends on the previous one)
-  cudaError_t rec_err = cudaSuccess;
+  GraphRec rec;                   // graph being recorded by build_graph (explicit kernel nodes)
   int graph_chunk = 0;
   double graph_kappa = 0;
   int graph_cand = -1;
@@ -709,34 +671,11 @@ struct Work {
   int64_t launches = 0;           // kernels launched by the current call (graph nodes included)
 };
 
-// Launch a kernel, or, while build_graph records (w.rec set), append it to the
-// graph as a kernel node after the previous one.  Recording builds the graph
-// with explicit nodes instead of stream capture, so nothing is ever capturing:
-// another thread's first launch of a lazily loaded kernel (a library or a torch
-// kernel) cannot collide with a capture in progress.
+// Launch a kernel, or, while build_graph records, append it to the graph as a
+// kernel node after the previous one (launch_rec).
 template <typename... KArgs, typename... Args>
 static void launch(Work& w, cudaStream_t st, void (*kernel)(KArgs...), dim3 grid, dim3 block, Args&&... args) {
-  if (!w.rec) {
-    kernel<<<grid, block, 0, st>>>(std::forward<Args>(args)...);
-    return;
-  }
-  std::tuple<KArgs...> vals(std::forward<Args>(args)...);
-  void* ptrs[sizeof...(KArgs)];
-  std::apply([&](auto&... v) {
-    int i = 0;
-    ((ptrs[i++] = (void*)&v), ...);
-  }, vals);
-  cudaKernelNodeParams p{};
-  p.func = (void*)kernel;
-  p.gridDim = grid;
-  p.blockDim = block;
-  p.sharedMemBytes = 0;
-  p.kernelParams = ptrs;
-  cudaGraphNode_t node = nullptr;
-  const cudaError_t e = cudaGraphAddKernelNode(&node, w.rec, w.rec_last ? &w.rec_last : nullptr,
-                                               w.rec_last ? 1 : 0, &p);
-  if (e != cudaSuccess && w.rec_err == cudaSuccess) w.rec_err = e;
-  if (e == cudaSuccess) w.rec_last = node;
+  launch_rec(w.rec, st, kernel, grid, block, std::forward<Args>(args)...);
 }
 
 template <int ND, int NC, int SP, bool COMP, int R, int MX>
@@ -1077,12 +1016,10 @@ static int build_graph(Work& w, int chunk, cudaStream_t st) {
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaGraphCreate(&graph, 0);
   if (e == cudaSuccess) {
-    w.rec = graph;
-    w.rec_last = nullptr;
-    w.rec_err = cudaSuccess;
+    w.rec = GraphRec{graph, nullptr, cudaSuccess};
     for (int i = 0; i < chunk; ++i) w.ops.iterate(w, st);
-    w.rec = nullptr;
-    e = w.rec_err;
+    e = w.rec.err;
+    w.rec = GraphRec{};
   }
   if (e == cudaSuccess) {
     e = cudaGraphInstantiate(&w.graph, graph, 0);
@@ -1480,6 +1417,7 @@ static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
 #undef LYM_PACK
   LYM_CHECK_LAUNCH();
   free_all_work(g);  // sloppy gauge pointers / compression may have changed
+  free_ms_works(g);
   return LYM_OK;
 }
 
@@ -1536,6 +1474,7 @@ int lym_gauge_destroy(lym_gauge* g) {
   if (!g) return LYM_OK;
   cudaDeviceSynchronize();
   free_all_work(g);
+  free_ms_works(g);
   if (g->uref) cudaFree(g->uref);
   if (g->u64) cudaFree(g->u64);
   if (g->u32) cudaFree(g->u32);

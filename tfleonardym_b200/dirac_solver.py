@@ -8,7 +8,9 @@
   on any other operator the loop calls ``operator.apply`` with lym vector kernels.
 * ``biconjugate_gradient`` -- BiCGStab of dirac_solver.py:56-110.
 * ``multishift_cg`` -- builder-defined drop-in for ``multishift_solver`` on
-  Q^2 + sigma (lym_multishift_solve); tolerance is relative, tol * |b|.
+  Q^2 + sigma (lym_multishift_solve, FP64; or with ``precision`` the even-odd
+  lym_multishift_solve_eo with FP64 / FP32 / FP16 / BF16 inner iterations and
+  batched sources); tolerance is relative, tol * |b|.
 * ``conjugate_gradient`` -- builder-defined even-odd CG for D x = b (or Q x = b)
   with FP64 reliable updates and FP64 / FP32 / FP16 / BF16 inner iterations
   (lym_wilson_solve).
@@ -147,18 +149,33 @@ class biconjugate_gradient:  # noqa: N801 - reference name
 
 class multishift_cg:  # noqa: N801 - named like the reference solvers
     """Multishift CG on (Q^2 + sigma_k): same interface as multishift_solver;
-    stops when every shift's residual is below tol * |source|."""
+    stops when every shift's residual is below tol * |source|.
 
-    def __init__(self, max_steps, tol):
+    ``precision=None``: the full-lattice FP64 multishift (lym_multishift_solve),
+    one source.  ``precision`` in {"f64", "f32", "f16", "bf16"}: the even-odd
+    multishift (lym_multishift_solve_eo) with inner iterations in that precision,
+    FP64 reliable updates and every shift's FP64 true residual verified (and
+    refined where needed); ``source`` may then be a batch (nrhs, ns, N, V), each
+    returned solution then has the batch shape.  ``reports`` holds one dict per
+    (rhs, shift) after an even-odd solve."""
+
+    def __init__(self, max_steps, tol, precision=None, delta=0.1, chunk=8, rhs_per_thread=0):
         self.max_steps = max_steps
         self.tol = tol
+        self.precision = precision
+        self.delta = delta
+        self.chunk = chunk
+        self.rhs_per_thread = rhs_per_thread
         self.last_steps = None
+        self.reports = None
 
     def solve(self, operator, source, shifts):
         q = _wilson_square(operator)
         if q is None:
             raise TypeError("multishift_cg needs SquareOperator(DiracWilsonOperator(hermitian=True))")
         source = _dev.as_c128(source)
+        if self.precision is not None:
+            return self._solve_eo(q, source, shifts)
         xs = torch.empty((len(shifts),) + tuple(source.shape), dtype=torch.complex128, device=source.device)
         it = ctypes.c_int()
         sh = (ctypes.c_double * len(shifts))(*[float(s) for s in shifts])
@@ -171,6 +188,30 @@ class multishift_cg:  # noqa: N801 - named like the reference solvers
         else:
             _lib.check(rc, "lym_multishift_solve")
         return [xs[i] for i in range(len(shifts))]
+
+    def _solve_eo(self, q, source, shifts):
+        batched = source.dim() == 4
+        bb = source if batched else source[None]
+        n, ns = bb.shape[0], len(shifts)
+        xs = torch.empty((n, ns) + tuple(bb.shape[1:]), dtype=torch.complex128, device=bb.device)
+        sh = (ctypes.c_double * ns)(*[float(s) for s in shifts])
+        prm = _lib.SolverParams(float(self.tol), int(self.max_steps), _lib.PREC[self.precision], float(self.delta),
+                                1, int(self.chunk), int(self.rhs_per_thread), 0, 0)
+        reps = (_lib.SolverReport * (n * ns))()
+        precs = () if self.precision == "f64" else (self.precision,)
+        rc = _lib.lib().lym_multishift_solve_eo(q.solver_gauge(precs), float(q.kappa), n, ns, sh, _dev.ptr(bb),
+                                                _dev.ptr(xs), ctypes.byref(prm), reps, _dev.stream())
+        self.reports = [dict(status=r.status, iterations=r.iterations, reliable_updates=r.reliable_updates,
+                             true_residual=r.true_residual, kernel_launches=r.kernel_launches,
+                             rhs_per_thread=r.rhs_per_thread, compressed_links=r.compressed_links) for r in reps]
+        self.last_steps = max(r.iterations for r in reps)
+        if rc == _lib.LYM_ERR_NOT_CONVERGED:
+            _print(f"multishift CG: failed to find convergence ({self.reports})")
+        else:
+            _lib.check(rc, "lym_multishift_solve_eo")
+        if batched:
+            return [xs[:, k] for k in range(ns)]
+        return [xs[0, k] for k in range(ns)]
 
 
 class conjugate_gradient:  # noqa: N801 - named like the reference solvers
