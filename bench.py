@@ -78,8 +78,18 @@ def parse_args():
                          "one JSON line")
     ap.add_argument("--precision-study", action="store_true",
                     help="24^3x48 SU(3), eps 0.3, kappa 0.12 and 0.13, 8 rhs: the even-odd CG with FP64 / FP32 / "
-                         "FP16 / BF16 inner iterations against the FP64 solution, and the FP64 multishift CG on "
-                         "Q^2 + sigma_k with the reference's 17-pole rational approximation; one JSON line per case")
+                         "FP16 / BF16 inner iterations against the FP64 solution, the full-lattice FP64 multishift CG "
+                         "and the even-odd multishift CG in four inner precisions on Q^2 + sigma_k with the "
+                         "reference's 17-pole rational approximation; one JSON line per case")
+    ap.add_argument("--multishift", action="store_true",
+                    help="24^3x48 SU(3), eps 0.3: the even-odd multishift CG on Q^2 + sigma_k with the reference's "
+                         "17 metropolis shifts, --ms-rhs sources in one call, for every --ms-precisions x "
+                         "--ms-switch; one JSON line per case")
+    ap.add_argument("--kappa", type=float, default=0.13, help="hopping parameter of --multishift")
+    ap.add_argument("--ms-rhs", type=int, default=8, help="sources of --multishift")
+    ap.add_argument("--ms-precisions", default="f64,f32,f16,bf16", help="inner precisions of --multishift")
+    ap.add_argument("--ms-switch", default="0",
+                    help="FP64-head switch residuals of --multishift (0: the library default, <0: no head)")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per rate")
     ap.add_argument("--serve-max-requests", type=int, default=600)
@@ -925,6 +935,93 @@ REFERENCE_17_POLES = [708.456969133708774250236839, 20.5545836704482543092111935
                       0.0000000269253347571438797470449799]
 
 
+def _multishift_case(sq, q, b, prec, switch, ref, stream):
+    """One timed even-odd multishift solve of all sources in b (after a warm-up
+    solve) on the 17 reference shifts; returns (JSON-ready dict, solutions
+    (rhs, shift, ...)).  ref: FP64 solutions to compare with, or None."""
+    import torch
+
+    from tfleonardym_b200 import dirac_solver
+    nrhs, nsh = b.shape[0], len(REFERENCE_17_POLES)
+    ms = dirac_solver.multishift_cg(20000, 1e-10, precision=prec, delta=0.01, switch_residual=switch)
+    ms.solve(sq, b, REFERENCE_17_POLES)  # warm-up: workspaces, graphs
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    xs = ms.solve(sq, b, REFERENCE_17_POLES)
+    e.record(stream)
+    torch.cuda.synchronize()
+    xs = torch.stack(xs, 1)  # (rhs, shift, ...)
+    reps = ms.reports
+    out = {"inner_precision": prec, "switch_residual": switch, "rhs": nrhs, "ms": s.elapsed_time(e),
+           "ms_per_rhs": s.elapsed_time(e) / nrhs,
+           "iterations_per_shift_max": [max(reps[i * nsh + k]["iterations"] for i in range(nrhs))
+                                        for k in range(nsh)],
+           "reliable_updates_max": max(r["reliable_updates"] for r in reps),
+           "true_residual_per_shift_max": [max(reps[i * nsh + k]["true_residual"] for i in range(nrhs))
+                                           for k in range(nsh)],
+           "kernel_launches": reps[0]["kernel_launches"],
+           "status_ok": all(r["status"] == 0 for r in reps)}
+    # independent FP64 check of source 0 through the reference-layout operator
+    bn = float(torch.linalg.vector_norm(b[0]))
+    out["rhs0_reference_layout_residual_max"] = max(
+        float(torch.linalg.vector_norm(b[0] - (q.apply(q.apply(xs[0, k])) + sg * xs[0, k]))) / bn
+        for k, sg in enumerate(REFERENCE_17_POLES))
+    if ref is not None:
+        out["rel_diff_to_fp64_per_shift_max"] = [
+            max(float(torch.linalg.vector_norm(xs[i, k] - ref[i, k]) / torch.linalg.vector_norm(ref[i, k]))
+                for i in range(nrhs)) for k in range(nsh)]
+    return out, xs
+
+
+def _study_setup(dev, nrhs):
+    """24^3 x 48 SU(3) links reunit(exp(i 0.3 H)) (seed 2026) and nrhs unit complex Gaussian sources (seed 7)."""
+    import torch
+
+    from tfleonardym_b200 import lattice as lt
+    geom = (24, 24, 24, 48)
+    vol = int(np.prod(geom))
+    links = _device_links(geom, NC, 0.3, 2026, dev)
+    cfg = lt.Configuration(links, geom, NC, 4)
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    b = torch.complex(torch.randn((nrhs, 4, NC, vol), generator=g, device=dev, dtype=torch.float64),
+                      torch.randn((nrhs, 4, NC, vol), generator=g, device=dev, dtype=torch.float64)) / np.sqrt(2)
+    return geom, cfg, b
+
+
+def run_multishift(args, local_rank):
+    """The even-odd multishift CG (lym_multishift_solve_eo) on 24^3 x 48 SU(3)
+    (links reunit(exp(i 0.3 H)), antiperiodic time) at --kappa, the reference's
+    17 metropolis shifts, --ms-rhs unit complex Gaussian sources in one call,
+    for each inner precision and FP64-head switch residual: time (CUDA events,
+    after a warm-up solve), iterations, the FP64 true residual of every (rhs,
+    shift) and, after an FP64 case, each shift's largest relative difference
+    to the FP64 solutions."""
+    import torch
+
+    from tfleonardym_b200 import boundary_conditions, dirac, dirac_solver
+    dirac_solver.VERBOSE = False
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    geom, cfg, b = _study_setup(dev, args.ms_rhs)
+    stream = torch.cuda.current_stream()
+    prov = boundary_conditions.time_antiperiodic_provider(-1)
+    q = dirac.DiracWilsonOperator(cfg, args.kappa, True, representation="fundamental",
+                                  boundary_condition_provider=prov)
+    sq = dirac.SquareOperator(q)
+    ref = None
+    for prec in args.ms_precisions.split(","):
+        for sw in (float(x) for x in args.ms_switch.split(",")):
+            if prec == "f64" and sw != float(args.ms_switch.split(",")[0]):
+                continue  # no head to switch from
+            out, xs = _multishift_case(sq, q, b, prec, sw, ref, stream)
+            if prec == "f64" and ref is None:
+                ref = xs.clone()
+            print(json.dumps({"multishift": "even-odd multishift CG, 17 reference shifts", "geometry": list(geom),
+                              "kappa": args.kappa, **out}), flush=True)
+    return 0
+
+
 def run_precision_study(args, local_rank):
     """BASELINE config 3 as far as it is built: on 24^3 x 48 SU(3) (links
     reunit(exp(i 0.3 H)), antiperiodic time) at kappa 0.12 and 0.13, 8 unit complex
@@ -939,18 +1036,10 @@ def run_precision_study(args, local_rank):
     import torch
 
     from tfleonardym_b200 import boundary_conditions, dirac, dirac_solver
-    from tfleonardym_b200 import lattice as lt
     dirac_solver.VERBOSE = False
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    geom = (24, 24, 24, 48)
-    nd, vol = 4, int(np.prod(geom))
-    links = _device_links(geom, NC, 0.3, 2026, dev)
-    cfg = lt.Configuration(links, geom, NC, nd)
-    g = torch.Generator(device=dev)
-    g.manual_seed(7)
-    b = torch.complex(torch.randn((8, 4, NC, vol), generator=g, device=dev, dtype=torch.float64),
-                      torch.randn((8, 4, NC, vol), generator=g, device=dev, dtype=torch.float64)) / np.sqrt(2)
+    geom, cfg, b = _study_setup(dev, 8)
     stream = torch.cuda.current_stream()
     prov = boundary_conditions.time_antiperiodic_provider(-1)
     for kappa in (0.12, 0.13):
@@ -998,35 +1087,11 @@ def run_precision_study(args, local_rank):
         # errors per shift against its FP64 solutions
         ref_ms = None
         for prec in ("f64", "f32", "f16", "bf16"):
-            ms = dirac_solver.multishift_cg(20000, 1e-10, precision=prec, delta=0.01)
-            ms.solve(sq, b, REFERENCE_17_POLES)  # warm-up: workspaces, graphs
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            xs = ms.solve(sq, b, REFERENCE_17_POLES)
-            e.record(stream)
-            torch.cuda.synchronize()
-            xs = torch.stack(xs, 1)  # (rhs, shift, ...)
+            out, xs = _multishift_case(sq, q, b, prec, 0.0, ref_ms, stream)
             if ref_ms is None:
                 ref_ms = xs.clone()
-            nsh = len(REFERENCE_17_POLES)
-            reps = ms.reports
-            diff = [max(float(torch.linalg.vector_norm(xs[i, k] - ref_ms[i, k]) /
-                              torch.linalg.vector_norm(ref_ms[i, k])) for i in range(8)) for k in range(nsh)]
-            # independent FP64 check of source 0 through the reference-layout operator
-            bn = float(torch.linalg.vector_norm(b[0]))
-            chk = [float(torch.linalg.vector_norm(b[0] - (q.apply(q.apply(xs[0, k])) + sg * xs[0, k]))) / bn
-                   for k, sg in enumerate(REFERENCE_17_POLES)]
             print(json.dumps({"precision_study": "even-odd multishift CG, 17 reference shifts", "geometry": list(geom),
-                              "kappa": kappa, "inner_precision": prec, "rhs": 8, "ms": s.elapsed_time(e),
-                              "ms_per_rhs": s.elapsed_time(e) / 8,
-                              "iterations_per_shift_max": [max(reps[i * nsh + k]["iterations"] for i in range(8))
-                                                           for k in range(nsh)],
-                              "reliable_updates_max": max(r["reliable_updates"] for r in reps),
-                              "true_residual_per_shift_max": [max(reps[i * nsh + k]["true_residual"]
-                                                                  for i in range(8)) for k in range(nsh)],
-                              "rhs0_reference_layout_residual_max": max(chk),
-                              "rel_diff_to_fp64_per_shift_max": diff,
-                              "status_ok": all(r["status"] == 0 for r in reps)}), flush=True)
+                              "kappa": kappa, **out}), flush=True)
     return 0
 
 
@@ -1123,6 +1188,8 @@ def main():
         return run_batch_lattices(args, local_rank)
     if args.precision_study:
         return run_precision_study(args, local_rank)
+    if args.multishift:
+        return run_multishift(args, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if world > 1:

@@ -157,6 +157,10 @@ typedef struct lym_solver_params {
   int mixed_fma;     /* with a forced tile and FP16 (full links): 0 = FP32 arithmetic on
                         converted values; 1 = half spinor in FP16, U h through f16 x f16 + f32
                         FMAs */
+  double switch_residual; /* lym_multishift_solve_eo with a reduced inner precision: the
+                        iterations run in FP64 until the true relative residual of the
+                        smallest shift is below this, then in the inner precision
+                        (0 = 1e-4 FP32, 1e-6 FP16, 1e-7 BF16; negative = from the start) */
 } lym_solver_params;
 
 typedef struct lym_solver_report {
@@ -203,6 +207,7 @@ int lym_multishift_solve(lym_gauge* g, double kappa, int nshift, const double* s
  * Replaces multishift_solver.solve on a SquareOperator(DiracWilsonOperator)
  * (dirac_solver.py:19-53) for positive shifts, several sources per call;
  * builder-defined algorithm (even-odd layout, Jegerlehner's recurrences).
+ * params->switch_residual sets where a reduced precision takes over from FP64;
  * params->hermitian, compressed_links and mixed_fma are not used;
  * rhs_per_thread = 1 forces one group per hop-kernel thread. */
 int lym_multishift_solve_eo(lym_gauge* g, double kappa, int nrhs, int nshift, const double* shifts,

@@ -244,6 +244,26 @@ def test_multishift_eo_padded_groups(cuda_device, precision, tile):
             assert res < 1e-10, (i, s, res, ms.reports[i * len(shifts) + k])
 
 
+@pytest.mark.parametrize("switch", [-1.0, 1e-3, 1e-12])
+def test_multishift_eo_switch_points(cuda_device, switch):
+    """Inner precision from the start (-1), after an FP64 head to 1e-3, and an
+    FP64 head past tol (the whole solve in FP64): 1e-10 for every shift."""
+    from tfleonardym_b200 import dirac, dirac_solver
+    g = load_golden("d4")
+    spec = GOLDEN_CASES["d4"]
+    op = make_op(g, spec)
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    shifts = [0.02, 0.001, 0.3]
+    b = np.stack([g["eta"], g["eta2"], g["eta"] - g["eta2"]])
+    ms = dirac_solver.multishift_cg(5000, 1e-10, precision="f16", delta=0.01, switch_residual=switch)
+    xs = ms.solve(dirac.SquareOperator(op), cu(b), shifts)
+    for k, s in enumerate(shifts):
+        x = np_(xs[k])
+        for i in range(3):
+            res = np.linalg.norm(setup.Q2(x[i]) + s * x[i] - b[i]) / np.linalg.norm(b[i])
+            assert res < 1e-10, (switch, i, s, res, ms.reports[i * len(shifts) + k])
+
+
 @pytest.mark.parametrize("precision", ["f64", "f32", "f16", "bf16"])
 @pytest.mark.parametrize("case", ["d2", "d4", "d4su2", "d2su3"])
 def test_eo_cg_true_residual(cuda_device, case, precision):

@@ -34,7 +34,7 @@ P = ctypes.POINTER
 class SolverParams(ctypes.Structure):
     _fields_ = [("tol", c_double), ("max_iter", c_int), ("precision", c_int),
                 ("delta", c_double), ("hermitian", c_int), ("chunk", c_int), ("rhs_per_thread", c_int),
-                ("compressed_links", c_int), ("mixed_fma", c_int)]
+                ("compressed_links", c_int), ("mixed_fma", c_int), ("switch_residual", c_double)]
 
 
 class SolverReport(ctypes.Structure):

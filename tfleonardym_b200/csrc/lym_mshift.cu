@@ -37,6 +37,14 @@
 // replaces the sloppy r; the directions and zetas carry on.  A group ends
 // when its true base residual is below tol |b|.
 //
+// FP64 head: with a reduced inner precision the shifted systems cannot see
+// the reliable updates (their residuals are only known as zeta_k r), so the
+// rounding of the early iterations, while |r| is still of order |b|, stays in
+// their solutions.  The iterations therefore run in FP64 until the base true
+// residual is below a switch point (params->switch_residual, by default 1e-4
+// for FP32, 1e-6 for FP16, 1e-7 for BF16), then the state (directions, zetas,
+// recurrences) moves to the inner precision and the solve carries on.
+//
 // Verification: the FP64 true residual of every (i, k).  Phase 2 -- every
 // (i, k) still above tol |b_i| (the shifted solutions drift with the inner
 // precision) runs a CG of its own on (Q^2 + sigma_k) from x_ik, again with
@@ -496,6 +504,28 @@ __global__ void __launch_bounds__(128) ms_sloppy_kernel(int64_t Vh, int nblk, in
   }
 }
 
+// The directions of an FP64 workspace (Gi groups) in the inner precision of
+// another (Go groups): the base direction and every shift's; grid (2 nblk, nreal)
+template <int SP, int NCOMP>
+__global__ void __launch_bounds__(128) ms_dirs_from64_kernel(int64_t Vh, int nblk, int Gi, int Go, int S,
+                                                             EoField pbi, EoField psi, EoField pbo, EoField pso) {
+  using RT = typename Prec<SP>::real;
+  const int par = eo_block_parity(nblk);
+  const int64_t cb = (blockIdx.x - par * nblk) * (int64_t)blockDim.x + threadIdx.x;
+  const int gi = blockIdx.y;
+  if (cb >= Vh) return;
+  for (int s = -1; s < S; ++s) {
+    cx<double> v[NCOMP];
+    if (s < 0) load_sp<SP64, NCOMP>(pbi, par * Gi + gi, cb, v);
+    else load_sp<SP64, NCOMP>(psi, par * Gi * S + gi * S + s, cb, v);
+    cx<RT> w[NCOMP];
+#pragma unroll
+    for (int k = 0; k < NCOMP; ++k) w[k] = {(RT)v[k].re, (RT)v[k].im};
+    if (s < 0) store_sp<SP, NCOMP>(pbo, par * Go + gi, cb, w);
+    else store_sp<SP, NCOMP>(pso, par * Go * S + gi * S + s, cb, w);
+  }
+}
+
 // reference layout (nrhs, ns, N, V) -> FP64 even-odd b64 (nbs slots per parity)
 template <int ND, int NC>
 __global__ void ms_from_ref_kernel(EoGeom g, int64_t V, const double2* __restrict__ ref, EoField b64, int nbs) {
@@ -547,10 +577,11 @@ struct MsOps {
   void (*sloppy)(MsWork&, cudaStream_t);
   void (*from_ref)(MsWork&, const void* ref, int nrhs, cudaStream_t);
   void (*to_ref)(MsWork&, void* ref, const int* out_slot, int nslot, cudaStream_t);
+  void (*dirs_from64)(MsWork& dst, const MsWork& src, int nreal, cudaStream_t);
   void (*preload)();
 };
 constexpr int kMsLaunchesPerIteration = 3;  // plus one ms_xpm every kMsBlock iterations
-constexpr size_t kMaxMsWorkspaces = 2;
+constexpr size_t kMaxMsWorkspaces = 3;  // a solve uses up to three: FP64 head, inner precision, refinement
 
 struct MsWork {
   lym_gauge* g = nullptr;
@@ -654,6 +685,11 @@ struct MsImpl {
     ms_to_ref_kernel<ND, NC><<<dim3(grid_for(w.g->V, 128), nslot), 128, 0, st>>>(w.g->geom, w.g->V, w.own_x64,
                                                                                 w.own_nxs, out_slot, (double2*)ref);
   }
+  static void dirs_from64(MsWork& w, const MsWork& src, int nreal, cudaStream_t st) {
+    w.launches += 1;
+    ms_dirs_from64_kernel<SP, NCOMP><<<dim3(2 * w.nblk, nreal), 128, 0, st>>>(w.Vh, w.nblk, src.G, w.G, w.S, src.pb,
+                                                                             src.ps, w.pb, w.ps);
+  }
   static void preload() {
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, ms_dp_kernel<ND, NC, SP, GP, COMP, R>);
@@ -661,7 +697,9 @@ struct MsImpl {
     cudaFuncGetAttributes(&a, ms_p0_kernel<SP, XP, NCOMP>);
     cudaFuncGetAttributes(&a, ms_xpm_kernel<SP, XP, NCOMP>);
   }
-  static MsOps table() { return MsOps{&iterate, &dx64, &res64, &flush, &sloppy, &from_ref, &to_ref, &preload}; }
+  static MsOps table() {
+    return MsOps{&iterate, &dx64, &res64, &flush, &sloppy, &from_ref, &to_ref, &dirs_from64, &preload};
+  }
 };
 
 template <int ND, int NC, int R>
@@ -755,7 +793,7 @@ void free_ms_works(lym_gauge* g) {
 
 // A workspace for up to `cap` groups of S shifts (Greal is set per run).
 // R: groups per hop-kernel thread (1, or 4 with the groups padded to a
-// multiple of 4).  `keep` is never evicted (the workspace a phase-2 one borrows from).
+// multiple of 4).  `keep` is never evicted (the workspace the others borrow from).
 static int ms_get(lym_gauge* g, int cap, int S, int sp, int store_rhs, int want_r, const MsWork* keep,
                   MsWork** out) {
   const int R = (sp == SP64 || cap < 4 || want_r == 1) ? 1 : 4;
@@ -907,15 +945,16 @@ struct MsOutcome {
   std::vector<double> tres;   // last true relative residual of the base
 };
 
-// Runs the group CGs of w (grp_h / shf_h hold sigma and the zeroed recurrences;
-// x64 holds each group's start) until each group's base true residual is below
-// tol |b| (bnorm2: |b|^2 per group, < 0 to take it from the first residual,
-// i.e. a zero start), it stalls (a group of several shifts: phase 2 takes over)
-// or runs out of iterations.
-static int ms_run(MsWork& w, const lym_solver_params* prm, std::vector<double>& bnorm2, MsOutcome& out,
-                  cudaStream_t st) {
+// Runs the group CGs of w (grp_h / shf_h hold sigma and the zeroed recurrences,
+// or with `resume` the state another workspace left; x64 holds each group's
+// start) until each group's base true residual is below group_tol |b|
+// (bnorm2: |b|^2 per group, < 0 to take it from the first residual, i.e. a
+// zero start), it stalls (a group of several shifts: phase 2 takes over) or
+// runs out of iterations.  The shifted systems stop on the final prm->tol.
+static int ms_run(MsWork& w, const lym_solver_params* prm, double group_tol, bool resume,
+                  std::vector<double>& bnorm2, MsOutcome& out, cudaStream_t st) {
   const int G = w.G, Gr = w.Greal, S = w.S;
-  const double tol2 = prm->tol * prm->tol;
+  const double tol2 = group_tol * group_tol, final2 = prm->tol * prm->tol;
   const double delta = prm->delta > 0 && prm->delta < 1 ? prm->delta : 0.1;
   // a chunk ends on a block boundary, so no shift update is pending between chunks
   const int chunk = (std::max(1, prm->chunk > 0 ? std::min(prm->chunk, 256) : 8) + kMsBlock - 1) / kMsBlock * kMsBlock;
@@ -926,7 +965,7 @@ static int ms_run(MsWork& w, const lym_solver_params* prm, std::vector<double>& 
   std::vector<int> ended(G, 0), restart(G, 0), iters_at_update(G, -1);
   std::vector<double> prev_q2(G, 0.0);
   for (int i = 0; i < G; ++i) {
-    w.upd_h[i] = i < Gr ? 3 : 0;
+    w.upd_h[i] = i < Gr ? 3 : 0;  // the first residual (and with a fresh start, every direction)
     if (i >= Gr) ended[i] = 1;
   }
   auto plan = [&](int i, double q2) {
@@ -974,9 +1013,9 @@ static int ms_run(MsWork& w, const lym_solver_params* prm, std::vector<double>& 
   if (rc) return rc;
   for (int i = 0; i < Gr; ++i) {
     if (bnorm2[i] < 0) bnorm2[i] = w.res_h[i];
-    for (int s = 1; s < S; ++s) w.shf_h[(size_t)i * S + s].stop2 = 0.25 * tol2 * bnorm2[i];
+    for (int s = 1; s < S; ++s) w.shf_h[(size_t)i * S + s].stop2 = 0.25 * final2 * bnorm2[i];
     plan(i, w.res_h[i]);
-    w.upd_h[i] = out.done[i] ? 0 : 3;
+    w.upd_h[i] = out.done[i] ? 0 : (resume ? 1 : 3);
   }
   LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_h, sizeof(int) * G, cudaMemcpyHostToDevice, st));
   LYM_CUDA(cudaMemcpyAsync(w.grp, w.grp_h, sizeof(MsGroup) * G, cudaMemcpyHostToDevice, st));
@@ -1091,8 +1130,53 @@ static int ms_solve_on(lym_gauge* g, double kappa, int nrhs, int nshift, const d
   auto trace_ms = [&]() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   };
-  rc = ms_run(w1, prm, bnorm2, o1, st);
+  // FP64 head (reduced inner precisions): the same groups in an FP64 workspace
+  // until the base true residual is below the switch point
+  double sw = prm->switch_residual;
+  if (sw == 0.0) sw = sp == SP32 ? 1e-4 : (sp == SP16 ? 1e-6 : 1e-7);
+  const bool head = sp != SP64 && sw > prm->tol;
+  std::vector<int> head_updates(nrhs, 0);
+  if (head) {
+    MsWork* whp;
+    rc = ms_get(g, nrhs, nshift, SP64, 0, prm->rhs_per_thread, &w1, &whp);
+    if (rc) return rc;
+    MsWork& wh = *whp;
+    wh.kappa = kappa;
+    wh.launches = 0;
+    wh.b64 = w1.own_b64;
+    wh.nbs = w1.own_nbs;
+    wh.x64 = w1.own_x64;
+    wh.nxs = w1.own_nxs;
+    wh.Greal = nrhs;
+    for (int i = 0; i < wh.G; ++i) {
+      wh.map_h[i] = std::min(i, nrhs - 1) * S;
+      wh.map_h[wh.G + i] = std::min(i, nrhs - 1);
+    }
+    LYM_CUDA(cudaMemcpyAsync(wh.xmap, wh.map_h, sizeof(int) * 2 * wh.G, cudaMemcpyHostToDevice, st));
+    LYM_CUDA(cudaMemsetAsync(wh.xs.data, 0, ms_field_bytes(SP64, g->ncomp, g->Vh, 2 * (int64_t)wh.G * S), st));
+    ms_init_states(wh, base_sigma, shift_sigma, prm->max_iter);
+    std::vector<double> bn_h(wh.G, -1.0);
+    MsOutcome oh;
+    rc = ms_run(wh, prm, sw, false, bn_h, oh, st);
+    if (rc) return rc;
+    // the state moves to the inner-precision workspace
+    LYM_CUDA(cudaMemcpyAsync(wh.shf_h, wh.shf, sizeof(MsShift) * (size_t)wh.G * S, cudaMemcpyDeviceToHost, st));
+    LYM_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < nrhs; ++i) {
+      w1.grp_h[i] = wh.grp_h[i];
+      w1.grp_h[i].nstep = 0;
+      for (int s = 0; s < S; ++s) w1.shf_h[(size_t)i * S + s] = wh.shf_h[(size_t)i * S + s];
+      bnorm2[i] = bn_h[i];
+      head_updates[i] = oh.updates[i];
+    }
+    w1.ops.dirs_from64(w1, wh, nrhs, st);
+    LYM_CHECK_LAUNCH();
+    w1.launches += wh.launches;
+    if (ms_trace()) std::fprintf(stderr, "lym_ms: FP64 head done at %.2f ms\n", trace_ms());
+  }
+  rc = ms_run(w1, prm, prm->tol, head, bnorm2, o1, st);
   if (rc) return rc;
+  for (int i = 0; i < nrhs; ++i) o1.updates[i] += head_updates[i];
   if (ms_trace()) std::fprintf(stderr, "lym_ms: phase 1 done at %.2f ms\n", trace_ms());
   if (ms_trace()) {
     LYM_CUDA(cudaMemcpyAsync(w1.shf_h, w1.shf, sizeof(MsShift) * (size_t)w1.G * S, cudaMemcpyDeviceToHost, st));
@@ -1170,7 +1254,7 @@ static int ms_solve_on(lym_gauge* g, double kappa, int nrhs, int nshift, const d
     LYM_CUDA(cudaMemsetAsync(w2.xs.data, 0, ms_field_bytes(w2.xp, g->ncomp, g->Vh, 2 * (int64_t)w2.G), st));
     ms_init_states(w2, bs, ss, std::max(1, prm->max_iter));
     MsOutcome o2;
-    rc = ms_run(w2, prm, bn2, o2, st);
+    rc = ms_run(w2, prm, prm->tol, false, bn2, o2, st);
     if (rc) return rc;
     for (int j = 0; j < batch; ++j) {
       const int k = todo[at + j];

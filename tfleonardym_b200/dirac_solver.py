@@ -156,16 +156,20 @@ class multishift_cg:  # noqa: N801 - named like the reference solvers
     multishift (lym_multishift_solve_eo) with inner iterations in that precision,
     FP64 reliable updates and every shift's FP64 true residual verified (and
     refined where needed); ``source`` may then be a batch (nrhs, ns, N, V), each
-    returned solution then has the batch shape.  ``reports`` holds one dict per
-    (rhs, shift) after an even-odd solve."""
+    returned solution then has the batch shape.  ``switch_residual``: FP64
+    iterations until the smallest shift's true relative residual is below it,
+    then the inner precision (0: the library's default per precision, < 0: the
+    inner precision from the start).  ``reports`` holds one dict per (rhs,
+    shift) after an even-odd solve."""
 
-    def __init__(self, max_steps, tol, precision=None, delta=0.1, chunk=8, rhs_per_thread=0):
+    def __init__(self, max_steps, tol, precision=None, delta=0.1, chunk=8, rhs_per_thread=0, switch_residual=0.0):
         self.max_steps = max_steps
         self.tol = tol
         self.precision = precision
         self.delta = delta
         self.chunk = chunk
         self.rhs_per_thread = rhs_per_thread
+        self.switch_residual = switch_residual
         self.last_steps = None
         self.reports = None
 
@@ -196,7 +200,7 @@ class multishift_cg:  # noqa: N801 - named like the reference solvers
         xs = torch.empty((n, ns) + tuple(bb.shape[1:]), dtype=torch.complex128, device=bb.device)
         sh = (ctypes.c_double * ns)(*[float(s) for s in shifts])
         prm = _lib.SolverParams(float(self.tol), int(self.max_steps), _lib.PREC[self.precision], float(self.delta),
-                                1, int(self.chunk), int(self.rhs_per_thread), 0, 0)
+                                1, int(self.chunk), int(self.rhs_per_thread), 0, 0, float(self.switch_residual))
         reps = (_lib.SolverReport * (n * ns))()
         precs = () if self.precision == "f64" else (self.precision,)
         rc = _lib.lib().lym_multishift_solve_eo(q.solver_gauge(precs), float(q.kappa), n, ns, sh, _dev.ptr(bb),
