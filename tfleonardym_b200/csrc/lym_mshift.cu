@@ -386,6 +386,84 @@ __global__ void __launch_bounds__(128) ms_xpm_kernel(int64_t Vh, int nblk, int G
   }
 }
 
+// ms_xpm for FP64 (no per-site norm): each thread takes one site and UPT of
+// its NU complex components (NG = NU / UPT threads per site, consecutive
+// sites in a block, so every load stays coalesced), which leaves room to hold
+// the pending ring residuals in registers for all shifts.  The coefficients
+// are real, so the update is component-wise.  Grid (2 nblk NG, G).
+template <int NCOMP, int NG>
+__global__ void __launch_bounds__(128) ms_xpm64_kernel(int64_t Vh, int nblk, int G, int S, EoField ring, EoField ps,
+                                                       EoField xs, MsGroup* grp, const MsShift* shf,
+                                                       unsigned* counters) {
+  static_assert(NCOMP % NG == 0, "components split evenly");
+  constexpr int UPT = NCOMP / NG;
+  const int part = blockIdx.x % NG;
+  const int rest = blockIdx.x / NG;
+  const int par = rest >= nblk ? 1 : 0;
+  const int64_t cb = (rest - par * nblk) * (int64_t)blockDim.x + threadIdx.x;
+  const int gi = blockIdx.y;
+  const int n = grp[gi].nstep;
+  if (n == 0) return;  // uniform per group
+  const int k0 = grp[gi].iters - n;
+  if (cb < Vh) {
+    const int64_t vh = Vh, unit0 = (int64_t)part * UPT;
+    auto field_at = [&](const EoField& f, int64_t slot) {
+      return reinterpret_cast<double2*>(f.data) + (slot * f.nunits + unit0) * vh + cb;
+    };
+    double2 rr[kMsBlock][UPT];
+#pragma unroll
+    for (int j = 0; j < kMsBlock; ++j) {
+      if (j >= n) break;
+      const double2* rp = field_at(ring, (int64_t)((k0 + j + 1) % kMsBlock) * 2 * G + par * G + gi);
+#pragma unroll
+      for (int u = 0; u < UPT; ++u) rr[j][u] = __ldg(rp + u * vh);
+    }
+    for (int s = 1; s < S; ++s) {
+      const MsShift& T = shf[(int64_t)gi * S + s];
+      if (!T.run[k0 % kMsBlock]) continue;
+      const int64_t slot = (int64_t)par * G * S + gi * S + s;
+      double2* pp = field_at(ps, slot);
+      double2* xp = field_at(xs, slot);
+      double2 pv[UPT], xv[UPT];
+#pragma unroll
+      for (int u = 0; u < UPT; ++u) {
+        pv[u] = pp[u * vh];
+        xv[u] = xp[u * vh];
+      }
+#pragma unroll
+      for (int j = 0; j < kMsBlock; ++j) {
+        if (j >= n) break;
+        const int ix = (k0 + j) % kMsBlock;
+        if (!T.run[ix]) break;  // the shift stopped after its previous step
+        const double a = T.a[ix], zn = T.zn[ix], b = T.b[ix];
+#pragma unroll
+        for (int u = 0; u < UPT; ++u) {
+          xv[u].x += a * pv[u].x;
+          xv[u].y += a * pv[u].y;
+          pv[u].x = zn * rr[j][u].x + b * pv[u].x;
+          pv[u].y = zn * rr[j][u].y + b * pv[u].y;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < UPT; ++u) {
+        pp[u * vh] = pv[u];
+        xp[u * vh] = xv[u];
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(counters + gi, 1u) == gridDim.x - 1) {
+      grp[gi].nstep = 0;
+      counters[gi] = 0u;  // ready for the next use of this slot
+    }
+  }
+}
+
+// threads per site of ms_xpm64: about three complex components each
+template <int NCOMP> constexpr int ms_xpm64_parts() { return NCOMP % 4 == 0 && NCOMP >= 8 ? 4 : 2; }
+
 // ---------------------------------------------------------------------------
 // FP64 kernels (reliable updates, verification); grids (2 nblk, G).
 // The solutions x64 (nxs slots per parity, group gi's shift s at xmap[gi] + s)
@@ -650,9 +728,16 @@ struct MsImpl {
               w.G, w.S, w.kappa, w.grp, w.shf, w.partials, w.counters + w.G, w.nblk);
     ms_launch(w, st, ms_p0_kernel<SP, XP, NCOMP>, grid, dim3(128), w.Vh, w.nblk, w.G, w.S, w.ring, w.pb, w.xs, w.grp,
               w.counters);
-    if ((i + 1) % kMsBlock == 0)
-      ms_launch(w, st, ms_xpm_kernel<SP, XP, NCOMP>, grid, dim3(128), w.Vh, w.nblk, w.G, w.S, w.ring, w.ps, w.xs,
-                w.grp, (const MsShift*)w.shf, w.counters);
+    if ((i + 1) % kMsBlock == 0) {
+      if constexpr (SP == SP64) {
+        constexpr int NG = ms_xpm64_parts<NCOMP>();
+        ms_launch(w, st, ms_xpm64_kernel<NCOMP, NG>, dim3(2 * w.nblk * NG, w.G), dim3(128), w.Vh, w.nblk, w.G, w.S,
+                  w.ring, w.ps, w.xs, w.grp, (const MsShift*)w.shf, w.counters);
+      } else {
+        ms_launch(w, st, ms_xpm_kernel<SP, XP, NCOMP>, grid, dim3(128), w.Vh, w.nblk, w.G, w.S, w.ring, w.ps, w.xs,
+                  w.grp, (const MsShift*)w.shf, w.counters);
+      }
+    }
   }
   static void dx64(MsWork& w, int s, cudaStream_t st) {
     w.launches += 1;
@@ -695,7 +780,8 @@ struct MsImpl {
     cudaFuncGetAttributes(&a, ms_dp_kernel<ND, NC, SP, GP, COMP, R>);
     cudaFuncGetAttributes(&a, ms_ap_kernel<ND, NC, SP, GP, COMP, R>);
     cudaFuncGetAttributes(&a, ms_p0_kernel<SP, XP, NCOMP>);
-    cudaFuncGetAttributes(&a, ms_xpm_kernel<SP, XP, NCOMP>);
+    if constexpr (SP == SP64) cudaFuncGetAttributes(&a, ms_xpm64_kernel<NCOMP, ms_xpm64_parts<NCOMP>()>);
+    else cudaFuncGetAttributes(&a, ms_xpm_kernel<SP, XP, NCOMP>);
   }
   static MsOps table() {
     return MsOps{&iterate, &dx64, &res64, &flush, &sloppy, &from_ref, &to_ref, &dirs_from64, &preload};

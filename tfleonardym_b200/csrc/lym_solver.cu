@@ -1343,6 +1343,9 @@ using namespace lym;
 // ---------------------------------------------------------------------------
 static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
   const int64_t V = g->V;
+  // what the solver workspaces (and their CUDA graphs) point at
+  const void* held[5] = {g->u32, g->u16, g->u32f, g->u16f, g->nbr};
+  const bool held_comp = g->comp;
   LYM_CUDA(cudaMemcpyAsync(g->uref, gauge, sizeof(double2) * g->nd * g->nc * g->nc * V, cudaMemcpyDeviceToDevice, st));
   // decide on link compression for the sloppy copies: links must be SU(N)
   Scratch* s;
@@ -1416,8 +1419,14 @@ static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
   else LYM_PACK(4, 3);
 #undef LYM_PACK
   LYM_CHECK_LAUNCH();
-  free_all_work(g);  // sloppy gauge pointers / compression may have changed
-  free_ms_works(g);
+  // The links were rewritten in place.  Workspaces stay valid unless a sloppy
+  // copy moved or the compression changed (their hop-kernel choices and graphs
+  // hold those pointers); keeping them spares an HMC step the workspace setup.
+  const void* now[5] = {g->u32, g->u16, g->u32f, g->u16f, g->nbr};
+  if (g->comp != held_comp || std::memcmp(held, now, sizeof(held)) != 0) {
+    free_all_work(g);
+    free_ms_works(g);
+  }
   return LYM_OK;
 }
 
