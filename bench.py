@@ -91,6 +91,9 @@ def parse_args():
     ap.add_argument("--ms-switch", default="0",
                     help="FP64-head switch residuals of --multishift (0: the library default, <0: no head)")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
+    ap.add_argument("--serve-shifted", default="full", choices=["full", "f64", "f32", "f16"],
+                    help="solver of --serve-sweep's shifted requests: the full-lattice FP64 multishift, or the "
+                         "even-odd multishift with that inner precision")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per rate")
     ap.add_argument("--serve-max-requests", type=int, default=600)
     ap.add_argument("--sweep-tiles", action="store_true",
@@ -758,11 +761,12 @@ def _request_specs(rng, n, max_bytes=2 << 30):
     return specs
 
 
-def _serve(specs, times, precision, workers, max_batch, dev, budget):
+def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision=None):
     import torch
 
     from tfleonardym_b200 import serving
-    srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=dev.index)
+    srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=dev.index,
+                              shifted_precision=shifted_precision)
     futs = []
     t0 = time.perf_counter()
     for sp, t in zip(specs, times):
@@ -799,7 +803,8 @@ def run_serve_sweep(args, local_rank):
     """Open-loop Poisson streams of mixed solve requests through the solve server at
     each rate of --serve-rates (arrivals over --serve-seconds, at most
     --serve-max-requests), inner precision FP16 for unshifted requests (shifted ones
-    run the FP64 multishift CG), every answer checked by its FP64 true residual.
+    run the full-lattice FP64 multishift CG, or with --serve-shifted a precision the
+    even-odd multishift in it), every answer checked by its FP64 true residual.
     Then the lowest rate's requests again as plain FP64 one-at-a-time solves (one
     worker, batches of one)."""
     import torch
@@ -810,8 +815,9 @@ def run_serve_sweep(args, local_rank):
     dev = torch.device("cuda", local_rank)
     budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
     rates = [float(r) for r in args.serve_rates.split(",")]
+    shifted = None if args.serve_shifted == "full" else args.serve_shifted
     warm = _request_specs(np.random.default_rng(1), 24)
-    _serve(warm, [0.0] * len(warm), "f16", args.workers, args.nrhs, dev, budget)  # compile-free warm-up of the path
+    _serve(warm, [0.0] * len(warm), "f16", args.workers, args.nrhs, dev, budget, shifted)  # warm-up of the path
     first = None
     for rate in rates:
         rng = np.random.default_rng(int(rate) + 7)
@@ -820,9 +826,9 @@ def run_serve_sweep(args, local_rank):
         specs = _request_specs(rng, len(times))
         if first is None:
             first = (specs, times)
-        r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget)
+        r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget, shifted)
         print(json.dumps({"serve_sweep": "mixed", "rate_per_s": rate, "workers": args.workers,
-                          "max_batch_rhs": args.nrhs, **r}), flush=True)
+                          "max_batch_rhs": args.nrhs, "shifted_solver": args.serve_shifted, **r}), flush=True)
     specs, times = first
     r = _serve(specs, times, "f64", 1, 1, dev, budget)
     print(json.dumps({"serve_sweep": "plain_fp64_one_at_a_time", "rate_per_s": rates[0], **r}), flush=True)

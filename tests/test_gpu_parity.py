@@ -400,6 +400,26 @@ def test_nf2_force_with_eo_square_solver(cuda_device, case, precision):
     assert solver.total_iterations > 0
 
 
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_rational_approximation_with_eo_square_solver(cuda_device, precision):
+    """RationalApproximation.apply (dirac.py:52-59) with positive poles: the even-odd
+    square solver (even-odd multishift) against the reference's MMMR."""
+    from tfleonardym_b200 import dirac, dirac_solver
+    dirac_solver.VERBOSE = False
+    g = load_golden("d4")
+    spec = GOLDEN_CASES["d4"]
+    q = make_op(g, spec)
+    # descending poles: the reference's MMMR iterates on the last (smallest) one
+    alphas, betas = [0.1, 0.25, 0.4], [1.5, 0.05, 0.002]
+    ra_ref = dirac.RationalApproximation(dirac.SquareOperator(q), alphas, betas, 0.3,
+                                         dirac_solver.multishift_solver(5000, 1e-24))
+    solver = dirac_solver.eo_square_solver(tol=1e-12, precision=precision)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), alphas, betas, 0.3, solver)
+    v = cu(g["eta"])
+    assert relerr(np_(ra.apply(v)), np_(ra_ref.apply(v))) < 1e-9
+    assert solver.total_iterations > 0
+
+
 @pytest.mark.parametrize("case", ["d2", "d4"])
 def test_md_trajectory_vs_reference(cuda_device, case):
     """integrate_om (hmc.py:133-162) with the Nf=2 and gauge actions from the golden inputs."""

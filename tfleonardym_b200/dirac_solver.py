@@ -266,8 +266,8 @@ class eo_square_solver:  # noqa: N801 - named like the reference solvers
     with the interface of multishift_solver (dirac_solver.py:19), so that it plugs
     into RationalApproximation and fermion_action.n_flavor.  sigma = 0: two
     even-odd CG solves Q y = b, Q x = y (conjugate_gradient, relative true residual
-    ``tol`` each, inner ``precision``); sigma > 0: multishift_cg (relative
-    tolerance ``tol``).  ``last_iterations`` holds the CG iterations of the last call."""
+    ``tol`` each, inner ``precision``); sigma > 0: the even-odd multishift_cg in the
+    same inner precision (relative tolerance ``tol`` per shift).  ``last_iterations`` holds the CG iterations of the last call."""
 
     def __init__(self, tol=1e-10, precision="f64", max_steps=20000, **cg_options):
         self.tol = tol
@@ -298,7 +298,8 @@ class eo_square_solver:  # noqa: N801 - named like the reference solvers
         if rest:
             if any(shifts[i] < 0 for i in rest):
                 raise ValueError("eo_square_solver takes shifts >= 0")
-            ms = multishift_cg(self.max_steps, self.tol)
+            ms = multishift_cg(self.max_steps, self.tol, precision=self.precision,
+                               delta=self.cg_options.get("delta", 0.1), chunk=self.cg_options.get("chunk", 8))
             xs = ms.solve(operator, source, [shifts[i] for i in rest])
             self.last_iterations += ms.last_steps
             for k, i in enumerate(rest):

@@ -98,11 +98,14 @@ class SolveResult:
         return r.t_end - r.t_submit
 
 
-def footprint_bytes(geometry, nc, nrhs, precision="f16", with_gauge=True, nshift=0):
+def footprint_bytes(geometry, nc, nrhs, precision="f16", with_gauge=True, nshift=0, shifted_precision=None):
     """Device bytes a request occupies: its sources and solutions, its share of
     the solver workspace and (when not resident yet) the gauge copies.  A
     shifted request holds nshift solutions and search vectors plus a few
-    full-lattice FP64 work vectors."""
+    full-lattice FP64 work vectors (shifted_precision None: the full-lattice
+    FP64 multishift), or with the even-odd multishift in shifted_precision its
+    FP64 solutions, the FP64 (head) workspace, the inner precision's and up to
+    nshift one-shift refinement groups."""
     vol = int(np.prod(geometry))
     nd = len(geometry)
     ns = 2 if nd == 2 else 4
@@ -110,7 +113,14 @@ def footprint_bytes(geometry, nc, nrhs, precision="f16", with_gauge=True, nshift
     spin = vol * ncomp * 16
     if nshift:
         link = nd * nc * nc * vol * 16
-        return int((2 * nshift + 6) * spin + (3 * link if with_gauge else 0))
+        if shifted_precision is None:
+            spins = 2 * nshift + 6
+        else:
+            spins = 9 + 3 * nshift  # FP64 store and FP64 (head) workspace
+            if shifted_precision != "f64":
+                ratio = {"f32": 0.5, "f16": 0.25 + 0.25 / ncomp, "bf16": 0.25 + 0.25 / ncomp}[shifted_precision]
+                spins += 2 + (6 + nshift) * ratio + 0.5 * nshift + nshift * (2 + 8 * ratio)
+        return int(spins * spin + (3 * link if with_gauge else 0))
     sloppy = {"f64": 16, "f32": 8, "f16": 4 + 4 / ncomp, "bf16": 4 + 4 / ncomp}[precision]
     per_rhs = 2 * spin + 7 * spin / 2 + 5 * (vol / 2) * ncomp * sloppy
     gauge = 0
@@ -150,8 +160,12 @@ class _Gauge:
 
 
 class SolveServer:
-    def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None):
+    def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
+                 shifted_precision=None):
         self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
+        # shifted requests: None = the full-lattice FP64 multishift (lym_multishift_solve); a precision =
+        # the even-odd multishift (lym_multishift_solve_eo) with that inner precision
+        self.shifted_precision = shifted_precision
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch)
         self.device = device  # CUDA device index; None: the caller's current device
@@ -208,7 +222,8 @@ class SolveServer:
     def _request_bytes(self, req):
         resident = req.gauge_key in self._gauges
         return footprint_bytes(req.geometry, req.nc, req.nrhs, req.precision, with_gauge=not resident,
-                               nshift=len(req.shifts) if req.shifts is not None else 0)
+                               nshift=len(req.shifts) if req.shifts is not None else 0,
+                               shifted_precision=self.shifted_precision)
 
     def _admit(self, req):
         self._in_use += req._bytes
@@ -310,19 +325,22 @@ class SolveServer:
                 self._release(batch)
 
     def _solve_shifted(self, req, g, widx):
-        """(Q^2 + sigma_k) x_k = b by multishift CG, then each true residual in FP64."""
+        """(Q^2 + sigma_k) x_k = b by multishift CG (the server's shifted_precision
+        picks the solver), then each true residual in FP64 through the
+        reference-layout operator."""
         from . import _dev, dirac, dirac_solver
         dev = torch.device("cuda", self.device)
         b = (req.b if req.b.dim() == 3 else req.b[0]).to(dev, non_blocking=True)
         op = g.op_for(widx, req.kappa, True)
-        ms = dirac_solver.multishift_cg(req.max_iter, req.tol)
+        ms = dirac_solver.multishift_cg(req.max_iter, req.tol, precision=self.shifted_precision, delta=0.01)
         xs = ms.solve(dirac.SquareOperator(op), b, req.shifts)
         bn = float(np.sqrt(abs(_dev.cdot(b, b))))
         reports = []
-        for s, x in zip(req.shifts, xs):
+        for k, (s, x) in enumerate(zip(req.shifts, xs)):
             r = _dev.axpby(1.0, b, -1.0, _dev.axpby(1.0, op.apply(op.apply(x)), s, x))
             res = float(np.sqrt(abs(_dev.cdot(r, r)))) / bn
-            reports.append(dict(status=0, iterations=ms.last_steps, true_residual=res, shift=s))
+            its = ms.reports[k]["iterations"] if ms.reports else ms.last_steps
+            reports.append(dict(status=0, iterations=its, true_residual=res, shift=s))
         x = torch.stack(xs)
         if req.out is not None:
             req.out.copy_(x, non_blocking=True)
