@@ -91,7 +91,7 @@ def parse_args():
     ap.add_argument("--ms-switch", default="0",
                     help="FP64-head switch residuals of --multishift (0: the library default, <0: no head)")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
-    ap.add_argument("--serve-shifted", default="full", choices=["full", "f64", "f32", "f16"],
+    ap.add_argument("--serve-shifted", default="f64", choices=["full", "f64", "f32", "f16"],
                     help="solver of --serve-sweep's shifted requests: the full-lattice FP64 multishift, or the "
                          "even-odd multishift with that inner precision")
     ap.add_argument("--serve-seconds", type=float, default=6.0, help="arrival window per rate")
@@ -761,7 +761,7 @@ def _request_specs(rng, n, max_bytes=2 << 30):
     return specs
 
 
-def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision=None):
+def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64"):
     import torch
 
     from tfleonardym_b200 import serving
@@ -803,8 +803,9 @@ def run_serve_sweep(args, local_rank):
     """Open-loop Poisson streams of mixed solve requests through the solve server at
     each rate of --serve-rates (arrivals over --serve-seconds, at most
     --serve-max-requests), inner precision FP16 for unshifted requests (shifted ones
-    run the full-lattice FP64 multishift CG, or with --serve-shifted a precision the
-    even-odd multishift in it), every answer checked by its FP64 true residual.
+    run the even-odd multishift CG in --serve-shifted's precision, FP64 by default, or
+    with --serve-shifted full the full-lattice FP64 multishift), every answer checked
+    by its FP64 true residual.
     Then the lowest rate's requests again as plain FP64 one-at-a-time solves (one
     worker, batches of one)."""
     import torch
@@ -830,7 +831,7 @@ def run_serve_sweep(args, local_rank):
         print(json.dumps({"serve_sweep": "mixed", "rate_per_s": rate, "workers": args.workers,
                           "max_batch_rhs": args.nrhs, "shifted_solver": args.serve_shifted, **r}), flush=True)
     specs, times = first
-    r = _serve(specs, times, "f64", 1, 1, dev, budget)
+    r = _serve(specs, times, "f64", 1, 1, dev, budget, None)  # plain: full-lattice FP64 multishift too
     print(json.dumps({"serve_sweep": "plain_fp64_one_at_a_time", "rate_per_s": rates[0], **r}), flush=True)
     return 0
 

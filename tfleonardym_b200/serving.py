@@ -14,8 +14,8 @@ tolerance, precision and operator form into one multi-right-hand-side solve
 (``lym_wilson_solve``), up to ``max_batch`` right-hand sides.  Requests that
 arrive while a batch runs join the next batch, and batches of different
 gauges run concurrently on different streams.  A request with ``shifts``
-solves (Q^2 + sigma_k) x_k = b for all its shifts in one multishift CG
-(lym_multishift_solve, FP64) and is served on its own.  Every answer carries
+solves (Q^2 + sigma_k) x_k = b for all its shifts in one multishift CG (by
+default the even-odd lym_multishift_solve_eo in FP64) and is served on its own.  Every answer carries
 the FP64 true residual (recomputed here for the shifted systems); a request
 whose residual misses its tolerance completes with status NOT_CONVERGED.
 
@@ -161,10 +161,11 @@ class _Gauge:
 
 class SolveServer:
     def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
-                 shifted_precision=None):
+                 shifted_precision="f64"):
         self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
-        # shifted requests: None = the full-lattice FP64 multishift (lym_multishift_solve); a precision =
-        # the even-odd multishift (lym_multishift_solve_eo) with that inner precision
+        # shifted requests: a precision = the even-odd multishift (lym_multishift_solve_eo) with that inner
+        # precision (FP64 by default: the fastest for the mixed request streams measured); None = the
+        # full-lattice FP64 multishift (lym_multishift_solve)
         self.shifted_precision = shifted_precision
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch)
