@@ -92,8 +92,9 @@ int lym_lattice_tables_device(const lym_lattice* lat, int64_t* sup_dev, int64_t*
  * D psi = psi + kappa sum_mu [U_mu(x)(1-g_mu)psi(x+mu) + U_mu(x-mu)^dag(1+g_mu)psi(x-mu)].
  * Replaces DiracWilsonOperator.multiply_in_fundamental_representation /
  * simple_multiply_in_fundamental_representation + apply_hermiticity
- * (dirac.py:458-523, 649-662).  nd in {2, 4}; nd = 3 is builder-defined
- * (Pauli gammas, no reference counterpart).  `in` and `out` must not alias. */
+ * (dirac.py:458-523, 649-662).  nd in {2, 4}, the reference's fermion
+ * dimensions; any other nd returns LYM_ERR_UNSUPPORTED with the reference's
+ * message (dirac.py:299-300).  `in` and `out` must not alias. */
 int lym_wilson_apply(const lym_lattice* lat, int nc, double kappa, int hermitian,
                      double bc_re, double bc_im, const void* gauge,
                      const void* in, void* out, void* stream);

@@ -110,15 +110,6 @@ template <> struct Gamma<2> {
   LYM_HD static int phase(int mu, int) { return mu == 0 ? 0 : 3; }
 };
 
-// D = 3 (builder-defined, no reference counterpart): 2-component spinors
-// with gamma_mu = Pauli sigma_{mu+1}.  sigma3 is diagonal, so the hop uses
-// the full 2-component projector instead of the half-spinor trick.
-template <> struct Gamma<3> {
-  static constexpr int NS = 2;
-  LYM_HD static int col(int, int) { return 1; }
-  LYM_HD static int phase(int mu, int) { return mu == 0 ? 0 : 3; }
-};
-
 // ---------------------------------------------------------------------------
 // error handling
 // ---------------------------------------------------------------------------
