@@ -223,9 +223,9 @@ def test_multishift_eo(cuda_device, case, precision):
 @pytest.mark.parametrize("precision", ["f32", "f16"])
 @pytest.mark.parametrize("tile", [0, 1])
 def test_multishift_eo_padded_groups(cuda_device, precision, tile):
-    """Five sources (four per hop thread, three padding groups, or one per
-    thread), 17 shifts from 1e-4 to 300 (a rational approximation's spread):
-    true residual 1e-10 each."""
+    """Five sources (FP32: four per hop thread and three padding groups, or
+    one per thread; FP16: one per thread, mixed-precision hop), 17 shifts from
+    1e-4 to 300 (a rational approximation's spread): true residual 1e-10 each."""
     from tfleonardym_b200 import dirac, dirac_solver
     g = load_golden("d4")
     spec = GOLDEN_CASES["d4"]
@@ -236,7 +236,8 @@ def test_multishift_eo_padded_groups(cuda_device, precision, tile):
     b = (rng.normal(size=(5,) + g["eta"].shape) + 1j * rng.normal(size=(5,) + g["eta"].shape)) / np.sqrt(2)
     ms = dirac_solver.multishift_cg(5000, 1e-10, precision=precision, delta=0.01, rhs_per_thread=tile)
     xs = ms.solve(dirac.SquareOperator(op), cu(b), shifts)
-    assert ms.reports[0]["rhs_per_thread"] == (1 if tile == 1 else 4)
+    # four groups per thread in FP32 unless forced to one; FP16 always one (mixed-precision hop)
+    assert ms.reports[0]["rhs_per_thread"] == (4 if precision == "f32" and tile == 0 else 1)
     for k, s in enumerate(shifts):
         x = np_(xs[k])
         for i in range(5):

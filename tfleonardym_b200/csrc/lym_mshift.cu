@@ -113,13 +113,27 @@ LYM_HD EoField sub(const EoField& f, int64_t slot) {
 
 LYM_D int eo_block_parity(int nblk) { return blockIdx.x >= (unsigned)nblk ? 1 : 0; }
 
+// The hop of the multishift kernels: FP32 arithmetic (MX = 0, hop_tile), or
+// for FP16 spinors with full links the mixed-precision form (MX = 1,
+// hop_tile_mx: f16 x f16 + f32 FMAs), as the CG's autotuner picks for FP16.
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
+LYM_D void ms_hop(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
+                  const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
+  if constexpr (MX != 0) {
+    static_assert(SP == SP16 && GP == SP16 && !COMP, "the mixed-precision hop takes FP16 spinors and full links");
+    hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+  } else {
+    hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // sloppy iteration kernels; grids (2 nblk, G / R): blocks [0, nblk) even sites,
 // [nblk, 2 nblk) odd sites, R groups per thread sharing each link
 // ---------------------------------------------------------------------------
 
 // w = p + kappa H p (p = the base direction); |w|^2 and |p|^2 -> alpha
-template <int ND, int NC, int SP, int GP, bool COMP, int R>
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
 __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0)
     ms_dp_kernel(EoGeom g, HopGauge hg, EoField pb, EoField w, int G, double kappa, MsGroup* grp,
                  double* partials, unsigned* counters, int nblk) {
@@ -142,7 +156,7 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0)
   for (int k = 0; k < 2 * R; ++k) n[k] = 0.0;
   if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    hop_tile<ND, NC, SP, GP, COMP, false, R>(g, hg, sub(pb, (1 - par) * G), g0, i, par, act, acc);
+    ms_hop<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, sub(pb, (1 - par) * G), g0, i, par, act, acc);
     const EoField pin = sub(pb, par * G), wout = sub(w, par * G);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -181,7 +195,7 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0)
 
 // r -= alpha (w + kappa gamma_d H gamma_d w + sigma_0 p); |r|^2 -> beta; the
 // last block then advances every shift's recurrences (one thread per shift)
-template <int ND, int NC, int SP, int GP, bool COMP, int R>
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
 __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0)
     ms_ap_kernel(EoGeom g, HopGauge hg, EoField w, EoField pb, EoField ring, int G, int S, double kappa,
                  MsGroup* grp, MsShift* shf, double* partials, unsigned* counters, int nblk) {
@@ -206,7 +220,7 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0)
   for (int q = 0; q < R; ++q) n[q] = 0.0;
   if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    hop_tile<ND, NC, SP, GP, COMP, true, R>(g, hg, sub(w, (1 - par) * G), g0, i, par, act, acc);
+    ms_hop<ND, NC, SP, GP, COMP, true, R, MX>(g, hg, sub(w, (1 - par) * G), g0, i, par, act, acc);
     const EoField wv = sub(w, par * G), pv = sub(pb, par * G);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
@@ -714,7 +728,7 @@ static void ms_launch(MsWork& w, cudaStream_t st, void (*kernel)(KArgs...), dim3
   launch_rec(w.rec, st, kernel, grid, block, std::forward<Args>(args)...);
 }
 
-template <int ND, int NC, int SP, bool COMP, int R>
+template <int ND, int NC, int SP, bool COMP, int R, int MX>
 struct MsImpl {
   static constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   static constexpr int GP = SP == SP64 ? SP64 : (SP == SP32 ? SP32 : SP16);
@@ -722,9 +736,9 @@ struct MsImpl {
 
   static void iterate(MsWork& w, cudaStream_t st, int i) {
     dim3 tile(2 * w.nblk, w.G / R), grid(2 * w.nblk, w.G);
-    ms_launch(w, st, ms_dp_kernel<ND, NC, SP, GP, COMP, R>, tile, dim3(128), w.g->geom, w.hgs, w.pb, w.w, w.G,
+    ms_launch(w, st, ms_dp_kernel<ND, NC, SP, GP, COMP, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.pb, w.w, w.G,
               w.kappa, w.grp, w.partials, w.counters + w.G, w.nblk);
-    ms_launch(w, st, ms_ap_kernel<ND, NC, SP, GP, COMP, R>, tile, dim3(128), w.g->geom, w.hgs, w.w, w.pb, w.ring,
+    ms_launch(w, st, ms_ap_kernel<ND, NC, SP, GP, COMP, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.w, w.pb, w.ring,
               w.G, w.S, w.kappa, w.grp, w.shf, w.partials, w.counters + w.G, w.nblk);
     ms_launch(w, st, ms_p0_kernel<SP, XP, NCOMP>, grid, dim3(128), w.Vh, w.nblk, w.G, w.S, w.ring, w.pb, w.xs, w.grp,
               w.counters);
@@ -777,8 +791,8 @@ struct MsImpl {
   }
   static void preload() {
     cudaFuncAttributes a;
-    cudaFuncGetAttributes(&a, ms_dp_kernel<ND, NC, SP, GP, COMP, R>);
-    cudaFuncGetAttributes(&a, ms_ap_kernel<ND, NC, SP, GP, COMP, R>);
+    cudaFuncGetAttributes(&a, ms_dp_kernel<ND, NC, SP, GP, COMP, R, MX>);
+    cudaFuncGetAttributes(&a, ms_ap_kernel<ND, NC, SP, GP, COMP, R, MX>);
     cudaFuncGetAttributes(&a, ms_p0_kernel<SP, XP, NCOMP>);
     if constexpr (SP == SP64) cudaFuncGetAttributes(&a, ms_xpm64_kernel<NCOMP, ms_xpm64_parts<NCOMP>()>);
     else cudaFuncGetAttributes(&a, ms_xpm_kernel<SP, XP, NCOMP>);
@@ -788,13 +802,17 @@ struct MsImpl {
   }
 };
 
+// FP64: one group per thread; FP32: R groups per thread, 12-real links when
+// the links allow; FP16: one group per thread, full links, mixed-precision hop;
+// BF16: one group per thread, full links (the 16-bit choices are the fastest
+// tiles of the CG's hop sweep)
 template <int ND, int NC, int R>
 static MsOps ms_pick_sp(int sp, bool comp) {
   switch (sp) {
-    case SP64: return MsImpl<ND, NC, SP64, false, 1>::table();
-    case SP32: return comp ? MsImpl<ND, NC, SP32, true, R>::table() : MsImpl<ND, NC, SP32, false, R>::table();
-    case SP16: return comp ? MsImpl<ND, NC, SP16, true, R>::table() : MsImpl<ND, NC, SP16, false, R>::table();
-    default: return comp ? MsImpl<ND, NC, SPB16, true, R>::table() : MsImpl<ND, NC, SPB16, false, R>::table();
+    case SP64: return MsImpl<ND, NC, SP64, false, 1, 0>::table();
+    case SP32: return comp ? MsImpl<ND, NC, SP32, true, R, 0>::table() : MsImpl<ND, NC, SP32, false, R, 0>::table();
+    case SP16: return MsImpl<ND, NC, SP16, false, 1, 1>::table();
+    default: return MsImpl<ND, NC, SPB16, false, 1, 0>::table();
   }
 }
 
@@ -882,9 +900,9 @@ void free_ms_works(lym_gauge* g) {
 // multiple of 4).  `keep` is never evicted (the workspace the others borrow from).
 static int ms_get(lym_gauge* g, int cap, int S, int sp, int store_rhs, int want_r, const MsWork* keep,
                   MsWork** out) {
-  const int R = (sp == SP64 || cap < 4 || want_r == 1) ? 1 : 4;
+  const int R = (sp == SP32 && cap >= 4 && want_r != 1) ? 4 : 1;
   const int G = (cap + R - 1) / R * R;
-  const bool comp = g->comp && sp != SP64;
+  const bool comp = g->comp && sp == SP32;
   for (size_t i = 0; i < g->ms_works.size(); ++i) {
     MsWork* w = g->ms_works[i];
     if (w->cap == cap && w->S == S && w->sp == sp && w->store_rhs == store_rhs && w->R == R) {
