@@ -67,7 +67,7 @@
 namespace lym {
 
 constexpr int kMsMaxShifts = 32;
-constexpr int kMsBlock = 4;  // iterations per blocked shift update (ms_xpm)
+constexpr int kMsBlock = 8;  // iterations per blocked shift update (ms_xpm)
 
 // LYM_MS_TRACE=1 in the environment prints every reliable-update decision and
 // the per-shift verification to stderr.
@@ -400,17 +400,42 @@ __global__ void __launch_bounds__(128) ms_xpm_kernel(int64_t Vh, int nblk, int G
   }
 }
 
-// ms_xpm for FP64 (no per-site norm): each thread takes one site and UPT of
-// its NU complex components (NG = NU / UPT threads per site, consecutive
-// sites in a block, so every load stays coalesced), which leaves room to hold
-// the pending ring residuals in registers for all shifts.  The coefficients
-// are real, so the update is component-wise.  Grid (2 nblk NG, G).
-template <int NCOMP, int NG>
-__global__ void __launch_bounds__(128) ms_xpm64_kernel(int64_t Vh, int nblk, int G, int S, EoField ring, EoField ps,
-                                                       EoField xs, MsGroup* grp, const MsShift* shf,
-                                                       unsigned* counters) {
-  static_assert(NCOMP % NG == 0, "components split evenly");
-  constexpr int UPT = NCOMP / NG;
+// ms_xpm for the precisions without a per-site norm (FP64, FP32; x in the
+// same precision): each thread takes one site and UPT of its NU 16-byte units
+// (NG = NU / UPT threads per site, consecutive sites in a block, so every load
+// stays coalesced), which leaves room to hold the pending ring residuals in
+// registers for all shifts.  The coefficients are real, so the update is
+// component-wise.  Grid (2 nblk NG, G).
+LYM_D void ms_axpy(double2& x, double a, const double2& p) {
+  x.x += a * p.x;
+  x.y += a * p.y;
+}
+LYM_D void ms_axpy(float4& x, float a, const float4& p) {
+  x.x += a * p.x;
+  x.y += a * p.y;
+  x.z += a * p.z;
+  x.w += a * p.w;
+}
+LYM_D void ms_lincomb(double2& p, double zn, const double2& r, double b) {
+  p.x = zn * r.x + b * p.x;
+  p.y = zn * r.y + b * p.y;
+}
+LYM_D void ms_lincomb(float4& p, float zn, const float4& r, float b) {
+  p.x = zn * r.x + b * p.x;
+  p.y = zn * r.y + b * p.y;
+  p.z = zn * r.z + b * p.z;
+  p.w = zn * r.w + b * p.w;
+}
+
+template <int SP, int NU, int NG>
+__global__ void __launch_bounds__(128) ms_xpm_split_kernel(int64_t Vh, int nblk, int G, int S, EoField ring,
+                                                           EoField ps, EoField xs, MsGroup* grp, const MsShift* shf,
+                                                           unsigned* counters) {
+  static_assert(SP == SP64 || SP == SP32, "no per-site norm");
+  static_assert(NU % NG == 0, "units split evenly");
+  using U = typename Prec<SP>::unit;
+  using RT = typename Prec<SP>::real;
+  constexpr int UPT = NU / NG;
   const int part = blockIdx.x % NG;
   const int rest = blockIdx.x / NG;
   const int par = rest >= nblk ? 1 : 0;
@@ -422,13 +447,13 @@ __global__ void __launch_bounds__(128) ms_xpm64_kernel(int64_t Vh, int nblk, int
   if (cb < Vh) {
     const int64_t vh = Vh, unit0 = (int64_t)part * UPT;
     auto field_at = [&](const EoField& f, int64_t slot) {
-      return reinterpret_cast<double2*>(f.data) + (slot * f.nunits + unit0) * vh + cb;
+      return reinterpret_cast<U*>(f.data) + (slot * f.nunits + unit0) * vh + cb;
     };
-    double2 rr[kMsBlock][UPT];
+    U rr[kMsBlock][UPT];
 #pragma unroll
     for (int j = 0; j < kMsBlock; ++j) {
       if (j >= n) break;
-      const double2* rp = field_at(ring, (int64_t)((k0 + j + 1) % kMsBlock) * 2 * G + par * G + gi);
+      const U* rp = field_at(ring, (int64_t)((k0 + j + 1) % kMsBlock) * 2 * G + par * G + gi);
 #pragma unroll
       for (int u = 0; u < UPT; ++u) rr[j][u] = __ldg(rp + u * vh);
     }
@@ -436,9 +461,9 @@ __global__ void __launch_bounds__(128) ms_xpm64_kernel(int64_t Vh, int nblk, int
       const MsShift& T = shf[(int64_t)gi * S + s];
       if (!T.run[k0 % kMsBlock]) continue;
       const int64_t slot = (int64_t)par * G * S + gi * S + s;
-      double2* pp = field_at(ps, slot);
-      double2* xp = field_at(xs, slot);
-      double2 pv[UPT], xv[UPT];
+      U* pp = field_at(ps, slot);
+      U* xp = field_at(xs, slot);
+      U pv[UPT], xv[UPT];
 #pragma unroll
       for (int u = 0; u < UPT; ++u) {
         pv[u] = pp[u * vh];
@@ -449,13 +474,11 @@ __global__ void __launch_bounds__(128) ms_xpm64_kernel(int64_t Vh, int nblk, int
         if (j >= n) break;
         const int ix = (k0 + j) % kMsBlock;
         if (!T.run[ix]) break;  // the shift stopped after its previous step
-        const double a = T.a[ix], zn = T.zn[ix], b = T.b[ix];
+        const RT a = (RT)T.a[ix], zn = (RT)T.zn[ix], b = (RT)T.b[ix];
 #pragma unroll
         for (int u = 0; u < UPT; ++u) {
-          xv[u].x += a * pv[u].x;
-          xv[u].y += a * pv[u].y;
-          pv[u].x = zn * rr[j][u].x + b * pv[u].x;
-          pv[u].y = zn * rr[j][u].y + b * pv[u].y;
+          ms_axpy(xv[u], a, pv[u]);
+          ms_lincomb(pv[u], zn, rr[j][u], b);
         }
       }
 #pragma unroll
@@ -475,8 +498,8 @@ __global__ void __launch_bounds__(128) ms_xpm64_kernel(int64_t Vh, int nblk, int
   }
 }
 
-// threads per site of ms_xpm64: about three complex components each
-template <int NCOMP> constexpr int ms_xpm64_parts() { return NCOMP % 4 == 0 && NCOMP >= 8 ? 4 : 2; }
+// threads per site of ms_xpm_split: at most three 16-byte units each
+template <int NU> constexpr int ms_xpm_parts() { return NU % 4 == 0 && NU >= 8 ? 4 : (NU % 2 == 0 && NU > 3 ? 2 : 1); }
 
 // ---------------------------------------------------------------------------
 // FP64 kernels (reliable updates, verification); grids (2 nblk, G).
@@ -743,10 +766,10 @@ struct MsImpl {
     ms_launch(w, st, ms_p0_kernel<SP, XP, NCOMP>, grid, dim3(128), w.Vh, w.nblk, w.G, w.S, w.ring, w.pb, w.xs, w.grp,
               w.counters);
     if ((i + 1) % kMsBlock == 0) {
-      if constexpr (SP == SP64) {
-        constexpr int NG = ms_xpm64_parts<NCOMP>();
-        ms_launch(w, st, ms_xpm64_kernel<NCOMP, NG>, dim3(2 * w.nblk * NG, w.G), dim3(128), w.Vh, w.nblk, w.G, w.S,
-                  w.ring, w.ps, w.xs, w.grp, (const MsShift*)w.shf, w.counters);
+      if constexpr (SP == SP64 || SP == SP32) {
+        constexpr int NU = units_for(NCOMP, Prec<SP>::CPU), NG = ms_xpm_parts<NU>();
+        ms_launch(w, st, ms_xpm_split_kernel<SP, NU, NG>, dim3(2 * w.nblk * NG, w.G), dim3(128), w.Vh, w.nblk, w.G,
+                  w.S, w.ring, w.ps, w.xs, w.grp, (const MsShift*)w.shf, w.counters);
       } else {
         ms_launch(w, st, ms_xpm_kernel<SP, XP, NCOMP>, grid, dim3(128), w.Vh, w.nblk, w.G, w.S, w.ring, w.ps, w.xs,
                   w.grp, (const MsShift*)w.shf, w.counters);
@@ -794,7 +817,10 @@ struct MsImpl {
     cudaFuncGetAttributes(&a, ms_dp_kernel<ND, NC, SP, GP, COMP, R, MX>);
     cudaFuncGetAttributes(&a, ms_ap_kernel<ND, NC, SP, GP, COMP, R, MX>);
     cudaFuncGetAttributes(&a, ms_p0_kernel<SP, XP, NCOMP>);
-    if constexpr (SP == SP64) cudaFuncGetAttributes(&a, ms_xpm64_kernel<NCOMP, ms_xpm64_parts<NCOMP>()>);
+    if constexpr (SP == SP64 || SP == SP32) {
+      constexpr int NU = units_for(NCOMP, Prec<SP>::CPU);
+      cudaFuncGetAttributes(&a, ms_xpm_split_kernel<SP, NU, ms_xpm_parts<NU>()>);
+    }
     else cudaFuncGetAttributes(&a, ms_xpm_kernel<SP, XP, NCOMP>);
   }
   static MsOps table() {
