@@ -46,6 +46,23 @@ def _req(key, geom=(4, 4, 4, 4), nrhs=1, kappa=0.12, tol=1e-10):
     return serving.SolveRequest(key, geom, 3, kappa, b, gauge=None, tol=tol)
 
 
+def test_shifted_footprint_follows_the_solver():
+    """A shifted request's HBM estimate: the even-odd multishift keeps its FP64
+    solutions, an FP64 (head) workspace and, for a reduced inner precision, that
+    workspace and the refinement groups; the full-lattice FP64 multishift less."""
+    geom, nc, nsh = (8, 8, 8, 16), 3, 12
+    spin = int(np.prod(geom)) * 4 * nc * 16
+    full = serving.footprint_bytes(geom, nc, 1, "f16", with_gauge=False, nshift=nsh, shifted_precision=None)
+    eo64 = serving.footprint_bytes(geom, nc, 1, "f16", with_gauge=False, nshift=nsh, shifted_precision="f64")
+    eo32 = serving.footprint_bytes(geom, nc, 1, "f16", with_gauge=False, nshift=nsh, shifted_precision="f32")
+    assert full == (2 * nsh + 6) * spin
+    assert eo64 == (9 + 3 * nsh) * spin
+    assert full < eo64 < eo32
+    link = 4 * nc * nc * int(np.prod(geom)) * 16
+    with_gauge = serving.footprint_bytes(geom, nc, 1, "f16", with_gauge=True, nshift=nsh, shifted_precision="f64")
+    assert with_gauge == eo64 + 3 * link
+
+
 def test_rejects_requests_that_can_never_fit():
     srv = _FakeServer(hbm_budget_bytes=10_000, workers=1)
     f = srv.submit(_req("g", geom=(16, 16, 16, 16)))

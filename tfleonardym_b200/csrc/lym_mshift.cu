@@ -31,8 +31,9 @@
 //           kMsBlock fields, the coefficients in per-shift rings), the same
 //           arithmetic in the same order.
 // All scalars stay on the device; iterations run in CUDA graphs of `chunk`
-// iterations (a multiple of kMsBlock, ending with ms_xpm).  A group pauses itself when its sloppy residual fell by delta;
-// the host then does an FP64 reliable update: x64_k += x_k for every shift,
+// iterations (a multiple of kMsBlock, ending with ms_xpm).  A group pauses
+// itself when its sloppy residual fell by delta; the host then does an FP64
+// reliable update: x64_k += x_k for every shift,
 // r = b - (Q^2 + sigma_0) x64_0 in FP64 (the true base residual), which
 // replaces the sloppy r; the directions and zetas carry on.  A group ends
 // when its true base residual is below tol |b|.
@@ -1220,6 +1221,17 @@ static void ms_init_states(MsWork& w, const std::vector<double>& group_base_sigm
   }
 }
 
+// Orders the caller's later work after everything the solve enqueued on its
+// own stream, on every way out of the solve (errors included).
+struct MsFence {
+  cudaEvent_t ev;
+  cudaStream_t from, to;
+  ~MsFence() {
+    cudaEventRecord(ev, from);
+    cudaStreamWaitEvent(to, ev, 0);
+  }
+};
+
 static int ms_solve_on(lym_gauge* g, double kappa, int nrhs, int nshift, const double* shifts, const void* b,
                        void* xs, const lym_solver_params* prm, lym_solver_report* rep, cudaStream_t caller) {
   const int sp = prm->precision;
@@ -1235,6 +1247,7 @@ static int ms_solve_on(lym_gauge* g, double kappa, int nrhs, int nshift, const d
   cudaStream_t st = w1.stream;
   LYM_CUDA(cudaEventRecord(w1.ev_in, caller));
   LYM_CUDA(cudaStreamWaitEvent(st, w1.ev_in, 0));
+  const MsFence fence{w1.ev_out, st, caller};
   w1.kappa = kappa;
   w1.launches = 0;
   w1.b64 = w1.own_b64;
@@ -1405,8 +1418,6 @@ static int ms_solve_on(lym_gauge* g, double kappa, int nrhs, int nshift, const d
   LYM_CHECK_LAUNCH();
   LYM_CUDA(cudaStreamSynchronize(st));
   launches += w1.launches;
-  cudaEventRecord(w1.ev_out, st);
-  cudaStreamWaitEvent(caller, w1.ev_out, 0);
   int result = LYM_OK;
   for (int i = 0; i < nrhs; ++i)
     for (int s = 0; s < S; ++s) {
