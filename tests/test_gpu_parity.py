@@ -245,6 +245,31 @@ def test_multishift_eo_padded_groups(cuda_device, precision, tile):
             assert res < 1e-10, (i, s, res, ms.reports[i * len(shifts) + k])
 
 
+def test_multishift_eo_edge_cases(cuda_device):
+    """A zero source gives zero solutions; one shift; a repeated shift gives the
+    same solution twice; too few iterations report NOT_CONVERGED per pair and
+    return the last iterate (as the reference's solvers do)."""
+    from tfleonardym_b200 import _lib, dirac, dirac_solver
+    dirac_solver.VERBOSE = False
+    g = load_golden("d4")
+    spec = GOLDEN_CASES["d4"]
+    sq = dirac.SquareOperator(make_op(g, spec))
+    setup = O.WilsonSetup(g["gauge"], spec["kappa"], spec["geometry"])
+    b = np.stack([np.zeros_like(g["eta"]), g["eta"]])
+    ms = dirac_solver.multishift_cg(5000, 1e-10, precision="f32")
+    xs = ms.solve(sq, cu(b), [0.1])
+    x = np_(xs[0])
+    assert np.all(x[0] == 0) and ms.reports[0]["status"] == 0
+    res = np.linalg.norm(setup.Q2(x[1]) + 0.1 * x[1] - b[1]) / np.linalg.norm(b[1])
+    assert res < 1e-10
+    xs = ms.solve(sq, cu(g["eta"]), [0.2, 0.05, 0.2])
+    assert relerr(np_(xs[0]), np_(xs[2])) < 1e-12
+    short = dirac_solver.multishift_cg(3, 1e-10, precision="f64")
+    xs = short.solve(sq, cu(g["eta"]), [0.05, 0.5])
+    assert all(r["status"] == _lib.LYM_ERR_NOT_CONVERGED for r in short.reports)
+    assert all(np.isfinite(np_(x)).all() and np.linalg.norm(np_(x)) > 0 for x in xs)
+
+
 @pytest.mark.parametrize("switch", [-1.0, 1e-3, 1e-12])
 def test_multishift_eo_switch_points(cuda_device, switch):
     """Inner precision from the start (-1), after an FP64 head to 1e-3, and an
