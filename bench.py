@@ -842,7 +842,9 @@ def run_batch_lattices(args, local_rank):
     is 2D SU(2) here), kappa in [0.10, 0.14], links reunit(exp(i eps H)) with eps in
     [0.1, 0.4] -- with 4 unit complex Gaussian rhs each (256 solves), submitted
     together to the solve server (4 workers, one CUDA stream each) with FP32 inner
-    and FP64 outer iterations to true relative residual 1e-10.  Then the same 256
+    and FP64 outer iterations to true relative residual 1e-10; the same 256 solves
+    with all lattices of one (D, N) class in the same launches
+    (dirac_solver.solve_lattices, two calls).  Then the same 256
     solves as plain FP64 one-at-a-time solves, and one gauge HMC step per lattice
     (staples and force fused into the momentum update, then the link update).
     Device time of each phase by CUDA events around it (the server's streams are
@@ -899,6 +901,34 @@ def run_batch_lattices(args, local_rank):
     wall = time.perf_counter() - t0
     ok = sum(r.status == serving.OK for r in res)
     worst = max(m["true_residual"] for r in res for m in r.reports)
+    # the same 256 solves with every lattice of one (D, N) class in the same launches
+    from tfleonardym_b200 import boundary_conditions, dirac
+    prov = boundary_conditions.time_antiperiodic_provider(-1)
+    ops = [dirac.DiracWilsonOperator(lt.Configuration(g, l["geometry"], l["nc"], len(l["geometry"])), l["kappa"],
+                                     False, representation="fundamental", boundary_condition_provider=prov)
+           for g, l in zip(gauges, lattices)]
+    classes = {}
+    for k, l in enumerate(lattices):
+        classes.setdefault((len(l["geometry"]), l["nc"]), []).append(k)
+
+    def solve_together():
+        worst_m, launches = 0.0, 0
+        for ks in classes.values():
+            _, reps = dirac_solver.solve_lattices([ops[k] for k in ks], [sources[k] for k in ks], tol=1e-10,
+                                                  precision="f32", delta=0.01)
+            worst_m = max([worst_m] + [m["true_residual"] for r in reps for m in r])
+            launches += reps[0][0]["kernel_launches"]
+            ok_m = all(m["status"] == 0 for r in reps for m in r)
+            if not ok_m:
+                return worst_m, launches, False
+        return worst_m, launches, True
+
+    solve_together()  # warm-up: workspaces
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    worst_multi, multi_launches, multi_ok = solve_together()
+    torch.cuda.synchronize()
+    multi_wall = time.perf_counter() - t0
     solve_all("f64", 1, 1)  # warm-up of the plain path
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -920,6 +950,11 @@ def run_batch_lattices(args, local_rank):
         torch.cuda.synchronize()
     print(json.dumps({"batch_lattices": "64 uneven lattices x 4 rhs", "solves": 256, "ok": ok,
                       "worst_true_residual": worst, "wall_s": wall, "solves_per_s": 256 / wall,
+                      "one_launch_per_class": {"what": "lym_wilson_solve_multi: the 32 2D SU(2) lattices in one "
+                                                       "set of launches, the 32 4D SU(3) in another",
+                                               "all_ok": multi_ok, "worst_true_residual": worst_multi,
+                                               "wall_s": multi_wall, "solves_per_s": 256 / multi_wall,
+                                               "kernel_launches": multi_launches},
                       "plain_fp64_one_at_a_time": {"ok": sum(r.status == serving.OK for r in plain),
                                                    "wall_s": plain_wall, "solves_per_s": 256 / plain_wall},
                       "gauge_hmc_step_all_lattices_ms": e0.elapsed_time(e1),

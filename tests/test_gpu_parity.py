@@ -342,6 +342,46 @@ def _smooth_links(geometry, nc, seed, spread=0.3):
     return u
 
 
+@pytest.mark.parametrize("precision", ["f64", "f32", "f16"])
+@pytest.mark.parametrize("nd_nc", [(4, 3), (2, 2)])
+def test_solve_lattices_together(cuda_device, precision, nd_nc):
+    """Independent lattices of different geometry, kappa and rhs count in the same
+    launches (lym_wilson_solve_multi): every solution meets 1e-10 by the oracle's
+    operator and matches the lattice solved alone."""
+    from tfleonardym_b200 import boundary_conditions as bc
+    from tfleonardym_b200 import dirac, dirac_solver
+    from tfleonardym_b200 import lattice as lt
+    nd, nc = nd_nc
+    geoms = [(4, 4, 4, 8), (6, 4, 2, 4), (4, 2, 4, 4)] if nd == 4 else [(8, 6), (16, 12), (6, 4)]
+    kappas, counts = [0.11, 0.13, 0.12], [2, 1, 3]
+    rng = np.random.default_rng(5)
+    ops, srcs, links = [], [], []
+    for k, geom in enumerate(geoms):
+        u = _smooth_links(geom, nc, seed=31 + k)
+        links.append(u)
+        cfg = lt.Configuration(cu(u), geom, nc, nd)
+        ops.append(dirac.DiracWilsonOperator(cfg, kappas[k], False, representation="fundamental",
+                                             boundary_condition_provider=bc.time_antiperiodic_provider(-1)))
+        ns = 2 if nd == 2 else 4
+        shape = (counts[k], ns, nc, int(np.prod(geom)))
+        b = (rng.normal(size=shape) + 1j * rng.normal(size=shape)) / np.sqrt(2)
+        srcs.append(b if counts[k] > 1 else b[0])
+    xs, reps = dirac_solver.solve_lattices(ops, [cu(b) for b in srcs], tol=1e-10, precision=precision, delta=0.01)
+    for k, geom in enumerate(geoms):
+        tables = O.lookup_tables(geom)
+        ub = O.apply_time_bc(links[k], O.antiperiodic_field(geom))
+        x, b = np_(xs[k]), srcs[k]
+        assert x.shape == b.shape
+        xb, bb = (x, b) if counts[k] > 1 else (x[None], b[None])
+        alone = np_(dirac_solver.conjugate_gradient(tol=1e-10, precision="f64").solve(ops[k], cu(b)))
+        alone = alone if counts[k] > 1 else alone[None]
+        for i in range(counts[k]):
+            res = np.linalg.norm(bb[i] - O.wilson_apply(ub, xb[i], kappas[k], False, tables)) / np.linalg.norm(bb[i])
+            assert res < 1e-10, (k, i, res, reps[k][i])
+            assert reps[k][i]["status"] == 0 and reps[k][i]["true_residual"] < 1e-10
+            assert relerr(xb[i], alone[i]) < 1e-8
+
+
 @pytest.mark.parametrize("geometry,nc", [((4, 4, 4, 8), 3), ((2, 4, 4, 6), 3), ((4, 4, 4, 4), 2),
                                          ((8, 6), 2), ((12, 4), 3)])
 def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):

@@ -71,14 +71,15 @@ LYM_D void block_sum(double (&v)[NV], double* sh) {
 // returns true in every thread of that block, with the totals in `v`
 // (thread 0) -- the caller then writes results.  No block ever waits for
 // another, so there is no spin loop.
+// grid_sum_n: the same for a slot of nb blocks numbered blk (several slots
+// may share one launch, e.g. the lattices of a multi-lattice launch).
 template <int NV>
-LYM_D bool grid_sum(double (&v)[NV], double* partials, unsigned* counter, double* sh) {
+LYM_D bool grid_sum_n(double (&v)[NV], double* partials, unsigned* counter, double* sh, int blk, int nb) {
   __shared__ bool last;
   block_sum<NV>(v, sh);
-  const int nb = gridDim.x;
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) partials[blockIdx.x * NV + k] = v[k];
+    for (int k = 0; k < NV; ++k) partials[blk * NV + k] = v[k];
     __threadfence();
     unsigned t = atomicAdd(counter, 1u);
     last = (t == (unsigned)nb - 1);
@@ -100,6 +101,11 @@ LYM_D bool grid_sum(double (&v)[NV], double* partials, unsigned* counter, double
     *counter = 0u;  // ready for the next use of this slot
   }
   return true;
+}
+
+template <int NV>
+LYM_D bool grid_sum(double (&v)[NV], double* partials, unsigned* counter, double* sh) {
+  return grid_sum_n<NV>(v, partials, counter, sh, blockIdx.x, gridDim.x);
 }
 
 LYM_D cx<double> ld(const double2* p) {

@@ -357,12 +357,15 @@ LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int r
 
 // s = H_oe G5IN(p) for the rhs tile blockIdx.y*R .. +R-1 (odd output);
 // st == nullptr: every rhs (profiling hook)
+// The kernel bodies below take the block's site block `bx` and rhs tile `by`
+// (and, for the reductions, the site-block count nblk) so that the
+// multi-lattice kernels can run them for any lattice of one launch.
 template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
-__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_hop_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
-                                                     const CGState* st) {
+LYM_D void cg_hop_body(const EoGeom& g, const HopGauge& hg, const EoField& in, const EoField& out, int par,
+                       const CGState* st, int bx, int by) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs0 = blockIdx.y * R;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int rhs0 = by * R;
   int act[R];
   int any = 0;
 #pragma unroll
@@ -386,14 +389,20 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_hop_kernel(EoGeom 
   }
 }
 
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_hop_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
+                                                     const CGState* st) {
+  cg_hop_body<ND, NC, SP, GP, COMP, G5IN, R, MX>(g, hg, in, out, par, st, blockIdx.x, blockIdx.y);
+}
+
 // t = p - kappa^2 H_eo s ; alpha = rr / |t|^2   (rhs tile of R)
 template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
-__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_t_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t, double k2,
-                                                   CGState* st, double* partials, unsigned* counters, int nblk) {
+LYM_D void cg_t_body(const EoGeom& g, const HopGauge& hg, const EoField& s, const EoField& p, const EoField& t,
+                     double k2, CGState* st, double* partials, unsigned* counters, int nblk, int bx, int by) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[R * 32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs0 = blockIdx.y * R;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int rhs0 = by * R;
   int act[R];
   int any = 0;
 #pragma unroll
@@ -426,7 +435,7 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_t_kernel(EoGeom g,
       store_sp<SP, NCOMP>(t, rhs0 + r, cb, v);
     }
   }
-  if (grid_sum<R>(n, partials + (int64_t)blockIdx.y * nblk * R, counters + blockIdx.y, sh) && threadIdx.x == 0) {
+  if (grid_sum_n<R>(n, partials + (int64_t)by * nblk * R, counters + by, sh, bx, nblk) && threadIdx.x == 0) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       if (!act[r]) continue;
@@ -441,15 +450,21 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_t_kernel(EoGeom g,
   }
 }
 
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_t_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t, double k2,
+                                                   CGState* st, double* partials, unsigned* counters, int nblk) {
+  cg_t_body<ND, NC, SP, GP, COMP, R, MX>(g, hg, s, p, t, k2, st, partials, counters, nblk, blockIdx.x, blockIdx.y);
+}
+
 // Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr   (rhs tile of R)
 template <int ND, int NC, int SP, int GP, bool COMP, int XP, int R, int MX>
-__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_update_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
-                                                        EoField x, EoField r, double k2, CGState* st,
-                                                        double* partials, unsigned* counters, int nblk) {
+LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s, const EoField& t, const EoField& p,
+                          const EoField& x, const EoField& r, double k2, CGState* st, double* partials,
+                          unsigned* counters, int nblk, int bx, int by) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[R * 32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs0 = blockIdx.y * R;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int rhs0 = by * R;
   int act[R];
   int any = 0;
 #pragma unroll
@@ -494,7 +509,7 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_update_kernel(EoGe
       store_sp<XP, NCOMP>(x, rhs0 + q, cb, xv);
     }
   }
-  if (grid_sum<R>(n, partials + (int64_t)blockIdx.y * nblk * R, counters + blockIdx.y, sh) && threadIdx.x == 0) {
+  if (grid_sum_n<R>(n, partials + (int64_t)by * nblk * R, counters + by, sh, bx, nblk) && threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       if (!act[q]) continue;
@@ -506,6 +521,14 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_update_kernel(EoGe
         S.active = 2;  // finish the p update, then stop
     }
   }
+}
+
+template <int ND, int NC, int SP, int GP, bool COMP, int XP, int R, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_update_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
+                                                        EoField x, EoField r, double k2, CGState* st,
+                                                        double* partials, unsigned* counters, int nblk) {
+  cg_update_body<ND, NC, SP, GP, COMP, XP, R, MX>(g, hg, s, t, p, x, r, k2, st, partials, counters, nblk, blockIdx.x,
+                                                  blockIdx.y);
 }
 
 // Reliable-update residual in the sloppy precision: r = t - kappa^2 gamma_d H_eo s
@@ -575,10 +598,9 @@ __global__ void __launch_bounds__(128) copy_sp_kernel(int64_t Vh, EoField src, E
 // after the p update" marker (active == 2) into a pause.  Every block of the rhs
 // read `active` before it counted itself, so the last one may change it.
 template <int SP, int NCOMP>
-__global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoField p, CGState* st,
-                                                   unsigned* counters) {
-  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
+LYM_D void cg_p_body(int64_t Vh, const EoField& r, const EoField& p, CGState* st, unsigned* counters, int bx, int rhs,
+                     int nblk) {
+  const int64_t cb = bx * (int64_t)blockDim.x + threadIdx.x;
   const int act = st[rhs].active;
   if (!act) return;  // uniform per rhs
   if (cb < Vh) {
@@ -594,11 +616,17 @@ __global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoFiel
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    if (atomicAdd(counters + rhs, 1u) == gridDim.x - 1) {
+    if (atomicAdd(counters + rhs, 1u) == (unsigned)nblk - 1) {
       if (act == 2) st[rhs].active = 0;
       counters[rhs] = 0u;  // ready for the next use of this slot
     }
   }
+}
+
+template <int SP, int NCOMP>
+__global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoField p, CGState* st,
+                                                   unsigned* counters) {
+  cg_p_body<SP, NCOMP>(Vh, r, p, st, counters, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1312,6 +1340,370 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
   return status;
 }
 
+// ---------------------------------------------------------------------------
+// Several lattices in the same launches (lym_wilson_solve_multi)
+//
+// Independent lattices of the same (nd, N) -- each with its own geometry,
+// kappa, links and right-hand sides -- run their sloppy CG iterations in the
+// same five launches per iteration: every lattice owns a contiguous range of
+// blocks (its site blocks x its right-hand sides) of one grid, a block finds
+// its lattice by binary search over the range starts and runs the same kernel
+// body as the single-lattice launch.  Setup, FP64 reliable updates and the
+// odd-site reconstruction stay per lattice (they are rare).  One rhs per
+// thread; FP32 takes the 12-real links when every lattice's links are SU(N),
+// FP16 the mixed-precision hop with full links.
+// ---------------------------------------------------------------------------
+struct CgLat {
+  EoGeom g;
+  HopGauge hg;
+  EoField p, s, t, r, xs;
+  CGState* st;
+  double* partials;
+  unsigned* counters;
+  int64_t Vh;
+  int nblk, nrhs;
+  double k2;
+  int b0;  // first block of this lattice: its blocks are b0 + rhs * nblk + site block
+};
+
+LYM_D int cg_lat_of(const CgLat* __restrict__ lats, int n, int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (lats[mid].b0 <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cgm_hop_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, by = local / D.nblk, bx = local - by * D.nblk;
+  cg_hop_body<ND, NC, SP, GP, COMP, G5IN, 1, MX>(D.g, D.hg, G5IN ? D.t : D.p, D.s, 1, D.st, bx, by);
+}
+
+template <int ND, int NC, int SP, int GP, bool COMP, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cgm_t_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, by = local / D.nblk, bx = local - by * D.nblk;
+  cg_t_body<ND, NC, SP, GP, COMP, 1, MX>(D.g, D.hg, D.s, D.p, D.t, D.k2, D.st, D.partials, D.counters, D.nblk, bx,
+                                         by);
+}
+
+template <int ND, int NC, int SP, int GP, bool COMP, int XP, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cgm_update_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, by = local / D.nblk, bx = local - by * D.nblk;
+  cg_update_body<ND, NC, SP, GP, COMP, XP, 1, MX>(D.g, D.hg, D.s, D.t, D.p, D.xs, D.r, D.k2, D.st, D.partials,
+                                                  D.counters, D.nblk, bx, by);
+}
+
+template <int SP, int NCOMP>
+__global__ void __launch_bounds__(128) cgm_p_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, rhs = local / D.nblk, bx = local - rhs * D.nblk;
+  cg_p_body<SP, NCOMP>(D.Vh, D.r, D.p, D.st, D.counters, bx, rhs, D.nblk);
+}
+
+struct MultiOps {
+  void (*iterate)(GraphRec&, cudaStream_t, const CgLat*, int n, int blocks);  // one iteration, 5 launches
+  void (*preload)();
+};
+
+template <int ND, int NC, int SP, bool COMP, int MX>
+struct MultiImpl {
+  static constexpr int NCOMP = Gamma<ND>::NS * NC;
+  static constexpr int GP = SP == SP64 ? SP64 : (SP == SP32 ? SP32 : SP16);
+  static constexpr int XP = (SP == SP16 || SP == SPB16) ? SP32 : SP;
+  static void iterate(GraphRec& rec, cudaStream_t st, const CgLat* lats, int n, int blocks) {
+    const dim3 grid(blocks), blk(128);
+    launch_rec(rec, st, cgm_hop_kernel<ND, NC, SP, GP, COMP, false, MX>, grid, blk, lats, n);
+    launch_rec(rec, st, cgm_t_kernel<ND, NC, SP, GP, COMP, MX>, grid, blk, lats, n);
+    launch_rec(rec, st, cgm_hop_kernel<ND, NC, SP, GP, COMP, true, MX>, grid, blk, lats, n);
+    launch_rec(rec, st, cgm_update_kernel<ND, NC, SP, GP, COMP, XP, MX>, grid, blk, lats, n);
+    launch_rec(rec, st, cgm_p_kernel<SP, NCOMP>, grid, blk, lats, n);
+  }
+  static void preload() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, cgm_hop_kernel<ND, NC, SP, GP, COMP, false, MX>);
+    cudaFuncGetAttributes(&a, cgm_t_kernel<ND, NC, SP, GP, COMP, MX>);
+    cudaFuncGetAttributes(&a, cgm_hop_kernel<ND, NC, SP, GP, COMP, true, MX>);
+    cudaFuncGetAttributes(&a, cgm_update_kernel<ND, NC, SP, GP, COMP, XP, MX>);
+    cudaFuncGetAttributes(&a, cgm_p_kernel<SP, NCOMP>);
+  }
+  static MultiOps table() { return MultiOps{&iterate, &preload}; }
+};
+
+template <int ND, int NC>
+static MultiOps multi_pick_sp(int sp, bool comp) {
+  switch (sp) {
+    case SP64: return MultiImpl<ND, NC, SP64, false, 0>::table();
+    case SP32: return comp ? MultiImpl<ND, NC, SP32, true, 0>::table() : MultiImpl<ND, NC, SP32, false, 0>::table();
+    case SP16: return MultiImpl<ND, NC, SP16, false, 1>::table();
+    default: return MultiImpl<ND, NC, SPB16, false, 0>::table();
+  }
+}
+
+static bool multi_pick(int nd, int nc, int sp, bool comp, MultiOps* out) {
+  if (nd == 2 && nc == 2) *out = multi_pick_sp<2, 2>(sp, comp);
+  else if (nd == 2 && nc == 3) *out = multi_pick_sp<2, 3>(sp, comp);
+  else if (nd == 4 && nc == 2) *out = multi_pick_sp<4, 2>(sp, comp);
+  else if (nd == 4 && nc == 3) *out = multi_pick_sp<4, 3>(sp, comp);
+  else return false;
+  return true;
+}
+
+// Per-lattice CG bookkeeping of the multi-lattice driver (the same decisions
+// as cg_solve_on's, for one workspace).
+struct MultiLat {
+  Work* w = nullptr;
+  int nreal = 0;
+  std::vector<double> bnorm2, tres, prev_q2;
+  std::vector<int> done, updates, restart;
+};
+
+static void multi_plan(MultiLat& L, const lym_solver_params* prm, double delta, int i, double q2, double r2) {
+  Work& w = *L.w;
+  CGState& S = w.st_host[i];
+  const int sp = w.sp;
+  const double want = prm->tol * prm->tol * L.bnorm2[i];
+  L.tres[i] = L.bnorm2[i] > 0 ? std::sqrt(q2 / L.bnorm2[i]) : 0.0;
+  L.restart[i] = (L.prev_q2[i] > 0.0 && q2 > 0.25 * L.prev_q2[i]) ? 1 : 0;
+  L.prev_q2[i] = q2;
+  if (q2 <= want || r2 == 0.0) {
+    L.done[i] = 1;
+    S.active = 0;
+    return;
+  }
+  const double est = r2 * (want / q2) * 0.25;
+  S.rr = r2;
+  S.pause2 = sp == SP64 ? est : std::max(est, delta * delta * r2);
+  S.pause_iter = S.iters + (sp == SP64 ? (1 << 30) : 50);
+  S.active = S.iters >= S.max_iter ? 0 : 1;
+}
+
+static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, const int* nrhs,
+                          const void* const* bs, void* const* xs, const lym_solver_params* prm,
+                          lym_solver_report* rep, cudaStream_t caller) {
+  const int sp = prm->precision;
+  const int nd = gs[0]->nd, nc = gs[0]->nc;
+  bool comp_all = sp == SP32;
+  for (int l = 0; l < nlat; ++l) {
+    LYM_REQUIRE(gs[l] && bs[l] && xs[l], LYM_ERR_BAD_ARG, "null argument (lattice %d)", l);
+    LYM_REQUIRE(gs[l]->nd == nd && gs[l]->nc == nc, LYM_ERR_BAD_ARG, "every lattice needs the same nd and N");
+    LYM_REQUIRE(nrhs[l] >= 1 && nrhs[l] <= 4096, LYM_ERR_BAD_ARG, "nrhs out of range (lattice %d)", l);
+    LYM_REQUIRE(sp == SP64 || (gs[l]->prec_mask >> sp) & 1u, LYM_ERR_BAD_ARG,
+                "precision %d was not enabled in lym_gauge_create (lattice %d)", sp, l);
+    for (int k = 0; k < l; ++k)
+      LYM_REQUIRE(gs[k] != gs[l], LYM_ERR_BAD_ARG, "a gauge object appears twice (lattices %d and %d)", k, l);
+    comp_all = comp_all && gs[l]->comp;
+  }
+  const int mx = sp == SP16 ? 1 : 0;
+  MultiOps ops;
+  LYM_REQUIRE(multi_pick(nd, nc, sp, comp_all, &ops), LYM_ERR_UNSUPPORTED, "unsupported (nd=%d, N=%d)", nd, nc);
+  std::vector<MultiLat> lats(nlat);
+  for (int l = 0; l < nlat; ++l) {
+    int rc = get_work(gs[l], nrhs[l], sp, &lats[l].w);
+    if (rc) return rc;
+    Work& w = *lats[l].w;
+    int pick = -1;
+    for (int i = 0; i < w.ncand; ++i)
+      if (w.rcand[i] == 1 && w.ccand[i] == comp_all && w.mcand[i] == mx) pick = i;
+    LYM_REQUIRE(pick >= 0, LYM_ERR_UNSUPPORTED, "no one-rhs hop tile for lattice %d", l);
+    select_cand(w, pick);
+  }
+  cudaStream_t st = lats[0].w->stream;
+  LYM_CUDA(cudaEventRecord(lats[0].w->ev_in, caller));
+  LYM_CUDA(cudaStreamWaitEvent(st, lats[0].w->ev_in, 0));
+  struct Fence {
+    cudaEvent_t ev;
+    cudaStream_t from, to;
+    ~Fence() {
+      cudaEventRecord(ev, from);
+      cudaStreamWaitEvent(to, ev, 0);
+    }
+  } fence{lats[0].w->ev_out, st, caller};
+  const double delta = prm->delta > 0 && prm->delta < 1 ? prm->delta : 0.1;
+  const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 8;
+  EoField none;
+  // per-lattice setup, as cg_solve_on: source, |b|^2, b', x = 0, first residual, p = r
+  for (int l = 0; l < nlat; ++l) {
+    MultiLat& L = lats[l];
+    Work& w = *L.w;
+    const int n = w.nrhs;
+    L.nreal = nrhs[l];
+    w.kappa = kappas[l];
+    w.launches = 0;
+    const double k = kappas[l];
+    w.ops.to_eo(w, bs[l], prm->hermitian ? 1 : 0, st);
+    w.ops.norm64(w, w.be, 0, st);
+    w.ops.norm64(w, w.bo, 1, st);
+    LYM_CHECK_LAUNCH();
+    int rc = fetch_res(w, n, st);
+    if (rc) return rc;
+    L.bnorm2.assign(w.res_host, w.res_host + n);
+    L.tres.assign(n, 0.0);
+    L.prev_q2.assign(n, 0.0);
+    L.done.assign(n, 0);
+    L.updates.assign(n, 0);
+    L.restart.assign(n, 0);
+    for (int i = 0; i < n; ++i) w.upd_host[i] = 1;
+    LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    w.ops.hop64(w, 0, w.bo, w.bp, w.be, none, 0.0, -k, false, false, false, st);
+    w.ops.zero64(w, w.x64, st);
+    if (sp != SP64) LYM_CUDA(cudaMemsetAsync(w.xs.data, 0, field_bytes(w.xp, gs[l]->ncomp, w.Vh, n), st));
+    LYM_CHECK_LAUNCH();
+    for (int i = 0; i < n; ++i) {
+      std::memset(&w.st_host[i], 0, sizeof(CGState));
+      w.st_host[i].max_iter = prm->max_iter;
+    }
+    rc = reliable_update(w, st);
+    if (rc) return rc;
+    for (int i = 0; i < n; ++i) multi_plan(L, prm, delta, i, w.res_host[i], w.res_host[n + i]);
+    LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * n, cudaMemcpyHostToDevice, st));
+    w.ops.copy_rp(w, st);
+    LYM_CHECK_LAUNCH();
+  }
+  // lattice descriptors and the graph of `chunk` iterations over all lattices
+  std::vector<CgLat> desc(nlat);
+  int blocks = 0;
+  for (int l = 0; l < nlat; ++l) {
+    Work& w = *lats[l].w;
+    CgLat& D = desc[l];
+    D.g = gs[l]->geom;
+    D.hg = w.hgs;
+    D.p = w.p;
+    D.s = w.s;
+    D.t = w.t;
+    D.r = w.r;
+    D.xs = w.xs;
+    D.st = w.st;
+    D.partials = w.partials;
+    D.counters = w.counters;
+    D.Vh = w.Vh;
+    D.nblk = w.nblk;
+    D.nrhs = w.nrhs;
+    D.k2 = kappas[l] * kappas[l];
+    D.b0 = blocks;
+    LYM_REQUIRE((int64_t)blocks + (int64_t)w.nblk * w.nrhs < (int64_t(1) << 31), LYM_ERR_UNSUPPORTED,
+                "too many blocks for one launch");
+    blocks += w.nblk * w.nrhs;
+  }
+  CgLat* d_desc = nullptr;
+  LYM_CUDA(cudaMallocAsync(&d_desc, sizeof(CgLat) * nlat, st));
+  struct Release {
+    CgLat* p;
+    cudaStream_t st;
+    cudaGraphExec_t exec = nullptr;
+    ~Release() {
+      if (exec) cudaGraphExecDestroy(exec);
+      cudaFreeAsync(p, st);
+    }
+  } release{d_desc, st};
+  LYM_CUDA(cudaMemcpyAsync(d_desc, desc.data(), sizeof(CgLat) * nlat, cudaMemcpyHostToDevice, st));
+  ops.preload();
+  {
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess) {
+      GraphRec rec{graph, nullptr, cudaSuccess};
+      for (int i = 0; i < chunk; ++i) ops.iterate(rec, st, d_desc, nlat, blocks);
+      e = rec.err;
+    }
+    if (e == cudaSuccess && cudaGraphInstantiate(&release.exec, graph, 0) != cudaSuccess) release.exec = nullptr;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();  // without a graph the iterations run as plain launches
+  }
+  int64_t launches = 0;
+  auto active_any = [&]() {
+    for (auto& L : lats)
+      for (int i = 0; i < L.w->nrhs; ++i)
+        if (!L.done[i] && L.w->st_host[i].active) return true;
+    return false;
+  };
+  while (active_any()) {
+    while (true) {
+      if (release.exec) {
+        LYM_CUDA(cudaGraphLaunch(release.exec, st));
+      } else {
+        GraphRec direct;
+        for (int i = 0; i < chunk; ++i) ops.iterate(direct, st, d_desc, nlat, blocks);
+        LYM_CHECK_LAUNCH();
+      }
+      launches += (int64_t)chunk * kLaunchesPerIteration;
+      for (auto& L : lats)
+        LYM_CUDA(cudaMemcpyAsync(L.w->st_host, L.w->st, sizeof(CGState) * L.w->nrhs, cudaMemcpyDeviceToHost, st));
+      LYM_CUDA(cudaStreamSynchronize(st));
+      bool running = false;
+      for (auto& L : lats)
+        for (int i = 0; i < L.w->nrhs; ++i) running = running || L.w->st_host[i].active;
+      if (!running) break;
+    }
+    // reliable updates, lattice by lattice, for every rhs that paused and is not done
+    for (auto& L : lats) {
+      Work& w = *L.w;
+      const int n = w.nrhs;
+      bool any = false;
+      for (int i = 0; i < n; ++i) {
+        w.upd_host[i] = !L.done[i] ? 1 : 0;  // as cg_solve_on: capped rhs get their last update too
+        any = any || w.upd_host[i];
+      }
+      if (!any) continue;
+      LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+      int rc = reliable_update(w, st);
+      if (rc) return rc;
+      std::vector<double> q2(w.res_host, w.res_host + n), r2(w.res_host + n, w.res_host + 2 * n);
+      for (int i = 0; i < n; ++i) {
+        if (!w.upd_host[i]) continue;
+        L.updates[i] += 1;
+        multi_plan(L, prm, delta, i, q2[i], r2[i]);
+      }
+      LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * n, cudaMemcpyHostToDevice, st));
+      bool any_restart = false;
+      for (int i = 0; i < n; ++i) {
+        w.upd_host[i] = (!L.done[i] && L.restart[i]) ? 1 : 0;
+        any_restart = any_restart || w.upd_host[i];
+      }
+      if (any_restart) {
+        LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        w.ops.copy_rp(w, st);
+      }
+      LYM_CHECK_LAUNCH();
+    }
+  }
+  // x_o = b_o - kappa H_oe x_e and the reference layout, lattice by lattice
+  int status = LYM_OK;
+  int64_t total_launches = launches;
+  for (int l = 0; l < nlat; ++l) {
+    Work& w = *lats[l].w;
+    for (int i = 0; i < w.nrhs; ++i) w.upd_host[i] = 1;
+    LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * w.nrhs, cudaMemcpyHostToDevice, st));
+    w.ops.hop64(w, 1, w.x64, w.xo, w.bo, none, 0.0, -kappas[l], false, false, false, st);
+    w.ops.from_eo(w, xs[l], st);
+    LYM_CHECK_LAUNCH();
+    total_launches += w.launches;
+  }
+  LYM_CUDA(cudaStreamSynchronize(st));
+  int k = 0;
+  for (int l = 0; l < nlat; ++l) {
+    MultiLat& L = lats[l];
+    Work& w = *L.w;
+    for (int i = 0; i < L.nreal; ++i, ++k) {
+      rep[k].status = L.done[i] ? LYM_OK : LYM_ERR_NOT_CONVERGED;
+      rep[k].iterations = w.st_host[i].iters;
+      rep[k].reliable_updates = L.updates[i];
+      rep[k].true_residual = L.tres[i];
+      rep[k].kernel_launches = total_launches;
+      rep[k].rhs_per_thread = 1;
+      rep[k].compressed_links = comp_all ? 1 : 0;
+      rep[k].mixed_fma = mx;
+      if (!L.done[i]) status = LYM_ERR_NOT_CONVERGED;
+    }
+  }
+  return status;
+}
+
 static int dslash_eo(lym_gauge* g, int precision, int nrhs, int repeats, cudaStream_t st) {
   LYM_REQUIRE(g && repeats >= 0, LYM_ERR_BAD_ARG, "bad argument");
   Work* w = find_work(g, nrhs, precision);
@@ -1498,6 +1890,16 @@ int lym_gauge_destroy(lym_gauge* g) {
 int lym_wilson_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x, const lym_solver_params* params,
                      lym_solver_report* reports, void* stream) {
   return cg_solve(g, kappa, nrhs, b, x, params, reports, (cudaStream_t)stream);
+}
+
+int lym_wilson_solve_multi(int nlat, lym_gauge* const* gauges, const double* kappas, const int* nrhs,
+                           const void* const* b, void* const* x, const lym_solver_params* params,
+                           lym_solver_report* reports, void* stream) {
+  LYM_REQUIRE(nlat >= 1 && nlat <= 1024, LYM_ERR_BAD_ARG, "nlat out of range");
+  LYM_REQUIRE(gauges && kappas && nrhs && b && x && params && reports, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(params->tol > 0 && params->max_iter > 0, LYM_ERR_BAD_ARG, "tol and max_iter must be positive");
+  LYM_REQUIRE(params->precision >= 0 && params->precision <= 3, LYM_ERR_BAD_ARG, "bad precision");
+  return cg_solve_multi(nlat, gauges, kappas, nrhs, b, x, params, reports, (cudaStream_t)stream);
 }
 
 int lym_dslash_eo(lym_gauge* g, int precision, int nrhs, int repeats, void* stream) {

@@ -14,6 +14,9 @@
 * ``conjugate_gradient`` -- builder-defined even-odd CG for D x = b (or Q x = b)
   with FP64 reliable updates and FP64 / FP32 / FP16 / BF16 inner iterations
   (lym_wilson_solve).
+* ``solve_lattices`` -- builder-defined: independent lattices (their own geometry,
+  kappa, links and sources) solved together, the CG iterations of all of them in
+  the same launches (lym_wilson_solve_multi).
 * ``eo_square_solver`` -- builder-defined drop-in for ``multishift_solver`` on
   SquareOperator(Q): shift 0 by two even-odd CG solves of Q, positive shifts by
   ``multishift_cg``.
@@ -259,6 +262,54 @@ class conjugate_gradient:  # noqa: N801 - named like the reference solvers
         else:
             _lib.check(rc, "lym_wilson_solve")
         return x if batched else x[0]
+
+
+def solve_lattices(operators, sources, tol=1e-10, precision="f32", max_steps=20000, delta=0.1, chunk=8):
+    """Independent lattices solved together (lym_wilson_solve_multi): D x = b (Q x = b
+    when the operators are hermitian) for every fundamental DiracWilsonOperator in
+    ``operators`` (distinct objects, same dimension and N, each with its own geometry,
+    kappa and links) and its ``sources[l]`` ((ns, N, V) or a batch (nrhs, ns, N, V)).
+    The sloppy CG iterations of all lattices run in the same launches.  Returns the
+    solutions (shaped like the sources) and one list of report dicts per lattice.
+    Builder-defined (the reference solves one lattice per process)."""
+    n = len(operators)
+    if n == 0 or len(sources) != n:
+        raise ValueError("one source (batch) per operator")
+    herm = bool(operators[0].hermitian)
+    for op in operators:
+        if not isinstance(op, DiracWilsonOperator) or op.representation != "fundamental":
+            raise TypeError("solve_lattices takes fundamental-representation DiracWilsonOperators")
+        if bool(op.hermitian) != herm:
+            raise ValueError("every operator needs the same hermitian flag")
+    bs = [_dev.as_c128(b) for b in sources]
+    batched = [b.dim() == 4 for b in bs]
+    bb = [b if bt else b[None] for b, bt in zip(bs, batched)]
+    xs = [torch.empty_like(b) for b in bb]
+    precs = () if precision == "f64" else (precision,)
+    handles = [op.solver_gauge(precs) for op in operators]
+    gauges = (ctypes.c_void_p * n)(*[h.value for h in handles])
+    kappas = (ctypes.c_double * n)(*[float(op.kappa) for op in operators])
+    nrhs = (ctypes.c_int * n)(*[int(b.shape[0]) for b in bb])
+    bptr = (ctypes.c_void_p * n)(*[b.data_ptr() for b in bb])
+    xptr = (ctypes.c_void_p * n)(*[x.data_ptr() for x in xs])
+    prm = _lib.SolverParams(float(tol), int(max_steps), _lib.PREC[precision], float(delta), int(herm), int(chunk),
+                            0, 0, 0, 0.0)
+    total = sum(int(b.shape[0]) for b in bb)
+    reps = (_lib.SolverReport * total)()
+    rc = _lib.lib().lym_wilson_solve_multi(n, gauges, kappas, nrhs, bptr, xptr, ctypes.byref(prm), reps,
+                                           _dev.stream())
+    flat = [dict(status=r.status, iterations=r.iterations, reliable_updates=r.reliable_updates,
+                 true_residual=r.true_residual, kernel_launches=r.kernel_launches) for r in reps]
+    if rc == _lib.LYM_ERR_NOT_CONVERGED:
+        _print("solve_lattices: failed to find convergence for some right-hand sides")
+    else:
+        _lib.check(rc, "lym_wilson_solve_multi")
+    out, reports, k = [], [], 0
+    for x, bt in zip(xs, batched):
+        out.append(x if bt else x[0])
+        reports.append(flat[k:k + x.shape[0]])
+        k += x.shape[0]
+    return out, reports
 
 
 class eo_square_solver:  # noqa: N801 - named like the reference solvers
