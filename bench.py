@@ -91,6 +91,9 @@ def parse_args():
     ap.add_argument("--ms-switch", default="0",
                     help="FP64-head switch residuals of --multishift (0: the library default, <0: no head)")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
+    ap.add_argument("--serve-multi", type=int, default=8,
+                    help="solve server: batches on up to this many different gauge fields of one class run as one "
+                         "multi-lattice solve (<= 1: each batch on its own)")
     ap.add_argument("--serve-shifted", default="f64", choices=["full", "f64", "f32", "f16"],
                     help="solver of --serve-sweep's shifted requests: the full-lattice FP64 multishift, or the "
                          "even-odd multishift with that inner precision")
@@ -761,12 +764,12 @@ def _request_specs(rng, n, max_bytes=2 << 30):
     return specs
 
 
-def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64"):
+def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=8):
     import torch
 
     from tfleonardym_b200 import serving
     srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=dev.index,
-                              shifted_precision=shifted_precision)
+                              shifted_precision=shifted_precision, multi_lattice=multi_lattice)
     futs = []
     t0 = time.perf_counter()
     for sp, t in zip(specs, times):
@@ -818,7 +821,7 @@ def run_serve_sweep(args, local_rank):
     rates = [float(r) for r in args.serve_rates.split(",")]
     shifted = None if args.serve_shifted == "full" else args.serve_shifted
     warm = _request_specs(np.random.default_rng(1), 24)
-    _serve(warm, [0.0] * len(warm), "f16", args.workers, args.nrhs, dev, budget, shifted)  # warm-up of the path
+    _serve(warm, [0.0] * len(warm), "f16", args.workers, args.nrhs, dev, budget, shifted, args.serve_multi)  # warm-up
     first = None
     for rate in rates:
         rng = np.random.default_rng(int(rate) + 7)
@@ -827,11 +830,12 @@ def run_serve_sweep(args, local_rank):
         specs = _request_specs(rng, len(times))
         if first is None:
             first = (specs, times)
-        r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget, shifted)
+        r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget, shifted, args.serve_multi)
         print(json.dumps({"serve_sweep": "mixed", "rate_per_s": rate, "workers": args.workers,
-                          "max_batch_rhs": args.nrhs, "shifted_solver": args.serve_shifted, **r}), flush=True)
+                          "max_batch_rhs": args.nrhs, "shifted_solver": args.serve_shifted,
+                          "multi_lattice": args.serve_multi, **r}), flush=True)
     specs, times = first
-    r = _serve(specs, times, "f64", 1, 1, dev, budget, None)  # plain: full-lattice FP64 multishift too
+    r = _serve(specs, times, "f64", 1, 1, dev, budget, None, 1)  # plain: one request at a time, full-lattice multishift
     print(json.dumps({"serve_sweep": "plain_fp64_one_at_a_time", "rate_per_s": rates[0], **r}), flush=True)
     return 0
 
@@ -880,8 +884,9 @@ def run_batch_lattices(args, local_rank):
                        / np.sqrt(2))
     budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
 
-    def solve_all(precision, workers, max_batch):
-        srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=local_rank)
+    def solve_all(precision, workers, max_batch, multi_lattice=8):
+        srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=local_rank,
+                                  multi_lattice=multi_lattice)
         futs = []
         for k, l in enumerate(lattices):
             reqs = [sources[k]] if max_batch >= 4 else [sources[k][j] for j in range(4)]
@@ -929,10 +934,10 @@ def run_batch_lattices(args, local_rank):
     worst_multi, multi_launches, multi_ok = solve_together()
     torch.cuda.synchronize()
     multi_wall = time.perf_counter() - t0
-    solve_all("f64", 1, 1)  # warm-up of the plain path
+    solve_all("f64", 1, 1, 1)  # warm-up of the plain path
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    plain = solve_all("f64", 1, 1)
+    plain = solve_all("f64", 1, 1, 1)
     torch.cuda.synchronize()
     plain_wall = time.perf_counter() - t0
     # one gauge HMC step per lattice: P += eps F (fused), U <- exp(eps P) U

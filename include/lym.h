@@ -185,17 +185,18 @@ int lym_wilson_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* 
                      const lym_solver_params* params, lym_solver_report* reports, void* stream);
 
 /* Several independent lattices at once: gauges[l] (distinct objects of the same nd and N,
- * each with its own geometry and links) with kappas[l] and nrhs[l] right-hand sides b[l]
- * (reference layout), solutions into x[l] -- the systems of lym_wilson_solve, solved
+ * each with its own geometry and links) with kappas[l], tolerance tols[l] (NULL: params->tol
+ * for every lattice) and nrhs[l] right-hand sides b[l] (reference layout), solutions into
+ * x[l] -- the systems of lym_wilson_solve, solved
  * together: the sloppy CG iterations of every lattice run in the same five launches per
  * iteration (each lattice owns a range of the blocks), in CUDA graphs; setup, FP64
  * reliable updates and the odd-site reconstruction run per lattice.  One rhs per hop
  * thread (FP32: 12-real links when every lattice's links are SU(N); FP16: the
  * mixed-precision hop).  `reports` has sum(nrhs) entries in lattice order.  No reference
  * counterpart (the reference solves one lattice per process). */
-int lym_wilson_solve_multi(int nlat, lym_gauge* const* gauges, const double* kappas, const int* nrhs,
-                           const void* const* b, void* const* x, const lym_solver_params* params,
-                           lym_solver_report* reports, void* stream);
+int lym_wilson_solve_multi(int nlat, lym_gauge* const* gauges, const double* kappas, const double* tols,
+                           const int* nrhs, const void* const* b, void* const* x,
+                           const lym_solver_params* params, lym_solver_report* reports, void* stream);
 
 /* Runs the solver's even-odd hopping kernel s_o = H_oe p_e `repeats` times on
  * the workspace left by the last lym_wilson_solve with this (precision, nrhs):

@@ -67,8 +67,8 @@ SIGNATURES = {
     "lym_wilson_solve": (c_int, [c_void_p, c_double, c_int, c_void_p, c_void_p, P(SolverParams),
                                  P(SolverReport), c_void_p]),
     "lym_dslash_eo": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p]),
-    "lym_wilson_solve_multi": (c_int, [c_int, P(c_void_p), P(c_double), P(c_int), P(c_void_p), P(c_void_p),
-                                       P(SolverParams), P(SolverReport), c_void_p]),
+    "lym_wilson_solve_multi": (c_int, [c_int, P(c_void_p), P(c_double), P(c_double), P(c_int), P(c_void_p),
+                                       P(c_void_p), P(SolverParams), P(SolverReport), c_void_p]),
     "lym_multishift_solve": (c_int, [c_void_p, c_double, c_int, P(c_double), c_void_p, c_void_p,
                                      c_double, c_int, P(c_int), c_void_p]),
     "lym_multishift_solve_eo": (c_int, [c_void_p, c_double, c_int, c_int, P(c_double), c_void_p, c_void_p,

@@ -1459,6 +1459,7 @@ static bool multi_pick(int nd, int nc, int sp, bool comp, MultiOps* out) {
 struct MultiLat {
   Work* w = nullptr;
   int nreal = 0;
+  double tol = 0;  // target true relative residual of this lattice
   std::vector<double> bnorm2, tres, prev_q2;
   std::vector<int> done, updates, restart;
 };
@@ -1467,7 +1468,7 @@ static void multi_plan(MultiLat& L, const lym_solver_params* prm, double delta, 
   Work& w = *L.w;
   CGState& S = w.st_host[i];
   const int sp = w.sp;
-  const double want = prm->tol * prm->tol * L.bnorm2[i];
+  const double want = L.tol * L.tol * L.bnorm2[i];
   L.tres[i] = L.bnorm2[i] > 0 ? std::sqrt(q2 / L.bnorm2[i]) : 0.0;
   L.restart[i] = (L.prev_q2[i] > 0.0 && q2 > 0.25 * L.prev_q2[i]) ? 1 : 0;
   L.prev_q2[i] = q2;
@@ -1483,8 +1484,8 @@ static void multi_plan(MultiLat& L, const lym_solver_params* prm, double delta, 
   S.active = S.iters >= S.max_iter ? 0 : 1;
 }
 
-static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, const int* nrhs,
-                          const void* const* bs, void* const* xs, const lym_solver_params* prm,
+static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, const double* tols,
+                          const int* nrhs, const void* const* bs, void* const* xs, const lym_solver_params* prm,
                           lym_solver_report* rep, cudaStream_t caller) {
   const int sp = prm->precision;
   const int nd = gs[0]->nd, nc = gs[0]->nc;
@@ -1497,6 +1498,7 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
                 "precision %d was not enabled in lym_gauge_create (lattice %d)", sp, l);
     for (int k = 0; k < l; ++k)
       LYM_REQUIRE(gs[k] != gs[l], LYM_ERR_BAD_ARG, "a gauge object appears twice (lattices %d and %d)", k, l);
+    LYM_REQUIRE(!tols || tols[l] > 0, LYM_ERR_BAD_ARG, "tolerance must be positive (lattice %d)", l);
     comp_all = comp_all && gs[l]->comp;
   }
   const int mx = sp == SP16 ? 1 : 0;
@@ -1533,6 +1535,7 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
     Work& w = *L.w;
     const int n = w.nrhs;
     L.nreal = nrhs[l];
+    L.tol = tols ? tols[l] : prm->tol;
     w.kappa = kappas[l];
     w.launches = 0;
     const double k = kappas[l];
@@ -1892,14 +1895,14 @@ int lym_wilson_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* 
   return cg_solve(g, kappa, nrhs, b, x, params, reports, (cudaStream_t)stream);
 }
 
-int lym_wilson_solve_multi(int nlat, lym_gauge* const* gauges, const double* kappas, const int* nrhs,
-                           const void* const* b, void* const* x, const lym_solver_params* params,
+int lym_wilson_solve_multi(int nlat, lym_gauge* const* gauges, const double* kappas, const double* tols,
+                           const int* nrhs, const void* const* b, void* const* x, const lym_solver_params* params,
                            lym_solver_report* reports, void* stream) {
   LYM_REQUIRE(nlat >= 1 && nlat <= 1024, LYM_ERR_BAD_ARG, "nlat out of range");
   LYM_REQUIRE(gauges && kappas && nrhs && b && x && params && reports, LYM_ERR_BAD_ARG, "null argument");
   LYM_REQUIRE(params->tol > 0 && params->max_iter > 0, LYM_ERR_BAD_ARG, "tol and max_iter must be positive");
   LYM_REQUIRE(params->precision >= 0 && params->precision <= 3, LYM_ERR_BAD_ARG, "bad precision");
-  return cg_solve_multi(nlat, gauges, kappas, nrhs, b, x, params, reports, (cudaStream_t)stream);
+  return cg_solve_multi(nlat, gauges, kappas, tols, nrhs, b, x, params, reports, (cudaStream_t)stream);
 }
 
 int lym_dslash_eo(lym_gauge* g, int precision, int nrhs, int repeats, void* stream) {

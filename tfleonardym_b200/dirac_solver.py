@@ -264,13 +264,14 @@ class conjugate_gradient:  # noqa: N801 - named like the reference solvers
         return x if batched else x[0]
 
 
-def solve_lattices(operators, sources, tol=1e-10, precision="f32", max_steps=20000, delta=0.1, chunk=8):
+def solve_lattices(operators, sources, tol=1e-10, precision="f32", max_steps=20000, delta=0.1, chunk=8, tols=None):
     """Independent lattices solved together (lym_wilson_solve_multi): D x = b (Q x = b
     when the operators are hermitian) for every fundamental DiracWilsonOperator in
     ``operators`` (distinct objects, same dimension and N, each with its own geometry,
     kappa and links) and its ``sources[l]`` ((ns, N, V) or a batch (nrhs, ns, N, V)).
     The sloppy CG iterations of all lattices run in the same launches.  Returns the
     solutions (shaped like the sources) and one list of report dicts per lattice.
+    ``tols``: one target true relative residual per lattice (default ``tol`` for all).
     Builder-defined (the reference solves one lattice per process)."""
     n = len(operators)
     if n == 0 or len(sources) != n:
@@ -296,7 +297,8 @@ def solve_lattices(operators, sources, tol=1e-10, precision="f32", max_steps=200
                             0, 0, 0, 0.0)
     total = sum(int(b.shape[0]) for b in bb)
     reps = (_lib.SolverReport * total)()
-    rc = _lib.lib().lym_wilson_solve_multi(n, gauges, kappas, nrhs, bptr, xptr, ctypes.byref(prm), reps,
+    tol_arr = None if tols is None else (ctypes.c_double * n)(*[float(t) for t in tols])
+    rc = _lib.lib().lym_wilson_solve_multi(n, gauges, kappas, tol_arr, nrhs, bptr, xptr, ctypes.byref(prm), reps,
                                            _dev.stream())
     flat = [dict(status=r.status, iterations=r.iterations, reliable_updates=r.reliable_updates,
                  true_residual=r.true_residual, kernel_launches=r.kernel_launches) for r in reps]

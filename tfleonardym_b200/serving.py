@@ -84,6 +84,11 @@ class SolveRequest:
             return ("multishift", self.id)  # served on its own
         return (self.gauge_key, self.kappa, self.tol, self.precision, self.hermitian, self.bc)
 
+    def class_key(self):
+        """Requests of one class can share a multi-lattice solve (same D, N, inner
+        precision and operator form; geometry, kappa, tolerance and field may differ)."""
+        return (len(self.geometry), self.nc, self.precision, self.hermitian)
+
 
 class SolveResult:
     def __init__(self, request, x, status, reports):
@@ -161,12 +166,15 @@ class _Gauge:
 
 class SolveServer:
     def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
-                 shifted_precision="f64"):
+                 shifted_precision="f64", multi_lattice=8):
         self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
         # shifted requests: a precision = the even-odd multishift (lym_multishift_solve_eo) with that inner
         # precision (FP64 by default: the fastest for the mixed request streams measured); None = the
         # full-lattice FP64 multishift (lym_multishift_solve)
         self.shifted_precision = shifted_precision
+        # batches on up to this many different gauge fields of one class run as one
+        # multi-lattice solve (lym_wilson_solve_multi); <= 1: each batch on its own
+        self.multi_lattice = int(multi_lattice)
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch)
         self.device = device  # CUDA device index; None: the caller's current device
@@ -274,6 +282,30 @@ class SolveServer:
             self._pending = keep
             return batch
 
+    def _take_companions(self, batch):
+        """With multi_lattice > 1: pending unshifted batches of the same class on other
+        gauge fields (one batch per field, at most multi_lattice - 1, each up to
+        max_batch rhs) join `batch` in one multi-lattice solve."""
+        first = batch[0]
+        if self.multi_lattice <= 1 or first.shifts is not None:
+            return [batch]
+        with self._lock:
+            cls = first.class_key()
+            comp = collections.OrderedDict()  # gauge key -> [batch key, requests, rhs]
+            keep = collections.deque()
+            for r in self._pending:
+                if r.shifts is None and r.gauge_key != first.gauge_key and r.class_key() == cls:
+                    c = comp.get(r.gauge_key)
+                    if c is None and len(comp) + 1 < self.multi_lattice:
+                        c = comp[r.gauge_key] = [r.batch_key(), [], 0]
+                    if c is not None and r.batch_key() == c[0] and c[2] + r.nrhs <= self.max_batch:
+                        c[1].append(r)
+                        c[2] += r.nrhs
+                        continue
+                keep.append(r)
+            self._pending = keep
+        return [batch] + [c[1] for c in comp.values()]
+
     def _gauge_for(self, req):
         with self._lock:
             g = self._gauges.get(req.gauge_key)
@@ -311,19 +343,24 @@ class SolveServer:
             batch = self._take_batch(widx)
             if batch is None:
                 return
+            batches = self._take_companions(batch)
+            reqs = [r for b in batches for r in b]
             t0 = time.perf_counter()
-            for r in batch:
+            for r in reqs:
                 r.t_start = t0
             try:
                 with torch.cuda.stream(stream):
-                    self._solve_batch(batch, widx)
+                    if len(batches) == 1:
+                        self._solve_batch(batch, widx)
+                    else:
+                        self._solve_multi(batches, widx)
             except Exception as exc:  # noqa: BLE001 - delivered to every waiter
-                for r in batch:
+                for r in reqs:
                     r.t_end = time.perf_counter()
                     if not r.future.done():
                         r.future.set_exception(exc)
             finally:
-                self._release(batch)
+                self._release(reqs)
 
     def _solve_shifted(self, req, g, widx):
         """(Q^2 + sigma_k) x_k = b by multishift CG (the server's shifted_precision
@@ -347,6 +384,52 @@ class SolveServer:
             req.out.copy_(x, non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return x, reports
+
+    def _solve_multi(self, batches, widx):
+        """Batches on different gauge fields of one class in one multi-lattice solve
+        (each batch one lattice: its field, kappa, tolerance and rhs)."""
+        from . import dirac_solver
+        dev = torch.device("cuda", self.device)
+        gs = []
+        try:
+            for bt in batches:
+                gs.append(self._gauge_for(bt[0]))
+            ops = [g.op_for(widx, bt[0].kappa, bt[0].hermitian) for g, bt in zip(gs, batches)]
+            bs = [torch.cat([(r.b if r.b.dim() == 4 else r.b[None]).to(dev, non_blocking=True) for r in bt])
+                  for bt in batches]
+            opts = {k: v for k, v in self.solver_options.items() if k in ("delta", "chunk")}
+            xs, reps = dirac_solver.solve_lattices(ops, bs, precision=batches[0][0].precision,
+                                                   max_steps=max(r.max_iter for bt in batches for r in bt),
+                                                   tols=[bt[0].tol for bt in batches], **opts)
+            outs = []
+            for bt, x in zip(batches, xs):
+                k = 0
+                for r in bt:  # caller-provided outputs (pinned host buffers on the host path)
+                    if r.out is not None:
+                        r.out.copy_(x[k:k + r.nrhs] if r.b.dim() == 4 else x[k], non_blocking=True)
+                    k += r.nrhs
+                if not bt[0].b.is_cuda and any(r.out is None for r in bt):
+                    x = x.to("cpu", non_blocking=True)
+                outs.append(x)
+            torch.cuda.current_stream().synchronize()
+        finally:
+            with self._lock:
+                for g in gs:
+                    g.users -= 1
+        t_end = time.perf_counter()
+        total_rhs = sum(r.nrhs for bt in batches for r in bt)
+        for bt, x, rp in zip(batches, outs, reps):
+            k = 0
+            for r in bt:
+                mine = rp[k:k + r.nrhs]
+                xr = r.out if r.out is not None else (x[k:k + r.nrhs] if r.b.dim() == 4 else x[k])
+                k += r.nrhs
+                ok = all(m["status"] == 0 and m["true_residual"] <= r.tol for m in mine)
+                r.t_end = t_end
+                res = SolveResult(r, xr, OK if ok else NOT_CONVERGED, mine)
+                res.batch_rhs = total_rhs
+                self.completed.append(res)
+                r.future.set_result(res)
 
     def _solve_batch(self, batch, widx=0):
         from . import dirac_solver
