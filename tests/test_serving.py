@@ -115,6 +115,81 @@ def test_workers_overlap_when_budget_allows():
     assert srv.max_concurrent >= 2
 
 
+class _FakeSolveServer(serving.SolveServer):
+    """The server's batch and companion selection with stand-in solves (no CUDA
+    stream: the worker loop below mirrors SolveServer._run without the device)."""
+
+    def __init__(self, *a, **k):
+        self.calls = []
+        super().__init__(*a, **k)
+
+    def _run(self, widx):
+        while True:
+            batch = self._take_batch(widx)
+            if batch is None:
+                return
+            batches = self._take_companions(batch)
+            if len(batches) == 1:
+                self._solve_batch(batch, widx)
+            else:
+                self._solve_multi(batches, widx)
+            self._release([r for b in batches for r in b])
+
+    def _finish(self, reqs):
+        for r in reqs:
+            r.t_end = time.perf_counter()
+            res = serving.SolveResult(r, r.b, serving.OK, [])
+            self.completed.append(res)
+            r.future.set_result(res)
+
+    def _solve_batch(self, batch, widx=0):
+        self.calls.append([[r.id for r in batch]])
+        self._finish(batch)
+
+    def _solve_multi(self, batches, widx):
+        self.calls.append([[r.id for r in b] for b in batches])
+        self._finish([r for b in batches for r in b])
+
+
+def _req3(key, geom=(4, 4, 4, 4), nc=3, kappa=0.12, tol=1e-10, precision="f16", shifts=None):
+    nd = len(geom)
+    ns = 2 if nd == 2 else 4
+    b = torch.zeros((ns, nc, int(np.prod(geom))), dtype=torch.complex128)
+    return serving.SolveRequest(key, geom, nc, kappa, b, gauge=None, tol=tol, precision=precision, shifts=shifts)
+
+
+def test_batches_on_other_fields_of_one_class_join_a_multi_lattice_solve():
+    srv = _FakeSolveServer(hbm_budget_bytes=1 << 40, workers=1, max_batch=2, multi_lattice=3)
+    srv._lock.acquire()  # every request pending before the worker looks
+    try:
+        a1 = srv.submit(_req3("a"))
+        a2 = srv.submit(_req3("a"))
+        b1 = srv.submit(_req3("b", geom=(4, 4, 2, 6), kappa=0.13, tol=1e-9))  # other field, same class
+        c1 = srv.submit(_req3("c", geom=(6, 4, 4, 4)))
+        d1 = srv.submit(_req3("d"))                                           # beyond multi_lattice = 3
+        e1 = srv.submit(_req3("e", nc=2))                                     # other class (N)
+        f1 = srv.submit(_req3("f", precision="f32"))                          # other class (precision)
+        s1 = srv.submit(_req3("g", shifts=[0.1]))                             # shifted: on its own
+        b2 = srv.submit(_req3("b", geom=(4, 4, 2, 6), kappa=0.14, tol=1e-9))  # same field, other kappa
+    finally:
+        srv._lock.release()
+    futs = [a1, a2, b1, c1, d1, e1, f1, s1, b2]
+    for f in futs:
+        assert f.result(timeout=5).status == serving.OK
+    srv.close()
+    ids = {f: f.result().request.id for f in futs}
+    first = srv.calls[0]
+    assert first == [[ids[a1], ids[a2]], [ids[b1]], [ids[c1]]]  # primary + two other fields
+    singles = [c for c in srv.calls[1:]]
+    flat = [i for c in singles for b in c for i in b]
+    assert sorted(flat) == sorted(ids[f] for f in (d1, e1, f1, s1, b2))
+    # the shifted request and the other classes never share a solve with anything
+    for c in singles:
+        members = [i for b in c for i in b]
+        if ids[s1] in members or ids[e1] in members or ids[f1] in members:
+            assert len(members) == 1
+
+
 @pytest.mark.gpu
 def test_same_answer_alone_and_in_the_mix(cuda_device):
     """Each request's solution alone equals its solution inside a mixed stream
