@@ -1018,7 +1018,9 @@ static int fetch_res(Work& w, int n, cudaStream_t st) {
 // (it only has to be accurate relative to |q|).  Leaves |q|^2 in
 // res_host[0..nrhs) and |r|^2 in res_host[nrhs..2 nrhs).  t and s serve as
 // temporaries: the next iteration recomputes both before reading them.
-static int reliable_update(Work& w, cudaStream_t st) {
+// sync = false: everything is only enqueued on st (the multi-lattice driver
+// enqueues every lattice's update and synchronises once).
+static int reliable_update(Work& w, cudaStream_t st, bool sync = true) {
   const double k = w.kappa, k2 = k * k;
   EoField none;
   w.ops.accumulate(w, st);
@@ -1029,7 +1031,7 @@ static int reliable_update(Work& w, cudaStream_t st) {
   w.ops.rnew(w, st);
   LYM_CUDA(cudaMemcpyAsync(w.res_host + w.nrhs, w.res, sizeof(double) * w.nrhs, cudaMemcpyDeviceToHost, st));
   LYM_CHECK_LAUNCH();
-  LYM_CUDA(cudaStreamSynchronize(st));
+  if (sync) LYM_CUDA(cudaStreamSynchronize(st));
   return LYM_OK;
 }
 
@@ -1529,7 +1531,8 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
   const double delta = prm->delta > 0 && prm->delta < 1 ? prm->delta : 0.1;
   const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 8;
   EoField none;
-  // per-lattice setup, as cg_solve_on: source, |b|^2, b', x = 0, first residual, p = r
+  // per-lattice setup, as cg_solve_on: source, |b|^2, b', x = 0, first residual, p = r;
+  // every lattice's work is enqueued first and the host waits once
   for (int l = 0; l < nlat; ++l) {
     MultiLat& L = lats[l];
     Work& w = *L.w;
@@ -1543,27 +1546,33 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
     w.ops.norm64(w, w.be, 0, st);
     w.ops.norm64(w, w.bo, 1, st);
     LYM_CHECK_LAUNCH();
-    int rc = fetch_res(w, n, st);
-    if (rc) return rc;
-    L.bnorm2.assign(w.res_host, w.res_host + n);
-    L.tres.assign(n, 0.0);
-    L.prev_q2.assign(n, 0.0);
-    L.done.assign(n, 0);
-    L.updates.assign(n, 0);
-    L.restart.assign(n, 0);
+    // |b|^2 to res_host[4n..5n) (the reliable update below fills [0..2n))
+    LYM_CUDA(cudaMemcpyAsync(w.res_host + 4 * n, w.res, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     for (int i = 0; i < n; ++i) w.upd_host[i] = 1;
     LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
     w.ops.hop64(w, 0, w.bo, w.bp, w.be, none, 0.0, -k, false, false, false, st);
     w.ops.zero64(w, w.x64, st);
     if (sp != SP64) LYM_CUDA(cudaMemsetAsync(w.xs.data, 0, field_bytes(w.xp, gs[l]->ncomp, w.Vh, n), st));
     LYM_CHECK_LAUNCH();
+    int rc = reliable_update(w, st, false);
+    if (rc) return rc;
+  }
+  LYM_CUDA(cudaStreamSynchronize(st));
+  for (int l = 0; l < nlat; ++l) {
+    MultiLat& L = lats[l];
+    Work& w = *L.w;
+    const int n = w.nrhs;
+    L.bnorm2.assign(w.res_host + 4 * n, w.res_host + 5 * n);
+    L.tres.assign(n, 0.0);
+    L.prev_q2.assign(n, 0.0);
+    L.done.assign(n, 0);
+    L.updates.assign(n, 0);
+    L.restart.assign(n, 0);
     for (int i = 0; i < n; ++i) {
       std::memset(&w.st_host[i], 0, sizeof(CGState));
       w.st_host[i].max_iter = prm->max_iter;
+      multi_plan(L, prm, delta, i, w.res_host[i], w.res_host[n + i]);
     }
-    rc = reliable_update(w, st);
-    if (rc) return rc;
-    for (int i = 0; i < n; ++i) multi_plan(L, prm, delta, i, w.res_host[i], w.res_host[n + i]);
     LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * n, cudaMemcpyHostToDevice, st));
     w.ops.copy_rp(w, st);
     LYM_CHECK_LAUNCH();
@@ -1643,8 +1652,11 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
         for (int i = 0; i < L.w->nrhs; ++i) running = running || L.w->st_host[i].active;
       if (!running) break;
     }
-    // reliable updates, lattice by lattice, for every rhs that paused and is not done
-    for (auto& L : lats) {
+    // reliable updates of every rhs that paused and is not done, all lattices
+    // enqueued, one host wait
+    std::vector<int> updated(nlat, 0);
+    for (int l = 0; l < nlat; ++l) {
+      MultiLat& L = lats[l];
       Work& w = *L.w;
       const int n = w.nrhs;
       bool any = false;
@@ -1653,14 +1665,21 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
         any = any || w.upd_host[i];
       }
       if (!any) continue;
+      updated[l] = 1;
       LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
-      int rc = reliable_update(w, st);
+      int rc = reliable_update(w, st, false);
       if (rc) return rc;
-      std::vector<double> q2(w.res_host, w.res_host + n), r2(w.res_host + n, w.res_host + 2 * n);
+    }
+    LYM_CUDA(cudaStreamSynchronize(st));
+    for (int l = 0; l < nlat; ++l) {
+      if (!updated[l]) continue;
+      MultiLat& L = lats[l];
+      Work& w = *L.w;
+      const int n = w.nrhs;
       for (int i = 0; i < n; ++i) {
         if (!w.upd_host[i]) continue;
         L.updates[i] += 1;
-        multi_plan(L, prm, delta, i, q2[i], r2[i]);
+        multi_plan(L, prm, delta, i, w.res_host[i], w.res_host[n + i]);
       }
       LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * n, cudaMemcpyHostToDevice, st));
       bool any_restart = false;
