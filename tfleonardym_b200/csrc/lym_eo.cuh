@@ -577,4 +577,18 @@ LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, i
   }
 }
 
+// The hop of the solver kernels for R right-hand sides at one site: FP32
+// arithmetic (MX = 0, hop_tile), or for FP16 spinors with full links the
+// mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx).
+template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
+LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
+                   const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
+  if constexpr (MX != 0) {
+    static_assert(SP == SP16 && GP == SP16 && !COMP, "the mixed-precision hop takes FP16 spinors and full links");
+    hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+  } else {
+    hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+  }
+}
+
 }  // namespace lym

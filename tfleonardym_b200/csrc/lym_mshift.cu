@@ -114,20 +114,6 @@ LYM_HD EoField sub(const EoField& f, int64_t slot) {
 
 LYM_D int eo_block_parity(int nblk) { return blockIdx.x >= (unsigned)nblk ? 1 : 0; }
 
-// The hop of the multishift kernels: FP32 arithmetic (MX = 0, hop_tile), or
-// for FP16 spinors with full links the mixed-precision form (MX = 1,
-// hop_tile_mx: f16 x f16 + f32 FMAs), as the CG's autotuner picks for FP16.
-template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
-LYM_D void ms_hop(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
-                  const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
-  if constexpr (MX != 0) {
-    static_assert(SP == SP16 && GP == SP16 && !COMP, "the mixed-precision hop takes FP16 spinors and full links");
-    hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
-  } else {
-    hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // sloppy iteration kernels; grids (2 nblk, G / R): blocks [0, nblk) even sites,
 // [nblk, 2 nblk) odd sites, R groups per thread sharing each link
@@ -157,7 +143,7 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0)
   for (int k = 0; k < 2 * R; ++k) n[k] = 0.0;
   if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    ms_hop<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, sub(pb, (1 - par) * G), g0, i, par, act, acc);
+    hop_any<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, sub(pb, (1 - par) * G), g0, i, par, act, acc);
     const EoField pin = sub(pb, par * G), wout = sub(w, par * G);
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -221,7 +207,7 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0)
   for (int q = 0; q < R; ++q) n[q] = 0.0;
   if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    ms_hop<ND, NC, SP, GP, COMP, true, R, MX>(g, hg, sub(w, (1 - par) * G), g0, i, par, act, acc);
+    hop_any<ND, NC, SP, GP, COMP, true, R, MX>(g, hg, sub(w, (1 - par) * G), g0, i, par, act, acc);
     const EoField wv = sub(w, par * G), pv = sub(pb, par * G);
 #pragma unroll
     for (int q = 0; q < R; ++q) {

@@ -341,25 +341,12 @@ __global__ void __launch_bounds__(128) norm64_kernel(int64_t Vh, EoField f, doub
 // (about 250 registers); the memory-bound FP64 hop runs ~20% faster at 32^4
 // that way.  Sloppy ones keep ptxas's default register target.
 //
-// The hop of the CG kernels for R right-hand sides at one site: FP32
-// arithmetic (MX = 0, hop_tile), or for FP16 spinors with full links the
-// mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx).
-template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
-LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
-                   const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
-  if constexpr (MX != 0) {
-    static_assert(SP == SP16 && GP == SP16 && !COMP, "the mixed-precision hop takes FP16 spinors and full links");
-    hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
-  } else {
-    hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
-  }
-}
-
-// s = H_oe G5IN(p) for the rhs tile blockIdx.y*R .. +R-1 (odd output);
-// st == nullptr: every rhs (profiling hook)
 // The kernel bodies below take the block's site block `bx` and rhs tile `by`
 // (and, for the reductions, the site-block count nblk) so that the
 // multi-lattice kernels can run them for any lattice of one launch.
+
+// s = H_oe G5IN(p) for the rhs tile by*R .. +R-1 (odd output);
+// st == nullptr: every rhs (profiling hook)
 template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
 LYM_D void cg_hop_body(const EoGeom& g, const HopGauge& hg, const EoField& in, const EoField& out, int par,
                        const CGState* st, int bx, int by) {
