@@ -91,7 +91,7 @@ def parse_args():
     ap.add_argument("--ms-switch", default="0",
                     help="FP64-head switch residuals of --multishift (0: the library default, <0: no head)")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
-    ap.add_argument("--serve-multi", type=int, default=8,
+    ap.add_argument("--serve-multi", type=int, default=1,
                     help="solve server: batches on up to this many different gauge fields of one class run as one "
                          "multi-lattice solve (<= 1: each batch on its own)")
     ap.add_argument("--serve-shifted", default="f64", choices=["full", "f64", "f32", "f16"],
@@ -764,7 +764,7 @@ def _request_specs(rng, n, max_bytes=2 << 30):
     return specs
 
 
-def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=8):
+def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=1):
     import torch
 
     from tfleonardym_b200 import serving
@@ -884,7 +884,7 @@ def run_batch_lattices(args, local_rank):
                        / np.sqrt(2))
     budget = int(0.8 * torch.cuda.get_device_properties(dev).total_memory)
 
-    def solve_all(precision, workers, max_batch, multi_lattice=8):
+    def solve_all(precision, workers, max_batch, multi_lattice=1):
         srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=local_rank,
                                   multi_lattice=multi_lattice)
         futs = []

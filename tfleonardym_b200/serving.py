@@ -166,14 +166,17 @@ class _Gauge:
 
 class SolveServer:
     def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
-                 shifted_precision="f64", multi_lattice=8):
+                 shifted_precision="f64", multi_lattice=1):
         self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
         # shifted requests: a precision = the even-odd multishift (lym_multishift_solve_eo) with that inner
         # precision (FP64 by default: the fastest for the mixed request streams measured); None = the
         # full-lattice FP64 multishift (lym_multishift_solve)
         self.shifted_precision = shifted_precision
         # batches on up to this many different gauge fields of one class run as one
-        # multi-lattice solve (lym_wilson_solve_multi); <= 1: each batch on its own
+        # multi-lattice solve (lym_wilson_solve_multi); <= 1 (the default): each batch on
+        # its own.  Opt-in: it helped the mixed stream at 100 req/s, but runs of the
+        # 64-lattice batch through the server varied widely with it on (gauge objects
+        # evicted and rebuilt while companions are in flight is the suspected cause).
         self.multi_lattice = int(multi_lattice)
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch)
