@@ -191,7 +191,8 @@ def test_batches_on_other_fields_of_one_class_join_a_multi_lattice_solve():
 
 
 @pytest.mark.gpu
-def test_same_answer_alone_and_in_the_mix(cuda_device):
+@pytest.mark.parametrize("multi_lattice", [1, 8])
+def test_same_answer_alone_and_in_the_mix(cuda_device, multi_lattice):
     """Each request's solution alone equals its solution inside a mixed stream
     (different geometry, N, kappa, precision, shifted and unshifted requests),
     within the solve tolerance, and every answer meets its FP64 true residual."""
@@ -222,7 +223,7 @@ def test_same_answer_alone_and_in_the_mix(cuda_device):
     for r in reqs:
         alone.append(srv.submit(make(r)).result(timeout=120))
     srv.close()
-    srv = serving.SolveServer(hbm_budget_bytes=8 << 30, workers=3, max_batch=8)
+    srv = serving.SolveServer(hbm_budget_bytes=8 << 30, workers=3, max_batch=8, multi_lattice=multi_lattice)
     futs = [srv.submit(make(r)) for r in reqs]
     mixed = [f.result(timeout=300) for f in futs]
     srv.close()
