@@ -175,8 +175,9 @@ class SolveServer:
         # batches on up to this many different gauge fields of one class run as one
         # multi-lattice solve (lym_wilson_solve_multi); <= 1 (the default): each batch on
         # its own.  Opt-in: it helped the mixed stream at 100 req/s, but runs of the
-        # 64-lattice batch through the server varied widely with it on (gauge objects
-        # evicted and rebuilt while companions are in flight is the suspected cause).
+        # 64-lattice batch through the server varied widely with it on: companions touch
+        # more gauge fields per solve, so more fields leave the cache, and destroying a
+        # field's lym_gauge synchronises the device (all workers' streams).
         self.multi_lattice = int(multi_lattice)
         self.budget = int(hbm_budget_bytes)
         self.max_batch = int(max_batch)
