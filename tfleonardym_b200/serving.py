@@ -324,6 +324,7 @@ class SolveServer:
             u = u.to(torch.device("cuda", self.device))
         g = _Gauge(req.gauge_key, u, req.geometry, req.nc, req.bc,
                    footprint_bytes(req.geometry, req.nc, 0, req.precision, True))
+        evicted = []
         with self._lock:
             old = self._gauges.get(req.gauge_key)
             if old is not None:  # another worker loaded it meanwhile
@@ -332,10 +333,14 @@ class SolveServer:
             self._gauges[req.gauge_key] = g
             g.users += 1
             while len(self._gauges) > self.cache_size:
-                k, victim = next(iter(self._gauges.items()))
-                if victim.users:
+                k = next(iter(self._gauges))
+                if self._gauges[k].users:
                     break
-                self._gauges.pop(k)
+                evicted.append(self._gauges.pop(k))
+        # the evicted fields' operators release their lym_gauge objects here, outside the
+        # server lock: lym_gauge_destroy synchronises the device, which must not hold up
+        # the other workers' batch selection
+        evicted.clear()
         return g
 
     def _run(self, widx):
