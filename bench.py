@@ -898,10 +898,10 @@ def run_batch_lattices(args, local_rank):
         srv.close()
         return res
 
-    solve_all("f32", 4, 16)  # warm-up: workspaces, autotuning, graphs
+    solve_all("f32", 4, 16, args.serve_multi)  # warm-up: workspaces, autotuning, graphs
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res = solve_all("f32", 4, 16)
+    res = solve_all("f32", 4, 16, args.serve_multi)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     ok = sum(r.status == serving.OK for r in res)
@@ -965,7 +965,8 @@ def run_batch_lattices(args, local_rank):
                       "gauge_hmc_step_all_lattices_ms": e0.elapsed_time(e1),
                       "config": {"lattices": "32 x 2D SU(2) 8^2..64^2 + 32 x 4D SU(3) 8^4..12^3x24",
                                  "inner_precision": "f32", "outer_precision": "f64", "tol": 1e-10,
-                                 "server_workers": 4, "max_batch_rhs": 16}}), flush=True)
+                                 "server_workers": 4, "max_batch_rhs": 16,
+                                 "server_multi_lattice": args.serve_multi}}), flush=True)
     return 0
 
 
