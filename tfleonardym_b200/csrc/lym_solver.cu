@@ -225,10 +225,9 @@ __global__ void eo_to_ref_kernel(EoGeom g, int64_t V, EoField e, EoField o, doub
 
 // dst (precision SP) = src (FP64); optionally also dst2 = src
 template <int SP, int NCOMP>
-__global__ void convert_kernel(int64_t Vh, EoField src, EoField dst, EoField dst2, const CGState* st, int only_update,
-                               const int* upd) {
-  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
+LYM_D void convert_body(int64_t Vh, const EoField& src, const EoField& dst, const EoField& dst2, int only_update,
+                        const int* upd, int bx, int rhs) {
+  const int64_t cb = bx * (int64_t)blockDim.x + threadIdx.x;
   if (cb >= Vh) return;
   if (only_update && !upd[rhs]) return;
   cx<double> v[NCOMP];
@@ -240,11 +239,16 @@ __global__ void convert_kernel(int64_t Vh, EoField src, EoField dst, EoField dst
   if (dst2.data) store_sp<SP, NCOMP>(dst2, rhs, cb, w);
 }
 
+template <int SP, int NCOMP>
+__global__ void convert_kernel(int64_t Vh, EoField src, EoField dst, EoField dst2, const CGState* st, int only_update,
+                               const int* upd) {
+  convert_body<SP, NCOMP>(Vh, src, dst, dst2, only_update, upd, blockIdx.x, blockIdx.y);
+}
+
 // x64 += xs; xs = 0  (for rhs with upd[rhs])
 template <int XP, int NCOMP>
-__global__ void accumulate_kernel(int64_t Vh, EoField xs, EoField x64, const int* upd) {
-  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
+LYM_D void accumulate_body(int64_t Vh, const EoField& xs, const EoField& x64, const int* upd, int bx, int rhs) {
+  const int64_t cb = bx * (int64_t)blockDim.x + threadIdx.x;
   if (cb >= Vh || !upd[rhs]) return;
   using R = typename Prec<XP>::real;
   cx<R> a[NCOMP];
@@ -259,6 +263,11 @@ __global__ void accumulate_kernel(int64_t Vh, EoField xs, EoField x64, const int
   }
   store_sp<SP64, NCOMP>(x64, rhs, cb, b);
   store_sp<XP, NCOMP>(xs, rhs, cb, z);
+}
+
+template <int XP, int NCOMP>
+__global__ void accumulate_kernel(int64_t Vh, EoField xs, EoField x64, const int* upd) {
+  accumulate_body<XP, NCOMP>(Vh, xs, x64, upd, blockIdx.x, blockIdx.y);
 }
 
 template <int NCOMP>
@@ -276,14 +285,12 @@ __global__ void zero64_kernel(int64_t Vh, EoField f) {
 //   out = z0 + a1 z1 + c * G5OUT(hop(G5IN(in)))  ; optional |out|^2 -> res[rhs]
 // ---------------------------------------------------------------------------
 template <int ND, int NC, bool G5IN, bool G5OUT>
-__global__ void __launch_bounds__(128, 1) hop64_lincomb_kernel(EoGeom g, HopGauge hg, EoField in, int par, EoField out,
-                                                            EoField z0, EoField z1, double a1, double c,
-                                                            const int* upd, double* partials, unsigned* counters,
-                                                            double* res, int nblk) {
+LYM_D void hop64_lincomb_body(const EoGeom& g, const HopGauge& hg, const EoField& in, int par, const EoField& out,
+                              const EoField& z0, const EoField& z1, double a1, double c, const int* upd,
+                              double* partials, unsigned* counters, double* res, int nblk, int bx, int rhs) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[32];
-  const int64_t cb = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int rhs = blockIdx.y;
+  const int64_t cb = bx * (int64_t)blockDim.x + threadIdx.x;
   if (upd && !upd[rhs]) return;  // uniform per block
   double nrm[1] = {0.0};
   if (cb < g.Vh) {
@@ -310,8 +317,18 @@ __global__ void __launch_bounds__(128, 1) hop64_lincomb_kernel(EoGeom g, HopGaug
     store_sp<SP64, NCOMP>(out, rhs, cb, v);
   }
   if (res) {
-    if (grid_sum<1>(nrm, partials + (int64_t)rhs * nblk, counters + rhs, sh) && threadIdx.x == 0) res[rhs] = nrm[0];
+    if (grid_sum_n<1>(nrm, partials + (int64_t)rhs * nblk, counters + rhs, sh, bx, nblk) && threadIdx.x == 0)
+      res[rhs] = nrm[0];
   }
+}
+
+template <int ND, int NC, bool G5IN, bool G5OUT>
+__global__ void __launch_bounds__(128, 1) hop64_lincomb_kernel(EoGeom g, HopGauge hg, EoField in, int par, EoField out,
+                                                            EoField z0, EoField z1, double a1, double c,
+                                                            const int* upd, double* partials, unsigned* counters,
+                                                            double* res, int nblk) {
+  hop64_lincomb_body<ND, NC, G5IN, G5OUT>(g, hg, in, par, out, z0, z1, a1, c, upd, partials, counters, res, nblk,
+                                          blockIdx.x, blockIdx.y);
 }
 
 // |f|^2 per rhs (FP64 field)
@@ -522,13 +539,13 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_update_kernel(EoGe
 // (t = q converted, s = H_oe gamma_d t), i.e. r = M^dag q, for rhs with upd[rhs];
 // res[rhs] = |r|^2.
 template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
-__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_rnew_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField r,
-                                                      double k2, const int* upd, double* partials,
-                                                      unsigned* counters, double* res, int nblk) {
+LYM_D void cg_rnew_body(const EoGeom& g, const HopGauge& hg, const EoField& s, const EoField& t, const EoField& r,
+                        double k2, const int* upd, double* partials, unsigned* counters, double* res, int nblk,
+                        int bx, int by) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[R * 32];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs0 = blockIdx.y * R;
+  const int i = bx * blockDim.x + threadIdx.x;
+  const int rhs0 = by * R;
   int act[R];
   int any = 0;
 #pragma unroll
@@ -563,11 +580,19 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_rnew_kernel(EoGeom
       store_sp<SP, NCOMP>(r, rhs0 + q, cb, v);
     }
   }
-  if (grid_sum<R>(n, partials + (int64_t)blockIdx.y * nblk * R, counters + blockIdx.y, sh) && threadIdx.x == 0) {
+  if (grid_sum_n<R>(n, partials + (int64_t)by * nblk * R, counters + by, sh, bx, nblk) && threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < R; ++q)
       if (act[q]) res[rhs0 + q] = n[q];
   }
+}
+
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_rnew_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField r,
+                                                      double k2, const int* upd, double* partials,
+                                                      unsigned* counters, double* res, int nblk) {
+  cg_rnew_body<ND, NC, SP, GP, COMP, R, MX>(g, hg, s, t, r, k2, upd, partials, counters, res, nblk, blockIdx.x,
+                                            blockIdx.y);
 }
 
 // dst = src (same precision) for rhs with upd[rhs]
@@ -1344,9 +1369,12 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
 // ---------------------------------------------------------------------------
 struct CgLat {
   EoGeom g;
-  HopGauge hg;
+  HopGauge hg, hg64;
   EoField p, s, t, r, xs;
+  EoField x64, s64, q, bp;  // FP64 fields of the reliable update
   CGState* st;
+  const int* upd;
+  double* res;
   double* partials;
   unsigned* counters;
   int64_t Vh;
@@ -1395,10 +1423,64 @@ __global__ void __launch_bounds__(128) cgm_p_kernel(const CgLat* __restrict__ la
   cg_p_body<SP, NCOMP>(D.Vh, D.r, D.p, D.st, D.counters, bx, rhs, D.nblk);
 }
 
+// The FP64 reliable update of every lattice (the rhs with upd set), as
+// reliable_update does for one: x64 += x_sloppy; s64 = H_oe x64;
+// q = b' - M x64 with |q|^2 -> res; t = q (sloppy); s = H_oe gamma_d t;
+// r = M^dag q with |r|^2 -> res.
+template <int XP, int NCOMP>
+__global__ void __launch_bounds__(128) cgm_accumulate_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, rhs = local / D.nblk, bx = local - rhs * D.nblk;
+  accumulate_body<XP, NCOMP>(D.Vh, D.xs, D.x64, D.upd, bx, rhs);
+}
+
+template <int ND, int NC>
+__global__ void __launch_bounds__(128, 1) cgm_hx64_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, rhs = local / D.nblk, bx = local - rhs * D.nblk;
+  const EoField none;
+  hop64_lincomb_body<ND, NC, false, false>(D.g, D.hg64, D.x64, 1, D.s64, none, none, 0.0, 1.0, D.upd, nullptr,
+                                           nullptr, nullptr, D.nblk, bx, rhs);
+}
+
+template <int ND, int NC>
+__global__ void __launch_bounds__(128, 1) cgm_q64_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, rhs = local / D.nblk, bx = local - rhs * D.nblk;
+  hop64_lincomb_body<ND, NC, false, false>(D.g, D.hg64, D.s64, 0, D.q, D.bp, D.x64, -1.0, D.k2, D.upd, D.partials,
+                                           D.counters, D.res, D.nblk, bx, rhs);
+}
+
+template <int SP, int NCOMP>
+__global__ void __launch_bounds__(128) cgm_convert_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, rhs = local / D.nblk, bx = local - rhs * D.nblk;
+  const EoField none;
+  convert_body<SP, NCOMP>(D.Vh, D.q, D.t, none, 1, D.upd, bx, rhs);
+}
+
+template <int ND, int NC, int SP, int GP, bool COMP, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cgm_hopt_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, by = local / D.nblk, bx = local - by * D.nblk;
+  cg_hop_body<ND, NC, SP, GP, COMP, true, 1, MX>(D.g, D.hg, D.t, D.s, 1, nullptr, bx, by);
+}
+
+template <int ND, int NC, int SP, int GP, bool COMP, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cgm_rnew_kernel(const CgLat* __restrict__ lats, int n) {
+  const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
+  const int local = blockIdx.x - D.b0, by = local / D.nblk, bx = local - by * D.nblk;
+  cg_rnew_body<ND, NC, SP, GP, COMP, 1, MX>(D.g, D.hg, D.s, D.t, D.r, D.k2, D.upd, D.partials, D.counters, D.res,
+                                            D.nblk, bx, by);
+}
+
 struct MultiOps {
   void (*iterate)(GraphRec&, cudaStream_t, const CgLat*, int n, int blocks);  // one iteration, 5 launches
+  void (*q_part)(cudaStream_t, const CgLat*, int n, int blocks);  // reliable update up to |q|^2
+  void (*r_part)(cudaStream_t, const CgLat*, int n, int blocks);  // the rest: r = M^dag q, |r|^2
   void (*preload)();
 };
+constexpr int kMultiUpdateLaunches = 6;
 
 template <int ND, int NC, int SP, bool COMP, int MX>
 struct MultiImpl {
@@ -1413,6 +1495,16 @@ struct MultiImpl {
     launch_rec(rec, st, cgm_update_kernel<ND, NC, SP, GP, COMP, XP, MX>, grid, blk, lats, n);
     launch_rec(rec, st, cgm_p_kernel<SP, NCOMP>, grid, blk, lats, n);
   }
+  static void q_part(cudaStream_t st, const CgLat* lats, int n, int blocks) {
+    if constexpr (SP != SP64) cgm_accumulate_kernel<XP, NCOMP><<<blocks, 128, 0, st>>>(lats, n);
+    cgm_hx64_kernel<ND, NC><<<blocks, 128, 0, st>>>(lats, n);
+    cgm_q64_kernel<ND, NC><<<blocks, 128, 0, st>>>(lats, n);
+  }
+  static void r_part(cudaStream_t st, const CgLat* lats, int n, int blocks) {
+    cgm_convert_kernel<SP, NCOMP><<<blocks, 128, 0, st>>>(lats, n);
+    cgm_hopt_kernel<ND, NC, SP, GP, COMP, MX><<<blocks, 128, 0, st>>>(lats, n);
+    cgm_rnew_kernel<ND, NC, SP, GP, COMP, MX><<<blocks, 128, 0, st>>>(lats, n);
+  }
   static void preload() {
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, cgm_hop_kernel<ND, NC, SP, GP, COMP, false, MX>);
@@ -1421,7 +1513,7 @@ struct MultiImpl {
     cudaFuncGetAttributes(&a, cgm_update_kernel<ND, NC, SP, GP, COMP, XP, MX>);
     cudaFuncGetAttributes(&a, cgm_p_kernel<SP, NCOMP>);
   }
-  static MultiOps table() { return MultiOps{&iterate, &preload}; }
+  static MultiOps table() { return MultiOps{&iterate, &q_part, &r_part, &preload}; }
 };
 
 template <int ND, int NC>
@@ -1518,53 +1610,7 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
   const double delta = prm->delta > 0 && prm->delta < 1 ? prm->delta : 0.1;
   const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 8;
   EoField none;
-  // per-lattice setup, as cg_solve_on: source, |b|^2, b', x = 0, first residual, p = r;
-  // every lattice's work is enqueued first and the host waits once
-  for (int l = 0; l < nlat; ++l) {
-    MultiLat& L = lats[l];
-    Work& w = *L.w;
-    const int n = w.nrhs;
-    L.nreal = nrhs[l];
-    L.tol = tols ? tols[l] : prm->tol;
-    w.kappa = kappas[l];
-    w.launches = 0;
-    const double k = kappas[l];
-    w.ops.to_eo(w, bs[l], prm->hermitian ? 1 : 0, st);
-    w.ops.norm64(w, w.be, 0, st);
-    w.ops.norm64(w, w.bo, 1, st);
-    LYM_CHECK_LAUNCH();
-    // |b|^2 to res_host[4n..5n) (the reliable update below fills [0..2n))
-    LYM_CUDA(cudaMemcpyAsync(w.res_host + 4 * n, w.res, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-    for (int i = 0; i < n; ++i) w.upd_host[i] = 1;
-    LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
-    w.ops.hop64(w, 0, w.bo, w.bp, w.be, none, 0.0, -k, false, false, false, st);
-    w.ops.zero64(w, w.x64, st);
-    if (sp != SP64) LYM_CUDA(cudaMemsetAsync(w.xs.data, 0, field_bytes(w.xp, gs[l]->ncomp, w.Vh, n), st));
-    LYM_CHECK_LAUNCH();
-    int rc = reliable_update(w, st, false);
-    if (rc) return rc;
-  }
-  LYM_CUDA(cudaStreamSynchronize(st));
-  for (int l = 0; l < nlat; ++l) {
-    MultiLat& L = lats[l];
-    Work& w = *L.w;
-    const int n = w.nrhs;
-    L.bnorm2.assign(w.res_host + 4 * n, w.res_host + 5 * n);
-    L.tres.assign(n, 0.0);
-    L.prev_q2.assign(n, 0.0);
-    L.done.assign(n, 0);
-    L.updates.assign(n, 0);
-    L.restart.assign(n, 0);
-    for (int i = 0; i < n; ++i) {
-      std::memset(&w.st_host[i], 0, sizeof(CGState));
-      w.st_host[i].max_iter = prm->max_iter;
-      multi_plan(L, prm, delta, i, w.res_host[i], w.res_host[n + i]);
-    }
-    LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * n, cudaMemcpyHostToDevice, st));
-    w.ops.copy_rp(w, st);
-    LYM_CHECK_LAUNCH();
-  }
-  // lattice descriptors and the graph of `chunk` iterations over all lattices
+  // lattice descriptors (device copy for the multi-lattice kernels)
   std::vector<CgLat> desc(nlat);
   int blocks = 0;
   for (int l = 0; l < nlat; ++l) {
@@ -1572,12 +1618,19 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
     CgLat& D = desc[l];
     D.g = gs[l]->geom;
     D.hg = w.hgs;
+    D.hg64 = w.hg64;
     D.p = w.p;
     D.s = w.s;
     D.t = w.t;
     D.r = w.r;
     D.xs = w.xs;
+    D.x64 = w.x64;
+    D.s64 = w.s64;
+    D.q = w.q;
+    D.bp = w.bp;
     D.st = w.st;
+    D.upd = w.upd;
+    D.res = w.res;
     D.partials = w.partials;
     D.counters = w.counters;
     D.Vh = w.Vh;
@@ -1601,6 +1654,69 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
     }
   } release{d_desc, st};
   LYM_CUDA(cudaMemcpyAsync(d_desc, desc.data(), sizeof(CgLat) * nlat, cudaMemcpyHostToDevice, st));
+  int64_t launches = 0;
+  // FP64 reliable update of every lattice's rhs with upd set, in launches over all
+  // lattices; |q|^2 lands in res_host[0..n), |r|^2 in res_host[n..2n)
+  auto fused_update = [&]() -> int {
+    ops.q_part(st, d_desc, nlat, blocks);
+    LYM_CHECK_LAUNCH();
+    for (auto& L : lats)
+      LYM_CUDA(cudaMemcpyAsync(L.w->res_host, L.w->res, sizeof(double) * L.w->nrhs, cudaMemcpyDeviceToHost, st));
+    ops.r_part(st, d_desc, nlat, blocks);
+    LYM_CHECK_LAUNCH();
+    for (auto& L : lats)
+      LYM_CUDA(cudaMemcpyAsync(L.w->res_host + L.w->nrhs, L.w->res, sizeof(double) * L.w->nrhs,
+                               cudaMemcpyDeviceToHost, st));
+    LYM_CUDA(cudaStreamSynchronize(st));
+    launches += kMultiUpdateLaunches;
+    return LYM_OK;
+  };
+  // per-lattice setup, as cg_solve_on: source, |b|^2, b', x = 0; then the first
+  // residual of every lattice at once, and p = r
+  for (int l = 0; l < nlat; ++l) {
+    MultiLat& L = lats[l];
+    Work& w = *L.w;
+    const int n = w.nrhs;
+    L.nreal = nrhs[l];
+    L.tol = tols ? tols[l] : prm->tol;
+    w.kappa = kappas[l];
+    w.launches = 0;
+    const double k = kappas[l];
+    w.ops.to_eo(w, bs[l], prm->hermitian ? 1 : 0, st);
+    w.ops.norm64(w, w.be, 0, st);
+    w.ops.norm64(w, w.bo, 1, st);
+    LYM_CHECK_LAUNCH();
+    // |b|^2 to res_host[4n..5n) (the reliable update fills [0..2n))
+    LYM_CUDA(cudaMemcpyAsync(w.res_host + 4 * n, w.res, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    for (int i = 0; i < n; ++i) w.upd_host[i] = 1;
+    LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+    w.ops.hop64(w, 0, w.bo, w.bp, w.be, none, 0.0, -k, false, false, false, st);
+    w.ops.zero64(w, w.x64, st);
+    if (sp != SP64) LYM_CUDA(cudaMemsetAsync(w.xs.data, 0, field_bytes(w.xp, gs[l]->ncomp, w.Vh, n), st));
+    LYM_CHECK_LAUNCH();
+  }
+  int rc = fused_update();
+  if (rc) return rc;
+  for (int l = 0; l < nlat; ++l) {
+    MultiLat& L = lats[l];
+    Work& w = *L.w;
+    const int n = w.nrhs;
+    L.bnorm2.assign(w.res_host + 4 * n, w.res_host + 5 * n);
+    L.tres.assign(n, 0.0);
+    L.prev_q2.assign(n, 0.0);
+    L.done.assign(n, 0);
+    L.updates.assign(n, 0);
+    L.restart.assign(n, 0);
+    for (int i = 0; i < n; ++i) {
+      std::memset(&w.st_host[i], 0, sizeof(CGState));
+      w.st_host[i].max_iter = prm->max_iter;
+      multi_plan(L, prm, delta, i, w.res_host[i], w.res_host[n + i]);
+    }
+    LYM_CUDA(cudaMemcpyAsync(w.st, w.st_host, sizeof(CGState) * n, cudaMemcpyHostToDevice, st));
+    w.ops.copy_rp(w, st);
+    LYM_CHECK_LAUNCH();
+  }
+  // the graph of `chunk` iterations over all lattices
   ops.preload();
   {
     cudaGraph_t graph = nullptr;
@@ -1614,7 +1730,6 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
     if (graph) cudaGraphDestroy(graph);
     cudaGetLastError();  // without a graph the iterations run as plain launches
   }
-  int64_t launches = 0;
   auto active_any = [&]() {
     for (auto& L : lats)
       for (int i = 0; i < L.w->nrhs; ++i)
@@ -1639,25 +1754,24 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
         for (int i = 0; i < L.w->nrhs; ++i) running = running || L.w->st_host[i].active;
       if (!running) break;
     }
-    // reliable updates of every rhs that paused and is not done, all lattices
-    // enqueued, one host wait
+    // reliable updates of every rhs that paused and is not done, all lattices in
+    // the same launches, one host wait
     std::vector<int> updated(nlat, 0);
+    bool any_update = false;
     for (int l = 0; l < nlat; ++l) {
       MultiLat& L = lats[l];
       Work& w = *L.w;
       const int n = w.nrhs;
-      bool any = false;
       for (int i = 0; i < n; ++i) {
         w.upd_host[i] = !L.done[i] ? 1 : 0;  // as cg_solve_on: capped rhs get their last update too
-        any = any || w.upd_host[i];
+        updated[l] = updated[l] || w.upd_host[i];
       }
-      if (!any) continue;
-      updated[l] = 1;
+      any_update = any_update || updated[l];
       LYM_CUDA(cudaMemcpyAsync(w.upd, w.upd_host, sizeof(int) * n, cudaMemcpyHostToDevice, st));
-      int rc = reliable_update(w, st, false);
-      if (rc) return rc;
     }
-    LYM_CUDA(cudaStreamSynchronize(st));
+    if (!any_update) break;
+    rc = fused_update();
+    if (rc) return rc;
     for (int l = 0; l < nlat; ++l) {
       if (!updated[l]) continue;
       MultiLat& L = lats[l];
