@@ -55,3 +55,27 @@ def test_bad_arguments_are_rejected():
     out = np.empty((2, 16), np.int64)
     assert lib.lym_lookup_tables(2, bad, out.ctypes.data, None, None) == _lib.LYM_ERR_BAD_ARG
     assert b"extent" in lib.lym_last_error()
+
+
+def test_solver_entry_points_validate_before_any_device_work():
+    """The multi-lattice and even-odd multishift entry points reject bad arguments
+    (null pointers, counts out of range) before touching a device."""
+    import ctypes
+    lib = _lib.lib()
+    prm = _lib.SolverParams(1e-10, 100, 1, 0.1, 0, 8, 0, 0, 0, 0.0)
+    reps = (_lib.SolverReport * 4)()
+    one = (ctypes.c_void_p * 1)(None)
+    k = (ctypes.c_double * 1)(0.1)
+    n = (ctypes.c_int * 1)(1)
+    assert lib.lym_wilson_solve_multi(0, one, k, None, n, one, one, ctypes.byref(prm), reps, None) == \
+        _lib.LYM_ERR_BAD_ARG
+    assert lib.lym_wilson_solve_multi(1, None, k, None, n, one, one, ctypes.byref(prm), reps, None) == \
+        _lib.LYM_ERR_BAD_ARG
+    assert lib.lym_wilson_solve_multi(1, one, k, None, n, one, one, None, reps, None) == _lib.LYM_ERR_BAD_ARG
+    sh = (ctypes.c_double * 1)(0.1)
+    assert lib.lym_multishift_solve_eo(None, 0.1, 1, 1, sh, None, None, ctypes.byref(prm), reps, None) == \
+        _lib.LYM_ERR_BAD_ARG
+    zero = _lib.SolverParams(0.0, 100, 1, 0.1, 0, 8, 0, 0, 0, 0.0)
+    assert lib.lym_wilson_solve_multi(1, one, k, None, n, one, one, ctypes.byref(zero), reps, None) == \
+        _lib.LYM_ERR_BAD_ARG
+    assert b"tol" in lib.lym_last_error()
