@@ -1071,7 +1071,7 @@ def run_multishift(args, local_rank):
 
 
 def run_precision_study(args, local_rank):
-    """BASELINE config 3 as far as it is built: on 24^3 x 48 SU(3) (links
+    """The precision study on 24^3 x 48 SU(3) (links
     reunit(exp(i 0.3 H)), antiperiodic time) at kappa 0.12 and 0.13, 8 unit complex
     Gaussian rhs: (a) the even-odd CG to true relative residual 1e-10 with FP64, FP32,
     FP16 and BF16 inner iterations (FP64 reliable updates), each solution's relative

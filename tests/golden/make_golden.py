@@ -38,7 +38,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REFERENCE = "/root/reference"
 
 CASES = {
-    # BASELINE config-1 geometry: D=2 24x16 SU(2), kappa=-0.15, beta=3.0
+    # the CPU-runnable HMC case: D=2 24x16 SU(2), kappa=-0.15, beta=3.0
     "d2": dict(geometry=(24, 16), nc=2, kappa=-0.15, beta=3.0, seed=11,
                hmc_steps=[4, 3], n_traj=10, shifts=[0.5, 0.1, 0.01]),
     # 4D SU(3) on an asymmetric small lattice, kappa=0.13, beta=5.6

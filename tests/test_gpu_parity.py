@@ -507,7 +507,7 @@ def test_md_trajectory_vs_reference(cuda_device, case):
 
 
 def test_hmc_chain_config1(cuda_device):
-    """BASELINE config 1 (D=2 24x16 SU(2), beta=3, kappa=-0.15, antiperiodic time,
+    """The CPU-runnable HMC case (D=2 24x16 SU(2), beta=3, kappa=-0.15, antiperiodic time,
     Omelyan [4,3], t=1): 10 trajectories fed the reference's momenta, eta and
     uniforms; dH, acceptance and plaquette per trajectory against the reference."""
     from tfleonardym_b200 import dirac, dirac_solver, fermion_action, gauge_action, hmc, measurements
