@@ -690,6 +690,7 @@ struct Work {
   EoField r, p, t, s, xs;
   CGState* st = nullptr;
   CGState* st_host = nullptr;
+  CGState* st_ahead = nullptr;    // pinned: the state after the chunk launched ahead (cg_solve_on)
   int* upd = nullptr;
   int* upd_host = nullptr;
   double* partials = nullptr;
@@ -708,6 +709,7 @@ struct Work {
   cudaStream_t graph_stream = nullptr;
   cudaStream_t stream = nullptr;  // solves run here (non-blocking, fenced to the caller's stream by events)
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaEvent_t ev_state[2] = {nullptr, nullptr};  // the two state copies in flight
   int64_t launches = 0;           // kernels launched by the current call (graph nodes included)
 };
 
@@ -883,6 +885,9 @@ static void free_work(Work* w) {
   if (w->pool) cudaFree(w->pool);
   if (w->ev_in) cudaEventDestroy(w->ev_in);
   if (w->ev_out) cudaEventDestroy(w->ev_out);
+  for (cudaEvent_t e : w->ev_state)
+    if (e) cudaEventDestroy(e);
+  if (w->st_ahead) cudaFreeHost(w->st_ahead);
   if (w->stream) cudaStreamDestroy(w->stream);
   if (w->st_host) cudaFreeHost(w->st_host);
   if (w->upd_host) cudaFreeHost(w->upd_host);
@@ -993,6 +998,9 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   // zero everything: reduction counters, and the padding rhs' sources stay zero for good
   if (cudaMemset(w->pool, 0, bytes) != cudaSuccess ||
       cudaMallocHost(&w->st_host, sizeof(CGState) * nrhs) != cudaSuccess ||
+      cudaMallocHost(&w->st_ahead, sizeof(CGState) * nrhs) != cudaSuccess ||
+      cudaEventCreateWithFlags(&w->ev_state[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&w->ev_state[1], cudaEventDisableTiming) != cudaSuccess ||
       cudaMallocHost(&w->upd_host, sizeof(int) * nrhs) != cudaSuccess ||
       cudaMallocHost(&w->res_host, sizeof(double) * nrhs * nres) != cudaSuccess ||
       cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1285,8 +1293,12 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
     bool any_active = false;
     for (int i = 0; i < nrhs; ++i) any_active = any_active || (!done[i] && w.st_host[i].active);
     if (!any_active) break;
-    // run chunks until every rhs paused, finished or hit max_iter
-    while (true) {
+    // run chunks until every rhs paused, finished or hit max_iter.  One chunk
+    // is always in flight ahead of the state the host looks at, so the device
+    // keeps iterating while the host thread wakes up; a chunk launched after
+    // every rhs paused does nothing (its blocks find no active rhs and return,
+    // the state stays as it was).
+    auto launch_chunk = [&](CGState* to, cudaEvent_t ev) -> int {
       if (w.graph) {
         LYM_CUDA(cudaGraphLaunch(w.graph, st));
       } else {
@@ -1294,12 +1306,27 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
         LYM_CHECK_LAUNCH();
       }
       w.launches += (int64_t)chunk * kLaunchesPerIteration;
-      LYM_CUDA(cudaMemcpyAsync(w.st_host, w.st, sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
-      LYM_CUDA(cudaStreamSynchronize(st));
+      LYM_CUDA(cudaMemcpyAsync(to, w.st, sizeof(CGState) * nrhs, cudaMemcpyDeviceToHost, st));
+      LYM_CUDA(cudaEventRecord(ev, st));
+      return LYM_OK;
+    };
+    CGState* bufs[2] = {w.st_host, w.st_ahead};
+    int cur = 0;
+    rc = launch_chunk(bufs[0], w.ev_state[0]);
+    if (rc) return rc;
+    while (true) {
+      rc = launch_chunk(bufs[1 - cur], w.ev_state[1 - cur]);  // ahead
+      if (rc) return rc;
+      LYM_CUDA(cudaEventSynchronize(w.ev_state[cur]));
       bool running = false;
-      for (int i = 0; i < nrhs; ++i) running = running || w.st_host[i].active;
-      if (!running) break;
+      for (int i = 0; i < nrhs; ++i) running = running || bufs[cur][i].active;
+      if (!running) {
+        LYM_CUDA(cudaEventSynchronize(w.ev_state[1 - cur]));  // the chunk ahead: no change
+        break;
+      }
+      cur = 1 - cur;
     }
+    if (bufs[cur] != w.st_host) std::memcpy(w.st_host, bufs[cur], sizeof(CGState) * nrhs);
     // reliable update for every rhs that paused and is not done
     bool any = false;
     for (int i = 0; i < nrhs; ++i) {
