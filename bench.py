@@ -37,8 +37,11 @@ BETA = 5.6
 EPS = 0.25
 TOL = 1e-10
 METRIC = "Wilson-CG solves/s at 1e-10 true relative residual"
-ITER_FILE = os.path.join(ROOT, "profiles", "wilson_cg_16x16x16x16_iterations.txt")
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dslash_eo_f16_16x16x16x16_traffic.txt")
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the solver hop
+# (16^4, 16 rhs, L2 cold), keyed by (precision, nrhs, hop form, tile, compressed links);
+# captured once per kernel change, the capture's summary is the file named here
+STORED_TRAFFIC_FILE = "profiles/dslash_eo_f16_16x16x16x16_traffic.txt"
+STORED_TRAFFIC = {("f16", 16, 1, 1, False): 40031488.0}
 
 
 def parse_args():
@@ -50,7 +53,13 @@ def parse_args():
     ap.add_argument("--nrhs", type=int, default=16)
     ap.add_argument("--precision", default="f16", choices=["f64", "f32", "f16", "bf16"])
     ap.add_argument("--plain-solves", type=int, default=4)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-sample", type=int, default=16,
+                    help="MMMR steps of the CPU baseline's timed sample (GPU arm)")
+    ap.add_argument("--ref-sample", type=int, default=4, help="MMMR steps per --impl reference step")
+    ap.add_argument("--ref-max-steps", type=int, default=3000, help="MMMR step cap of the reference's whole solve")
+    ap.add_argument("--step-requests", type=int, default=128,
+                    help="single-rhs requests per timed step of the headline (served in batches of --nrhs)")
+    ap.add_argument("--repeats", type=int, default=3, help="timed regions of the headline; value = their median")
     ap.add_argument("--delta", type=float, default=0.01, help="reliable-update trigger of the mixed solver")
     ap.add_argument("--chunk", type=int, default=8, help="CG iterations per CUDA graph launch")
     ap.add_argument("--workers", type=int, default=2, help="solve-server worker streams")
@@ -178,76 +187,71 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle's even-odd CG on the same workload (bounded sample)
+# CPU baseline: the reference's own solve path, restated in the oracle, on the
+# host's threads
 # ---------------------------------------------------------------------------
-def oracle_cg_iteration_seconds(seconds, seed=2026):
-    """Time CG iterations of the oracle (oracle.lym_oracle.eo_solve's CGNR on the
-    16^4 even-odd system) for about ``seconds`` of CPU work; returns (s/iteration, n)."""
-    import scipy.linalg
+def host_threads():
+    return max(1, len(os.sched_getaffinity(0)))
 
-    from oracle import lym_oracle as O
+
+def host_exp_links(seed):
+    """The links of the GPU arm on the host: exp(i eps H) for the same H, by
+    eigendecomposition (the GPU arm's Cayley-Hamilton exponential followed by
+    reunitarisation gives the same SU(3) links up to rounding); (nd, N, N, V)."""
     h = host_links(seed)
-    u = scipy.linalg.expm(1j * EPS * h)  # (nd, V, N, N)
-    u = O.unitary_sqrt_projection(np.ascontiguousarray(np.transpose(u, (0, 2, 3, 1))))
-    setup = O.WilsonSetup(u, KAPPA, GEOMETRY, bc_factor=-1, hermitian=False)
-    b = host_sources(seed + 1, 1)[0]
-    par, cb, eo = O.parity_maps(GEOMETRY)
-    k = KAPPA
+    w, v = np.linalg.eigh(h)
+    u = np.einsum("...ik,...k,...jk->...ij", v, np.exp(1j * EPS * w), np.conj(v))
+    return np.ascontiguousarray(np.transpose(u, (0, 2, 3, 1)))
 
-    def h_eo(vo):
-        full = O.from_eo(np.zeros_like(vo), vo, eo)
-        return O.hopping(setup.gauge_bc, full, setup.tables)[..., eo[0]]
 
-    def h_oe(ve):
-        full = O.from_eo(ve, np.zeros_like(ve), eo)
-        return O.hopping(setup.gauge_bc, full, setup.tables)[..., eo[1]]
+class HostWilson:
+    """The oracle's restatement of the reference's Wilson operator (dirac.py:458-523,
+    649-662) with every apply split over `threads` host threads by output sites
+    (numpy releases the GIL inside its kernels), as TensorFlow's intra-op threads
+    split the reference's einsums."""
 
-    def m(ve):
-        return ve - k * k * h_eo(h_oe(ve))
+    def __init__(self, seed, threads):
+        from concurrent.futures import ThreadPoolExecutor
 
-    def mdag(ve):
-        return O.gamma_d(m(O.gamma_d(ve)))
+        from oracle import lym_oracle as O
+        self.O = O
+        self.tables = O.lookup_tables(GEOMETRY)
+        self.gauge = O.apply_time_bc(host_exp_links(seed), O.antiperiodic_field(GEOMETRY))
+        vol = int(np.prod(GEOMETRY))
+        self.chunks = np.array_split(np.arange(vol), threads)
+        self.pool = ThreadPoolExecutor(threads)
+        self.threads = threads
 
-    be, bo = O.to_eo(b, eo)
-    bp = be - k * h_eo(bo)
-    x = np.zeros_like(bp)
-    r = mdag(bp)
-    p = r.copy()
-    rr = np.real(O.dot(r, r))
+    def apply(self, v, hermitian):
+        O = self.O
+        parts = self.pool.map(lambda s: O.wilson_apply_sites(self.gauge, v, KAPPA, hermitian, self.tables, s),
+                              self.chunks)
+        return np.concatenate(list(parts), axis=-1)
+
+    def close(self):
+        self.pool.shutdown()
+
+
+def host_mmmr(op, b, max_steps):
+    """D x = b the reference's way: multishift_solver.solve (dirac_solver.py:19-53,
+    oracle.mmmr_multishift) on SquareOperator(Q) (dirac.py:27-37), Q = gamma_d D, with
+    source gamma_d b and the single shift 0, stopping at |<r,r>| < 1e-20 |b|^2 (true
+    relative residual 1e-10); then x = Q y.  Returns (x, MMMR steps, converged, seconds)."""
+    O = op.O
+    precision = 1e-20 * float(np.vdot(b, b).real)
     t0 = time.perf_counter()
-    n = 0
-    while True:  # the loop body of oracle.lym_oracle.cg_normal
-        t = m(p)
-        alpha = rr / np.real(O.dot(t, t))
-        x = x + alpha * p
-        r = r - alpha * mdag(t)
-        rr_new = np.real(O.dot(r, r))
-        p = r + (rr_new / rr) * p
-        rr = rr_new
-        n += 1
-        if time.perf_counter() - t0 > seconds and n >= 2:
-            break
-    return (time.perf_counter() - t0) / n, n
+    ys, steps, conv = O.mmmr_multishift(lambda v: op.apply(op.apply(v, True), True), O.gamma_d(b), [0.0],
+                                        max_steps, precision)
+    x = op.apply(ys[0], True)
+    return x, steps, conv, time.perf_counter() - t0
 
 
-def read_iterations(default=80):
-    try:
-        for line in open(ITER_FILE):
-            if line.startswith("fp64_iterations="):
-                return int(line.split("=")[1])
-    except OSError:
-        pass
-    return default
-
-
-def read_traffic():
-    try:
-        for line in open(TRAFFIC_FILE):
-            if line.startswith("bytes_per_launch="):
-                return float(line.split("=")[1])
-    except OSError:
-        pass
-    return None
+def host_mmmr_seconds_per_step(op, b, steps):
+    """Seconds per MMMR step of host_mmmr, timed over `steps` steps (a bounded sample)."""
+    O = op.O
+    t0 = time.perf_counter()
+    O.mmmr_multishift(lambda v: op.apply(op.apply(v, True), True), O.gamma_d(b), [0.0], steps, 0.0)
+    return (time.perf_counter() - t0) / steps
 
 
 def max_over_ranks(ms, world, device):
@@ -270,7 +274,7 @@ def workload_config(args, world):
     """The workload both arms report (the reference arm solves the same systems with
     the oracle port of the reference's algorithm on the host cores)."""
     return {"workload": "served wilson-eo-cg 16^4 SU(3) kappa=0.13 tol=1e-10", "geometry": list(GEOMETRY),
-            "step": f"{args.nrhs} single-rhs requests", "max_batch_rhs": args.max_batch or args.nrhs,
+            "step": f"{args.step_requests} single-rhs requests", "max_batch_rhs": args.max_batch or args.nrhs,
             "server_workers": args.workers,
             "inner_precision": args.precision, "outer_precision": "f64",
             "reliable_update_delta": args.delta, "graph_chunk": args.chunk,
@@ -279,38 +283,42 @@ def workload_config(args, world):
             "l2": "inputs larger than L2 (the sources and solutions of the timed requests exceed 126 MB)"}
 
 
-def _ref_worker(args):
-    seconds, seed = args
-    os.environ.setdefault("OMP_NUM_THREADS", "1")
-    return oracle_cg_iteration_seconds(seconds, seed)
-
-
 def run_reference(args, rank, world):
-    """--impl reference: the oracle restatement of the reference's algorithm on
-    all host cores (one process per core, each on its own right-hand side)."""
+    """--impl reference: the reference's own algorithm for this solve (its MMMR
+    multishift solver on Q^2 and its Wilson operator, restated in the oracle) on the
+    host with all its threads, on the GPU arm's workload.  Each step times a bounded
+    sample of --ref-sample MMMR steps; after the timed steps one whole solve runs to
+    the 1e-10 true residual, which gives the MMMR step count per solve (and its
+    wall time as a cross-check).  value = 1 / (seconds per MMMR step x steps per solve)."""
     if rank != 0:
         return 0
-    import multiprocessing as mp
-    cores = len(os.sched_getaffinity(0))
-    procs = max(1, min(cores, 32))
-    iters = read_iterations()
+    threads = host_threads()
+    op = HostWilson(1234, threads)
+    b = host_sources(99, 1)[0]
     per_step = []
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(procs) as pool:
-        for step in range(args.warmup + args.steps):
-            res = pool.map(_ref_worker, [(max(1.0, args.cpu_seconds / 4), 100 + i) for i in range(procs)])
-            if step >= args.warmup:
-                per_step.append(sum(1.0 / (s * iters) for s, _ in res))
-    value = statistics.mean(per_step)
+    for step in range(args.warmup + args.steps):
+        sec = host_mmmr_seconds_per_step(op, b, args.ref_sample)
+        if step >= args.warmup:
+            per_step.append(sec)
+    x, steps, conv, full_s = host_mmmr(op, b, args.ref_max_steps)
+    res = float(np.linalg.norm(b - op.apply(x, False)) / np.linalg.norm(b))
+    op.close()
+    executed = steps + 1
+    sec_step = statistics.mean(per_step)
+    value = 1.0 / (sec_step * executed)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f64",
-        "data": "synthetic", "scaling": "weak", "vs_baseline": None,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_step * args.ref_sample * 1e3,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic", "scaling": "weak", "vs_baseline": None,
         "config": workload_config(args, world),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "port",
-                         "sample": f"{procs} processes x CG iterations of the oracle's even-odd CGNR on 16^4 "
-                                   f"(about {max(1.0, args.cpu_seconds / 4):.0f} s each per step), extrapolated "
-                                   f"with {iters} iterations per solve"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"the reference's solve path (multishift_solver MMMR on SquareOperator(Q), shift "
+                                   f"0, then x = Q y; dirac_solver.py:19-53, dirac.py:27-37,458-523) restated in "
+                                   f"the oracle, each Wilson apply split over {threads} host threads; each step "
+                                   f"times {args.ref_sample} MMMR steps ({sec_step:.3f} s per MMMR step), "
+                                   f"extrapolated with the {executed} MMMR steps one whole solve took in this run "
+                                   f"(true residual {res:.2e}, {full_s:.1f} s wall, converged={conv})"},
+        "full_solve_s": full_s, "mmmr_steps_per_solve": executed, "true_residual": res,
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -419,26 +427,34 @@ def run_lym(args, rank, world, local_rank):
 
     served(2 * B * args.workers, b_dev)  # warm the server: gauge copies, workspaces, graphs, autotuning
     torch.cuda.synchronize()
+    nstep = args.step_requests
+
+    # --repeats timed regions of exactly --steps steps each (a step = --step-requests
+    # single-rhs requests); value = the median region's rate
     clocks = ClockSampler(local_rank)
     clocks.start()
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t_wall = time.perf_counter()
-    ev0.record(stream)
-    # process-wide NVTX start/end range (covers the server's worker threads):
-    # ncu --nvtx --nvtx-include timed selects the timed region's launches
-    nvtx_timed = torch.cuda.nvtx.range_start("timed")
-    res = served(args.steps * B, b_dev)
-    torch.cuda.synchronize()
-    torch.cuda.nvtx.range_end(nvtx_timed)
-    ev1.record(stream)
-    ev1.synchronize()
-    barrier()
-    t_wall = time.perf_counter() - t_wall
+    regions = []
+    for rep in range(max(1, args.repeats)):
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_wall = time.perf_counter()
+        ev0.record(stream)
+        # process-wide NVTX start/end range (covers the server's worker threads):
+        # ncu --nvtx --nvtx-include timed selects the timed region's launches
+        nvtx_timed = torch.cuda.nvtx.range_start("timed")
+        res = served(args.steps * nstep, b_dev)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_end(nvtx_timed)
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+        t_wall = time.perf_counter() - t_wall
+        ms = max_over_ranks(ev0.elapsed_time(ev1), world, dev)
+        regions.append((replica_throughput(world, args.steps * nstep, ms), ms, t_wall, res))
     clk = clocks.stop()
-    total_ms = max_over_ranks(ev0.elapsed_time(ev1), world, dev)
-    value = replica_throughput(world, args.steps * B, total_ms)
+    ordered = sorted(regions, key=lambda t: t[0])
+    value, total_ms, t_wall, res = ordered[len(ordered) // 2]
     launches = sum(r.reports[0]["kernel_launches"] / r.batch_rhs for r in res)
     iters = [m["iterations"] for r in res for m in r.reports]
     rupd = [m["reliable_updates"] for r in res for m in r.reports]
@@ -453,14 +469,14 @@ def run_lym(args, rank, world, local_rank):
     # ---- end to end through the serving API with host buffers ----
     torch.cuda.synchronize()
     ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    n_e2e = max(2, args.steps // 2) * B
+    e2e_steps = max(2, args.steps // 4)
     ev2.record(stream)
-    served(n_e2e, b_host)
+    served(e2e_steps * nstep, b_host)
     torch.cuda.synchronize()
     ev3.record(stream)
     ev3.synchronize()
     e2e_total = max_over_ranks(ev2.elapsed_time(ev3), world, dev)
-    e2e_value = replica_throughput(world, n_e2e, e2e_total)
+    e2e_value = replica_throughput(world, e2e_steps * nstep, e2e_total)
     srv.close()
 
     # ---- the same solves as direct batched calls (no server) ----
@@ -468,10 +484,11 @@ def run_lym(args, rank, world, local_rank):
         mixed.solve(op, b_dev)
     torch.cuda.synchronize()
     direct_ms = []
+    x_mixed = None
     for _ in range(max(2, args.steps // 2)):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        mixed.solve(op, b_dev)
+        x_mixed = mixed.solve(op, b_dev)
         e.record(stream)
         torch.cuda.synchronize()
         check(mixed.reports)
@@ -479,16 +496,19 @@ def run_lym(args, rank, world, local_rank):
     direct_value = B / (statistics.mean(direct_ms) / 1e3)
 
     # ---- plain FP64 one solve at a time ----
-    plain_ms, plain_iters = [], []
+    plain_ms, plain_iters, mixed_vs_fp64 = [], [], []
     for i in range(args.plain_solves):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        plain.solve(op, b_dev[i % B])
+        x_plain = plain.solve(op, b_dev[i % B])
         e.record(stream)
         torch.cuda.synchronize()
         check(plain.reports)
         plain_ms.append(s.elapsed_time(e))
         plain_iters.append(plain.reports[0]["iterations"])
+        # the mixed-precision solution's distance from the FP64 one (same rhs)
+        mixed_vs_fp64.append(float(torch.linalg.vector_norm(x_mixed[i % B] - x_plain) /
+                                   torch.linalg.vector_norm(x_plain)))
     plain_value = 1e3 / statistics.mean(plain_ms)
 
     # ---- roofline: the solver's dslash timed alone, L2 flushed between launches ----
@@ -510,7 +530,8 @@ def run_lym(args, rank, world, local_rank):
     bs = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}[args.precision]
     spinor_bytes = spin_reals * bs + (4 if args.precision in ("f16", "bf16") else 0)
     # links as the tuned kernel reads them: N-1 rows (12 reals for SU(3)) or the full 18
-    comp = bool(mixed.reports[0]["compressed_links"])
+    rep0 = mixed.reports[0]
+    comp = bool(rep0["compressed_links"])
     link_bytes = ((12 if NC == 3 else 4) if comp else 2 * NC * NC) * bs
     algo_bytes = B * (vol // 2) * 2 * spinor_bytes + nd * vol * link_bytes
     peaks = {}
@@ -520,18 +541,34 @@ def run_lym(args, rank, world, local_rank):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = algo_bytes / hop_s / 1e9
-    # ncu DRAM bytes of one launch of this kernel (FP16, 16 rhs, the tuned tile), captured once
-    traffic = read_traffic() if (args.precision == "f16" and B == 16 and mixed.reports[0]["mixed_fma"]) else None
+    kind = {0: "FP32-arithmetic", 1: "mixed-precision (f16 x f16 + f32 FMA)", 2: "tensor-core (mma.sync f16, f32 accum)"}
+    traffic = STORED_TRAFFIC.get((args.precision, B, rep0["mixed_fma"], rep0["rhs_per_thread"], comp))
 
-    # ---- CPU baseline (rank 0, N = 1 only) ----
+    # ---- CPU baseline (rank 0, N = 1 only): the reference's solve path on the host ----
     cpu = None
     if rank == 0 and world == 1:
-        sec_per_it, nit = oracle_cg_iteration_seconds(args.cpu_seconds)
-        it_per_solve = statistics.mean(plain_iters)
-        cpu = {"value": 1.0 / (sec_per_it * it_per_solve), "unit": "solves/s", "cores": 1, "kind": "port",
-               "sample": f"{nit} CG iterations of the oracle's even-odd CGNR on 16^4 (numpy, one core), "
-                         f"{sec_per_it:.2f} s each, extrapolated with the {it_per_solve:.0f} iterations the "
-                         f"plain FP64 GPU solve took"}
+        # MMMR steps per solve of this workload, from the reference's algorithm on the
+        # device (lym_mmmr_solve: multishift_solver's arithmetic in its order)
+        q_op = dirac.DiracWilsonOperator(cfg, KAPPA, True, representation="fundamental",
+                                         boundary_condition_provider=boundary_conditions.time_antiperiodic_provider(-1))
+        b0 = b_dev[0]
+        mmmr = dirac_solver.multishift_solver(args.ref_max_steps, 1e-20 * float(torch.vdot(b0.flatten(),
+                                                                                          b0.flatten()).real))
+        g5b = b0.clone()
+        g5b[2:] *= -1
+        y = mmmr.solve(dirac.SquareOperator(q_op), g5b, [0.0])[0]
+        mres = float(torch.linalg.vector_norm(b0 - op.apply(q_op.apply(y))) / torch.linalg.vector_norm(b0))
+        executed = mmmr.last_steps + 1
+        threads = host_threads()
+        hop_cpu = HostWilson(1234 + rank, threads)
+        sec_step = host_mmmr_seconds_per_step(hop_cpu, host_sources(99 + rank, 1)[0], args.cpu_sample)
+        hop_cpu.close()
+        cpu = {"value": 1.0 / (sec_step * executed), "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"the reference's solve path (multishift_solver MMMR on SquareOperator(Q), shift 0, then "
+                         f"x = Q y; dirac_solver.py:19-53, dirac.py:27-37,458-523) restated in the oracle, each "
+                         f"Wilson apply split over {threads} host threads: {args.cpu_sample} MMMR steps timed "
+                         f"({sec_step:.3f} s each), extrapolated with the {executed} MMMR steps the same algorithm "
+                         f"took on this workload on the device in this run (true residual {mres:.2e})"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -539,6 +576,10 @@ def run_lym(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": f"{args.precision}+f64",
         "data": "synthetic",
         "config": workload_config(args, world),
+        "repeats": {"values": [r[0] for r in regions], "median": value,
+                    "spread": (ordered[-1][0] - ordered[0][0]) / value,
+                    "timed_s": [r[1] / 1e3 for r in regions],
+                    "what": f"{len(regions)} timed regions of {args.steps} steps x {nstep} requests; value = median"},
         "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                        "what": f"request latency, Poisson arrivals at {rate:.0f} req/s (half the saturated rate)"},
         "batch_rhs_seen": batch_sizes,
@@ -547,22 +588,28 @@ def run_lym(args, rank, world, local_rank):
         "plain_fp64": {"value": world * plain_value, "unit": "solves/s", "ms_per_solve": statistics.mean(plain_ms),
                        "iterations": plain_iters},
         "speedup_vs_plain_fp64": value / (world * plain_value),
+        "mixed_vs_fp64": {"max_rel_diff": max(mixed_vs_fp64), "rhs": len(mixed_vs_fp64),
+                          "what": "|x_mixed - x_fp64| / |x_fp64| per rhs, both solved to true residual 1e-10"},
         "iterations_per_solve": {"mean": statistics.mean(iters), "max": max(iters),
                                  "reliable_updates_mean": statistics.mean(rupd)},
         "autotuned": tuned,
         "gpu_launches": int(launches),
         "e2e": {"value": e2e_value, "unit": "solves/s",
-                "h2d_bytes_per_step": int(b_host.numel() * 16), "d2h_bytes_per_step": int(b_host.numel() * 16),
+                "h2d_bytes_per_step": int(nstep * b_host[0].numel() * 16),
+                "d2h_bytes_per_step": int(nstep * b_host[0].numel() * 16),
                 "what": "the served path with pinned host sources; solutions come back to host memory"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
-                     "kernel": f"cg_hop_kernel 4D SU(3) {args.precision} s_o = H_oe p_e, {B} rhs, "
-                               f"{mixed.reports[0]['rhs_per_thread']} rhs per thread, "
-                               f"{'compressed' if comp else 'full'} links"
-                               f"{', mixed-precision FP16 hop' if mixed.reports[0]['mixed_fma'] else ''}, "
+                     "traffic_source": (f"stored: ncu dram__bytes of one launch of this kernel and tile "
+                                        f"({STORED_TRAFFIC_FILE})") if traffic else None,
+                     "kernel": f"solver hop 4D SU(3) {args.precision} s_o = H_oe p_e, {B} rhs, "
+                               f"{kind.get(rep0['mixed_fma'], '')} "
+                               f"{'rhs per CTA' if rep0['mixed_fma'] == 2 else 'rhs per thread'} "
+                               f"{rep0['rhs_per_thread']}, {'compressed' if comp else 'full'} links, "
                                f"L2 flushed before each launch",
                      "algorithmic_bytes_per_launch": algo_bytes, "launch_us": hop_s * 1e6,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback"},
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy), of measured" if peaks
+                     else "fallback 6650 GB/s"},
         "clocks": clk,
         "wall_s_timed": t_wall,
     }

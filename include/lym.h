@@ -121,7 +121,8 @@ int lym_caxpby(int64_t n, const double* a, const void* x, const double* b, void*
  * would not see a cudaMalloc) or under a fixed device-memory budget.  It allocates
  * nothing: its reduction scratch is a static device array of about 263 KB that every
  * GPU loading the library keeps until exit, which limits nvec to 64 (larger nvec
- * returns LYM_ERR_BAD_ARG).  The first call on a device looks up the array's address;
+ * returns LYM_ERR_BAD_ARG).  The first call on each device also looks up the array's
+ * device address (cudaGetSymbolAddress, once per device, cached for later calls);
  * make that first call before any stream capture.  All calls share the array, so
  * calls that overlap on the GPU (other streams, other host threads) race.
  * Synchronises `stream`. */

@@ -119,6 +119,28 @@ def wilson_apply(gauge_bc, psi, kappa, hermitian, tables):
     return gamma_d(out) if hermitian else out
 
 
+def wilson_apply_sites(gauge_bc, psi, kappa, hermitian, tables, sites):
+    """wilson_apply restricted to the output sites ``sites`` (int array): returns
+    (ns, N, len(sites)).  The same formula (dirac.py:503-523 + 649-662) evaluated
+    site by site, so that lattices too large for a whole-field numpy apply can be
+    checked at a sample of sites."""
+    nd = gauge_bc.shape[0]
+    g, _ = gammas(nd)
+    ident = np.eye(g.shape[1])
+    sup, sdn, _ = tables
+    sites = np.asarray(sites, dtype=np.int64)
+    out = np.array(psi[:, :, sites], dtype=np.complex128, copy=True)
+    hop = np.zeros_like(out)
+    for mu in range(nd):
+        up, dn = sup[mu][sites], sdn[mu][sites]
+        fwd = np.einsum("mn,njc->mjc", ident - g[mu], psi[:, :, up])
+        hop += np.einsum("ijc,mjc->mic", gauge_bc[mu][:, :, sites], fwd)
+        bwd = np.einsum("mn,njc->mjc", ident + g[mu], psi[:, :, dn])
+        hop += np.einsum("jic,mjc->mic", np.conj(gauge_bc[mu][:, :, dn]), bwd)
+    out = out + kappa * hop
+    return gamma_d(out) if hermitian else out
+
+
 def dot(v1, v2):
     """sum conj(v1) v2 over all indices (algebra_utils.py:5-11)."""
     if v1.shape != v2.shape:

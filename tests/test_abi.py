@@ -72,7 +72,11 @@ def test_solver_entry_points_validate_before_any_device_work():
     assert lib.lym_wilson_solve_multi(1, None, k, None, n, one, one, ctypes.byref(prm), reps, None) == \
         _lib.LYM_ERR_BAD_ARG
     assert lib.lym_wilson_solve_multi(1, one, k, None, n, one, one, None, reps, None) == _lib.LYM_ERR_BAD_ARG
-    sh = (ctypes.c_double * 1)(0.1)
+    # a null first gauge object is refused before its fields are read
+    assert lib.lym_wilson_solve_multi(1, one, k, None, n, one, one, ctypes.byref(prm), reps, None) == \
+        _lib.LYM_ERR_BAD_ARG
+    assert b"lattice 0" in lib.lym_last_error()
+    sh =(ctypes.c_double * 1)(0.1)
     assert lib.lym_multishift_solve_eo(None, 0.1, 1, 1, sh, None, None, ctypes.byref(prm), reps, None) == \
         _lib.LYM_ERR_BAD_ARG
     zero = _lib.SolverParams(0.0, 100, 1, 0.1, 0, 8, 0, 0, 0, 0.0)

@@ -417,6 +417,43 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
         assert abs(its - base) <= max(3, base // 10), (arith, tile, its, base)
 
 
+@pytest.mark.parametrize("geometry,nrhs", [((4, 4, 4, 8), 16), ((2, 4, 4, 6), 8), ((6, 4, 2, 4), 4),
+                                           ((4, 4, 4, 6), 12)])
+def test_eo_cg_tensor_core_hop(cuda_device, geometry, nrhs):
+    """The tensor-core FP16 hop (4D SU(3); projected FP16 spinors x FP16 links on
+    mma.sync, FP32 accumulation; 16, 8 or 4 rhs per CTA) meets the oracle's true
+    residual for every rhs in about the iterations of the FP32-arithmetic FP16 hop;
+    sites past a CTA's last full tile (6 x 4 x 2 x 4: 96 sites per parity) and
+    rhs groups of 4 are covered."""
+    from tfleonardym_b200 import boundary_conditions as bcs
+    from tfleonardym_b200 import dirac, dirac_solver
+    from tfleonardym_b200 import lattice as lt
+    nc = 3
+    u = _smooth_links(geometry, nc, seed=sum(geometry) + nrhs)
+    kappa = 0.12
+    tables = O.lookup_tables(geometry)
+    ub = O.apply_time_bc(u, O.antiperiodic_field(geometry))
+    cfg = lt.Configuration(cu(u), tuple(geometry), nc, len(geometry))
+    rng = np.random.default_rng(nrhs)
+    b = rng.normal(size=(nrhs, 4, nc, u.shape[-1])) + 1j * rng.normal(size=(nrhs, 4, nc, u.shape[-1]))
+    for herm in (False, True):
+        op = dirac.DiracWilsonOperator(cfg, kappa, herm, representation="fundamental",
+                                       boundary_condition_provider=bcs.time_antiperiodic_provider(-1))
+        ref = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=1)
+        ref.solve(op, cu(b))
+        base = max(r["iterations"] for r in ref.reports)
+        tcg = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=16, mixed_fma=2)
+        x = np_(tcg.solve(op, cu(b)))
+        rep = tcg.reports[0]
+        assert rep["mixed_fma"] == 2 and rep["compressed_links"] == 0, rep
+        assert rep["rhs_per_thread"] == max(g for g in (4, 8, 16) if nrhs % g == 0), rep
+        for i in range(nrhs):
+            res = np.linalg.norm(b[i] - O.wilson_apply(ub, x[i], kappa, herm, tables)) / np.linalg.norm(b[i])
+            assert res < 1e-10, (herm, i, res, tcg.reports[i])
+        its = max(r["iterations"] for r in tcg.reports)
+        assert abs(its - base) <= max(3, base // 10), (herm, its, base)
+
+
 def test_eo_cg_batch_equals_single(cuda_device):
     """A right-hand side gives the same answer alone and inside a batch."""
     from tfleonardym_b200 import dirac_solver

@@ -3,6 +3,7 @@
 // even-odd multishift CG (lym_mshift.cu).
 #pragma once
 
+#include <mutex>
 #include <tuple>
 #include <utility>
 #include <vector>
@@ -36,6 +37,11 @@ struct lym_gauge {
   int* nbr = nullptr;      // even-odd neighbour table (EoGeom::nbr)
   std::vector<lym::Work*> works;      // CG workspaces, most recently used first
   std::vector<lym::MsWork*> ms_works; // multishift workspaces, most recently used first
+  // Held for the whole of every call that uses or changes the workspaces or the
+  // packed links (solves, lym_dslash_eo, lym_gauge_update): two host threads that
+  // share a gauge object take turns instead of sharing one workspace's stream,
+  // pinned state buffers and graphs.
+  std::recursive_mutex mu;
 };
 
 namespace lym {
@@ -54,11 +60,12 @@ struct GraphRec {
   cudaError_t err = cudaSuccess;    // first error while adding nodes
 };
 
+// smem: dynamic shared memory bytes of the launch
 template <typename... KArgs, typename... Args>
-inline void launch_rec(GraphRec& rec, cudaStream_t st, void (*kernel)(KArgs...), dim3 grid, dim3 block,
-                       Args&&... args) {
+inline void launch_rec_smem(GraphRec& rec, cudaStream_t st, void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                            size_t smem, Args&&... args) {
   if (!rec.graph) {
-    kernel<<<grid, block, 0, st>>>(std::forward<Args>(args)...);
+    kernel<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
     return;
   }
   std::tuple<KArgs...> vals(std::forward<Args>(args)...);
@@ -71,13 +78,19 @@ inline void launch_rec(GraphRec& rec, cudaStream_t st, void (*kernel)(KArgs...),
   p.func = (void*)kernel;
   p.gridDim = grid;
   p.blockDim = block;
-  p.sharedMemBytes = 0;
+  p.sharedMemBytes = (unsigned)smem;
   p.kernelParams = ptrs;
   cudaGraphNode_t node = nullptr;
   const cudaError_t e = cudaGraphAddKernelNode(&node, rec.graph, rec.last ? &rec.last : nullptr,
                                                rec.last ? 1 : 0, &p);
   if (e != cudaSuccess && rec.err == cudaSuccess) rec.err = e;
   if (e == cudaSuccess) rec.last = node;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_rec(GraphRec& rec, cudaStream_t st, void (*kernel)(KArgs...), dim3 grid, dim3 block,
+                       Args&&... args) {
+  launch_rec_smem(rec, st, kernel, grid, block, 0, std::forward<Args>(args)...);
 }
 
 }  // namespace lym

@@ -1440,6 +1440,7 @@ int lym_multishift_solve_eo(lym_gauge* g, double kappa, int nrhs, int nshift, co
               "precision %d was not enabled in lym_gauge_create", params->precision);
   for (int s = 0; s < nshift; ++s)
     LYM_REQUIRE(shifts[s] >= 0, LYM_ERR_BAD_ARG, "negative shifts need BiCGStab (dirac_solver.py:26-30)");
+  std::lock_guard<std::recursive_mutex> own(g->mu);
   return ms_solve_on(g, kappa, nrhs, nshift, shifts, b, xs, params, reports, (cudaStream_t)stream);
 }
 

@@ -25,6 +25,7 @@
 
 #include "lym_eo.cuh"
 #include "lym_gauge_obj.cuh"
+#include "lym_hop_tc.cuh"
 #include "lym_internal.cuh"
 #include "lym_kernels.cuh"
 
@@ -642,6 +643,178 @@ __global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoFiel
 }
 
 // ---------------------------------------------------------------------------
+// tensor-core FP16 hop kernels (4D SU(3), FP16 spinors, full FP16 links; the hop
+// core and its layout are in lym_hop_tc.cuh).  One thread per (site, rhs), a
+// CTA per (S sites, RG rhs); the epilogues are the one-rhs forms of the bodies
+// above.
+// ---------------------------------------------------------------------------
+template <int RG>
+LYM_D double* tc_red(char* smem) {
+  using P = tc::Plan<RG>;
+  return reinterpret_cast<double*>(smem + 2 * P::kTile + P::kLinks + P::kCodes);
+}
+
+// the block-uniform "any rhs of this group active" test (every thread reads the same flags)
+template <int RG>
+LYM_D bool tc_any(const CGState* st, const int* upd) {
+  int any = 0;
+#pragma unroll
+  for (int k = 0; k < RG; ++k) {
+    const int q = blockIdx.y * RG + k;
+    any |= upd ? upd[q] : (st ? st[q].active : 1);
+  }
+  return any != 0;
+}
+
+// s = H G5IN(p) (output parity par); st == nullptr: every rhs
+template <bool G5IN, int RG>
+__global__ void __launch_bounds__(256) cg_hop_tc_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
+                                                        const CGState* st) {
+  extern __shared__ __align__(16) char smem[];
+  constexpr int S = 256 / RG, NCOMP = 12;
+  if (!tc_any<RG>(st, nullptr)) return;
+  const int i = threadIdx.x % S, r = threadIdx.x / S, rhs = blockIdx.y * RG + r;
+  const bool act = st ? st[rhs].active != 0 : true;
+  const int cb = blockIdx.x * S + i;
+  cx<float> acc[4][3];
+  tc::hop_tc<G5IN, RG>(g, hg, in, par, blockIdx.x * S, blockIdx.y * RG, i, r, act, smem, acc);
+  if (!act || cb >= g.Vh) return;
+  cx<float> v[NCOMP];
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[s * 3 + c] = acc[s][c];
+  store_sp<SP16, NCOMP>(out, rhs, cb, v);
+}
+
+// t = p - kappa^2 H_eo s ; alpha = rr / |t|^2
+template <int RG>
+__global__ void __launch_bounds__(256) cg_t_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t,
+                                                      double k2, CGState* st, double* partials,
+                                                      unsigned* counters, int nblk) {
+  extern __shared__ __align__(16) char smem[];
+  constexpr int S = 256 / RG, NCOMP = 12;
+  if (!tc_any<RG>(st, nullptr)) return;
+  const int i = threadIdx.x % S, r = threadIdx.x / S, rhs = blockIdx.y * RG + r;
+  const bool act = st[rhs].active != 0;
+  const int cb = blockIdx.x * S + i;
+  cx<float> acc[4][3];
+  tc::hop_tc<false, RG>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, r, act, smem, acc);
+  double n = 0.0;
+  if (act && cb < g.Vh) {
+    cx<float> v[NCOMP];
+    load_sp<SP16, NCOMP>(p, rhs, cb, v);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cx<float>& w = v[a * 3 + c];
+        w -= (float)k2 * acc[a][c];
+        n += (double)w.re * w.re + (double)w.im * w.im;
+      }
+    store_sp<SP16, NCOMP>(t, rhs, cb, v);
+  }
+  double tot = 0.0;
+  if (tc::grid_rhs_sum<RG>(n, tc_red<RG>(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
+    CGState& Sx = st[blockIdx.y * RG + threadIdx.x];
+    if (Sx.active) {
+      if (tot > 0.0 && Sx.rr > 0.0) {
+        Sx.alpha = Sx.rr / tot;
+      } else {
+        Sx.alpha = 0.0;
+        Sx.active = 0;  // p = 0: nothing left to do
+      }
+    }
+  }
+}
+
+// Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr
+template <int RG>
+__global__ void __launch_bounds__(256) cg_update_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
+                                                           EoField x, EoField r, double k2, CGState* st,
+                                                           double* partials, unsigned* counters, int nblk) {
+  extern __shared__ __align__(16) char smem[];
+  constexpr int S = 256 / RG, NCOMP = 12;
+  if (!tc_any<RG>(st, nullptr)) return;
+  const int i = threadIdx.x % S, q = threadIdx.x / S, rhs = blockIdx.y * RG + q;
+  const bool act = st[rhs].active != 0;
+  const int cb = blockIdx.x * S + i;
+  cx<float> acc[4][3];
+  tc::hop_tc<false, RG>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, q, act, smem, acc);
+  double n = 0.0;
+  if (act && cb < g.Vh) {
+    const double alpha = st[rhs].alpha;
+    cx<float> tv[NCOMP], pv[NCOMP], rv[NCOMP], xv[NCOMP];
+    load_sp<SP16, NCOMP>(t, rhs, cb, tv);
+    load_sp<SP16, NCOMP>(p, rhs, cb, pv);
+    load_sp<SP16, NCOMP>(r, rhs, cb, rv);
+    load_sp<SP32, NCOMP>(x, rhs, cb, xv);
+    const float a = (float)alpha;
+#pragma unroll
+    for (int sp = 0; sp < 4; ++sp)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int k = sp * 3 + c;
+        cx<float> h = acc[sp][c];
+        if (sp >= 2) h = -h;
+        const cx<float> ap = tv[k] - (float)k2 * h;
+        rv[k] -= a * ap;
+        xv[k] += (float)alpha * pv[k];
+        n += (double)rv[k].re * rv[k].re + (double)rv[k].im * rv[k].im;
+      }
+    store_sp<SP16, NCOMP>(r, rhs, cb, rv);
+    store_sp<SP32, NCOMP>(x, rhs, cb, xv);
+  }
+  double tot = 0.0;
+  if (tc::grid_rhs_sum<RG>(n, tc_red<RG>(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
+    CGState& Sx = st[blockIdx.y * RG + threadIdx.x];
+    if (Sx.active) {
+      Sx.beta = tot / Sx.rr;
+      Sx.rr = tot;
+      Sx.iters += 1;
+      if (Sx.rr < Sx.pause2 || Sx.iters >= Sx.max_iter || Sx.iters >= Sx.pause_iter)
+        Sx.active = 2;  // finish the p update, then stop
+    }
+  }
+}
+
+// r = t - kappa^2 gamma_d H_eo s for rhs with upd[rhs]; res[rhs] = |r|^2
+template <int RG>
+__global__ void __launch_bounds__(256) cg_rnew_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField r,
+                                                         double k2, const int* upd, double* partials,
+                                                         unsigned* counters, double* res, int nblk) {
+  extern __shared__ __align__(16) char smem[];
+  constexpr int S = 256 / RG, NCOMP = 12;
+  if (!tc_any<RG>(nullptr, upd)) return;
+  const int i = threadIdx.x % S, q = threadIdx.x / S, rhs = blockIdx.y * RG + q;
+  const bool act = upd[rhs] != 0;
+  const int cb = blockIdx.x * S + i;
+  cx<float> acc[4][3];
+  tc::hop_tc<false, RG>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, q, act, smem, acc);
+  double n = 0.0;
+  if (act && cb < g.Vh) {
+    cx<float> v[NCOMP];
+    load_sp<SP16, NCOMP>(t, rhs, cb, v);
+#pragma unroll
+    for (int sp = 0; sp < 4; ++sp)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cx<float> h = acc[sp][c];
+        if (sp >= 2) h = -h;
+        cx<float>& w = v[sp * 3 + c];
+        w -= (float)k2 * h;
+        n += (double)w.re * w.re + (double)w.im * w.im;
+      }
+    store_sp<SP16, NCOMP>(r, rhs, cb, v);
+  }
+  double tot = 0.0;
+  if (tc::grid_rhs_sum<RG>(n, tc_red<RG>(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
+    const int q2 = blockIdx.y * RG + threadIdx.x;
+    if (upd[q2]) res[q2] = tot;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // per-(ND, NC, SP, COMP) operation table
 // ---------------------------------------------------------------------------
 struct Work;
@@ -675,9 +848,9 @@ struct Work {
   int tuned_i = 0;
   // hop-kernel candidates: right-hand sides per thread x compressed / full links
   // (x FP32 / mixed-precision arithmetic for FP16)
-  static constexpr int kMaxCand = 10;
+  static constexpr int kMaxCand = 13;
   int ncand = 0, cur = 0;
-  int rcand[kMaxCand] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int rcand[kMaxCand] = {1};
   bool ccand[kMaxCand] = {};
   int mcand[kMaxCand] = {};
   CgOps ops_r[kMaxCand]{};
@@ -694,6 +867,7 @@ struct Work {
   int* upd = nullptr;
   int* upd_host = nullptr;
   double* partials = nullptr;
+  double* partials_tc = nullptr;  // per rhs and 16-site block: the tensor-core hop's reductions
   unsigned* counters = nullptr;
   double* res = nullptr;       // per rhs, several result slots
   double* res_host = nullptr;
@@ -718,6 +892,12 @@ struct Work {
 template <typename... KArgs, typename... Args>
 static void launch(Work& w, cudaStream_t st, void (*kernel)(KArgs...), dim3 grid, dim3 block, Args&&... args) {
   launch_rec(w.rec, st, kernel, grid, block, std::forward<Args>(args)...);
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_smem(Work& w, cudaStream_t st, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                        Args&&... args) {
+  launch_rec_smem(w.rec, st, kernel, grid, block, smem, std::forward<Args>(args)...);
 }
 
 template <int ND, int NC, int SP, bool COMP, int R, int MX>
@@ -824,6 +1004,70 @@ struct Impl {
   static CgOps table() {
     return CgOps{&iterate, &hop64, &to_eo, &from_eo, &norm64, &convert, &accumulate, &zero64, &dslash, &rnew,
                  &copy_rp, &preload};
+  }
+};
+
+// The tensor-core FP16 hop (4D SU(3), full FP16 links): iterate / dslash / rnew
+// run the cg_*_tc kernels with RG right-hand sides per CTA; everything else is
+// the FP16 mixed-precision table's.
+template <int RG>
+struct ImplTC {
+  using Base = Impl<4, 3, SP16, false, 1, 1>;
+  using P = tc::Plan<RG>;
+  static constexpr int S = P::S;
+  static unsigned nblk(const Work& w) { return (unsigned)((w.Vh + S - 1) / S); }
+  // the kernels take more than 48 KB of dynamic shared memory
+  static void prepare() {
+    cudaFuncSetAttribute(cg_hop_tc_kernel<false, RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_hop_tc_kernel<true, RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_t_tc_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_update_tc_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_rnew_tc_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+  }
+  static void iterate(Work& w, cudaStream_t st) {
+    const double k2 = w.kappa * w.kappa;
+    const dim3 grid(w.nblk, w.nrhs), tile(nblk(w), w.nrhs / RG);
+    const int nb = (int)nblk(w);
+    const CGState* cst = w.st;
+    launch_smem(w, st, cg_hop_tc_kernel<false, RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.p, w.s, 1, cst);
+    launch_smem(w, st, cg_t_tc_kernel<RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st,
+                w.partials_tc, w.counters, nb);
+    launch_smem(w, st, cg_hop_tc_kernel<true, RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.t, w.s, 1, cst);
+    launch_smem(w, st, cg_update_tc_kernel<RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.s, w.t, w.p, w.xs,
+                w.r, k2, w.st, w.partials_tc, w.counters, nb);
+    launch(w, st, cg_p_kernel<SP16, 12>, grid, dim3(128), w.Vh, w.r, w.p, w.st, w.counters);
+  }
+  static void dslash(Work& w, cudaStream_t st) {
+    prepare();
+    w.launches += 1;
+    cg_hop_tc_kernel<false, RG><<<dim3(nblk(w), w.nrhs / RG), 256, P::kBytes, st>>>(w.g->geom, w.hgs, w.p, w.s, 1,
+                                                                                   nullptr);
+  }
+  static void rnew(Work& w, cudaStream_t st) {
+    prepare();
+    const double k2 = w.kappa * w.kappa;
+    const dim3 tile(nblk(w), w.nrhs / RG);
+    w.launches += 2;
+    cg_hop_tc_kernel<true, RG><<<tile, 256, P::kBytes, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, nullptr);
+    cg_rnew_tc_kernel<RG><<<tile, 256, P::kBytes, st>>>(w.g->geom, w.hgs, w.s, w.t, w.r, k2, w.upd, w.partials_tc,
+                                                        w.counters, w.res, (int)nblk(w));
+  }
+  static void preload() {
+    Base::preload();
+    prepare();
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, cg_hop_tc_kernel<false, RG>);
+    cudaFuncGetAttributes(&a, cg_hop_tc_kernel<true, RG>);
+    cudaFuncGetAttributes(&a, cg_t_tc_kernel<RG>);
+    cudaFuncGetAttributes(&a, cg_update_tc_kernel<RG>);
+  }
+  static CgOps table() {
+    CgOps t = Base::table();
+    t.iterate = &iterate;
+    t.dslash = &dslash;
+    t.rnew = &rnew;
+    t.preload = &preload;
+    return t;
   }
 };
 
@@ -952,6 +1196,19 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
       }
     }
   }
+  // the tensor-core hop: 4D SU(3), FP16 spinors, full links, RG = 4, 8 or 16 rhs per CTA
+  if (sp == SP16 && g->nd == 4 && g->nc == 3) {
+    for (int RG : {4, 8, 16}) {
+      if (nrhs % RG != 0) continue;
+      w->ops_r[nc_] = RG == 4 ? ImplTC<4>::table() : (RG == 8 ? ImplTC<8>::table() : ImplTC<16>::table());
+      w->rcand[nc_] = RG;
+      w->ccand[nc_] = false;
+      w->mcand[nc_] = 2;
+      ++nc_;
+    }
+  }
+  const bool has_tc = nc_ > 0 && w->mcand[nc_ - 1] == 2;
+  const size_t ntc = has_tc ? (size_t)nrhs * (size_t)((g->Vh + 15) / 16) : 0;
   w->ncand = nc_;
   w->ops = w->ops_r[0];
   w->R = w->rcand[0];
@@ -966,6 +1223,7 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   bytes += ((sizeof(double) * (size_t)nrhs * w->nblk + 255) & ~(size_t)255);
   bytes += ((sizeof(unsigned) * nrhs + 255) & ~(size_t)255);
   bytes += ((sizeof(double) * nrhs * nres + 255) & ~(size_t)255);
+  bytes += ((sizeof(double) * ntc + 255) & ~(size_t)255);
   if (cudaMalloc(&w->pool, bytes) != cudaSuccess) {
     cudaGetLastError();
     delete w;
@@ -995,6 +1253,8 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   w->counters = reinterpret_cast<unsigned*>(cur);
   cur += (sizeof(unsigned) * nrhs + 255) & ~(size_t)255;
   w->res = reinterpret_cast<double*>(cur);
+  cur += (sizeof(double) * nrhs * nres + 255) & ~(size_t)255;
+  w->partials_tc = ntc ? reinterpret_cast<double*>(cur) : nullptr;
   // zero everything: reduction counters, and the padding rhs' sources stay zero for good
   if (cudaMemset(w->pool, 0, bytes) != cudaSuccess ||
       cudaMallocHost(&w->st_host, sizeof(CGState) * nrhs) != cudaSuccess ||
@@ -1205,6 +1465,7 @@ static int cg_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x
   const int sp = prm->precision;
   LYM_REQUIRE(sp == SP64 || (g->prec_mask >> sp) & 1u, LYM_ERR_BAD_ARG,
               "precision %d was not enabled in lym_gauge_create", sp);
+  std::lock_guard<std::recursive_mutex> own(g->mu);
   Work* wp;
   int rc = get_work(g, nrhs, sp, &wp);
   if (rc) return rc;
@@ -1596,6 +1857,7 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
                           const int* nrhs, const void* const* bs, void* const* xs, const lym_solver_params* prm,
                           lym_solver_report* rep, cudaStream_t caller) {
   const int sp = prm->precision;
+  LYM_REQUIRE(gs[0], LYM_ERR_BAD_ARG, "null argument (lattice 0)");
   const int nd = gs[0]->nd, nc = gs[0]->nc;
   bool comp_all = sp == SP32;
   for (int l = 0; l < nlat; ++l) {
@@ -1609,6 +1871,12 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
     LYM_REQUIRE(!tols || tols[l] > 0, LYM_ERR_BAD_ARG, "tolerance must be positive (lattice %d)", l);
     comp_all = comp_all && gs[l]->comp;
   }
+  // take every gauge object's lock in address order (no two callers can wait on each other)
+  std::vector<lym_gauge*> order(gs, gs + nlat);
+  std::sort(order.begin(), order.end());
+  std::vector<std::unique_lock<std::recursive_mutex>> own;
+  own.reserve(nlat);
+  for (lym_gauge* g : order) own.emplace_back(g->mu);
   const int mx = sp == SP16 ? 1 : 0;
   MultiOps ops;
   LYM_REQUIRE(multi_pick(nd, nc, sp, comp_all, &ops), LYM_ERR_UNSUPPORTED, "unsupported (nd=%d, N=%d)", nd, nc);
@@ -1856,6 +2124,7 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
 
 static int dslash_eo(lym_gauge* g, int precision, int nrhs, int repeats, cudaStream_t st) {
   LYM_REQUIRE(g && repeats >= 0, LYM_ERR_BAD_ARG, "bad argument");
+  std::lock_guard<std::recursive_mutex> own(g->mu);
   Work* w = find_work(g, nrhs, precision);
   LYM_REQUIRE(w, LYM_ERR_BAD_ARG,
               "no solver workspace for precision %d and %d right-hand sides", precision, nrhs);
@@ -2018,6 +2287,7 @@ int lym_gauge_create(const lym_lattice* lat, int nc, const void* gauge, double b
 
 int lym_gauge_update(lym_gauge* g, const void* gauge, void* stream) {
   LYM_REQUIRE(g && gauge, LYM_ERR_BAD_ARG, "null argument");
+  std::lock_guard<std::recursive_mutex> own(g->mu);
   return pack_gauge(g, gauge, (cudaStream_t)stream);
 }
 
