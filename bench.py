@@ -95,6 +95,9 @@ def parse_args():
                          "17 metropolis shifts, --ms-rhs sources in one call, for every --ms-precisions x "
                          "--ms-switch; one JSON line per case")
     ap.add_argument("--kappa", type=float, default=0.13, help="hopping parameter of --multishift")
+    ap.add_argument("--poles", default="zolotarev12", choices=["zolotarev12", "reference17"],
+                    help="shifts of --multishift / --precision-study: the 12 poles of x^(-1/2) on [1e-4, 1] or the "
+                         "reference's 17 metropolis shifts")
     ap.add_argument("--ms-rhs", type=int, default=8, help="sources of --multishift")
     ap.add_argument("--ms-precisions", default="f64,f32,f16,bf16", help="inner precisions of --multishift")
     ap.add_argument("--ms-switch", default="0",
@@ -1030,19 +1033,30 @@ REFERENCE_17_POLES = [708.456969133708774250236839, 20.5545836704482543092111935
                       0.0000000269253347571438797470449799]
 
 
-def _multishift_case(sq, q, b, prec, switch, ref, stream):
+def study_shifts(name):
+    """(label, shifts) of the multishift studies: "zolotarev12" = the 12 poles of
+    x^(-1/2) on [1e-4, 1] (approximations.inverse_sqrt_rational_approximation_coefficients),
+    "reference17" = the reference's 17 metropolis shifts."""
+    if name == "reference17":
+        return "17 reference shifts", list(REFERENCE_17_POLES)
+    from tfleonardym_b200 import approximations
+    _, betas = approximations.split(approximations.inverse_sqrt_rational_approximation_coefficients)
+    return "12 poles of x^(-1/2) on [1e-4, 1]", [float(x) for x in betas]
+
+
+def _multishift_case(sq, q, b, prec, switch, ref, stream, shifts):
     """One timed even-odd multishift solve of all sources in b (after a warm-up
-    solve) on the 17 reference shifts; returns (JSON-ready dict, solutions
-    (rhs, shift, ...)).  ref: FP64 solutions to compare with, or None."""
+    solve) on `shifts`; returns (JSON-ready dict, solutions (rhs, shift, ...)).
+    ref: FP64 solutions to compare with, or None."""
     import torch
 
     from tfleonardym_b200 import dirac_solver
-    nrhs, nsh = b.shape[0], len(REFERENCE_17_POLES)
+    nrhs, nsh = b.shape[0], len(shifts)
     ms = dirac_solver.multishift_cg(20000, 1e-10, precision=prec, delta=0.01, switch_residual=switch)
-    ms.solve(sq, b, REFERENCE_17_POLES)  # warm-up: workspaces, graphs
+    ms.solve(sq, b, shifts)  # warm-up: workspaces, graphs
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record(stream)
-    xs = ms.solve(sq, b, REFERENCE_17_POLES)
+    xs = ms.solve(sq, b, shifts)
     e.record(stream)
     torch.cuda.synchronize()
     xs = torch.stack(xs, 1)  # (rhs, shift, ...)
@@ -1060,7 +1074,8 @@ def _multishift_case(sq, q, b, prec, switch, ref, stream):
     bn = float(torch.linalg.vector_norm(b[0]))
     out["rhs0_reference_layout_residual_max"] = max(
         float(torch.linalg.vector_norm(b[0] - (q.apply(q.apply(xs[0, k])) + sg * xs[0, k]))) / bn
-        for k, sg in enumerate(REFERENCE_17_POLES))
+        for k, sg in enumerate(shifts))
+    out["shifts"] = shifts
     if ref is not None:
         out["rel_diff_to_fp64_per_shift_max"] = [
             max(float(torch.linalg.vector_norm(xs[i, k] - ref[i, k]) / torch.linalg.vector_norm(ref[i, k]))
@@ -1104,15 +1119,16 @@ def run_multishift(args, local_rank):
     q = dirac.DiracWilsonOperator(cfg, args.kappa, True, representation="fundamental",
                                   boundary_condition_provider=prov)
     sq = dirac.SquareOperator(q)
+    label, shifts = study_shifts(args.poles)
     ref = None
     for prec in args.ms_precisions.split(","):
         for sw in (float(x) for x in args.ms_switch.split(",")):
             if prec == "f64" and sw != float(args.ms_switch.split(",")[0]):
                 continue  # no head to switch from
-            out, xs = _multishift_case(sq, q, b, prec, sw, ref, stream)
+            out, xs = _multishift_case(sq, q, b, prec, sw, ref, stream, shifts)
             if prec == "f64" and ref is None:
                 ref = xs.clone()
-            print(json.dumps({"multishift": "even-odd multishift CG, 17 reference shifts", "geometry": list(geom),
+            print(json.dumps({"multishift": f"even-odd multishift CG, {label}", "geometry": list(geom),
                               "kappa": args.kappa, **out}), flush=True)
     return 0
 
@@ -1123,8 +1139,8 @@ def run_precision_study(args, local_rank):
     Gaussian rhs: (a) the even-odd CG to true relative residual 1e-10 with FP64, FP32,
     FP16 and BF16 inner iterations (FP64 reliable updates), each solution's relative
     difference to the FP64 one; (b) the FP64 multishift CG on Q^2 + sigma_k (Q = gamma_d D)
-    for the 17 shifts of the reference's metropolis rational approximation, per-shift
-    FP64 true residual; (c) the even-odd multishift CG on the same 17 shifts, all 8 rhs in
+    for the shifts of --poles (default: the 12 poles of x^(-1/2) on [1e-4, 1]), per-shift
+    FP64 true residual; (c) the even-odd multishift CG on the same shifts, all 8 rhs in
     one call, inner iterations in FP64, FP32, FP16 and BF16 with FP64 reliable updates,
     each (rhs, shift) verified by its FP64 true residual, and each shift's largest
     relative difference to the FP64 solutions."""
@@ -1162,30 +1178,32 @@ def run_precision_study(args, local_rank):
         q = dirac.DiracWilsonOperator(cfg, kappa, True, representation="fundamental", boundary_condition_provider=prov)
         ms_cg = dirac_solver.multishift_cg(20000, 1e-10)
         sq = dirac.SquareOperator(q)
-        ms_cg.solve(sq, b[0], REFERENCE_17_POLES)  # warm-up
+        label, shifts = study_shifts(args.poles)
+        ms_cg.solve(sq, b[0], shifts)  # warm-up
         res, times, iters = [], [], []
         for i in range(2):
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
-            xs = ms_cg.solve(sq, b[i], REFERENCE_17_POLES)
+            xs = ms_cg.solve(sq, b[i], shifts)
             e.record(stream)
             torch.cuda.synchronize()
             times.append(s.elapsed_time(e))
             iters.append(ms_cg.last_steps)
             bn = float(torch.linalg.vector_norm(b[i]))
             res.append([float(torch.linalg.vector_norm(b[i] - (q.apply(q.apply(x)) + sg * x))) / bn
-                        for sg, x in zip(REFERENCE_17_POLES, xs)])
-        print(json.dumps({"precision_study": "multishift CG FP64, 17 reference shifts", "geometry": list(geom),
+                        for sg, x in zip(shifts, xs)])
+        print(json.dumps({"precision_study": f"multishift CG FP64 (full lattice), {label}", "geometry": list(geom),
                           "kappa": kappa, "rhs": 2, "ms_per_rhs": statistics.mean(times), "iterations": iters,
-                          "true_residual_per_shift_max": [max(r[k] for r in res) for k in range(17)]}), flush=True)
+                          "true_residual_per_shift_max": [max(r[k] for r in res) for k in range(len(shifts))]}),
+              flush=True)
         # the even-odd multishift, all 8 sources in one call, inner precision swept;
         # errors per shift against its FP64 solutions
         ref_ms = None
         for prec in ("f64", "f32", "f16", "bf16"):
-            out, xs = _multishift_case(sq, q, b, prec, 0.0, ref_ms, stream)
+            out, xs = _multishift_case(sq, q, b, prec, 0.0, ref_ms, stream, shifts)
             if ref_ms is None:
                 ref_ms = xs.clone()
-            print(json.dumps({"precision_study": "even-odd multishift CG, 17 reference shifts", "geometry": list(geom),
+            print(json.dumps({"precision_study": f"even-odd multishift CG, {label}", "geometry": list(geom),
                               "kappa": kappa, **out}), flush=True)
     return 0
 

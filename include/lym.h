@@ -253,6 +253,16 @@ int lym_gauge_force(const lym_lattice* lat, int nc, double beta, const void* gau
 int lym_staples(const lym_lattice* lat, int nc, const void* gauge, int no_direction,
                 void* staples, void* stream);
 
+/* The per-plane staple terms of staples.py:23-58 (get_staple_fields), in its list
+ * order: terms (nd, 2(nd-1), N, N, V), where for direction mu != no_direction the
+ * planes (mu, nu), nu != mu and nu != no_direction in increasing nu, give slot 2k the
+ * term U_nu(x) U_mu(x+nu) U_nu(x+mu)^dag (sup_staple_trace, staples.py:13-15) and slot
+ * 2k+1 the term U_nu(x-nu)^dag U_mu(x-nu) U_nu(x-nu+mu) (sdn_staple_trace, :18-20).
+ * Slots without a plane (all of direction no_direction, and the last two of the
+ * others when no_direction is a direction) are not written. */
+int lym_staple_terms(const lym_lattice* lat, int nc, const void* gauge, int no_direction,
+                     void* terms, void* stream);
+
 /* out[0] (host) = sum_{x, mu<nu} Re Tr P_mu,nu(x); out[1] = Im (gauge_action.py:110-113
  * summed as in measurements.py:22-43 and gauge_action.py:26-39).  Synchronises. */
 int lym_plaquette_sum(const lym_lattice* lat, int nc, const void* gauge, double* out, void* stream);

@@ -237,6 +237,26 @@ def staples(gauge, tables, no_direction=None):
     return out
 
 
+def staple_terms(gauge, tables, no_direction=None):
+    """The per-direction lists of per-plane staple terms of staples.py:23-58, in its
+    order: for each plane (mu, nu) with mu, nu != no_direction, the up term then the
+    down term; an empty list for mu == no_direction."""
+    nd = gauge.shape[0]
+    out = [[] for _ in range(nd)]
+    for mu in range(nd):
+        for nu in range(nd):
+            if mu == no_direction or nu == no_direction or nu == mu:
+                continue
+            u_mu_xnu = translate(gauge[mu], tables, nu, +1)
+            u_nu_xmu = translate(gauge[nu], tables, mu, +1)
+            out[mu].append(np.einsum("kmc,mnc,pnc->kpc", gauge[nu], u_mu_xnu, np.conj(u_nu_xmu)))
+            u_nu_dn = translate(gauge[nu], tables, nu, -1)
+            u_mu_dn = translate(gauge[mu], tables, nu, -1)
+            u_nu_dn_up = translate(u_nu_dn, tables, mu, +1)
+            out[mu].append(np.einsum("mkc,mnc,npc->kpc", np.conj(u_nu_dn), u_mu_dn, u_nu_dn_up))
+    return out
+
+
 def gauge_force(gauge, beta, tables):
     """Wilson gauge force (gauge_action.py:13-24,42-53):
     W = U S^dag, F = -beta/(4N) (W^dag - W) with the trace/N removed from the diagonal."""

@@ -1,10 +1,11 @@
 """Generate golden vectors by running the unmodified reference on CPU.
 
-Test infrastructure only.  Run in the build container (where the reference
-tree is mounted read-only at /root/reference):
+Test infrastructure only.  Run where a checkout of the reference tree is
+available, naming it with --reference (or the LYM_REFERENCE_DIR environment
+variable):
 
-    python tests/golden/make_golden.py            # all cases
-    python tests/golden/make_golden.py --case d2  # one case
+    python tests/golden/make_golden.py --reference <reference tree>            # all cases
+    python tests/golden/make_golden.py --reference <reference tree> --case d2  # one case
 
 Each case runs in its own subprocess because the reference binds its
 lookup tables at import time (``from translate import lookup_tables`` in
@@ -35,7 +36,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = "/root/reference"
+REFERENCE = os.environ.get("LYM_REFERENCE_DIR", "")
 
 CASES = {
     # the CPU-runnable HMC case: D=2 24x16 SU(2), kappa=-0.15, beta=3.0
@@ -211,6 +212,13 @@ def run_case(name):
         st3 = staples.get_staple_fields(cfg)  # default no_direction=3 (staples.py:23)
         out["staples_no3"] = np.asarray([np.sum([np.asarray(s) for s in elem], axis=0) if elem else
                                          np.zeros((nc, nc, cfg.gauge_field.shape[-1]), complex) for elem in st3])
+        # the per-plane terms themselves, in the reference's list order (staples.py:49-58)
+        for mu, elem in enumerate(st3):
+            out[f"staple_terms_no3/{mu}"] = (np.stack([np.asarray(s) for s in elem]) if elem else
+                                             np.zeros((0, nc, nc, cfg.gauge_field.shape[-1]), complex))
+    st_all = staples.get_staple_fields(cfg, no_direction=nd)
+    for mu, elem in enumerate(st_all):
+        out[f"staple_terms_all/{mu}"] = np.stack([np.asarray(s) for s in elem])
 
     mom = hmc.random_momenta(nc, nd)
     out["momenta"] = np.asarray(mom)
@@ -497,7 +505,13 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", default=None)
     ap.add_argument("--inproc", action="store_true")
+    ap.add_argument("--reference", default=os.environ.get("LYM_REFERENCE_DIR"),
+                    help="the reference source tree (default: $LYM_REFERENCE_DIR)")
     args = ap.parse_args()
+    global REFERENCE
+    if not args.reference or not os.path.isdir(args.reference):
+        ap.error("give the reference tree with --reference or LYM_REFERENCE_DIR")
+    REFERENCE = os.path.abspath(args.reference)
     if args.case and args.inproc:
         if args.case == "tables":
             run_tables()
@@ -515,7 +529,8 @@ def main():
     names = [args.case] if args.case else (["tables"] + list(CASES) + list(ADJOINT_CASES) + list(MEASUREMENT_CASES)
                                            + list(XDR_CASES) + list(OBSERVABLE_CASES))
     for n in names:
-        subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc"], check=True)
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc", "--reference", REFERENCE],
+                       check=True)
 
 
 if __name__ == "__main__":

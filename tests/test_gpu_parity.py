@@ -117,9 +117,20 @@ def test_gauge_side_vs_reference(cuda_device, case):
     assert relerr(np_(ym.force()), g["gauge_force"]) < TOL
     assert abs(ym.energy() - g["gauge_energy"]) < 1e-12 * abs(g["gauge_energy"])
     assert abs(measurements.plaquette(cfg).value - g["plaquette"]) < 1e-14
-    assert relerr(np_(staples.get_staple_fields(cfg, no_direction=nd)), g["staples_all"]) < TOL
+    assert relerr(np_(staples.get_staple_sums(cfg, no_direction=nd)), g["staples_all"]) < TOL
     if "staples_no3" in g:
-        assert relerr(np_(staples.get_staple_fields(cfg)), g["staples_no3"]) < TOL
+        assert relerr(np_(staples.get_staple_sums(cfg)), g["staples_no3"]) < TOL
+    # the reference's return value: per direction, the list of per-plane terms (staples.py:49-58)
+    for key, nodir in (("staple_terms_all", nd), ("staple_terms_no3", 3)):
+        if f"{key}/0" not in g:
+            continue
+        lists = staples.get_staple_fields(cfg, no_direction=nodir)
+        assert len(lists) == nd
+        for mu in range(nd):
+            want = g[f"{key}/{mu}"]
+            assert len(lists[mu]) == want.shape[0], (key, mu)
+            for k, term in enumerate(lists[mu]):
+                assert relerr(np_(term), want[k]) < TOL, (key, mu, k)
     assert abs(hmc.momenta_energy(cu(g["momenta"])) - g["momenta_energy"]) < 1e-12 * abs(g["momenta_energy"])
     assert relerr(np_(hmc.update_momenta(cu(g["momenta"]), cu(g["gauge_force"]), -0.05)), g["update_momenta"]) < TOL
     assert relerr(np_(hmc.update_link_field(cu(g["gauge"]), cu(g["momenta"]), 0.1)), g["update_link_field"]) < 1e-13
@@ -775,6 +786,18 @@ def test_gauge_observables_vs_reference(cuda_device, case):
         assert relerr(np_(line), O.path_product(g["gauge"], tables, [3] * (k + 1))) < 1e-14
     sm = smearing.ape_smearing(cfg, 0.3, no_smear_direction=3)
     assert relerr(np_(sm.gauge_field), g["ape/gauge"]) < 1e-13
+    # a caller that consumes get_staple_fields the way smearing.py:38-44 does (len of
+    # each direction's list, their sum) gets the reference's APE links too
+    from tfleonardym_b200 import staples
+    rho = 0.3
+    fat = []
+    for mu, elem in enumerate(staples.get_staple_fields(cfg, 3)):
+        if len(elem) != 0:
+            fat.append((rho / 6) * torch.stack(elem).sum(0))
+        else:
+            fat.append(rho * cfg.gauge_field[mu])
+    unitary = smearing.unitary_sqrt_projection(torch.stack(fat) + (1 - rho) * cfg.gauge_field)
+    assert relerr(np_(unitary), g["ape/gauge"]) < 1e-13
     res = smearing.multi_smearing_operators(cfg, [lambda c: M.glueball_operators(c, 2)], smearing_levels=2, rho=0.3,
                                             no_smear_direction=3, skip=1)
     assert relerr(np.stack([m.value for m in res]), g["multi/values"]) < 1e-12

@@ -55,6 +55,15 @@ def test_gauge_side(case):
     assert relerr(O.staples(u, tables), g["staples_all"]) < TOL
     if "staples_no3" in g:
         assert relerr(O.staples(u, tables, no_direction=3), g["staples_no3"]) < TOL
+    for key, nodir in (("staple_terms_all", len(geom)), ("staple_terms_no3", 3)):
+        if f"{key}/0" not in g:
+            continue
+        lists = O.staple_terms(u, tables, no_direction=nodir)
+        for mu, elem in enumerate(lists):
+            want = g[f"{key}/{mu}"]
+            assert len(elem) == want.shape[0], (key, mu)
+            for k, term in enumerate(elem):
+                assert relerr(term, want[k]) < TOL, (key, mu, k)
     assert relerr(O.gauge_force(u, spec["beta"], tables), g["gauge_force"]) < TOL
     assert abs(O.gauge_energy(u, spec["beta"], tables) - g["gauge_energy"]) < 1e-12 * abs(g["gauge_energy"])
     assert abs(O.momenta_energy(g["momenta"]) - g["momenta_energy"]) < 1e-12 * abs(g["momenta_energy"])
@@ -269,3 +278,18 @@ def test_gauge_observables_and_smearing(case):
         vals.extend(O.glueball_operators(v, tables, geometry, 2))
     assert relerr(np.stack(vals), g["multi/values"]) < 1e-12
     assert list(g["multi/levels"]) == [0, 0, 0, 0, 1, 1]
+
+
+@pytest.mark.parametrize("case", list(GOLDEN_CASES))
+def test_wilson_apply_sites_matches_golden(case):
+    """The site-restricted oracle apply (used at lattice sizes too large for a
+    whole-field numpy apply) reproduces the reference's apply at every site."""
+    g = load_golden(case)
+    spec = GOLDEN_CASES[case]
+    geom = spec["geometry"]
+    tables = O.lookup_tables(geom)
+    ub = O.apply_time_bc(g["gauge"], O.antiperiodic_field(geom))
+    sites = np.arange(int(np.prod(geom)))[::3]
+    for herm in (0, 1):
+        out = O.wilson_apply_sites(ub, g["eta"], spec["kappa"], bool(herm), tables, sites)
+        assert relerr(out, g[f"apply/h{herm}/anti/projected"][:, :, sites]) < TOL

@@ -236,3 +236,58 @@ def test_same_answer_alone_and_in_the_mix(cuda_device, multi_lattice):
             assert xm.shape[0] == len(r[6]) and m.request.solves == len(r[6])
     st = srv.stats()
     assert st["completed"] == len(reqs) and st["p99_ms"] >= st["p50_ms"]
+
+
+@pytest.mark.gpu
+def test_concurrent_solves_on_two_threads_match_serial(cuda_device):
+    """Two host threads solving at once -- on two gauge objects, and on one shared
+    gauge object (calls on one object take turns under its lock) -- give the
+    serial answers (both to true residual 1e-10, so within 1e-8 of each other)."""
+    import threading
+
+    from oracle import lym_oracle as O
+    from tfleonardym_b200 import boundary_conditions as bcs
+    from tfleonardym_b200 import dirac, dirac_solver
+    from tfleonardym_b200 import lattice as lt
+    geom, nc, kappa = (4, 4, 4, 8), 3, 0.12
+    rng = np.random.default_rng(17)
+    vol = int(np.prod(geom))
+    u = O.unitary_sqrt_projection(rng.normal(size=(4, nc, nc, vol)) + 1j * rng.normal(size=(4, nc, nc, vol)))
+    b = [torch.from_numpy(rng.normal(size=(4, 4, nc, vol)) + 1j * rng.normal(size=(4, 4, nc, vol))).cuda()
+         for _ in range(2)]
+
+    def op():
+        cfg = lt.Configuration(torch.from_numpy(u).cuda(), geom, nc, 4)
+        return dirac.DiracWilsonOperator(cfg, kappa, False, representation="fundamental",
+                                         boundary_condition_provider=bcs.time_antiperiodic_provider(-1))
+
+    def solve(o, src):
+        s = torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            x = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", delta=0.01).solve(o, src)
+        s.synchronize()
+        return x
+
+    ops = [op(), op()]
+    serial = [solve(ops[k], b[k]).cpu() for k in range(2)]
+    for shared in (False, True):
+        targets = [ops[0], ops[0]] if shared else ops
+        out = [None, None]
+        errors = []
+
+        def work(k):
+            try:
+                for _ in range(3):
+                    out[k] = solve(targets[k], b[k]).cpu()
+            except Exception as e:  # surfaced below
+                errors.append(e)
+
+        th = [threading.Thread(target=work, args=(k,)) for k in range(2)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert not errors, errors
+        for k in range(2):
+            diff = float(torch.linalg.vector_norm(out[k] - serial[k]) / torch.linalg.vector_norm(serial[k]))
+            assert diff < 1e-8, (shared, k, diff)

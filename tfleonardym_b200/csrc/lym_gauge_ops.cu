@@ -48,6 +48,39 @@ __global__ void __launch_bounds__(128) staples_kernel(const int32_t* __restrict_
   store_link<NC>(out, mu, s, V, S);
 }
 
+// The per-plane staple terms themselves, in the reference's list order
+// (staples.py:23-58): for direction mu, the planes (mu, nu) with nu != mu,
+// no_dir in increasing nu, each giving the "up" term U_nu(x) U_mu(x+nu)
+// U_nu(x+mu)^dag (sup_staple_trace) then the "down" term U_nu(x-nu)^dag
+// U_mu(x-nu) U_nu(x-nu+mu) (sdn_staple_trace).  out is (nd, 2(nd-1), N, N, V);
+// slot 2k / 2k+1 holds plane k's terms; the slots of an excluded direction and
+// the last two slots of the others when no_dir is a direction are left as they are.
+template <int ND, int NC>
+__global__ void __launch_bounds__(128) staple_terms_kernel(const int32_t* __restrict__ tab, int64_t V,
+                                                           const double2* __restrict__ U, int no_dir,
+                                                           double2* __restrict__ out) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (s >= V || mu == no_dir) return;
+  constexpr int NT = 2 * (ND - 1);
+  const int64_t xmu = tab[mu * V + s];
+  int k = 0;
+#pragma unroll
+  for (int nu = 0; nu < ND; ++nu) {
+    if (nu == mu || nu == no_dir) continue;
+    const int64_t xnu = tab[nu * V + s];
+    const int64_t xmnu = tab[ND * V + nu * V + s];
+    const int64_t xmnu_pmu = tab[mu * V + xmnu];
+    const Mat<NC> up = mul_nd(mul(load_link<NC>(U, nu, s, V), load_link<NC>(U, mu, xnu, V)),
+                              load_link<NC>(U, nu, xmu, V));
+    const Mat<NC> dn = mul(mul_dn(load_link<NC>(U, nu, xmnu, V), load_link<NC>(U, mu, xmnu, V)),
+                           load_link<NC>(U, nu, xmnu_pmu, V));
+    store_link<NC>(out, mu * NT + 2 * k, s, V, up);
+    store_link<NC>(out, mu * NT + 2 * k + 1, s, V, dn);
+    ++k;
+  }
+}
+
 // F = -beta/(4N) (W^dag - W) - trace/N, W = U S^dag (gauge_action.py:42-53).
 // With mom != null: mom += eps F instead of storing F (hmc.py:59-61).
 template <int ND, int NC>
@@ -427,6 +460,18 @@ __global__ void __launch_bounds__(128) fermion_force_kernel(
 using namespace lym;
 
 extern "C" {
+
+int lym_staple_terms(const lym_lattice* lat, int nc, const void* gauge, int no_direction, void* terms,
+                     void* stream) {
+  LYM_REQUIRE(lat && gauge && terms, LYM_ERR_BAD_ARG, "null argument");
+  LYM_REQUIRE(gauge != terms, LYM_ERR_BAD_ARG, "gauge and terms must not alias");
+  cudaStream_t st = (cudaStream_t)stream;
+  dim3 grid(grid_for(lat->V, 128), lat->nd);
+  LYM_DISPATCH_ND_NC(lat->nd, nc, (staple_terms_kernel<ND, NC><<<grid, 128, 0, st>>>(
+                                      lat->d_tab, lat->V, (const double2*)gauge, no_direction, (double2*)terms)));
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
 
 int lym_staples(const lym_lattice* lat, int nc, const void* gauge, int no_direction, void* staples,
                 void* stream) {

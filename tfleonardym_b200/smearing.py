@@ -1,8 +1,9 @@
 """Reunitarisation and APE smearing (mirror of the reference's smearing.py on the GPU).
 
 ``unitary_sqrt_projection`` (smearing.py:17-31): X (X^dag X)^{-1/2} / det^{1/N}
-(lym_unitary_projection).  ``ape_smearing`` (smearing.py:34-51): staples
-(lym_staples), the fat-link combination (lym_caxpby) and the projection.
+(lym_unitary_projection).  ``ape_smearing`` (smearing.py:34-51): summed staples
+(staples.get_staple_sums, lym_staples), the fat-link combination (lym_caxpby) and
+the projection.
 ``multi_smearing_operators`` (smearing.py:54-86) keeps the reference's loop.
 """
 import torch
@@ -23,11 +24,11 @@ def unitary_sqrt_projection(link_config):
 def ape_smearing(cfg, rho, no_smear_direction=3):
     """P_SU(N)[(rho/6) S_mu + (1 - rho) U_mu]; a direction without staples (the
     no-smear one) gets rho U_mu + (1 - rho) U_mu, as in the reference."""
-    from .staples import get_staple_fields
+    from .staples import get_staple_sums
     u = _dev.as_c128(cfg.gauge_field)
     nd = u.shape[0]
     nodir = no_smear_direction if 0 <= no_smear_direction < nd else -1
-    st = get_staple_fields(cfg, nodir)
+    st = get_staple_sums(cfg, nodir)
     fat = torch.empty_like(u)
     for mu in range(nd):
         if mu == nodir:
