@@ -297,7 +297,7 @@ def run_reference(args, rank, world):
         return 0
     threads = host_threads()
     op = HostWilson(1234, threads)
-    b = host_sources(99, 1)[0]
+    b = host_sources(99, args.nrhs)[0]  # the GPU arm's first source
     per_step = []
     for step in range(args.warmup + args.steps):
         sec = host_mmmr_seconds_per_step(op, b, args.ref_sample)
@@ -564,7 +564,7 @@ def run_lym(args, rank, world, local_rank):
         executed = mmmr.last_steps + 1
         threads = host_threads()
         hop_cpu = HostWilson(1234 + rank, threads)
-        sec_step = host_mmmr_seconds_per_step(hop_cpu, host_sources(99 + rank, 1)[0], args.cpu_sample)
+        sec_step = host_mmmr_seconds_per_step(hop_cpu, host_sources(99 + rank, B)[0], args.cpu_sample)
         hop_cpu.close()
         cpu = {"value": 1.0 / (sec_step * executed), "unit": "solves/s", "cores": threads, "kind": "port",
                "sample": f"the reference's solve path (multishift_solver MMMR on SquareOperator(Q), shift 0, then "
@@ -697,7 +697,9 @@ def run_dslash_sweep(args, local_rank):
                                   "gflops": nvec * vol * (flops_site + 4 * ns * NC) / t / 1e9}), flush=True)
             del x, y
         # (rhs per thread, compressed links, mixed-precision FP16 hop); None: the autotuner's pick
-        forced = [None, (1, 0, 0), (1, 1, 0), (2, 0, 0), (4, 0, 0), (1, 0, 1), (2, 0, 1), (4, 0, 1)]
+        # (rhs per CTA, 0, 2): the tensor-core FP16 hop
+        forced = [None, (1, 0, 0), (1, 1, 0), (2, 0, 0), (4, 0, 0), (1, 0, 1), (2, 0, 1), (4, 0, 1),
+                  (4, 0, 2), (8, 0, 2), (16, 0, 2)]
         for prec, nrhs in (("f64", 1), ("f32", 1), ("f16", 1), ("f32", 16), ("f16", 16)):
             b = torch.randn((nrhs, ns, NC, vol), dtype=torch.complex128, device=dev)
             tiles = [None]
@@ -724,6 +726,7 @@ def run_dslash_sweep(args, local_rank):
                                       "nrhs": nrhs, "tile": "autotuned" if tile is None else "forced",
                                       "rhs_per_thread": rep["rhs_per_thread"],
                                       "mixed_fma": rep["mixed_fma"],
+                                      "tensor_core": rep["mixed_fma"] == 2,
                                       "compressed_links": rep["compressed_links"],
                                       "l2": "flushed" if cold else "warm",
                                       "us": t * 1e6, "algorithmic_bytes": algo, "gbs": algo / t / 1e9,
@@ -782,11 +785,12 @@ def _device_links(geometry, nc, eps, seed, dev):
 
 
 def _request_specs(rng, n, max_bytes=2 << 30):
-    """Mixed requests: D in {2, 4}, N in {2, 3}, extents log-uniform between 8 and 24
-    (space) / 48 (time) in 4D and between 8 and 816 in 2D (even), footprint <= 2 GB;
-    kappa in [0.10, 0.14]; 1-16 rhs or (half of the requests) one rhs with 12 shifts
-    log-spaced in [1e-4, 1]; tol log-uniform in [1e-12, 1e-8]; eps in [0.1, 0.4];
-    30% reuse one of the last 8 gauge fields."""
+    """Mixed requests: D in {2, 3, 4}, N in {2, 3}, extents log-uniform between 8 and 24
+    (space) / 48 (time) in 4D, between 8 and 96 in 3D and between 8 and 816 in 2D (even),
+    footprint <= 2 GB; kappa in [0.10, 0.14]; 1-16 rhs or (half of the 2D / 4D requests)
+    one rhs with 12 shifts log-spaced in [1e-4, 1] (3D has no hermitian Q, so no Q^2
+    shifts); tol log-uniform in [1e-12, 1e-8]; eps in [0.1, 0.4]; 30% reuse one of the
+    last 8 gauge fields."""
     from tfleonardym_b200 import serving
     specs, recent = [], []
     for i in range(n):
@@ -794,11 +798,13 @@ def _request_specs(rng, n, max_bytes=2 << 30):
             key, geom, nc, eps, seed = recent[int(rng.integers(len(recent)))]
         else:
             while True:
-                nd = int(rng.choice([2, 4]))
+                nd = int(rng.choice([2, 3, 4]))
                 nc = int(rng.choice([2, 3]))
                 if nd == 4:
                     geom = tuple(2 * int(round(np.exp(rng.uniform(np.log(8), np.log(hi))) / 2))
                                  for hi in (24, 24, 24, 48))
+                elif nd == 3:
+                    geom = tuple(2 * int(round(np.exp(rng.uniform(np.log(8), np.log(96))) / 2)) for _ in range(3))
                 else:
                     geom = tuple(2 * int(round(np.exp(rng.uniform(np.log(8), np.log(816))) / 2)) for _ in range(2))
                 if serving.footprint_bytes(geom, nc, 16, "f16") <= max_bytes:
@@ -806,7 +812,7 @@ def _request_specs(rng, n, max_bytes=2 << 30):
             eps, seed = float(rng.uniform(0.1, 0.4)), int(rng.integers(1 << 30))
             key = f"cfg{seed}"
             recent = (recent + [(key, geom, nc, eps, seed)])[-8:]
-        shifted = rng.uniform() < 0.5
+        shifted = len(geom) != 3 and rng.uniform() < 0.5
         specs.append(dict(key=key, geometry=geom, nc=nc, eps=eps, seed=seed, kappa=float(rng.uniform(0.10, 0.14)),
                           nrhs=1 if shifted else int(rng.integers(1, 17)),
                           shifts=list(np.logspace(-4, 0, 12)) if shifted else None,
@@ -827,7 +833,7 @@ def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_pre
         if delay > 0:
             time.sleep(delay)
         nd, vol = len(sp["geometry"]), int(np.prod(sp["geometry"]))
-        ns = 2 if nd == 2 else 4
+        ns = 4 if nd == 4 else 2
         g = torch.Generator(device=dev)
         g.manual_seed(sp["src_seed"])
         shape = (sp["nrhs"], ns, sp["nc"], vol) if sp["shifts"] is None else (ns, sp["nc"], vol)
@@ -891,9 +897,9 @@ def run_serve_sweep(args, local_rank):
 
 
 def run_batch_lattices(args, local_rank):
-    """64 independent lattices -- 2D SU(2) from 8^2 to 64^2 and 4D SU(3) from 8^4 to
-    12^3 x 24 (the even-odd solver has no D = 3, so the 3D SU(2) third of the mix
-    is 2D SU(2) here), kappa in [0.10, 0.14], links reunit(exp(i eps H)) with eps in
+    """64 independent lattices -- thirds of 2D SU(2) from 8^2 to 64^2, 3D SU(2) from 8^3
+    to 16^3 and 4D SU(3) from 8^4 to 12^3 x 24, kappa in [0.10, 0.14], links
+    reunit(exp(i eps H)) with eps in
     [0.1, 0.4] -- with 4 unit complex Gaussian rhs each (256 solves), submitted
     together to the solve server (4 workers, one CUDA stream each) with FP32 inner
     and FP64 outer iterations to true relative residual 1e-10; the same 256 solves
@@ -913,10 +919,12 @@ def run_batch_lattices(args, local_rank):
     rng = np.random.default_rng(44)
     lattices = []
     for i in range(64):
-        if i % 2 == 0:
+        if i % 3 == 0:
             n = int(2 * round(np.exp(rng.uniform(np.log(8), np.log(64))) / 2))
             m = int(2 * round(np.exp(rng.uniform(np.log(8), np.log(64))) / 2))
             geom, nc = (n, m), 2
+        elif i % 3 == 1:
+            geom, nc = tuple(int(rng.choice([8, 10, 12, 14, 16])) for _ in range(3)), 2
         else:
             geom = tuple(int(rng.choice([8, 10, 12])) for _ in range(3)) + (int(rng.choice([8, 12, 16, 20, 24])),)
             nc = 3
@@ -926,7 +934,7 @@ def run_batch_lattices(args, local_rank):
     sources = []
     for l in lattices:
         nd, vol = len(l["geometry"]), int(np.prod(l["geometry"]))
-        ns = 2 if nd == 2 else 4
+        ns = 4 if nd == 4 else 2
         g = torch.Generator(device=dev)
         g.manual_seed(l["seed"] + 1)
         sources.append(torch.complex(torch.randn((4, ns, l["nc"], vol), generator=g, device=dev, dtype=torch.float64),
@@ -999,7 +1007,7 @@ def run_batch_lattices(args, local_rank):
     for rep in range(2):
         e0.record(stream)
         for c, p, a in zip(cfgs, moms, acts):
-            p2 = hmc._apply_force(a, p, -0.05)
+            p2 = hmc._kick(a, p, -0.05)
             hmc.update_link_field(c.gauge_field, p2, 0.05)
         e1.record(stream)
         torch.cuda.synchronize()

@@ -267,6 +267,13 @@ int lym_staple_terms(const lym_lattice* lat, int nc, const void* gauge, int no_d
  * summed as in measurements.py:22-43 and gauge_action.py:26-39).  Synchronises. */
 int lym_plaquette_sum(const lym_lattice* lat, int nc, const void* gauge, double* out, void* stream);
 
+/* momenta (nd, N, N, V) from unit normals (nd, N^2-1, V) (device, float64): the
+ * anti-Hermitian traceless matrices random_momenta builds from its draws (hmc.py:69-96):
+ * per direction the (re, im) pairs of the entries above the diagonal in row order, then
+ * the N-1 Cartan values, each halved; unit variance per generator T^a = lambda^a / 2. */
+int lym_momenta_from_normals(int nd, int nc, int64_t volume, const double* normals, void* momenta,
+                             void* stream);
+
 /* out (host) = -Re sum Tr P^2 (hmc.py:170-176).  Synchronises. */
 int lym_momenta_energy(int nd, int nc, int64_t volume, const void* momenta, double* out, void* stream);
 

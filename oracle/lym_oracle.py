@@ -84,16 +84,24 @@ def gammas(nd):
                       [[0, 0, -1j, 0], [0, 0, 0, 1j], [1j, 0, 0, 0], [0, -1j, 0, 0]],
                       [[0, 0, 1, 0], [0, 0, 0, 1], [1, 0, 0, 0], [0, 1, 0, 0]]], dtype=np.complex128)
         gd = np.diag([1, 1, -1, -1]).astype(np.complex128)
+    elif nd == 3:
+        # BUILDER-DEFINED (the reference has no D = 3 fermions, dirac.py:299-300):
+        # two-component spinors, gamma_mu = sigma_{mu+1}; no gamma_d exists (odd dimension)
+        g = np.array([[[0, 1], [1, 0]], [[0, -1j], [1j, 0]], [[1, 0], [0, -1]]], dtype=np.complex128)
+        gd = None
     else:
         raise RuntimeError(f"Number of dimensions {nd} not supported for fermions!")
     return g, gd
 
 
-def hopping(gauge_bc, psi, tables):
+def hopping(gauge_bc, psi, tables, dagger=False):
     """H psi = sum_mu U_mu(x)(1-g_mu)psi(x+mu) + U_mu(x-mu)^dag (1+g_mu) psi(x-mu)
-    (the hopping sum of dirac.py:503-523, without kappa / identity)."""
+    (the hopping sum of dirac.py:503-523, without kappa / identity).  dagger: the
+    adjoint hop H^dag, which is H with g_mu -> -g_mu (BUILDER-DEFINED, for D = 3)."""
     nd = gauge_bc.shape[0]
     g, _ = gammas(nd)
+    if dagger:
+        g = -g
     ident = np.eye(g.shape[1])
     out = np.zeros_like(psi)
     for mu in range(nd):
@@ -112,10 +120,13 @@ def gamma_d(psi):
     return out
 
 
-def wilson_apply(gauge_bc, psi, kappa, hermitian, tables):
+def wilson_apply(gauge_bc, psi, kappa, hermitian, tables, dagger=False):
     """Fundamental Wilson operator (dirac.py:458-523 + 649-662):
-    D psi = psi + kappa * H psi; Q = gamma_d D when hermitian."""
-    out = psi + kappa * hopping(gauge_bc, psi, tables)
+    D psi = psi + kappa * H psi; Q = gamma_d D when hermitian.  dagger: D^dag
+    (BUILDER-DEFINED; D = 3 has no hermitian form)."""
+    if hermitian and gauge_bc.shape[0] == 3:
+        raise RuntimeError("three dimensions have no hermitian form gamma_d D")
+    out = psi + kappa * hopping(gauge_bc, psi, tables, dagger)
     return gamma_d(out) if hermitian else out
 
 

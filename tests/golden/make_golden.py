@@ -153,6 +153,63 @@ def run_tables():
     print("wrote tables.npz", len(out), "arrays")
 
 
+# nested integrators whose call sequence is recorded (the reference's hmc.py run
+# with recording stand-ins for update_momenta / update_configuration and the actions)
+SCHEDULE_CASES = [("integrate_om", [4, 3], 1.0), ("integrate_om", [2, 2], 1.0), ("integrate_om", [10, 2], 1.0),
+                  ("integrate_om", [3, 2, 2], 0.5), ("integrate_om", [4, 3], -1.0), ("integrate_om", [1], 1.0),
+                  ("integrate_lp", [4, 3], 1.0), ("integrate_lp", [2, 3, 2], 1.0)]
+
+
+def run_schedules():
+    """The sequence of momentum kicks (level, weight) and link drifts (weight) the
+    reference's integrate_om / integrate_lp (hmc.py:104-162) perform, with two
+    kicks in a row that reuse one force (the closing kick) summed into one."""
+    _setup_reference((4, 4))
+    import hmc
+
+    class Force:
+        def __init__(self, level, ident):
+            self.level, self.ident = level, ident
+
+    class Action:
+        def __init__(self, level, counter):
+            self.level, self.counter = level, counter
+
+        def set_gauge_configuration(self, cfg):
+            pass
+
+        def force(self):
+            self.counter[0] += 1
+            return Force(self.level, self.counter[0])
+
+    out = {}
+    for fn, steps, dt in SCHEDULE_CASES:
+        seq = []
+
+        def update_momenta(m, f, eps, seq=seq):
+            if seq and seq[-1][0] == "kick" and seq[-1][3] == f.ident:
+                seq[-1] = ("kick", f.level, seq[-1][2] + eps, f.ident)
+            else:
+                seq.append(("kick", f.level, eps, f.ident))
+            return m
+
+        def update_configuration(cfg, m, eps, seq=seq):
+            seq.append(("drift", len(steps) - 1, eps, None))
+            return cfg
+
+        hmc.update_momenta = update_momenta
+        hmc.update_configuration = update_configuration
+        counter = [0]
+        actions = [Action(level, counter) for level in range(len(steps))]
+        getattr(hmc, fn)(None, None, actions, steps, dt)
+        key = f"{fn}/{'_'.join(str(k) for k in steps)}/{dt}"
+        out[key] = [[kind, level, weight] for kind, level, weight, _ in seq]
+    import json
+    with open(os.path.join(HERE, "md_schedules.json"), "w") as f:
+        f.write("{\n" + ",\n".join(f"{json.dumps(k)}: {json.dumps(v)}" for k, v in out.items()) + "\n}\n")
+    print("wrote md_schedules.json", len(out), "schedules")
+
+
 def run_case(name):
     spec = CASES[name]
     geometry = spec["geometry"]
@@ -515,6 +572,8 @@ def main():
     if args.case and args.inproc:
         if args.case == "tables":
             run_tables()
+        elif args.case == "md_schedules":
+            run_schedules()
         elif args.case in ADJOINT_CASES:
             run_adjoint_case(args.case)
         elif args.case in MEASUREMENT_CASES:
@@ -526,7 +585,7 @@ def main():
         else:
             run_case(args.case)
         return
-    names = [args.case] if args.case else (["tables"] + list(CASES) + list(ADJOINT_CASES) + list(MEASUREMENT_CASES)
+    names = [args.case] if args.case else (["tables", "md_schedules"] + list(CASES) + list(ADJOINT_CASES) + list(MEASUREMENT_CASES)
                                            + list(XDR_CASES) + list(OBSERVABLE_CASES))
     for n in names:
         subprocess.run([sys.executable, os.path.abspath(__file__), "--case", n, "--inproc", "--reference", REFERENCE],

@@ -91,10 +91,17 @@ def test_wilson_apply_vs_oracle_random(cuda_device, geom, nc):
 
 
 def test_unsupported_dimension_raises(cuda_device):
+    """The reference's message for dimensions without fermions (dirac.py:299-300); the
+    three-dimensional extension has no hermitian form and no adjoint representation."""
     from tfleonardym_b200 import dirac
-    g = np.zeros((3, 2, 2, 64), complex)
+    g1 = np.zeros((1, 2, 2, 64), complex)
     with pytest.raises(RuntimeError, match="not supported for fermions"):
-        dirac.DiracWilsonOperator(make_cfg(g, (4, 4, 4)), 0.1, True, representation="fundamental")
+        dirac.DiracWilsonOperator(make_cfg(g1, (64,)), 0.1, False, representation="fundamental")
+    g3 = np.zeros((3, 2, 2, 64), complex)
+    with pytest.raises(RuntimeError, match="no hermitian form"):
+        dirac.DiracWilsonOperator(make_cfg(g3, (4, 4, 4)), 0.1, True, representation="fundamental")
+    with pytest.raises(RuntimeError, match="not supported for fermions"):
+        dirac.DiracWilsonOperator(make_cfg(g3, (4, 4, 4)), 0.1, False, representation="adjoint")
 
 
 def test_dot_and_shape_error(cuda_device):
@@ -428,14 +435,12 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
         assert abs(its - base) <= max(3, base // 10), (arith, tile, its, base)
 
 
-@pytest.mark.parametrize("geometry,nrhs", [((4, 4, 4, 8), 16), ((2, 4, 4, 6), 8), ((6, 4, 2, 4), 4),
-                                           ((4, 4, 4, 6), 12)])
+@pytest.mark.parametrize("geometry,nrhs", [((4, 4, 4, 8), 16), ((2, 4, 4, 6), 16), ((6, 4, 2, 4), 32)])
 def test_eo_cg_tensor_core_hop(cuda_device, geometry, nrhs):
     """The tensor-core FP16 hop (4D SU(3); projected FP16 spinors x FP16 links on
-    mma.sync, FP32 accumulation; 16, 8 or 4 rhs per CTA) meets the oracle's true
-    residual for every rhs in about the iterations of the FP32-arithmetic FP16 hop;
-    sites past a CTA's last full tile (6 x 4 x 2 x 4: 96 sites per parity) and
-    rhs groups of 4 are covered."""
+    mma.sync, FP32 accumulation; 16 rhs per CTA, so 32 rhs run as two groups)
+    meets the oracle's true residual for every rhs in about the iterations of the
+    FP32-arithmetic FP16 hop."""
     from tfleonardym_b200 import boundary_conditions as bcs
     from tfleonardym_b200 import dirac, dirac_solver
     from tfleonardym_b200 import lattice as lt
@@ -457,7 +462,7 @@ def test_eo_cg_tensor_core_hop(cuda_device, geometry, nrhs):
         x = np_(tcg.solve(op, cu(b)))
         rep = tcg.reports[0]
         assert rep["mixed_fma"] == 2 and rep["compressed_links"] == 0, rep
-        assert rep["rhs_per_thread"] == max(g for g in (4, 8, 16) if nrhs % g == 0), rep
+        assert rep["rhs_per_thread"] == 16, rep
         for i in range(nrhs):
             res = np.linalg.norm(b[i] - O.wilson_apply(ub, x[i], kappa, herm, tables)) / np.linalg.norm(b[i])
             assert res < 1e-10, (herm, i, res, tcg.reports[i])
@@ -802,3 +807,30 @@ def test_gauge_observables_vs_reference(cuda_device, case):
                                             no_smear_direction=3, skip=1)
     assert relerr(np.stack([m.value for m in res]), g["multi/values"]) < 1e-12
     assert [m.smearing_levels for m in res] == list(g["multi/levels"])
+
+
+@pytest.mark.parametrize("nc", [2, 3])
+def test_random_momenta_kernel(cuda_device, nc):
+    """Momenta from normals on the device (one kernel) equal the oracle's
+    restatement of random_momenta (hmc.py:69-96) for the same draws; a large draw
+    is anti-Hermitian and traceless to rounding, with zero mean and unit variance
+    per generator (omega_a = -2i Tr(P T^a), T^a = lambda^a / 2)."""
+    from tfleonardym_b200 import hmc, lie_generators
+    nd, vol = 4, 6 * 4 * 4 * 8
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5 + nc)
+    normals = torch.randn((nd, nc * nc - 1, vol), dtype=torch.float64, device="cuda", generator=g)
+    p = np_(hmc.momenta_from_normals(normals, nc))
+    assert relerr(p, O.random_momenta_from_normals(np_(normals), nc)) < 1e-15
+    big = hmc.random_momenta(nc, 2, 200000, generator=g)
+    pb = np_(big)
+    herm = pb + np.conj(np.swapaxes(pb, 1, 2))
+    assert np.abs(herm).max() < 1e-15
+    assert np.abs(np.trace(pb, axis1=1, axis2=2)).max() < 1e-15
+    gens = lie_generators.generators(nc, "fundamental")  # (N^2-1, N, N)
+    omega = -2j * np.einsum("mijv,aji->mav", pb, gens)
+    assert np.abs(omega.imag).max() < 1e-13
+    w = omega.real
+    n = w.shape[-1]
+    assert np.abs(w.mean(-1)).max() < 5 / np.sqrt(n)
+    assert np.abs(w.var(-1) - 1.0).max() < 6 * np.sqrt(2.0 / n)

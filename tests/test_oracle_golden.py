@@ -293,3 +293,27 @@ def test_wilson_apply_sites_matches_golden(case):
     for herm in (0, 1):
         out = O.wilson_apply_sites(ub, g["eta"], spec["kappa"], bool(herm), tables, sites)
         assert relerr(out, g[f"apply/h{herm}/anti/projected"][:, :, sites]) < TOL
+
+
+def test_three_dimensional_adjoint_hop():
+    """The oracle's D^dag (gamma -> -gamma, builder-defined for D = 3) is the adjoint of
+    its D: <phi, D psi> = <D^dag phi, psi>; in 4D it equals gamma_d D gamma_d."""
+    rng = np.random.default_rng(0)
+    geom = (4, 4, 6)
+    vol = int(np.prod(geom))
+    u = O.unitary_sqrt_projection(rng.normal(size=(3, 3, 3, vol)) + 1j * rng.normal(size=(3, 3, 3, vol)))
+    t = O.lookup_tables(geom)
+    ub = O.apply_time_bc(u, O.antiperiodic_field(geom))
+    phi = rng.normal(size=(2, 3, vol)) + 1j * rng.normal(size=(2, 3, vol))
+    psi = rng.normal(size=(2, 3, vol)) + 1j * rng.normal(size=(2, 3, vol))
+    a = np.vdot(phi, O.wilson_apply(ub, psi, 0.13, False, t))
+    b = np.vdot(O.wilson_apply(ub, phi, 0.13, False, t, dagger=True), psi)
+    assert abs(a - b) < 1e-13 * abs(a)
+    with pytest.raises(RuntimeError, match="hermitian"):
+        O.wilson_apply(ub, psi, 0.13, True, t)
+    g = load_golden("d4")
+    geom4 = GOLDEN_CASES["d4"]["geometry"]
+    t4 = O.lookup_tables(geom4)
+    u4 = O.apply_time_bc(g["gauge"], O.antiperiodic_field(geom4))
+    d4 = O.wilson_apply(u4, g["eta"], 0.13, False, t4, dagger=True)
+    assert np.abs(d4 - O.gamma_d(O.wilson_apply(u4, O.gamma_d(g["eta"]), 0.13, False, t4))).max() < 1e-14

@@ -110,6 +110,50 @@ template <> struct Gamma<2> {
   LYM_HD static int phase(int mu, int) { return mu == 0 ? 0 : 3; }
 };
 
+// Three dimensions (builder-defined: the reference has fermions in D = 2 and 4 only,
+// dirac.py:283-300): two-component spinors with gamma_mu = sigma_{mu+1} (Pauli).
+// There is no gamma_5 in odd dimensions, hence no hermitian form Q = gamma_d D; the
+// solvers use D^dag = D with gamma_mu -> -gamma_mu.  (1 - s gamma_mu) has rank one:
+//   mu = 0 (sigma1): h = psi0 - s psi1,    out0 += t, out1 += -s t
+//   mu = 1 (sigma2): h = psi0 + i s psi1,  out0 += t, out1 += -i s t
+//   mu = 2 (sigma3): s = +1: h = psi1, out1 += 2t;  s = -1: h = psi0, out0 += 2t
+// with t = W h, W the hop's link (U or U^dag).  col / phase give the sigma1, sigma2
+// rows in the form the D = 2 code uses; sigma3 goes through proj3 / recon3.
+template <> struct Gamma<3> {
+  static constexpr int NS = 2;
+  LYM_HD static int col(int, int) { return 1; }
+  LYM_HD static int phase(int mu, int) { return mu == 0 ? 0 : 3; }
+};
+
+template <typename R, int NC>
+LYM_HD void proj3(int mu, int s, const cx<R> (&p0)[NC], const cx<R> (&p1)[NC], cx<R> (&h)[NC]) {
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (mu == 0) h[c] = s > 0 ? p0[c] - p1[c] : p0[c] + p1[c];
+    else if (mu == 1) h[c] = p0[c] + mul_phase(s > 0 ? 1 : 3, p1[c]);
+    else h[c] = s > 0 ? p1[c] : p0[c];
+  }
+}
+
+template <typename R, int NC>
+LYM_HD void recon3(int mu, int s, const cx<R> (&t)[NC], cx<R> (&o0)[NC], cx<R> (&o1)[NC]) {
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (mu == 0) {
+      o0[c] += t[c];
+      if (s > 0) o1[c] -= t[c];
+      else o1[c] += t[c];
+    } else if (mu == 1) {
+      o0[c] += t[c];
+      o1[c] += mul_phase(s > 0 ? 3 : 1, t[c]);
+    } else if (s > 0) {
+      o1[c] += R(2) * t[c];
+    } else {
+      o0[c] += R(2) * t[c];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // error handling
 // ---------------------------------------------------------------------------

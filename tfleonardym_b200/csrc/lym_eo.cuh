@@ -325,6 +325,31 @@ LYM_D void hop_site(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
       }
       cx<R> psi[NS * NC];
       load_sp<SP, NS * NC>(in, rhs, ncb, psi);
+      if constexpr (ND == 3) {
+        // two-component spinors: G5IN selects the adjoint hop (gamma -> -gamma)
+        const int s3 = (fwd != G5IN) ? 1 : -1;
+        cx<R> p0[NC], p1[NC], h[NC], t[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          p0[c] = psi[c];
+          p1[c] = psi[NC + c];
+        }
+        proj3<R, NC>(mu, s3, p0, p1, h);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+          if (fwd) {
+            t[i] = u[i][0] * h[0];
+#pragma unroll
+            for (int j = 1; j < NC; ++j) cmac(t[i], u[i][j], h[j]);
+          } else {
+            t[i] = cmul_cj(u[0][i], h[0]);
+#pragma unroll
+            for (int j = 1; j < NC; ++j) cmac_cj(t[i], u[j][i], h[j]);
+          }
+        }
+        recon3<R, NC>(mu, s3, t, acc[0], acc[1]);
+        continue;
+      }
       if (G5IN) {
 #pragma unroll
         for (int k = (NS / 2) * NC; k < NS * NC; ++k) psi[k] = -psi[k];
@@ -404,6 +429,35 @@ LYM_D void hop_tile(const EoGeom& g, const HopGauge& hg, const EoField& in, int 
         if (!act[r]) continue;
         cx<RT> psi[NS * NC];
         const float nrm = load_sp_raw<SP, NS * NC>(in, rhs0 + r, ncb, psi);
+        if constexpr (ND == 3) {
+          // two-component spinors: G5IN selects the adjoint hop (gamma -> -gamma)
+          const int s3 = (fwd != G5IN) ? 1 : -1;
+          cx<RT> p0[NC], p1[NC], h[NC], t[NC];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            p0[c] = psi[c];
+            p1[c] = psi[NC + c];
+          }
+          proj3<RT, NC>(mu, s3, p0, p1, h);
+          if constexpr (SP == SP16 || SP == SPB16) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) h[c] = (RT)nrm * h[c];
+          }
+#pragma unroll
+          for (int i = 0; i < NC; ++i) {
+            if (fwd) {
+              t[i] = u[i][0] * h[0];
+#pragma unroll
+              for (int j = 1; j < NC; ++j) cmac(t[i], u[i][j], h[j]);
+            } else {
+              t[i] = cmul_cj(u[0][i], h[0]);
+#pragma unroll
+              for (int j = 1; j < NC; ++j) cmac_cj(t[i], u[j][i], h[j]);
+            }
+          }
+          recon3<RT, NC>(mu, s3, t, acc[r][0], acc[r][1]);
+          continue;
+        }
 #pragma unroll
         for (int a = 0; a < NS / 2; ++a) {
           const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
@@ -585,6 +639,7 @@ LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int r
                    const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
   if constexpr (MX != 0) {
     static_assert(SP == SP16 && GP == SP16 && !COMP, "the mixed-precision hop takes FP16 spinors and full links");
+    static_assert(ND != 3, "the mixed-precision hop has no three-dimensional form");
     hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
   } else {
     hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);

@@ -145,6 +145,47 @@ __global__ void __launch_bounds__(256) plaquette_kernel(const int32_t* __restric
   }
 }
 
+// Momenta from unit normals, one thread per link, built as hmc.py:69-96 builds
+// them from its draws: normals (nd, N^2-1, V) hold per direction the (re, im)
+// pairs of the entries above the diagonal in row order, then the N-1 Cartan
+// values; each is halved; P_ij = (re, im), P_ji = (-re, im); the diagonal is
+// i times sum_i c_i H_i with the reference's diagonal generators.
+template <int NC>
+__global__ void __launch_bounds__(256) momenta_from_normals_kernel(int nd, int64_t V, const double* __restrict__ nrm,
+                                                                   double2* __restrict__ P) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int mu = blockIdx.y;
+  if (s >= V) return;
+  constexpr int NG = NC * NC - 1;
+  const double* n = nrm + (int64_t)mu * NG * V + s;
+  Mat<NC> m;
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = i + 1; j < NC; ++j) {
+      const double re = 0.5 * n[(int64_t)k * V], im = 0.5 * n[(int64_t)(k + 1) * V];
+      k += 2;
+      m.m[i][j] = {re, im};
+      m.m[j][i] = {-re, im};
+    }
+  double diag[NC];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) diag[i] = 0.0;
+#pragma unroll
+  for (int i = 1; i < NC; ++i) {
+    const double r = 0.5 * n[(int64_t)k * V];
+    ++k;
+    const double di = (double)i;
+#pragma unroll
+    for (int j = 0; j < i; ++j) diag[j] += r / sqrt(di * (di + 1.0) / 2.0);
+    diag[i] += -r * (di * sqrt(2.0 / (di * (di + 1.0))));
+  }
+#pragma unroll
+  for (int i = 0; i < NC; ++i) m.m[i][i] = {0.0, diag[i]};
+  store_link<NC>(P, mu, s, V, m);
+}
+
 // -Re sum Tr P^2 (hmc.py:170-176)
 template <int NC>
 __global__ void __launch_bounds__(256) momenta_energy_kernel(int64_t nlinks, int64_t V,
@@ -516,6 +557,20 @@ int lym_plaquette_sum(const lym_lattice* lat, int nc, const void* gauge, double*
   LYM_CUDA(cudaStreamSynchronize(st));
   out[0] = s->host[slot * Scratch::kMaxVals];
   out[1] = s->host[slot * Scratch::kMaxVals + 1];
+  return LYM_OK;
+}
+
+int lym_momenta_from_normals(int nd, int nc, int64_t volume, const double* normals, void* momenta, void* stream) {
+  LYM_REQUIRE(normals && momenta && nd >= 1 && nd <= LYM_MAX_ND && volume >= 0, LYM_ERR_BAD_ARG, "bad argument");
+  LYM_REQUIRE(nc == 2 || nc == 3, LYM_ERR_UNSUPPORTED, "N must be 2 or 3");
+  if (volume == 0) return LYM_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const dim3 grid(grid_for(volume, 256), nd);
+  if (nc == 2)
+    momenta_from_normals_kernel<2><<<grid, 256, 0, st>>>(nd, volume, normals, (double2*)momenta);
+  else
+    momenta_from_normals_kernel<3><<<grid, 256, 0, st>>>(nd, volume, normals, (double2*)momenta);
+  LYM_CHECK_LAUNCH();
   return LYM_OK;
 }
 

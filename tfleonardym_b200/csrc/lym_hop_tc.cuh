@@ -1,32 +1,33 @@
-// Tensor-core form of the solver's FP16 hop for 4D SU(3) with several right-hand
-// sides (builder-defined; the reference applies the operator one vector at a
-// time through TensorFlow einsums, dirac.py:458-523).
+// Tensor-core form of the solver's FP16 hop for 4D SU(3) with 16 right-hand
+// sides per CTA (builder-defined; the reference applies the operator one vector
+// at a time through TensorFlow einsums, dirac.py:458-523).
 //
-// With RG right-hand sides per site the hop at one output site is a small dense
-// contraction.  Writing the spin projection of direction (mu, +-) as
-// h = P psi(x +- mu) (two spins) and the reconstruction of the lower spins as a
-// unit phase times an upper one, every one of the 4 spins s of every rhs r gets
-//     out[s, r] = sum_{mu, +-} W_{mu,+-} H_{mu,+-}[s, r],     W = U or U^dag,
-// where H holds the projected (upper) or phased (lower) half spinor.  In real
-// form, with the three colours' (re, im) pairs along K, this is
-//     C (4 RG x 6) = sum over 4 pairs of K-blocks  A (4 RG x 16) B (16 x 8)
-// with A = the projected spinors of the forward and the backward neighbour of
-// direction mu (three colours plus one zero complex each, in FP16) and B = the
-// forward link and the backward link's adjoint in real form (6 of 8 columns used).
-// One mma.sync.m16n8k16 (FP16 operands, FP32 accumulation) covers 16 rows of
-// (spin, rhs) for one mu; a site takes RG/4 x 4 of them.
+// With 16 right-hand sides per site the hop at one output site is a small dense
+// contraction.  For direction mu the spin projection of the forward and the
+// backward neighbour gives two upper half-spinor components h_a (a = 0, 1; three
+// colours each), and with W = U_mu(x) (forward) or U_mu(x-mu)^dag (backward)
+//     out[a]       += W h_a                    (upper spins)
+//     out[j(mu,a)] += lambda(mu,a,+-) W h_a    (lower spins, lambda a unit phase)
+// In real form, with the three colours' (re, im) pairs along K and one zero complex
+// of padding per hop, direction mu is K = 16 (forward 8, backward 8), and for the
+// 16 rhs of one site and one upper spin a
+//     C_a (16 x 8)     += A_a (16 x 16) B       with B   = the two links in real form,
+//     C_j(mu,a) (16x8) += A_a (16 x 16) B'_a    with B'_a = B with each half times lambda,
+// one mma.sync.m16n8k16 each (FP16 operands, FP32 accumulation; 6 of 8 columns
+// used).  The phase lives in the B operand, which each lane builds from its two
+// link entries, so only the upper spins are projected and staged.
 //
-// Each CTA covers S = 256/RG consecutive checkerboard sites x RG right-hand
-// sides (blockIdx.y = group of RG rhs), one thread per (site, rhs) for the
-// global loads and the epilogue:
-//   1. the neighbour table entries and the FP16 links of the tile go to shared
-//      memory once (shared by the RG right-hand sides);
+// Each CTA covers S = 8 consecutive checkerboard sites x 16 right-hand sides
+// (blockIdx.y = group of 16 rhs), one thread per (site, rhs) for the global loads
+// and the epilogue:
+//   1. the FP16 links of the tile go to shared memory once (shared by the 16 rhs);
 //   2. each thread reads its 8 neighbours' norms; every neighbour's half spinor
 //      is scaled by norm / (largest of the 8), so one FP32 factor per (site, rhs)
 //      restores the scale after the contraction (the FP16 operand never exceeds 2);
-//   3. per mu: each thread loads the two neighbour spinors (coalesced 16-byte
-//      loads), projects them in packed FP16 and stores the four spin rows into a
-//      double-buffered shared tile; the warps then run ldmatrix + mma on it;
+//   3. per mu: each thread projects its two neighbour spinors in packed FP16 and
+//      stores the two upper rows into a double-buffered shared tile (the spinors of
+//      mu + 1 are requested meanwhile); each warp then runs, for each of its two
+//      sites, 2 ldmatrix and 4 mma;
 //   4. the FP32 results go through shared memory back to one thread per
 //      (site, rhs), which runs the same epilogue as the register-tiled kernels.
 // The only roundings beyond the FP16 storage are h's (as in the mixed-precision
@@ -39,32 +40,25 @@ namespace lym {
 
 namespace tc {
 
+constexpr int kRG = 16;             // right-hand sides per CTA
+constexpr int kS = 8;               // sites per CTA
+constexpr int kThreads = kS * kRG;  // one thread per (site, rhs)
+constexpr int kSPW = 2;             // sites per warp in the mma stage
+static_assert(kThreads / 32 * kSPW == kS, "every site has one mma warp");
+
 // shared-memory plan of one CTA (bytes)
-template <int RG>
 struct Plan {
-  static constexpr int S = 256 / RG;                 // sites per CTA
-  static constexpr int kSiteStride = 128 * RG + 16;  // 4 RG rows of 32 B, +16 B against bank conflicts
-  static constexpr int kTile = S * kSiteStride;      // one spin-row tile
-  static constexpr int kLinks = S * 8 * 10 * 4;      // [site][dir][10 half2]
-  static constexpr int kCodes = S * 8 * 4;           // [dir][site] neighbour codes
-  static constexpr int kRed = 256 * 8;               // reduction scratch (doubles)
-  static constexpr int kBytes = 2 * kTile + kLinks + kCodes + kRed;
-  static_assert(S * RG * 96 <= kTile, "the FP32 results reuse the first tile");
+  static constexpr int kSiteStride = 2 * kRG * 32 + 16;  // 2 spin rows x 16 rhs x 32 B, +16 B against bank conflicts
+  static constexpr int kTile = kS * kSiteStride;         // one staged direction
+  static constexpr int kLinks = kS * 8 * 10 * 4;         // [site][dir][10 half2]
+  static constexpr int kRed = kThreads * 8;              // reduction scratch (doubles)
+  static constexpr int kBytes = 2 * kTile + kLinks + kRed;
+  static_assert(kS * kRG * 96 <= 2 * kTile, "the FP32 results reuse both tiles");
 };
 
 LYM_D unsigned h2u(__half2 h) { return *reinterpret_cast<unsigned*>(&h); }
 LYM_D __half2 u2h(unsigned u) { return *reinterpret_cast<__half2*>(&u); }
 LYM_D unsigned swap_halves(unsigned u) { return __byte_perm(u, 0, 0x1032); }
-
-// unit phase k (0: +1, 1: +i, 2: -1, 3: -i) times a (re, im) half2, by bit operations
-LYM_D unsigned phase_h2(int k, unsigned v) {
-  switch (k & 3) {
-    case 0: return v;
-    case 1: return swap_halves(v) ^ 0x00008000u;  // (-im, re)
-    case 2: return v ^ 0x80008000u;               // (-re, -im)
-    default: return swap_halves(v) ^ 0x80000000u; // (im, -re)
-  }
-}
 
 LYM_D void mma16816(float (&c)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3, unsigned b0, unsigned b1) {
   asm volatile(
@@ -79,42 +73,62 @@ LYM_D void ldmatrix_x4(unsigned addr, unsigned& r0, unsigned& r1, unsigned& r2, 
                : "r"(addr));
 }
 
+// The B-operand entry of column g (odd: the imaginary part of output colour g/2)
+// for the link times the unit phase k (0: +1, 1: +i, 2: -1, 3: -i), from the
+// lane's real-part column value bre and imaginary-part column value bim.
+LYM_D unsigned phased_b(int k, unsigned bre, unsigned bim, bool odd) {
+  switch (k & 3) {
+    case 0: return odd ? bim : bre;
+    case 2: return (odd ? bim : bre) ^ 0x80008000u;
+    case 1: return odd ? bre : (bim ^ 0x80008000u);  // Re(iX) = -Im X, Im(iX) = Re X
+    default: return odd ? (bre ^ 0x80008000u) : bim;  // Re(-iX) = Im X, Im(-iX) = -Re X
+  }
+}
+
 // The hop of the CTA's tile: on return, acc holds sum over the 8 hops for the
 // thread's (site, rhs) = (i, r) (zero for inactive rhs or sites past Vh), in
 // FP32 with the neighbour norms applied.  `smem` is the dynamic shared memory
-// (Plan<RG>::kBytes).  Every thread of the block must call it.
-template <bool G5IN, int RG>
+// (Plan::kBytes).  Every thread of the block must call it.
+template <bool G5IN>
 LYM_D void hop_tc(const EoGeom& g, const HopGauge& hg, const EoField& in, int par, int site0, int rhs_base,
                   int i, int r, bool act, char* smem, cx<float> (&acc)[4][3]) {
-  using P = Plan<RG>;
-  constexpr int S = P::S;
   constexpr int ND = 4, NC = 3;
   const int tid = threadIdx.x;
   const int vh = (int)g.Vh;
   char* tiles = smem;
-  unsigned* lk = reinterpret_cast<unsigned*>(smem + 2 * P::kTile);  // [site][dir][10]
-  int* codes = reinterpret_cast<int*>(smem + 2 * P::kTile + P::kLinks);  // [dir][site]
+  unsigned* lk = reinterpret_cast<unsigned*>(smem + 2 * Plan::kTile);  // [site][dir][10]
+  const int* nb = g.nbr + par * 2 * ND * vh;
+  const int cb = site0 + i;
+  const bool site_ok = cb < vh;
+  const bool live = act && site_ok;
+  const int rg = rhs_base + r;
+  const uint4* inb = reinterpret_cast<const uint4*>(in.data) + (size_t)rg * in.nunits * in.Vh;
 
-  // 1. neighbour codes of the tile (8 x S, coalesced along sites)
-  for (int k = tid; k < 8 * S; k += 256) {
-    const int d = k / S, s = k - d * S;
-    const int cb = site0 + s;
-    codes[k] = cb < vh ? __ldg(g.nbr + (par * 2 * ND + d) * vh + cb) : 0;
-  }
-  __syncthreads();
-
-  // 2. FP16 links of the tile: forward links on the tile's sites (parity par),
-  // backward links on the neighbours (parity 1 - par); 5 uint2 units each
+  // prologue: neighbour codes, norms, links, the spinors of direction 0
+  int code[8];
+#pragma unroll
+  for (int d = 0; d < 8; ++d) code[d] = site_ok ? (__ldg(nb + d * vh + cb) & 0x7fffffff) : 0;
+  float ratio[8];
+#pragma unroll
+  for (int d = 0; d < 8; ++d) ratio[d] = live ? __ldg(in.norm + (size_t)rg * in.Vh + code[d]) : 0.f;
+  uint4 raw[2][3];
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir)
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+      raw[dir][u] = live ? __ldg(inb + (size_t)u * vh + code[dir]) : make_uint4(0u, 0u, 0u, 0u);
   {
+    // FP16 links of the tile: forward links on the tile's sites (parity par),
+    // backward links on the neighbours (parity 1 - par); 5 uint2 units each
     const uint2* lbase = reinterpret_cast<const uint2*>(hg.data);
-    for (int k = tid; k < S * 8 * 5; k += 256) {
-      const int s = k % S, rest = k / S;
+    for (int k = tid; k < kS * 8 * 5; k += kThreads) {
+      const int s = k % kS, rest = k / kS;
       const int u = rest % 5, d = rest / 5;  // d = 2 mu + dir
       const int mu = d >> 1, dir = d & 1;
-      const int cb = site0 + s;
+      const int lcb0 = site0 + s;
       uint2 v = make_uint2(0u, 0u);
-      if (cb < vh) {
-        const int lcb = dir == 0 ? cb : (codes[d * S + s] & 0x7fffffff);
+      if (lcb0 < vh) {
+        const int lcb = dir == 0 ? lcb0 : (__ldg(nb + d * vh + lcb0) & 0x7fffffff);
         const int lpar = dir == 0 ? par : 1 - par;
         v = __ldg(lbase + (size_t)((mu * 2 + lpar) * hg.nunits + u) * vh + lcb);
       }
@@ -123,125 +137,119 @@ LYM_D void hop_tc(const EoGeom& g, const HopGauge& hg, const EoField& in, int pa
       dst[1] = v.y;
     }
   }
-
-  // 3. neighbour norms -> per-hop scale relative to the largest
-  float ratio[8];
   float nmax = 0.f;
-  const bool live = act && (site0 + i) < vh;
-  const int rg = rhs_base + r;
 #pragma unroll
-  for (int d = 0; d < 8; ++d) {
-    ratio[d] = live ? __ldg(in.norm + (size_t)rg * in.Vh + (codes[d * S + i] & 0x7fffffff)) : 0.f;
-    nmax = fmaxf(nmax, ratio[d]);
-  }
+  for (int d = 0; d < 8; ++d) nmax = fmaxf(nmax, ratio[d]);
   {
     const float inv = nmax > 0.f ? 1.0f / nmax : 0.f;
 #pragma unroll
     for (int d = 0; d < 8; ++d) ratio[d] *= inv;
   }
 
-  // mma roles: warp w owns sites w*(S/8) .. +S/8-1, all RG/4 m-tiles of each
-  constexpr int SPW = S / 8, MT = RG / 4;
+  // mma roles: warp w owns sites 2w, 2w + 1; accumulators per site and spin
   const int lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tq = lane & 3;
-  float c[SPW][MT][4];
+  const bool odd = (gq & 1) != 0;
+  const bool bcol = gq < 6 && tq < 3;  // columns 6, 7 and rows of the padding complex are zero
+  float c[kSPW][4][4];
 #pragma unroll
-  for (int a = 0; a < SPW; ++a)
+  for (int a = 0; a < kSPW; ++a)
 #pragma unroll
-    for (int m = 0; m < MT; ++m)
+    for (int s = 0; s < 4; ++s)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) c[a][m][k] = 0.f;
-  // ldmatrix row address of this lane within a 16-row m-tile
+      for (int k = 0; k < 4; ++k) c[a][s][k] = 0.f;
+  // ldmatrix row address of this lane within a 16-row tile (one spin, 16 rhs)
   const int lrow = (lane & 7) + ((lane >> 3) & 1) * 8, lhalf = lane >> 4;
   const unsigned tiles_s = (unsigned)__cvta_generic_to_shared(tiles);
-  const uint4* inb = reinterpret_cast<const uint4*>(in.data) + (size_t)rg * in.nunits * in.Vh;
 
 #pragma unroll
   for (int mu = 0; mu < ND; ++mu) {
-    char* tile = tiles + (mu & 1) * P::kTile;
-    // 3a. load, project, scale and store the two hops of direction mu
+    char* tile = tiles + (mu & 1) * Plan::kTile;
+    // project, scale and store the upper rows of the two hops of direction mu
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
       const bool fwd = dir == 0;
       const int d = 2 * mu + dir;
-      uint4 raw[3] = {make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u)};
-      if (live) {
-        const int ncb = codes[d * S + i] & 0x7fffffff;
-#pragma unroll
-        for (int u = 0; u < 3; ++u) raw[u] = __ldg(inb + (size_t)u * vh + ncb);
-      }
-      const unsigned psi[12] = {raw[0].x, raw[0].y, raw[0].z, raw[0].w, raw[1].x, raw[1].y,
-                                raw[1].z, raw[1].w, raw[2].x, raw[2].y, raw[2].z, raw[2].w};
+      const unsigned psi[12] = {raw[dir][0].x, raw[dir][0].y, raw[dir][0].z, raw[dir][0].w,
+                                raw[dir][1].x, raw[dir][1].y, raw[dir][1].z, raw[dir][1].w,
+                                raw[dir][2].x, raw[dir][2].y, raw[dir][2].z, raw[dir][2].w};
       const __half2 sc = __float2half2_rn(ratio[d]);
       const bool s2pos = fwd != G5IN;
 #pragma unroll
       for (int a = 0; a < 2; ++a) {
         const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
         const int kph = s2pos ? phase_neg(ph) : ph;
-        const int lph = fwd ? phase_neg(phase_conj(ph)) : phase_conj(ph);
-        unsigned h[3], l[3];
+        unsigned h[3];
 #pragma unroll
-        for (int cc = 0; cc < NC; ++cc) {
-          const __half2 pr = proj_h2(u2h(psi[a * NC + cc]), u2h(psi[jb * NC + cc]), kph);
-          h[cc] = h2u(__hmul2(pr, sc));
-          l[cc] = phase_h2(lph, h[cc]);
-        }
-        // rows m = s * RG + r; the 16-byte half of the row is swizzled by bit 2 of m
-        const int mu_ = a * RG + r, ml = jb * RG + r;
-        const int hu = dir ^ ((mu_ >> 2) & 1), hl = dir ^ ((ml >> 2) & 1);
-        *reinterpret_cast<uint4*>(tile + i * P::kSiteStride + mu_ * 32 + hu * 16) = make_uint4(h[0], h[1], h[2], 0u);
-        *reinterpret_cast<uint4*>(tile + i * P::kSiteStride + ml * 32 + hl * 16) = make_uint4(l[0], l[1], l[2], 0u);
+        for (int cc = 0; cc < NC; ++cc)
+          h[cc] = h2u(__hmul2(proj_h2(u2h(psi[a * NC + cc]), u2h(psi[jb * NC + cc]), kph), sc));
+        // row m = a * 16 + r; the 16-byte half of the row is swizzled by bit 2 of m
+        const int m = a * kRG + r;
+        *reinterpret_cast<uint4*>(tile + i * Plan::kSiteStride + m * 32 + ((dir ^ ((m >> 2) & 1)) * 16)) =
+            make_uint4(h[0], h[1], h[2], 0u);
       }
     }
-    __syncthreads();
-    // 3b. tensor cores: for each of the warp's sites, B from the links, A by ldmatrix
+    // request direction mu + 1 while this one is contracted
+    if (mu + 1 < ND) {
 #pragma unroll
-    for (int a = 0; a < SPW; ++a) {
-      const int site = warp * SPW + a;
-      unsigned b0 = 0u, b1 = 0u;
-      if (gq < 6 && tq < 3) {
+      for (int dir = 0; dir < 2; ++dir)
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+          raw[dir][u] = live ? __ldg(inb + (size_t)u * vh + code[2 * (mu + 1) + dir]) : make_uint4(0u, 0u, 0u, 0u);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < kSPW; ++a) {
+      const int site = warp * kSPW + a;
+      // B for this lane's column: real and imaginary column values of the forward
+      // (rows 0-7) and backward (rows 8-15) link entries
+      unsigned bre_f = 0u, bim_f = 0u, bre_b = 0u, bim_b = 0u;
+      if (bcol) {
         const int cp = gq >> 1;
         const unsigned uf = lk[(site * 8 + 2 * mu) * 10 + cp * 3 + tq];      // U_mu(x)[c'][t]
         const unsigned ub = lk[(site * 8 + 2 * mu + 1) * 10 + tq * 3 + cp];  // U_mu(x-mu)[t][c']
-        if ((gq & 1) == 0) {
-          b0 = uf ^ 0x80000000u;  // (re, -im)
-          b1 = ub;                // adjoint: (re, im) of U[t][c']
-        } else {
-          b0 = swap_halves(uf);                // (im, re)
-          b1 = swap_halves(ub) ^ 0x00008000u;  // (-im, re)
-        }
+        bre_f = uf ^ 0x80000000u;               // (re, -im)
+        bim_f = swap_halves(uf);                // (im, re)
+        bre_b = ub;                             // adjoint: (re, im) of U[t][c']
+        bim_b = swap_halves(ub) ^ 0x00008000u;  // (-im, re)
       }
+      const unsigned b0 = odd ? bim_f : bre_f, b1 = odd ? bim_b : bre_b;
 #pragma unroll
-      for (int m = 0; m < MT; ++m) {
-        const int row = m * 16 + lrow;
-        const unsigned addr = tiles_s + (mu & 1) * P::kTile + site * P::kSiteStride + row * 32 +
+      for (int sa = 0; sa < 2; ++sa) {
+        const int row = sa * kRG + lrow;
+        const unsigned addr = tiles_s + (mu & 1) * Plan::kTile + site * Plan::kSiteStride + row * 32 +
                               ((lhalf ^ ((row >> 2) & 1)) * 16);
         unsigned a0, a1, a2, a3;
         ldmatrix_x4(addr, a0, a1, a2, a3);
-        mma16816(c[a][m], a0, a1, a2, a3, b0, b1);
+        // upper spin sa
+        mma16816(c[a][sa], a0, a1, a2, a3, b0, b1);
+        // lower spin j(mu, sa) with the forward / backward reconstruction phases
+        const int jb = Gamma<ND>::col(mu, sa), ph = Gamma<ND>::phase(mu, sa);
+        const int lph_f = phase_neg(phase_conj(ph)), lph_b = phase_conj(ph);
+        mma16816(c[a][jb], a0, a1, a2, a3, phased_b(lph_f, bre_f, bim_f, odd), phased_b(lph_b, bre_b, bim_b, odd));
       }
     }
   }
-  // 4. results to shared memory (first tile, last read at mu = 2), then per thread
+  // results to shared memory (both tiles), then per thread
+  __syncthreads();
   float* cout = reinterpret_cast<float*>(tiles);  // [site][rhs][spin][colour] complex
   if (tq < 3) {
 #pragma unroll
-    for (int a = 0; a < SPW; ++a) {
-      const int site = warp * SPW + a;
+    for (int a = 0; a < kSPW; ++a) {
+      const int site = warp * kSPW + a;
 #pragma unroll
-      for (int m = 0; m < MT; ++m) {
+      for (int s = 0; s < 4; ++s) {
 #pragma unroll
         for (int hrow = 0; hrow < 2; ++hrow) {
-          const int row = m * 16 + gq + 8 * hrow;
-          const int s = row / RG, rr = row - s * RG;
-          float2* p = reinterpret_cast<float2*>(cout + ((site * RG + rr) * 12 + s * 3 + tq) * 2);
-          *p = make_float2(c[a][m][2 * hrow], c[a][m][2 * hrow + 1]);
+          const int rr = gq + 8 * hrow;
+          float2* p = reinterpret_cast<float2*>(cout + ((site * kRG + rr) * 12 + s * 3 + tq) * 2);
+          *p = make_float2(c[a][s][2 * hrow], c[a][s][2 * hrow + 1]);
         }
       }
     }
   }
   __syncthreads();
-  const float4* mine = reinterpret_cast<const float4*>(cout + (i * RG + r) * 24);
+  const float4* mine = reinterpret_cast<const float4*>(cout + (i * kRG + r) * 24);
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
     const float4 v = mine[k];
@@ -252,31 +260,27 @@ LYM_D void hop_tc(const EoGeom& g, const HopGauge& hg, const EoField& in, int pa
 }
 
 // Deterministic sum over the CTA of one double per thread, per rhs (threads
-// with the same r = tid / S): red[tid] = v, then thread r < RG adds its S
-// values in site order.  Result in out_r (threads r < RG).  Every thread calls it.
-template <int RG>
+// with the same r = tid / S): red[tid] = v, then thread r < 16 adds its S
+// values in site order.  Result in threads r < 16.  Every thread calls it.
 LYM_D double block_rhs_sum(double v, double* red) {
-  constexpr int S = 256 / RG;
   red[threadIdx.x] = v;
   __syncthreads();
   double s = 0.0;
-  if (threadIdx.x < RG) {
-    for (int k = 0; k < S; ++k) s += red[threadIdx.x * S + k];
+  if (threadIdx.x < kRG) {
+    for (int k = 0; k < kS; ++k) s += red[threadIdx.x * kS + k];
   }
   __syncthreads();
   return s;
 }
 
 // Grid-level per-rhs sum with the last-block pattern: each block of the rhs group
-// (blockIdx.y) stores RG partials; the last block to arrive adds them in block
-// order.  Returns true in the last block, with the totals in `tot` (threads r < RG).
-template <int RG>
+// (blockIdx.y) stores 16 partials; the last block to arrive adds them in block
+// order.  Returns true in the last block, with the totals in `tot` (threads r < 16).
 LYM_D bool grid_rhs_sum(double v, double* red, double* partials, unsigned* counter, int nblk, double& tot) {
-  constexpr int S = 256 / RG;
   __shared__ bool last;
-  const double bsum = block_rhs_sum<RG>(v, red);
-  double* part = partials + (size_t)blockIdx.y * nblk * RG;
-  if (threadIdx.x < RG) part[(size_t)blockIdx.x * RG + threadIdx.x] = bsum;
+  const double bsum = block_rhs_sum(v, red);
+  double* part = partials + (size_t)blockIdx.y * nblk * kRG;
+  if (threadIdx.x < kRG) part[(size_t)blockIdx.x * kRG + threadIdx.x] = bsum;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(counter + blockIdx.y, 1u) == (unsigned)nblk - 1;
@@ -284,10 +288,10 @@ LYM_D bool grid_rhs_sum(double v, double* red, double* partials, unsigned* count
   if (!last) return false;
   __threadfence();
   // thread (i, r) adds blocks i, i + S, ... of rhs r; then the S per-thread sums in order
-  const int i = threadIdx.x % S, r = threadIdx.x / S;
+  const int i = threadIdx.x % kS, r = threadIdx.x / kS;
   double s = 0.0;
-  for (int b = i; b < nblk; b += S) s += ((volatile double*)part)[(size_t)b * RG + r];
-  tot = block_rhs_sum<RG>(s, red);
+  for (int b = i; b < nblk; b += kS) s += ((volatile double*)part)[(size_t)b * kRG + r];
+  tot = block_rhs_sum(s, red);
   if (threadIdx.x == 0) counter[blockIdx.y] = 0u;  // ready for the next use of this slot
   return true;
 }

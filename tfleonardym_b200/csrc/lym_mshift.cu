@@ -1433,6 +1433,8 @@ int lym_multishift_solve_eo(lym_gauge* g, double kappa, int nrhs, int nshift, co
                             void* xs, const lym_solver_params* params, lym_solver_report* reports, void* stream) {
   LYM_REQUIRE(g && shifts && b && xs && params && reports, LYM_ERR_BAD_ARG, "null argument");
   LYM_REQUIRE(nrhs >= 1 && nrhs <= 1024, LYM_ERR_BAD_ARG, "nrhs out of range");
+  LYM_REQUIRE(g->nd != 3, LYM_ERR_UNSUPPORTED,
+              "Q^2 + sigma needs the hermitian Q = gamma_d D, which three dimensions do not have");
   LYM_REQUIRE(nshift >= 1 && nshift <= kMsMaxShifts, LYM_ERR_BAD_ARG, "nshift must be in [1, %d]", kMsMaxShifts);
   LYM_REQUIRE(params->tol > 0 && params->max_iter > 0, LYM_ERR_BAD_ARG, "tol and max_iter must be positive");
   LYM_REQUIRE(params->precision >= 0 && params->precision <= 3, LYM_ERR_BAD_ARG, "bad precision");

@@ -149,6 +149,8 @@ int lym_multishift_solve(lym_gauge* g, double kappa, int nshift, const double* s
   GaugeView gv;
   int rc = gauge_view(g, &gv);
   if (rc) return rc;
+  LYM_REQUIRE(gv.lat->nd != 3, LYM_ERR_UNSUPPORTED,
+              "Q^2 + sigma needs the hermitian Q = gamma_d D, which three dimensions do not have");
   int base = 0;
   for (int s = 0; s < nshift; ++s) {
     LYM_REQUIRE(shifts[s] >= 0, LYM_ERR_BAD_ARG, "negative shifts need BiCGStab (dirac_solver.py:26-30)");
@@ -266,6 +268,8 @@ int lym_mmmr_solve(lym_gauge* g, double kappa, int nshift, const double* shifts,
   GaugeView gv;
   int rc = gauge_view(g, &gv);
   if (rc) return rc;
+  LYM_REQUIRE(gv.lat->nd != 3, LYM_ERR_UNSUPPORTED,
+              "Q^2 + sigma needs the hermitian Q = gamma_d D, which three dimensions do not have");
   cudaStream_t st = (cudaStream_t)stream;
   const int64_t n = gv.V * gv.ncomp;
   std::lock_guard<std::mutex> lk(host_reduce_mutex());

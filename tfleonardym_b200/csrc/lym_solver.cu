@@ -485,7 +485,9 @@ LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s,
   for (int q = 0; q < R; ++q) n[q] = 0.0;
   if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    hop_any<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, s, rhs0, i, 0, act, acc);
+    // M^dag = gamma_d M gamma_d in 2 and 4 dimensions (gamma_d on the output below);
+    // in 3 the adjoint hop itself
+    hop_any<ND, NC, SP, GP, COMP, ND == 3, R, MX>(g, hg, s, rhs0, i, 0, act, acc);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       const int m = q, cb = i;
@@ -504,7 +506,7 @@ LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s,
         for (int c = 0; c < NC; ++c) {
           const int k = sp * NC + c;
           cx<RT> h = acc[m][sp][c];
-          if (sp >= NS / 2) h = -h;
+          if (ND != 3 && sp >= NS / 2) h = -h;
           cx<RT> ap = tv[k] - (RT)k2 * h;
           rv[k] -= a * ap;
           xv[k] += (XR)alpha * cx<XR>{(XR)pv[k].re, (XR)pv[k].im};
@@ -561,7 +563,7 @@ LYM_D void cg_rnew_body(const EoGeom& g, const HopGauge& hg, const EoField& s, c
   for (int q = 0; q < R; ++q) n[q] = 0.0;
   if (i < g.Vh) {
     cx<RT> acc[R][NS][NC];
-    hop_any<ND, NC, SP, GP, COMP, false, R, MX>(g, hg, s, rhs0, i, 0, act, acc);
+    hop_any<ND, NC, SP, GP, COMP, ND == 3, R, MX>(g, hg, s, rhs0, i, 0, act, acc);
 #pragma unroll
     for (int q = 0; q < R; ++q) {
       const int m = q, cb = i;
@@ -573,7 +575,7 @@ LYM_D void cg_rnew_body(const EoGeom& g, const HopGauge& hg, const EoField& s, c
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           cx<RT> h = acc[m][sp][c];
-          if (sp >= NS / 2) h = -h;
+          if (ND != 3 && sp >= NS / 2) h = -h;
           cx<RT>& w = v[sp * NC + c];
           w -= (RT)k2 * h;
           n[q] += (double)w.re * w.re + (double)w.im * w.im;
@@ -645,39 +647,27 @@ __global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoFiel
 // ---------------------------------------------------------------------------
 // tensor-core FP16 hop kernels (4D SU(3), FP16 spinors, full FP16 links; the hop
 // core and its layout are in lym_hop_tc.cuh).  One thread per (site, rhs), a
-// CTA per (S sites, RG rhs); the epilogues are the one-rhs forms of the bodies
+// CTA per (8 sites, 16 rhs); the epilogues are the one-rhs forms of the bodies
 // above.
 // ---------------------------------------------------------------------------
-template <int RG>
 LYM_D double* tc_red(char* smem) {
-  using P = tc::Plan<RG>;
-  return reinterpret_cast<double*>(smem + 2 * P::kTile + P::kLinks + P::kCodes);
+  using P = tc::Plan;
+  return reinterpret_cast<double*>(smem + 2 * P::kTile + P::kLinks);
 }
 
-// the block-uniform "any rhs of this group active" test (every thread reads the same flags)
-template <int RG>
-LYM_D bool tc_any(const CGState* st, const int* upd) {
-  int any = 0;
-#pragma unroll
-  for (int k = 0; k < RG; ++k) {
-    const int q = blockIdx.y * RG + k;
-    any |= upd ? upd[q] : (st ? st[q].active : 1);
-  }
-  return any != 0;
-}
 
 // s = H G5IN(p) (output parity par); st == nullptr: every rhs
-template <bool G5IN, int RG>
-__global__ void __launch_bounds__(256) cg_hop_tc_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
+template <bool G5IN>
+__global__ void __launch_bounds__(tc::kThreads) cg_hop_tc_kernel(EoGeom g, HopGauge hg, EoField in, EoField out, int par,
                                                         const CGState* st) {
   extern __shared__ __align__(16) char smem[];
-  constexpr int S = 256 / RG, NCOMP = 12;
-  if (!tc_any<RG>(st, nullptr)) return;
+  constexpr int S = tc::kS, RG = tc::kRG, NCOMP = 12;
   const int i = threadIdx.x % S, r = threadIdx.x / S, rhs = blockIdx.y * RG + r;
   const bool act = st ? st[rhs].active != 0 : true;
+  if (!__syncthreads_or(act)) return;  // no rhs of this group active (uniform per block)
   const int cb = blockIdx.x * S + i;
   cx<float> acc[4][3];
-  tc::hop_tc<G5IN, RG>(g, hg, in, par, blockIdx.x * S, blockIdx.y * RG, i, r, act, smem, acc);
+  tc::hop_tc<G5IN>(g, hg, in, par, blockIdx.x * S, blockIdx.y * RG, i, r, act, smem, acc);
   if (!act || cb >= g.Vh) return;
   cx<float> v[NCOMP];
 #pragma unroll
@@ -688,18 +678,17 @@ __global__ void __launch_bounds__(256) cg_hop_tc_kernel(EoGeom g, HopGauge hg, E
 }
 
 // t = p - kappa^2 H_eo s ; alpha = rr / |t|^2
-template <int RG>
-__global__ void __launch_bounds__(256) cg_t_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t,
+__global__ void __launch_bounds__(tc::kThreads) cg_t_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField p, EoField t,
                                                       double k2, CGState* st, double* partials,
                                                       unsigned* counters, int nblk) {
   extern __shared__ __align__(16) char smem[];
-  constexpr int S = 256 / RG, NCOMP = 12;
-  if (!tc_any<RG>(st, nullptr)) return;
+  constexpr int S = tc::kS, RG = tc::kRG, NCOMP = 12;
   const int i = threadIdx.x % S, r = threadIdx.x / S, rhs = blockIdx.y * RG + r;
   const bool act = st[rhs].active != 0;
+  if (!__syncthreads_or(act)) return;  // uniform per block
   const int cb = blockIdx.x * S + i;
   cx<float> acc[4][3];
-  tc::hop_tc<false, RG>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, r, act, smem, acc);
+  tc::hop_tc<false>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, r, act, smem, acc);
   double n = 0.0;
   if (act && cb < g.Vh) {
     cx<float> v[NCOMP];
@@ -715,7 +704,7 @@ __global__ void __launch_bounds__(256) cg_t_tc_kernel(EoGeom g, HopGauge hg, EoF
     store_sp<SP16, NCOMP>(t, rhs, cb, v);
   }
   double tot = 0.0;
-  if (tc::grid_rhs_sum<RG>(n, tc_red<RG>(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
+  if (tc::grid_rhs_sum(n, tc_red(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
     CGState& Sx = st[blockIdx.y * RG + threadIdx.x];
     if (Sx.active) {
       if (tot > 0.0 && Sx.rr > 0.0) {
@@ -729,18 +718,17 @@ __global__ void __launch_bounds__(256) cg_t_tc_kernel(EoGeom g, HopGauge hg, EoF
 }
 
 // Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr
-template <int RG>
-__global__ void __launch_bounds__(256) cg_update_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
+__global__ void __launch_bounds__(tc::kThreads) cg_update_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
                                                            EoField x, EoField r, double k2, CGState* st,
                                                            double* partials, unsigned* counters, int nblk) {
   extern __shared__ __align__(16) char smem[];
-  constexpr int S = 256 / RG, NCOMP = 12;
-  if (!tc_any<RG>(st, nullptr)) return;
+  constexpr int S = tc::kS, RG = tc::kRG, NCOMP = 12;
   const int i = threadIdx.x % S, q = threadIdx.x / S, rhs = blockIdx.y * RG + q;
   const bool act = st[rhs].active != 0;
+  if (!__syncthreads_or(act)) return;  // uniform per block
   const int cb = blockIdx.x * S + i;
   cx<float> acc[4][3];
-  tc::hop_tc<false, RG>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, q, act, smem, acc);
+  tc::hop_tc<false>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, q, act, smem, acc);
   double n = 0.0;
   if (act && cb < g.Vh) {
     const double alpha = st[rhs].alpha;
@@ -766,7 +754,7 @@ __global__ void __launch_bounds__(256) cg_update_tc_kernel(EoGeom g, HopGauge hg
     store_sp<SP32, NCOMP>(x, rhs, cb, xv);
   }
   double tot = 0.0;
-  if (tc::grid_rhs_sum<RG>(n, tc_red<RG>(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
+  if (tc::grid_rhs_sum(n, tc_red(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
     CGState& Sx = st[blockIdx.y * RG + threadIdx.x];
     if (Sx.active) {
       Sx.beta = tot / Sx.rr;
@@ -779,18 +767,17 @@ __global__ void __launch_bounds__(256) cg_update_tc_kernel(EoGeom g, HopGauge hg
 }
 
 // r = t - kappa^2 gamma_d H_eo s for rhs with upd[rhs]; res[rhs] = |r|^2
-template <int RG>
-__global__ void __launch_bounds__(256) cg_rnew_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField r,
+__global__ void __launch_bounds__(tc::kThreads) cg_rnew_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField r,
                                                          double k2, const int* upd, double* partials,
                                                          unsigned* counters, double* res, int nblk) {
   extern __shared__ __align__(16) char smem[];
-  constexpr int S = 256 / RG, NCOMP = 12;
-  if (!tc_any<RG>(nullptr, upd)) return;
+  constexpr int S = tc::kS, RG = tc::kRG, NCOMP = 12;
   const int i = threadIdx.x % S, q = threadIdx.x / S, rhs = blockIdx.y * RG + q;
   const bool act = upd[rhs] != 0;
+  if (!__syncthreads_or(act)) return;  // uniform per block
   const int cb = blockIdx.x * S + i;
   cx<float> acc[4][3];
-  tc::hop_tc<false, RG>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, q, act, smem, acc);
+  tc::hop_tc<false>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, q, act, smem, acc);
   double n = 0.0;
   if (act && cb < g.Vh) {
     cx<float> v[NCOMP];
@@ -808,7 +795,7 @@ __global__ void __launch_bounds__(256) cg_rnew_tc_kernel(EoGeom g, HopGauge hg, 
     store_sp<SP16, NCOMP>(r, rhs, cb, v);
   }
   double tot = 0.0;
-  if (tc::grid_rhs_sum<RG>(n, tc_red<RG>(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
+  if (tc::grid_rhs_sum(n, tc_red(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
     const int q2 = blockIdx.y * RG + threadIdx.x;
     if (upd[q2]) res[q2] = tot;
   }
@@ -867,7 +854,7 @@ struct Work {
   int* upd = nullptr;
   int* upd_host = nullptr;
   double* partials = nullptr;
-  double* partials_tc = nullptr;  // per rhs and 16-site block: the tensor-core hop's reductions
+  double* partials_tc = nullptr;  // per rhs and 8-site block: the tensor-core hop's reductions
   unsigned* counters = nullptr;
   double* res = nullptr;       // per rhs, several result slots
   double* res_host = nullptr;
@@ -1008,39 +995,38 @@ struct Impl {
 };
 
 // The tensor-core FP16 hop (4D SU(3), full FP16 links): iterate / dslash / rnew
-// run the cg_*_tc kernels with RG right-hand sides per CTA; everything else is
+// run the cg_*_tc kernels with 16 right-hand sides per CTA; everything else is
 // the FP16 mixed-precision table's.
-template <int RG>
 struct ImplTC {
   using Base = Impl<4, 3, SP16, false, 1, 1>;
-  using P = tc::Plan<RG>;
-  static constexpr int S = P::S;
+  using P = tc::Plan;
+  static constexpr int S = tc::kS, RG = tc::kRG;
   static unsigned nblk(const Work& w) { return (unsigned)((w.Vh + S - 1) / S); }
   // the kernels take more than 48 KB of dynamic shared memory
   static void prepare() {
-    cudaFuncSetAttribute(cg_hop_tc_kernel<false, RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
-    cudaFuncSetAttribute(cg_hop_tc_kernel<true, RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
-    cudaFuncSetAttribute(cg_t_tc_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
-    cudaFuncSetAttribute(cg_update_tc_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
-    cudaFuncSetAttribute(cg_rnew_tc_kernel<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_hop_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_hop_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_t_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_update_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
+    cudaFuncSetAttribute(cg_rnew_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P::kBytes);
   }
   static void iterate(Work& w, cudaStream_t st) {
     const double k2 = w.kappa * w.kappa;
     const dim3 grid(w.nblk, w.nrhs), tile(nblk(w), w.nrhs / RG);
     const int nb = (int)nblk(w);
     const CGState* cst = w.st;
-    launch_smem(w, st, cg_hop_tc_kernel<false, RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.p, w.s, 1, cst);
-    launch_smem(w, st, cg_t_tc_kernel<RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st,
+    launch_smem(w, st, cg_hop_tc_kernel<false>, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.p, w.s, 1, cst);
+    launch_smem(w, st, cg_t_tc_kernel, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st,
                 w.partials_tc, w.counters, nb);
-    launch_smem(w, st, cg_hop_tc_kernel<true, RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.t, w.s, 1, cst);
-    launch_smem(w, st, cg_update_tc_kernel<RG>, tile, dim3(256), P::kBytes, w.g->geom, w.hgs, w.s, w.t, w.p, w.xs,
+    launch_smem(w, st, cg_hop_tc_kernel<true>, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.t, w.s, 1, cst);
+    launch_smem(w, st, cg_update_tc_kernel, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.s, w.t, w.p, w.xs,
                 w.r, k2, w.st, w.partials_tc, w.counters, nb);
     launch(w, st, cg_p_kernel<SP16, 12>, grid, dim3(128), w.Vh, w.r, w.p, w.st, w.counters);
   }
   static void dslash(Work& w, cudaStream_t st) {
     prepare();
     w.launches += 1;
-    cg_hop_tc_kernel<false, RG><<<dim3(nblk(w), w.nrhs / RG), 256, P::kBytes, st>>>(w.g->geom, w.hgs, w.p, w.s, 1,
+    cg_hop_tc_kernel<false><<<dim3(nblk(w), w.nrhs / RG), tc::kThreads, P::kBytes, st>>>(w.g->geom, w.hgs, w.p, w.s, 1,
                                                                                    nullptr);
   }
   static void rnew(Work& w, cudaStream_t st) {
@@ -1048,18 +1034,18 @@ struct ImplTC {
     const double k2 = w.kappa * w.kappa;
     const dim3 tile(nblk(w), w.nrhs / RG);
     w.launches += 2;
-    cg_hop_tc_kernel<true, RG><<<tile, 256, P::kBytes, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, nullptr);
-    cg_rnew_tc_kernel<RG><<<tile, 256, P::kBytes, st>>>(w.g->geom, w.hgs, w.s, w.t, w.r, k2, w.upd, w.partials_tc,
+    cg_hop_tc_kernel<true><<<tile, tc::kThreads, P::kBytes, st>>>(w.g->geom, w.hgs, w.t, w.s, 1, nullptr);
+    cg_rnew_tc_kernel<<<tile, tc::kThreads, P::kBytes, st>>>(w.g->geom, w.hgs, w.s, w.t, w.r, k2, w.upd, w.partials_tc,
                                                         w.counters, w.res, (int)nblk(w));
   }
   static void preload() {
     Base::preload();
     prepare();
     cudaFuncAttributes a;
-    cudaFuncGetAttributes(&a, cg_hop_tc_kernel<false, RG>);
-    cudaFuncGetAttributes(&a, cg_hop_tc_kernel<true, RG>);
-    cudaFuncGetAttributes(&a, cg_t_tc_kernel<RG>);
-    cudaFuncGetAttributes(&a, cg_update_tc_kernel<RG>);
+    cudaFuncGetAttributes(&a, cg_hop_tc_kernel<false>);
+    cudaFuncGetAttributes(&a, cg_hop_tc_kernel<true>);
+    cudaFuncGetAttributes(&a, cg_t_tc_kernel);
+    cudaFuncGetAttributes(&a, cg_update_tc_kernel);
   }
   static CgOps table() {
     CgOps t = Base::table();
@@ -1077,7 +1063,9 @@ static CgOps pick_sp(int sp, bool comp, int mx) {
     case SP64: return Impl<ND, NC, SP64, false, 1, 0>::table();  // FP64 keeps one rhs per thread (registers)
     case SP32: return comp ? Impl<ND, NC, SP32, true, R, 0>::table() : Impl<ND, NC, SP32, false, R, 0>::table();
     case SP16:
-      if (mx) return Impl<ND, NC, SP16, false, R, 1>::table();
+      if constexpr (ND != 3) {
+        if (mx) return Impl<ND, NC, SP16, false, R, 1>::table();
+      }
       return comp ? Impl<ND, NC, SP16, true, R, 0>::table() : Impl<ND, NC, SP16, false, R, 0>::table();
     default: return comp ? Impl<ND, NC, SPB16, true, R, 0>::table() : Impl<ND, NC, SPB16, false, R, 0>::table();
   }
@@ -1087,6 +1075,8 @@ template <int R>
 static bool pick_ops_r(int nd, int nc, int sp, bool comp, int mx, CgOps* out) {
   if (nd == 2 && nc == 2) *out = pick_sp<2, 2, R>(sp, comp, mx);
   else if (nd == 2 && nc == 3) *out = pick_sp<2, 3, R>(sp, comp, mx);
+  else if (nd == 3 && nc == 2) *out = pick_sp<3, 2, R>(sp, comp, mx);
+  else if (nd == 3 && nc == 3) *out = pick_sp<3, 3, R>(sp, comp, mx);
   else if (nd == 4 && nc == 2) *out = pick_sp<4, 2, R>(sp, comp, mx);
   else if (nd == 4 && nc == 3) *out = pick_sp<4, 3, R>(sp, comp, mx);
   else return false;
@@ -1181,7 +1171,7 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   for (int comp = 0; comp < 2; ++comp) {
     if (comp && !(g->comp && sp != SP64)) continue;  // compressed links need SU(N) links and a sloppy precision
     for (int mx = 0; mx < 2; ++mx) {
-      if (mx && (sp != SP16 || comp)) continue;  // the mixed-precision hop: FP16 spinors, full links
+      if (mx && (sp != SP16 || comp || g->nd == 3)) continue;  // the mixed-precision hop: FP16 spinors, full links, 2 or 4 dimensions
       for (int R : {1, 2, 4}) {
         if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
         if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, mx, &w->ops_r[nc_])) {
@@ -1196,19 +1186,16 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
       }
     }
   }
-  // the tensor-core hop: 4D SU(3), FP16 spinors, full links, RG = 4, 8 or 16 rhs per CTA
-  if (sp == SP16 && g->nd == 4 && g->nc == 3) {
-    for (int RG : {4, 8, 16}) {
-      if (nrhs % RG != 0) continue;
-      w->ops_r[nc_] = RG == 4 ? ImplTC<4>::table() : (RG == 8 ? ImplTC<8>::table() : ImplTC<16>::table());
-      w->rcand[nc_] = RG;
-      w->ccand[nc_] = false;
-      w->mcand[nc_] = 2;
-      ++nc_;
-    }
+  // the tensor-core hop: 4D SU(3), FP16 spinors, full links, 16 rhs per CTA
+  if (sp == SP16 && g->nd == 4 && g->nc == 3 && nrhs % tc::kRG == 0) {
+    w->ops_r[nc_] = ImplTC::table();
+    w->rcand[nc_] = tc::kRG;
+    w->ccand[nc_] = false;
+    w->mcand[nc_] = 2;
+    ++nc_;
   }
   const bool has_tc = nc_ > 0 && w->mcand[nc_ - 1] == 2;
-  const size_t ntc = has_tc ? (size_t)nrhs * (size_t)((g->Vh + 15) / 16) : 0;
+  const size_t ntc = has_tc ? (size_t)nrhs * (size_t)((g->Vh + tc::kS - 1) / tc::kS) : 0;
   w->ncand = nc_;
   w->ops = w->ops_r[0];
   w->R = w->rcand[0];
@@ -1465,6 +1452,8 @@ static int cg_solve(lym_gauge* g, double kappa, int nrhs, const void* b, void* x
   const int sp = prm->precision;
   LYM_REQUIRE(sp == SP64 || (g->prec_mask >> sp) & 1u, LYM_ERR_BAD_ARG,
               "precision %d was not enabled in lym_gauge_create", sp);
+  LYM_REQUIRE(g->nd != 3 || !prm->hermitian, LYM_ERR_UNSUPPORTED,
+              "three dimensions have no hermitian form gamma_d D (two-component spinors, no gamma_5)");
   std::lock_guard<std::recursive_mutex> own(g->mu);
   Work* wp;
   int rc = get_work(g, nrhs, sp, &wp);
@@ -1809,7 +1798,9 @@ static MultiOps multi_pick_sp(int sp, bool comp) {
   switch (sp) {
     case SP64: return MultiImpl<ND, NC, SP64, false, 0>::table();
     case SP32: return comp ? MultiImpl<ND, NC, SP32, true, 0>::table() : MultiImpl<ND, NC, SP32, false, 0>::table();
-    case SP16: return MultiImpl<ND, NC, SP16, false, 1>::table();
+    case SP16:
+      if constexpr (ND == 3) return MultiImpl<ND, NC, SP16, false, 0>::table();
+      else return MultiImpl<ND, NC, SP16, false, 1>::table();
     default: return MultiImpl<ND, NC, SPB16, false, 0>::table();
   }
 }
@@ -1817,6 +1808,8 @@ static MultiOps multi_pick_sp(int sp, bool comp) {
 static bool multi_pick(int nd, int nc, int sp, bool comp, MultiOps* out) {
   if (nd == 2 && nc == 2) *out = multi_pick_sp<2, 2>(sp, comp);
   else if (nd == 2 && nc == 3) *out = multi_pick_sp<2, 3>(sp, comp);
+  else if (nd == 3 && nc == 2) *out = multi_pick_sp<3, 2>(sp, comp);
+  else if (nd == 3 && nc == 3) *out = multi_pick_sp<3, 3>(sp, comp);
   else if (nd == 4 && nc == 2) *out = multi_pick_sp<4, 2>(sp, comp);
   else if (nd == 4 && nc == 3) *out = multi_pick_sp<4, 3>(sp, comp);
   else return false;
@@ -1859,6 +1852,8 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
   const int sp = prm->precision;
   LYM_REQUIRE(gs[0], LYM_ERR_BAD_ARG, "null argument (lattice 0)");
   const int nd = gs[0]->nd, nc = gs[0]->nc;
+  LYM_REQUIRE(nd != 3 || !prm->hermitian, LYM_ERR_UNSUPPORTED,
+              "three dimensions have no hermitian form gamma_d D (two-component spinors, no gamma_5)");
   bool comp_all = sp == SP32;
   for (int l = 0; l < nlat; ++l) {
     LYM_REQUIRE(gs[l] && bs[l] && xs[l], LYM_ERR_BAD_ARG, "null argument (lattice %d)", l);
@@ -1877,7 +1872,7 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
   std::vector<std::unique_lock<std::recursive_mutex>> own;
   own.reserve(nlat);
   for (lym_gauge* g : order) own.emplace_back(g->mu);
-  const int mx = sp == SP16 ? 1 : 0;
+  const int mx = (sp == SP16 && nd != 3) ? 1 : 0;
   MultiOps ops;
   LYM_REQUIRE(multi_pick(nd, nc, sp, comp_all, &ops), LYM_ERR_UNSUPPORTED, "unsupported (nd=%d, N=%d)", nd, nc);
   std::vector<MultiLat> lats(nlat);
@@ -2216,6 +2211,7 @@ static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
     g->geom.nbr = g->nbr;
     dim3 tg(grid_for(g->Vh, 128), 2);
     if (g->nd == 2) build_nbr_kernel<2><<<tg, 128, 0, st>>>(g->geom, g->nbr);
+    else if (g->nd == 3) build_nbr_kernel<3><<<tg, 128, 0, st>>>(g->geom, g->nbr);
     else build_nbr_kernel<4><<<tg, 128, 0, st>>>(g->geom, g->nbr);
     LYM_CHECK_LAUNCH();
   }
@@ -2226,6 +2222,8 @@ static int pack_gauge(lym_gauge* g, const void* gauge, cudaStream_t st) {
                                                     g->u16f, g->n16f)
   if (g->nd == 2 && nc == 2) LYM_PACK(2, 2);
   else if (g->nd == 2 && nc == 3) LYM_PACK(2, 3);
+  else if (g->nd == 3 && nc == 2) LYM_PACK(3, 2);
+  else if (g->nd == 3 && nc == 3) LYM_PACK(3, 3);
   else if (g->nd == 4 && nc == 2) LYM_PACK(4, 2);
   else LYM_PACK(4, 3);
 #undef LYM_PACK
@@ -2246,20 +2244,21 @@ extern "C" {
 int lym_gauge_create(const lym_lattice* lat, int nc, const void* gauge, double bc_re, double bc_im,
                      unsigned prec_mask, void* stream, lym_gauge** out) {
   LYM_REQUIRE(lat && gauge && out, LYM_ERR_BAD_ARG, "null argument");
-  if (lat->nd != 2 && lat->nd != 4) {
+  if (lat->nd < 2 || lat->nd > 4) {
     set_error("Number of dimensions %d not supported for fermions!", lat->nd);
     return LYM_ERR_UNSUPPORTED;
   }
   LYM_REQUIRE(nc == 2 || nc == 3, LYM_ERR_UNSUPPORTED, "N=%d not supported (2 or 3)", nc);
   LYM_REQUIRE(lat->even, LYM_ERR_UNSUPPORTED, "even-odd ordering needs every extent even");
+  const int ns = lat->nd == 4 ? 4 : 2;  // two-component spinors in 2 and 3 dimensions
   // the hop kernels index one rhs of a field with 32-bit offsets
-  LYM_REQUIRE((int64_t)(lat->nd == 2 ? 2 : 4) * nc * (lat->V / 2) < (int64_t(1) << 31), LYM_ERR_UNSUPPORTED,
+  LYM_REQUIRE((int64_t)ns * nc * (lat->V / 2) < (int64_t(1) << 31), LYM_ERR_UNSUPPORTED,
               "lattice too large for 32-bit field offsets");
   lym_gauge* g = new lym_gauge();
   g->lat = lat;
   g->nc = nc;
   g->nd = lat->nd;
-  g->ns = lat->nd == 2 ? 2 : 4;
+  g->ns = ns;
   g->ncomp = g->ns * nc;
   g->V = lat->V;
   g->Vh = lat->V / 2;

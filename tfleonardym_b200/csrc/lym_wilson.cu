@@ -83,6 +83,22 @@ __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
 #pragma unroll
           for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
       }
+      if constexpr (ND == 3) {
+        cx<double> p0[NC], p1[NC], h[NC], t[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          p0[c] = ld(psi + (size_t)c * V + y);
+          p1[c] = ld(psi + (size_t)(NC + c) * V + y);
+        }
+        proj3<double, NC>(mu, +1, p0, p1, h);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+          t[i] = u[i][0] * h[0];
+#pragma unroll
+          for (int j = 1; j < NC; ++j) cmac(t[i], u[i][j], h[j]);
+        }
+        recon3<double, NC>(mu, +1, t, acc[0], acc[1]);
+      } else {
 #pragma unroll
       for (int a = 0; a < NS / 2; ++a) {
         const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
@@ -100,6 +116,7 @@ __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
           acc[jb][i] += mul_phase(phase_neg(phase_conj(ph)), t);
         }
       }
+      }
     }
     // backward: U_mu(x - mu)^dag (1 + g_mu) psi(x - mu)
     {
@@ -115,6 +132,22 @@ __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
 #pragma unroll
           for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
       }
+      if constexpr (ND == 3) {
+        cx<double> p0[NC], p1[NC], h[NC], t[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          p0[c] = ld(psi + (size_t)c * V + y);
+          p1[c] = ld(psi + (size_t)(NC + c) * V + y);
+        }
+        proj3<double, NC>(mu, -1, p0, p1, h);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+          t[i] = cmul_cj(u[0][i], h[0]);
+#pragma unroll
+          for (int j = 1; j < NC; ++j) cmac_cj(t[i], u[j][i], h[j]);
+        }
+        recon3<double, NC>(mu, -1, t, acc[0], acc[1]);
+      } else {
 #pragma unroll
       for (int a = 0; a < NS / 2; ++a) {
         const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
@@ -131,6 +164,7 @@ __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
           acc[a][i] += t;
           acc[jb][i] += mul_phase(phase_conj(ph), t);
         }
+      }
       }
     }
   }
@@ -166,11 +200,15 @@ int wilson_full(const lym_lattice* lat, int nc, double kappa, int herm, double b
   LYM_REQUIRE(lat && gauge && in && out, LYM_ERR_BAD_ARG, "null argument");
   LYM_REQUIRE(in != out, LYM_ERR_BAD_ARG, "in and out must not alias");
   LYM_REQUIRE(nvec >= 1 && nvec <= 65535, LYM_ERR_BAD_ARG, "nvec out of range");
-  if (lat->nd != 2 && lat->nd != 4) {
+  if (lat->nd < 2 || lat->nd > 4) {
     set_error("Number of dimensions %d not supported for fermions!", lat->nd);
     return LYM_ERR_UNSUPPORTED;
   }
+  LYM_REQUIRE(lat->nd != 3 || !herm, LYM_ERR_UNSUPPORTED,
+              "three dimensions have no hermitian form gamma_d D (two-component spinors, no gamma_5)");
   LYM_REQUIRE(nc == 2 || nc == 3, LYM_ERR_UNSUPPORTED, "N=%d not supported (2 or 3)", nc);
+  if (lat->nd == 3 && nc == 2) return launch_full<3, 2>(lat, kappa, 0, bcr, bci, gauge, nvec, in, out, st);
+  if (lat->nd == 3 && nc == 3) return launch_full<3, 3>(lat, kappa, 0, bcr, bci, gauge, nvec, in, out, st);
   if (lat->nd == 2 && nc == 2) return launch_full<2, 2>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);
   if (lat->nd == 2 && nc == 3) return launch_full<2, 3>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);
   if (lat->nd == 4 && nc == 2) return launch_full<4, 2>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);

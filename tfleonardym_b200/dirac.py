@@ -116,6 +116,13 @@ class DiracWilsonOperator(Operator):
             self.spinor_dimension = 2
         elif self.number_of_dimensions == 4:
             self.spinor_dimension = 4
+        elif self.number_of_dimensions == 3 and self.representation == "fundamental":
+            # builder-defined extension (the reference stops here): two-component
+            # spinors with gamma_mu = sigma_{mu+1}; odd dimensions have no gamma_5,
+            # so only D itself (hermitian=False) exists
+            if self.hermitian:
+                raise RuntimeError("Number of dimensions 3 has no hermitian form gamma_d D (two-component spinors)")
+            self.spinor_dimension = 2
         else:
             raise RuntimeError(f"Number of dimensions {self.number_of_dimensions} not supported for fermions!")
 

@@ -4,8 +4,10 @@ The per-link kernels replace the reference's TF ops: ``update_link_field``
 (hmc.py:40-43, tf.linalg.expm) runs lym_update_links (SU(2) closed form,
 SU(3) Cayley-Hamilton), ``update_momenta`` (hmc.py:59-61) runs
 lym_update_momenta, ``momenta_energy`` (hmc.py:170-176) lym_momenta_energy.
-The integrators and ``hybrid_mc`` / ``reversibility_check`` keep the
-reference's control flow (hmc.py:104-278) over these device tensors.
+The integrators are compiled into flat schedules of drifts and kicks (below)
+and run over these device tensors; ``integrate_om`` / ``integrate_lp`` /
+``hybrid_mc`` / ``reversibility_check`` keep the reference's signatures and
+results (hmc.py:104-278).
 """
 import copy
 import ctypes
@@ -46,27 +48,16 @@ def update_momenta(momenta, gauge_force, epsilon):
 
 
 def momenta_from_normals(normals, nc):
-    """Anti-Hermitian traceless momenta from unit normals (nd, N*N-1, V), built
-    exactly as random_momenta does from its draws (hmc.py:69-96)."""
-    nd, _, vol = normals.shape
-    p = torch.zeros((nd, nc, nc, vol), dtype=torch.complex128, device=normals.device)
-    for mu in range(nd):
-        k = 0
-        for i in range(nc):
-            for j in range(i + 1, nc):
-                re, im = normals[mu, k] / 2, normals[mu, k + 1] / 2
-                k += 2
-                p[mu, i, j] = torch.complex(re, im)
-                p[mu, j, i] = torch.complex(-re, im)
-        diag = torch.zeros((nc, vol), dtype=torch.float64, device=normals.device)
-        for i in range(1, nc):
-            r = normals[mu, k] / 2
-            k += 1
-            for j in range(i):
-                diag[j] += r / np.sqrt(i * (i + 1) / 2.0)
-            diag[i] += -r * (i * np.sqrt(2.0 / (i * (i + 1))))
-        for i in range(nc):
-            p[mu, i, i] = torch.complex(torch.zeros_like(diag[i]), diag[i])
+    """Anti-Hermitian traceless momenta from unit normals (nd, N*N-1, V) on the
+    device, built as random_momenta builds them from its draws (hmc.py:69-96)
+    in one kernel (lym_momenta_from_normals)."""
+    nrm = normals.to(torch.float64).contiguous()
+    nd, ng, vol = nrm.shape
+    if ng != nc * nc - 1:
+        raise ValueError(f"normals need N*N-1 = {nc * nc - 1} rows per direction, got {ng}")
+    p = torch.empty((nd, nc, nc, vol), dtype=torch.complex128, device=nrm.device)
+    _lib.check(_lib.lib().lym_momenta_from_normals(nd, nc, vol, nrm.data_ptr(), _dev.ptr(p), _dev.stream()),
+               "lym_momenta_from_normals")
     return p
 
 
@@ -128,60 +119,118 @@ def generate_random_vector(nc=3, spinor_dimension=4, representation="fundamental
     return torch.complex(re, im)
 
 
-def _apply_force(action, momenta, eps):
-    """momenta + eps * action.force(), fusing the update when the action allows it."""
+# ---------------------------------------------------------------------------
+# Molecular dynamics as a flat schedule
+#
+# The reference integrates recursively, calling update_momenta and
+# update_configuration as it goes (hmc.py:104-162).  Here an integrator is first
+# compiled into a flat list of operations -- a drift U <- exp(w P) U, or a kick
+# P <- P + w F_level(U) -- and then run.  Compilation writes each step as the
+# symmetric product of the scheme and fuses neighbouring kicks of one level that
+# no drift separates into one kick with the summed weight: the reference's closing
+# kick reuses the force of the kick just before it (hmc.py:122, 160), so the fused
+# list asks for exactly the force evaluations the reference makes.  The runner
+# sets an action's gauge configuration only when the links changed since it last
+# saw them, and applies each kick through the action's fused force-into-momenta
+# kernel where it has one.
+# ---------------------------------------------------------------------------
+DRIFT, KICK = 0, 1
+
+
+class Op:
+    __slots__ = ("kind", "level", "weight")
+
+    def __init__(self, kind, level, weight):
+        self.kind, self.level, self.weight = kind, level, weight
+
+    def __repr__(self):
+        return f"{'drift' if self.kind == DRIFT else 'kick'}({self.level}, {self.weight!r})"
+
+
+def _fuse(ops):
+    out = []
+    for op in ops:
+        if out and op.kind == KICK and out[-1].kind == KICK and out[-1].level == op.level:
+            out[-1] = Op(KICK, op.level, out[-1].weight + op.weight)
+        else:
+            out.append(op)
+    return out
+
+
+def _compile(scheme, steps, delta_t, level=0):
+    """The flat schedule of `scheme` ("omelyan" or "leapfrog") on nested levels:
+    level l takes steps[l] steps of delta_t / steps[l] (times the scheme's inner
+    fractions for the levels below); the last level's inner move is the drift."""
+    n = steps[level]
+    eps = delta_t / n
+    last = level == len(steps) - 1
+
+    def inner(dt):
+        return [Op(DRIFT, level, dt)] if last else _compile(scheme, steps, dt, level + 1)
+
+    one = []
+    if scheme == "omelyan":
+        lam = OMELYAN_LAMBDA
+        # K(lam e) I(e/2) K((1 - 2 lam) e) I(e/2) K(lam e); kick weights carry the
+        # force's sign convention of hmc.py (P + w F with w = -c e)
+        one = [Op(KICK, level, -lam * eps)] + inner(eps / 2) + [Op(KICK, level, -(1 - 2 * lam) * eps)] + \
+            inner(eps / 2) + [Op(KICK, level, -lam * eps)]
+    elif scheme == "leapfrog":
+        one = [Op(KICK, level, -eps / 2)] + inner(eps) + [Op(KICK, level, -eps / 2)]
+    else:
+        raise ValueError(f"unknown integrator {scheme!r}")
+    return _fuse(one * n)
+
+
+def schedule(scheme, steps, delta_t):
+    """Compiled molecular-dynamics schedule (a list of Op) for `steps` per level."""
+    if not steps or any(int(k) < 1 for k in steps):
+        raise ValueError("every level needs at least one step")
+    return _compile(scheme, [int(k) for k in steps], float(delta_t))
+
+
+def force_evaluations(ops):
+    """Forces a schedule evaluates, per level."""
+    counts = {}
+    for op in ops:
+        if op.kind == KICK:
+            counts[op.level] = counts.get(op.level, 0) + 1
+    return counts
+
+
+def _kick(action, momenta, w):
     fused = getattr(action, "force_into_momenta", None)
     if fused is not None:
-        out = momenta.clone()
-        return fused(out, eps)
-    return update_momenta(momenta, action.force(), eps)
+        return fused(momenta.clone(), w)
+    return update_momenta(momenta, action.force(), w)
 
 
-def integrate_lp(config, momenta, actions, steps, delta_t, action_index=0):
-    """Leap-frog (hmc.py:104-124)."""
-    epsilon = delta_t / steps[action_index]
-    actions[action_index].set_gauge_configuration(config)
-    momenta = _apply_force(actions[action_index], momenta, -(epsilon / 2))
-    for k in range(steps[action_index]):
-        if action_index == len(actions) - 1:
-            config = update_configuration(config, momenta, epsilon)
-        else:
-            config, momenta = integrate_lp(config, momenta, actions, steps, epsilon, action_index + 1)
-        actions[action_index].set_gauge_configuration(config)
-        # -eps inside the loop; after the last step also the closing +eps/2 with the same force
-        w = -epsilon if k < steps[action_index] - 1 else -epsilon / 2
-        momenta = _apply_force(actions[action_index], momenta, w)
+def run_schedule(config, momenta, actions, ops, level_offset=0):
+    """Run a compiled schedule; kick level l uses actions[level_offset + l]."""
+    version, seen = 0, {}
+    for op in ops:
+        if op.kind == DRIFT:
+            config = update_configuration(config, momenta, op.weight)
+            version += 1
+            continue
+        a = level_offset + op.level
+        if seen.get(a) != version:
+            actions[a].set_gauge_configuration(config)
+            seen[a] = version
+        momenta = _kick(actions[a], momenta, op.weight)
     return config, momenta
 
 
 def integrate_om(config, momenta, actions, steps, delta_t, action_index=0):
-    """Nested Omelyan integrator (hmc.py:133-162).
+    """Nested Omelyan integrator with the reference's interface (hmc.py:133-162)."""
+    return run_schedule(config, momenta, actions, schedule("omelyan", steps[action_index:len(actions)], delta_t),
+                        action_index)
 
-    The reference evaluates the last force of the loop twice in a row with the
-    same links (once inside the loop, once for the closing +lambda*eps kick);
-    here the closing kick reuses that force through eps-weight merging, which
-    is the same arithmetic on the momenta."""
-    ll = OMELYAN_LAMBDA
-    epsilon = delta_t / steps[action_index]
-    last = action_index == len(actions) - 1
-    actions[action_index].set_gauge_configuration(config)
-    momenta = _apply_force(actions[action_index], momenta, -ll * epsilon)
-    for k in range(steps[action_index]):
-        if last:
-            config = update_configuration(config, momenta, epsilon / 2)
-        else:
-            config, momenta = integrate_om(config, momenta, actions, steps, epsilon / 2, action_index + 1)
-        actions[action_index].set_gauge_configuration(config)
-        momenta = _apply_force(actions[action_index], momenta, -(1 - 2 * ll) * epsilon)
-        if last:
-            config = update_configuration(config, momenta, epsilon / 2)
-        else:
-            config, momenta = integrate_om(config, momenta, actions, steps, epsilon / 2, action_index + 1)
-        actions[action_index].set_gauge_configuration(config)
-        # -2 ll eps inside the loop and, after the last step, +ll eps with the same force
-        w = -2 * ll * epsilon if k < steps[action_index] - 1 else -ll * epsilon
-        momenta = _apply_force(actions[action_index], momenta, w)
-    return config, momenta
+
+def integrate_lp(config, momenta, actions, steps, delta_t, action_index=0):
+    """Nested leap-frog integrator with the reference's interface (hmc.py:104-124)."""
+    return run_schedule(config, momenta, actions, schedule("leapfrog", steps[action_index:len(actions)], delta_t),
+                        action_index)
 
 
 def gauge_energy(cfg, beta):
@@ -190,44 +239,47 @@ def gauge_energy(cfg, beta):
     return -beta * (nd - 1) * nd / 2 * cfg.gauge_field.shape[-1] * plaquette(cfg).value
 
 
-def _metropolis(new_energy, old_energy, uniform=None):
-    """metropolis.py:11-18; ``uniform`` may be supplied by the caller."""
-    if new_energy < old_energy:
+def hamiltonian(config, momenta, actions):
+    """Kinetic energy of the momenta plus every action's energy on `config`."""
+    h = momenta_energy(momenta)
+    for a in actions:
+        a.set_gauge_configuration(config)
+        h += a.energy()
+    return h
+
+
+def accept(delta_h, uniform=None):
+    """Metropolis test on delta_h = H_new - H_old (metropolis.py:11-18); the caller
+    may supply the uniform deviate."""
+    if delta_h < 0:
         return True
     u = np.random.uniform(0, 1) if uniform is None else uniform
-    return bool(u < np.exp(-(new_energy - old_energy)))
+    return bool(u < np.exp(-delta_h))
+
+
+def _fresh_momenta(config):
+    return random_momenta(config.colors, config.number_of_dimensions, config.gauge_field.shape[-1])
 
 
 def hybrid_mc(config, actions, steps, delta_t, momenta=None, uniform=None):
-    """One HMC trajectory (hmc.py:218-246).  Returns (cfg, -dH, accepted)."""
-    if momenta is None:
-        momenta = random_momenta(config.colors, config.number_of_dimensions, config.gauge_field.shape[-1])
-    old_energy = momenta_energy(momenta)
-    for action in actions:
-        action.set_gauge_configuration(config)
-        old_energy += action.energy()
-    new_config, new_momenta = integrate_om(config, momenta, actions, steps, delta_t)
-    new_energy = momenta_energy(new_momenta)
-    for action in actions:
-        action.set_gauge_configuration(new_config)
-        new_energy += action.energy()
-    if _metropolis(new_energy, old_energy, uniform):
-        return new_config, -(new_energy - old_energy), True
-    return copy.copy(config), -(new_energy - old_energy), False
+    """One HMC trajectory with the reference's interface and result (hmc.py:218-246):
+    returns (configuration, -dH, accepted)."""
+    p0 = _fresh_momenta(config) if momenta is None else momenta
+    h0 = hamiltonian(config, p0, actions)
+    ops = schedule("omelyan", steps[:len(actions)], delta_t)
+    cfg1, p1 = run_schedule(config, p0, actions, ops)
+    dh = hamiltonian(cfg1, p1, actions) - h0
+    if accept(dh, uniform):
+        return cfg1, -dh, True
+    return copy.copy(config), -dh, False
 
 
 def reversibility_check(config, actions, steps, delta_t, momenta=None):
-    """Forward then backward trajectory; returns H_end - H_start (hmc.py:249-278)."""
-    if momenta is None:
-        momenta = random_momenta(config.colors, config.number_of_dimensions, config.gauge_field.shape[-1])
-    old_energy = momenta_energy(momenta)
-    for action in actions:
-        action.set_gauge_configuration(config)
-        old_energy += action.energy()
-    new_config, new_momenta = integrate_om(config, momenta, actions, steps, delta_t)
-    new_config, new_momenta = integrate_om(new_config, new_momenta, actions, steps, -delta_t)
-    new_energy = momenta_energy(new_momenta)
-    for action in actions:
-        action.set_gauge_configuration(new_config)
-        new_energy += action.energy()
-    return new_energy - old_energy
+    """H after integrating forward by delta_t and back by -delta_t, minus H before
+    (hmc.py:249-278)."""
+    p0 = _fresh_momenta(config) if momenta is None else momenta
+    h0 = hamiltonian(config, p0, actions)
+    lv = steps[:len(actions)]
+    cfg1, p1 = run_schedule(config, p0, actions, schedule("omelyan", lv, delta_t))
+    cfg2, p2 = run_schedule(cfg1, p1, actions, schedule("omelyan", lv, -delta_t))
+    return hamiltonian(cfg2, p2, actions) - h0

@@ -89,7 +89,8 @@ class Lattice:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h is not None and _lib._lib is not None:
+        # at interpreter exit the module globals may already be gone
+        if h is not None and _lib is not None and getattr(_lib, "_lib", None) is not None:
             try:
                 torch.cuda.synchronize()
             except Exception:

@@ -113,7 +113,7 @@ def footprint_bytes(geometry, nc, nrhs, precision="f16", with_gauge=True, nshift
     nshift one-shift refinement groups."""
     vol = int(np.prod(geometry))
     nd = len(geometry)
-    ns = 2 if nd == 2 else 4
+    ns = 4 if nd == 4 else 2
     ncomp = ns * nc
     spin = vol * ncomp * 16
     if nshift:
