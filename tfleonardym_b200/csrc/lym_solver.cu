@@ -1410,11 +1410,13 @@ static int autotune(Work& w, cudaStream_t st, int forced_rhs, int forced_comp, i
   cudaEvent_t e0, e1;
   LYM_CUDA(cudaEventCreate(&e0));
   LYM_CUDA(cudaEventCreate(&e1));
-  // three interleaved rounds, best time per candidate: robust against a
-  // concurrent solve on another stream slowing one measurement down
+  // five interleaved rounds, median time per candidate: robust against a
+  // concurrent solve on another stream slowing a measurement down, and against
+  // one lucky round deciding between candidates a few per cent apart
+  constexpr int kRounds = 5;
+  float times[Work::kMaxCand][kRounds];
   float tbest[Work::kMaxCand];
-  for (float& t : tbest) t = 1e30f;
-  for (int round = 0; round < 3; ++round) {
+  for (int round = 0; round < kRounds; ++round) {
     for (int i = 0; i < w.ncand; ++i) {
       select_cand(w, i);
       w.ops.dslash(w, st);
@@ -1424,8 +1426,12 @@ static int autotune(Work& w, cudaStream_t st, int forced_rhs, int forced_comp, i
       cudaEventSynchronize(e1);
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
-      tbest[i] = std::min(tbest[i], ms);
+      times[i][round] = ms;
     }
+  }
+  for (int i = 0; i < w.ncand; ++i) {
+    std::sort(times[i], times[i] + kRounds);
+    tbest[i] = times[i][kRounds / 2];
   }
   int bi = 0;
   for (int i = 1; i < w.ncand; ++i)

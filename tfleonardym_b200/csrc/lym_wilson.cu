@@ -47,9 +47,73 @@ int scratch_get(Scratch** out) {
 // ---------------------------------------------------------------------------
 // full-lattice hop, reference layout
 // ---------------------------------------------------------------------------
-// One resident block per SM is declared enough, so ptxas keeps every
-// neighbour's loads in flight at once (memory-bound FP64 stencil).
-template <int ND, int NC, bool HERM>
+// One hop of the full-lattice operator for R vectors at one site: acc[r] +=
+// W (1 - s g_mu) psi_r(y), W = U (s = +1, forward) or U^dag (s = -1, backward);
+// the link is loaded once by the caller and applied to the R vectors.
+template <int ND, int NC, int R>
+LYM_D void full_hop(int mu, int s, const cx<double> (&u)[NC][NC], const double2* const (&psi)[R], int V, int y,
+                    cx<double> (&acc)[R][Gamma<ND>::NS][NC]) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if constexpr (ND == 3) {
+      cx<double> p0[NC], p1[NC], h[NC], t[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        p0[c] = ld(psi[r] + (size_t)c * V + y);
+        p1[c] = ld(psi[r] + (size_t)(NC + c) * V + y);
+      }
+      proj3<double, NC>(mu, s, p0, p1, h);
+#pragma unroll
+      for (int i = 0; i < NC; ++i) {
+        if (s > 0) {
+          t[i] = u[i][0] * h[0];
+#pragma unroll
+          for (int j = 1; j < NC; ++j) cmac(t[i], u[i][j], h[j]);
+        } else {
+          t[i] = cmul_cj(u[0][i], h[0]);
+#pragma unroll
+          for (int j = 1; j < NC; ++j) cmac_cj(t[i], u[j][i], h[j]);
+        }
+      }
+      recon3<double, NC>(mu, s, t, acc[r][0], acc[r][1]);
+    } else {
+#pragma unroll
+      for (int a = 0; a < Gamma<ND>::NS / 2; ++a) {
+        const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+        cx<double> h[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const cx<double> pb = mul_phase(ph, ld(psi[r] + (size_t)(jb * NC + c) * V + y));
+          const cx<double> pa = ld(psi[r] + (size_t)(a * NC + c) * V + y);
+          h[c] = s > 0 ? pa - pb : pa + pb;
+        }
+        // lower row: -s conj(g_a)
+        const int lph = s > 0 ? phase_neg(phase_conj(ph)) : phase_conj(ph);
+#pragma unroll
+        for (int i = 0; i < NC; ++i) {
+          cx<double> t;
+          if (s > 0) {
+            t = u[i][0] * h[0];
+#pragma unroll
+            for (int j = 1; j < NC; ++j) cmac(t, u[i][j], h[j]);
+          } else {
+            t = cmul_cj(u[0][i], h[0]);
+#pragma unroll
+            for (int j = 1; j < NC; ++j) cmac_cj(t, u[j][i], h[j]);
+          }
+          acc[r][a][i] += t;
+          acc[r][jb][i] += mul_phase(lph, t);
+        }
+      }
+    }
+  }
+}
+
+// One thread per site and R vectors (blockIdx.y selects the group of R): every
+// link is read once per group instead of once per vector.  One resident block per
+// SM is declared enough, so ptxas keeps every neighbour's loads in flight at once
+// (memory-bound FP64 stencil).
+template <int ND, int NC, bool HERM, int R>
 __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
     const int32_t* __restrict__ tab, int V, int Lt, double kappa, double bcr, double bci,
     const double2* __restrict__ U, const double2* __restrict__ in, double2* __restrict__ out) {
@@ -57,140 +121,84 @@ __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= V) return;
   const size_t vec = (size_t)NS * NC * V;
-  const double2* psi = in + blockIdx.y * vec;
-  double2* res = out + blockIdx.y * vec;
+  const double2* psi[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) psi[r] = in + ((size_t)blockIdx.y * R + r) * vec;
   const cx<double> bc{bcr, bci};
 
-  cx<double> acc[NS][NC];
+  cx<double> acc[R][NS][NC];
 #pragma unroll
-  for (int a = 0; a < NS; ++a)
+  for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int c = 0; c < NC; ++c) acc[a][c] = czero<double>();
+    for (int a = 0; a < NS; ++a)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[r][a][c] = czero<double>();
 
 #pragma unroll
   for (int mu = 0; mu < ND; ++mu) {
-    // forward: U_mu(x) (1 - g_mu) psi(x + mu)
-    {
-      const int y = tab[mu * V + s];
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      // forward: U_mu(x) (1 - g_mu) psi(x + mu); backward: U_mu(x - mu)^dag (1 + g_mu) psi(x - mu)
+      const bool fwd = dir == 0;
+      const int y = fwd ? tab[mu * V + s] : tab[ND * V + mu * V + s];
+      const int ls = fwd ? s : y;  // the link lives on x (forward) or x - mu (backward)
       cx<double> u[NC][NC];
 #pragma unroll
       for (int i = 0; i < NC; ++i)
 #pragma unroll
-        for (int j = 0; j < NC; ++j) u[i][j] = ld(U + ((size_t)(mu * NC + i) * NC + j) * V + s);
-      if (mu == ND - 1 && (s % Lt) == Lt - 1) {
+        for (int j = 0; j < NC; ++j) u[i][j] = ld(U + ((size_t)(mu * NC + i) * NC + j) * V + ls);
+      if (mu == ND - 1 && (s % Lt) == (fwd ? Lt - 1 : 0)) {
 #pragma unroll
         for (int i = 0; i < NC; ++i)
 #pragma unroll
           for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
       }
-      if constexpr (ND == 3) {
-        cx<double> p0[NC], p1[NC], h[NC], t[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          p0[c] = ld(psi + (size_t)c * V + y);
-          p1[c] = ld(psi + (size_t)(NC + c) * V + y);
-        }
-        proj3<double, NC>(mu, +1, p0, p1, h);
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-          t[i] = u[i][0] * h[0];
-#pragma unroll
-          for (int j = 1; j < NC; ++j) cmac(t[i], u[i][j], h[j]);
-        }
-        recon3<double, NC>(mu, +1, t, acc[0], acc[1]);
-      } else {
-#pragma unroll
-      for (int a = 0; a < NS / 2; ++a) {
-        const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
-        cx<double> h[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c)
-          h[c] = ld(psi + (size_t)(a * NC + c) * V + y) -
-                 mul_phase(ph, ld(psi + (size_t)(jb * NC + c) * V + y));
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-          cx<double> t = u[i][0] * h[0];
-#pragma unroll
-          for (int j = 1; j < NC; ++j) cmac(t, u[i][j], h[j]);
-          acc[a][i] += t;
-          acc[jb][i] += mul_phase(phase_neg(phase_conj(ph)), t);
-        }
-      }
-      }
-    }
-    // backward: U_mu(x - mu)^dag (1 + g_mu) psi(x - mu)
-    {
-      const int y = tab[ND * V + mu * V + s];
-      cx<double> u[NC][NC];
-#pragma unroll
-      for (int i = 0; i < NC; ++i)
-#pragma unroll
-        for (int j = 0; j < NC; ++j) u[i][j] = ld(U + ((size_t)(mu * NC + i) * NC + j) * V + y);
-      if (mu == ND - 1 && (s % Lt) == 0) {
-#pragma unroll
-        for (int i = 0; i < NC; ++i)
-#pragma unroll
-          for (int j = 0; j < NC; ++j) u[i][j] = bc * u[i][j];
-      }
-      if constexpr (ND == 3) {
-        cx<double> p0[NC], p1[NC], h[NC], t[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-          p0[c] = ld(psi + (size_t)c * V + y);
-          p1[c] = ld(psi + (size_t)(NC + c) * V + y);
-        }
-        proj3<double, NC>(mu, -1, p0, p1, h);
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-          t[i] = cmul_cj(u[0][i], h[0]);
-#pragma unroll
-          for (int j = 1; j < NC; ++j) cmac_cj(t[i], u[j][i], h[j]);
-        }
-        recon3<double, NC>(mu, -1, t, acc[0], acc[1]);
-      } else {
-#pragma unroll
-      for (int a = 0; a < NS / 2; ++a) {
-        const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
-        cx<double> h[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c)
-          h[c] = ld(psi + (size_t)(a * NC + c) * V + y) +
-                 mul_phase(ph, ld(psi + (size_t)(jb * NC + c) * V + y));
-#pragma unroll
-        for (int i = 0; i < NC; ++i) {
-          cx<double> t = cmul_cj(u[0][i], h[0]);
-#pragma unroll
-          for (int j = 1; j < NC; ++j) cmac_cj(t, u[j][i], h[j]);
-          acc[a][i] += t;
-          acc[jb][i] += mul_phase(phase_conj(ph), t);
-        }
-      }
-      }
+      full_hop<ND, NC, R>(mu, fwd ? 1 : -1, u, psi, V, y, acc);
     }
   }
 #pragma unroll
-  for (int a = 0; a < NS; ++a)
+  for (int r = 0; r < R; ++r) {
+    double2* res = out + ((size_t)blockIdx.y * R + r) * vec;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      cx<double> v = ld(psi + (size_t)(a * NC + c) * V + s) + kappa * acc[a][c];
-      if (HERM && a >= NS / 2) v = -v;
-      st(res + (size_t)(a * NC + c) * V + s, v);
-    }
+    for (int a = 0; a < NS; ++a)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        cx<double> v = ld(psi[r] + (size_t)(a * NC + c) * V + s) + kappa * acc[r][a][c];
+        if (HERM && a >= NS / 2) v = -v;
+        st(res + (size_t)(a * NC + c) * V + s, v);
+      }
+  }
 }
 
+template <int ND, int NC, int R>
+static void launch_full_r(const lym_lattice* lat, double kappa, int herm, double bcr, double bci, const void* gauge,
+                          int ngroups, const void* in, void* out, cudaStream_t st) {
+  dim3 grid(grid_for(lat->V, 128), ngroups);
+  const int Lt = lat->dims[ND - 1];
+  if (herm)
+    wilson_full_kernel<ND, NC, true, R><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
+                                                             (const double2*)gauge, (const double2*)in,
+                                                             (double2*)out);
+  else
+    wilson_full_kernel<ND, NC, false, R><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
+                                                              (const double2*)gauge, (const double2*)in,
+                                                              (double2*)out);
+}
+
+// nvec vectors: groups of 2 (4D, four-component spinors) or 4 (2D, 3D) vectors per
+// thread share the links (sized to the 255-register budget); a remainder runs one
+// vector per thread
 template <int ND, int NC>
 static int launch_full(const lym_lattice* lat, double kappa, int herm, double bcr, double bci,
                        const void* gauge, int nvec, const void* in, void* out, cudaStream_t st) {
-  dim3 grid(grid_for(lat->V, 128), nvec);
-  const int Lt = lat->dims[ND - 1];
-  if (herm)
-    wilson_full_kernel<ND, NC, true><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
-                                                          (const double2*)gauge, (const double2*)in,
-                                                          (double2*)out);
-  else
-    wilson_full_kernel<ND, NC, false><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
-                                                           (const double2*)gauge, (const double2*)in,
-                                                           (double2*)out);
+  constexpr int R = ND == 4 ? 2 : 4;
+  const size_t vec = (size_t)Gamma<ND>::NS * NC * lat->V * sizeof(double2);
+  const int ng = nvec / R;
+  if (ng > 0) launch_full_r<ND, NC, R>(lat, kappa, herm, bcr, bci, gauge, ng, in, out, st);
+  const int rest = nvec - ng * R;
+  if (rest > 0)
+    launch_full_r<ND, NC, 1>(lat, kappa, herm, bcr, bci, gauge, rest, (const char*)in + (size_t)ng * R * vec,
+                             (char*)out + (size_t)ng * R * vec, st);
   LYM_CHECK_LAUNCH();
   return LYM_OK;
 }
