@@ -109,21 +109,24 @@ LYM_D void full_hop(int mu, int s, const cx<double> (&u)[NC][NC], const double2*
   }
 }
 
-// One thread per site and R vectors (blockIdx.y selects the group of R): every
-// link is read once per group instead of once per vector.  One resident block per
-// SM is declared enough, so ptxas keeps every neighbour's loads in flight at once
-// (memory-bound FP64 stencil).
+// One thread per site and R vectors.  The grid is one-dimensional with the vector
+// group fastest (block b: group b % ngroups, site block b / ngroups), so the blocks
+// that read one site block's links run back to back and all but the first find the
+// links in L2: each link crosses HBM about once per launch, not once per vector.
+// One resident block per SM is declared enough, so ptxas keeps every neighbour's
+// loads in flight at once (memory-bound FP64 stencil).
 template <int ND, int NC, bool HERM, int R>
 __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
     const int32_t* __restrict__ tab, int V, int Lt, double kappa, double bcr, double bci,
-    const double2* __restrict__ U, const double2* __restrict__ in, double2* __restrict__ out) {
+    const double2* __restrict__ U, const double2* __restrict__ in, double2* __restrict__ out, int ngroups) {
   constexpr int NS = Gamma<ND>::NS;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int group = (int)(blockIdx.x % (unsigned)ngroups);
+  const int s = (int)(blockIdx.x / (unsigned)ngroups) * blockDim.x + threadIdx.x;
   if (s >= V) return;
   const size_t vec = (size_t)NS * NC * V;
   const double2* psi[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) psi[r] = in + ((size_t)blockIdx.y * R + r) * vec;
+  for (int r = 0; r < R; ++r) psi[r] = in + ((size_t)group * R + r) * vec;
   const cx<double> bc{bcr, bci};
 
   cx<double> acc[R][NS][NC];
@@ -158,7 +161,7 @@ __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
   }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    double2* res = out + ((size_t)blockIdx.y * R + r) * vec;
+    double2* res = out + ((size_t)group * R + r) * vec;
 #pragma unroll
     for (int a = 0; a < NS; ++a)
 #pragma unroll
@@ -173,32 +176,25 @@ __global__ void __launch_bounds__(128, 1) wilson_full_kernel(
 template <int ND, int NC, int R>
 static void launch_full_r(const lym_lattice* lat, double kappa, int herm, double bcr, double bci, const void* gauge,
                           int ngroups, const void* in, void* out, cudaStream_t st) {
-  dim3 grid(grid_for(lat->V, 128), ngroups);
+  const unsigned grid = grid_for(lat->V, 128) * (unsigned)ngroups;
   const int Lt = lat->dims[ND - 1];
   if (herm)
     wilson_full_kernel<ND, NC, true, R><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
                                                              (const double2*)gauge, (const double2*)in,
-                                                             (double2*)out);
+                                                             (double2*)out, ngroups);
   else
     wilson_full_kernel<ND, NC, false, R><<<grid, 128, 0, st>>>(lat->d_tab, (int)lat->V, Lt, kappa, bcr, bci,
                                                               (const double2*)gauge, (const double2*)in,
-                                                              (double2*)out);
+                                                              (double2*)out, ngroups);
 }
 
-// nvec vectors: groups of 2 (4D, four-component spinors) or 4 (2D, 3D) vectors per
-// thread share the links (sized to the 255-register budget); a remainder runs one
-// vector per thread
+// nvec vectors, one per thread (R = 1), the vectors of a site block in consecutive
+// blocks (their links shared through L2).  Measured at 32^4 SU(3): two vectors per
+// thread (links in registers) spill at the 255-register budget and gain no bandwidth.
 template <int ND, int NC>
 static int launch_full(const lym_lattice* lat, double kappa, int herm, double bcr, double bci,
                        const void* gauge, int nvec, const void* in, void* out, cudaStream_t st) {
-  constexpr int R = ND == 4 ? 2 : 4;
-  const size_t vec = (size_t)Gamma<ND>::NS * NC * lat->V * sizeof(double2);
-  const int ng = nvec / R;
-  if (ng > 0) launch_full_r<ND, NC, R>(lat, kappa, herm, bcr, bci, gauge, ng, in, out, st);
-  const int rest = nvec - ng * R;
-  if (rest > 0)
-    launch_full_r<ND, NC, 1>(lat, kappa, herm, bcr, bci, gauge, rest, (const char*)in + (size_t)ng * R * vec,
-                             (char*)out + (size_t)ng * R * vec, st);
+  launch_full_r<ND, NC, 1>(lat, kappa, herm, bcr, bci, gauge, nvec, in, out, st);
   LYM_CHECK_LAUNCH();
   return LYM_OK;
 }

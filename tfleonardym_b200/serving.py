@@ -164,6 +164,13 @@ class _Gauge:
         return op
 
 
+class _Done:
+    __slots__ = ("latency", "status")
+
+    def __init__(self, res):
+        self.latency, self.status = res.latency, res.status
+
+
 class SolveServer:
     def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
                  shifted_precision="f64", multi_lattice=1):
@@ -189,7 +196,9 @@ class SolveServer:
         self._in_use = 0
         self._gauges = collections.OrderedDict()
         self._closed = False
-        self.completed = []
+        # latency and status of finished requests (not the results: a result holds its
+        # solution tensor, which the caller owns and frees); bounded
+        self.completed = collections.deque(maxlen=1 << 18)
         if self.device is None and torch.cuda.is_available():
             self.device = torch.cuda.current_device()
         self._workers = [threading.Thread(target=self._run, args=(i,), daemon=True) for i in range(workers)]
@@ -437,7 +446,7 @@ class SolveServer:
                 r.t_end = t_end
                 res = SolveResult(r, xr, OK if ok else NOT_CONVERGED, mine)
                 res.batch_rhs = total_rhs
-                self.completed.append(res)
+                self.completed.append(_Done(res))
                 r.future.set_result(res)
 
     def _solve_batch(self, batch, widx=0):
@@ -454,7 +463,7 @@ class SolveServer:
             ok = all(m["true_residual"] <= first.tol for m in reps)
             res = SolveResult(first, first.out if first.out is not None else x, OK if ok else NOT_CONVERGED, reps)
             res.batch_rhs = 1
-            self.completed.append(res)
+            self.completed.append(_Done(res))
             first.future.set_result(res)
             return
         dev = torch.device("cuda", self.device)
@@ -489,5 +498,5 @@ class SolveServer:
             r.t_end = t_end
             res = SolveResult(r, xr, OK if ok else NOT_CONVERGED, mine)
             res.batch_rhs = batch_rhs
-            self.completed.append(res)
+            self.completed.append(_Done(res))
             r.future.set_result(res)
