@@ -103,6 +103,8 @@ def parse_args():
     ap.add_argument("--ms-switch", default="0",
                     help="FP64-head switch residuals of --multishift (0: the library default, <0: no head)")
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
+    ap.add_argument("--serve-max-queue", type=int, default=2000,
+                    help="solve server: requests that find this many queued are rejected (overload shedding)")
     ap.add_argument("--serve-multi", type=int, default=1,
                     help="solve server: batches on up to this many different gauge fields of one class run as one "
                          "multi-lattice solve (<= 1: each batch on its own)")
@@ -829,12 +831,13 @@ def _request_specs(rng, n, max_bytes=2 << 30):
     return specs
 
 
-def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=1):
+def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=1,
+           max_queue=None):
     import torch
 
     from tfleonardym_b200 import serving
     srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=dev.index,
-                              shifted_precision=shifted_precision, multi_lattice=multi_lattice)
+                              shifted_precision=shifted_precision, multi_lattice=multi_lattice, max_queue=max_queue)
     futs = []
     t0 = time.perf_counter()
     for sp, t in zip(specs, times):
@@ -843,15 +846,21 @@ def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_pre
             time.sleep(delay)
         nd, vol = len(sp["geometry"]), int(np.prod(sp["geometry"]))
         ns = 4 if nd == 4 else 2
-        g = torch.Generator(device=dev)
-        g.manual_seed(sp["src_seed"])
         shape = (sp["nrhs"], ns, sp["nc"], vol) if sp["shifts"] is None else (ns, sp["nc"], vol)
-        b = torch.complex(torch.randn(shape, generator=g, device=dev, dtype=torch.float64),
-                          torch.randn(shape, generator=g, device=dev, dtype=torch.float64)) / np.sqrt(2)
+
+        def source(shape=shape, seed=sp["src_seed"]):
+            # produced when the request runs, so that a backlog holds no source memory
+            g = torch.Generator(device=dev)
+            g.manual_seed(seed)
+            return torch.complex(torch.randn(shape, generator=g, device=dev, dtype=torch.float64),
+                                 torch.randn(shape, generator=g, device=dev, dtype=torch.float64)) / np.sqrt(2)
+
         gauge = (lambda s=sp: _device_links(s["geometry"], s["nc"], s["eps"], s["seed"], dev))
-        futs.append(srv.submit(serving.SolveRequest(sp["key"], sp["geometry"], sp["nc"], sp["kappa"], b, gauge=gauge,
-                                                    tol=sp["tol"], precision=precision, bc=-1.0, max_iter=4000,
-                                                    shifts=sp["shifts"])))
+        f = srv.submit(serving.SolveRequest(sp["key"], sp["geometry"], sp["nc"], sp["kappa"], source, gauge=gauge,
+                                            tol=sp["tol"], precision=precision, bc=-1.0, max_iter=4000,
+                                            shifts=sp["shifts"], nrhs=sp["nrhs"]))
+        f.add_done_callback(_drop_solution)
+        futs.append(f)
     res = [f.result() for f in futs]
     wall = time.perf_counter() - t0
     srv.close()
@@ -895,8 +904,10 @@ def run_serve_sweep(args, local_rank):
         specs = _request_specs(rng, len(times))
         if first is None:
             first = (specs, times)
-        r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget, shifted, args.serve_multi)
+        r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget, shifted, args.serve_multi,
+                   args.serve_max_queue)
         print(json.dumps({"serve_sweep": "mixed", "rate_per_s": rate, "workers": args.workers,
+                          "window_s": args.serve_seconds, "max_queue": args.serve_max_queue,
                           "max_batch_rhs": args.nrhs, "shifted_solver": args.serve_shifted,
                           "multi_lattice": args.serve_multi, **r}), flush=True)
     specs, times = first

@@ -63,6 +63,39 @@ def test_shifted_footprint_follows_the_solver():
     assert with_gauge == eo64 + 3 * link
 
 
+def test_overload_sheds_requests_beyond_the_queue_limit():
+    """With max_queue, a request that finds that many queued is rejected at once;
+    the queued ones are still served."""
+    srv = _FakeServer(hbm_budget_bytes=1 << 40, workers=1, max_queue=3)
+    futs = [srv.submit(_req("g", kappa=0.1 + 0.01 * k)) for k in range(12)]
+    res = [f.result(timeout=10) for f in futs]
+    srv.close()
+    rejected = [r for r in res if r.status == serving.REJECTED]
+    served = [r for r in res if r.status == serving.OK]
+    assert rejected and served and len(rejected) + len(served) == 12
+    assert all(r.latency < 1.0 for r in rejected)
+
+
+def test_callable_source_is_made_when_the_request_runs():
+    """A source given as a callable is produced by the worker (a backlog holds no
+    source memory) and released after the batch."""
+    made = []
+
+    def src():
+        made.append(time.perf_counter())
+        return torch.zeros((2, 4, 3, 256), dtype=torch.complex128)
+
+    r = serving.SolveRequest("g", (4, 4, 4, 4), 3, 0.12, src, nrhs=2)
+    assert r.nrhs == 2 and r.batched and not made
+    with pytest.raises(ValueError):
+        serving.SolveRequest("g", (4, 4, 4, 4), 3, 0.12, src)
+    assert r.source().shape == (2, 4, 3, 256) and len(made) == 1
+    r.source()
+    assert len(made) == 1
+    r.release_source()
+    assert r.b is None
+
+
 def test_rejects_requests_that_can_never_fit():
     srv = _FakeServer(hbm_budget_bytes=10_000, workers=1)
     f = srv.submit(_req("g", geom=(16, 16, 16, 16)))

@@ -44,13 +44,16 @@ class SolveRequest:
     (complex128 (nd, N, N, V) CUDA tensor or a zero-argument callable
     producing it) is only used when the key is not cached.  ``b`` is one
     spinor (ns, N, V) or several (k, ns, N, V) on the device (one spinor for a
-    shifted request; its solution is (nshift, ns, N, V)).
+    shifted request; its solution is (nshift, ns, N, V)), or a zero-argument
+    callable producing it when the request runs -- then ``nrhs`` gives the count
+    (k >= 1: a (k, ns, N, V) source; a shifted request's callable gives one
+    spinor) -- so that a queue of pending requests holds no source memory.
     """
 
     _ids = itertools.count()
 
     def __init__(self, gauge_key, geometry, nc, kappa, b, gauge=None, tol=1e-10, precision="f16",
-                 hermitian=False, bc=-1.0, max_iter=5000, out=None, shifts=None):
+                 hermitian=False, bc=-1.0, max_iter=5000, out=None, shifts=None, nrhs=None):
         self.id = next(self._ids)
         self.gauge_key = gauge_key
         self.geometry = tuple(int(g) for g in geometry)
@@ -64,7 +67,16 @@ class SolveRequest:
         self.bc = complex(bc)
         self.max_iter = int(max_iter)
         self.out = out  # optional tensor (e.g. pinned host memory) the solution is copied into
-        self.nrhs = 1 if b.dim() == 3 else int(b.shape[0])
+        if callable(b):
+            if nrhs is None:
+                raise ValueError("a source given as a callable needs nrhs")
+            self.nrhs = int(nrhs)
+            self.batched = shifts is None
+            self.on_device = True
+        else:
+            self.nrhs = 1 if b.dim() == 3 else int(b.shape[0])
+            self.batched = b.dim() == 4
+            self.on_device = b.is_cuda
         self.shifts = None if shifts is None else [float(s) for s in shifts]
         if self.shifts is not None:
             if self.nrhs != 1 or any(s < 0 for s in self.shifts):
@@ -73,6 +85,16 @@ class SolveRequest:
             self.precision = "f64"
         self.t_submit = self.t_admit = self.t_start = self.t_end = None
         self.future = concurrent.futures.Future()
+
+    def source(self):
+        """The source tensor (a callable source is produced here, once)."""
+        if callable(self.b):
+            self.b = self.b()
+        return self.b
+
+    def release_source(self):
+        """Drop the source once the request ran (a produced one is freed)."""
+        self.b = None
 
     @property
     def solves(self):
@@ -173,7 +195,7 @@ class _Done:
 
 class SolveServer:
     def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
-                 shifted_precision="f64", multi_lattice=1):
+                 shifted_precision="f64", multi_lattice=1, max_queue=None):
         self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
         # shifted requests: a precision = the even-odd multishift (lym_multishift_solve_eo) with that inner
         # precision (FP64 by default: the fastest for the mixed request streams measured); None = the
@@ -187,6 +209,9 @@ class SolveServer:
         # field's lym_gauge synchronises the device (all workers' streams).
         self.multi_lattice = int(multi_lattice)
         self.budget = int(hbm_budget_bytes)
+        # overload: a request that finds this many requests queued (admitted and waiting)
+        # is rejected at once instead of joining an ever longer queue (None: no limit)
+        self.max_queue = None if max_queue is None else int(max_queue)
         self.max_batch = int(max_batch)
         self.device = device  # CUDA device index; None: the caller's current device
         self.cache_size = int(gauge_cache)
@@ -216,6 +241,10 @@ class SolveServer:
         with self._lock:
             if self._closed:
                 raise RuntimeError("server closed")
+            if self.max_queue is not None and len(self._pending) + len(self._waiting) >= self.max_queue:
+                req.t_end = time.perf_counter()
+                req.future.set_result(SolveResult(req, None, REJECTED, []))
+                return req.future
             req._bytes = need
             if self._in_use + need <= self.budget and not self._waiting:
                 self._admit(req)
@@ -378,6 +407,8 @@ class SolveServer:
                     if not r.future.done():
                         r.future.set_exception(exc)
             finally:
+                for r in reqs:
+                    r.release_source()
                 self._release(reqs)
 
     def _solve_shifted(self, req, g, widx):
@@ -386,7 +417,8 @@ class SolveServer:
         reference-layout operator."""
         from . import _dev, dirac, dirac_solver
         dev = torch.device("cuda", self.device)
-        b = (req.b if req.b.dim() == 3 else req.b[0]).to(dev, non_blocking=True)
+        src = req.source()
+        b = (src if src.dim() == 3 else src[0]).to(dev, non_blocking=True)
         op = g.op_for(widx, req.kappa, True)
         ms = dirac_solver.multishift_cg(req.max_iter, req.tol, precision=self.shifted_precision, delta=0.01)
         xs = ms.solve(dirac.SquareOperator(op), b, req.shifts)
@@ -413,8 +445,8 @@ class SolveServer:
             for bt in batches:
                 gs.append(self._gauge_for(bt[0]))
             ops = [g.op_for(widx, bt[0].kappa, bt[0].hermitian) for g, bt in zip(gs, batches)]
-            bs = [torch.cat([(r.b if r.b.dim() == 4 else r.b[None]).to(dev, non_blocking=True) for r in bt])
-                  for bt in batches]
+            bs = [torch.cat([(r.source() if r.batched else r.source()[None]).to(dev, non_blocking=True)
+                             for r in bt]) for bt in batches]
             opts = {k: v for k, v in self.solver_options.items() if k in ("delta", "chunk")}
             xs, reps = dirac_solver.solve_lattices(ops, bs, precision=batches[0][0].precision,
                                                    max_steps=max(r.max_iter for bt in batches for r in bt),
@@ -424,9 +456,9 @@ class SolveServer:
                 k = 0
                 for r in bt:  # caller-provided outputs (pinned host buffers on the host path)
                     if r.out is not None:
-                        r.out.copy_(x[k:k + r.nrhs] if r.b.dim() == 4 else x[k], non_blocking=True)
+                        r.out.copy_(x[k:k + r.nrhs] if r.batched else x[k], non_blocking=True)
                     k += r.nrhs
-                if not bt[0].b.is_cuda and any(r.out is None for r in bt):
+                if not bt[0].on_device and any(r.out is None for r in bt):
                     x = x.to("cpu", non_blocking=True)
                 outs.append(x)
             torch.cuda.current_stream().synchronize()
@@ -440,7 +472,7 @@ class SolveServer:
             k = 0
             for r in bt:
                 mine = rp[k:k + r.nrhs]
-                xr = r.out if r.out is not None else (x[k:k + r.nrhs] if r.b.dim() == 4 else x[k])
+                xr = r.out if r.out is not None else (x[k:k + r.nrhs] if r.batched else x[k])
                 k += r.nrhs
                 ok = all(m["status"] == 0 and m["true_residual"] <= r.tol for m in mine)
                 r.t_end = t_end
@@ -467,10 +499,11 @@ class SolveServer:
             first.future.set_result(res)
             return
         dev = torch.device("cuda", self.device)
-        host = not first.b.is_cuda
+        host = not first.on_device
         try:
             # host sources (the reference-facing path) cross here, on this worker's stream
-            b = torch.cat([(r.b if r.b.dim() == 4 else r.b[None]).to(dev, non_blocking=True) for r in batch])
+            b = torch.cat([(r.source() if r.batched else r.source()[None]).to(dev, non_blocking=True)
+                           for r in batch])
             solver = dirac_solver.conjugate_gradient(max_steps=max(r.max_iter for r in batch), tol=first.tol,
                                                      precision=first.precision, **self.solver_options)
             op = g.op_for(widx, first.kappa, first.hermitian)
@@ -478,7 +511,7 @@ class SolveServer:
             k = 0
             for r in batch:  # caller-provided outputs (pinned host buffers on the host path)
                 if r.out is not None:
-                    r.out.copy_(x[k:k + r.nrhs] if r.b.dim() == 4 else x[k], non_blocking=True)
+                    r.out.copy_(x[k:k + r.nrhs] if r.batched else x[k], non_blocking=True)
                 k += r.nrhs
             if host and any(r.out is None for r in batch):
                 x = x.to("cpu", non_blocking=True)
@@ -492,7 +525,7 @@ class SolveServer:
         k = 0
         for r in batch:
             mine = reps[k:k + r.nrhs]
-            xr = r.out if r.out is not None else (x[k:k + r.nrhs] if r.b.dim() == 4 else x[k])
+            xr = r.out if r.out is not None else (x[k:k + r.nrhs] if r.batched else x[k])
             k += r.nrhs
             ok = all(m["status"] == 0 and m["true_residual"] <= r.tol for m in mine)
             r.t_end = t_end
