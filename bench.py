@@ -75,6 +75,7 @@ def parse_args():
                          "[10, 2], t = 1, even-odd CG at 1e-10): one JSON line, no solve timing")
     ap.add_argument("--trajectories", type=int, default=5)
     ap.add_argument("--hmc-inner", type=int, default=2, help="gauge steps per fermion step of the integrator")
+    ap.add_argument("--hmc-outer", type=int, default=10, help="fermion steps per trajectory of the integrator")
     ap.add_argument("--hmc-precision", default="f64", choices=["f64", "f32", "f16", "bf16"],
                     help="inner precision of the HMC's CG solves (f64: the plain FP64 method)")
     ap.add_argument("--serve-sweep", action="store_true",
@@ -925,8 +926,10 @@ def run_batch_lattices(args, local_rank):
     and FP64 outer iterations to true relative residual 1e-10; the same 256 solves
     with all lattices of one (D, N) class in the same launches
     (dirac_solver.solve_lattices, two calls).  Then the same 256
-    solves as plain FP64 one-at-a-time solves, and one gauge HMC step per lattice
-    (staples and force fused into the momentum update, then the link update).
+    solves as plain FP64 one-at-a-time solves, and one gauge HMC step on every lattice
+    (staples and force fused into the momentum update, then the link update): lattice
+    by lattice (128 launches), and all lattices together (lym_gauge_hmc_step_multi,
+    two launches).
     Device time of each phase by CUDA events around it (the server's streams are
     joined by a device synchronise)."""
     import torch
@@ -1031,6 +1034,14 @@ def run_batch_lattices(args, local_rank):
             hmc.update_link_field(c.gauge_field, p2, 0.05)
         e1.record(stream)
         torch.cuda.synchronize()
+    per_lattice_ms = e0.elapsed_time(e1)
+    betas = [5.6 if l["nc"] == 3 else 2.3 for l in lattices]
+    for rep in range(3):
+        e0.record(stream)
+        hmc.gauge_step_lattices(cfgs, moms, betas, -0.05, 0.05)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    two_launch_ms = e0.elapsed_time(e1)
     print(json.dumps({"batch_lattices": "64 uneven lattices x 4 rhs", "solves": 256, "ok": ok,
                       "worst_true_residual": worst, "wall_s": wall, "solves_per_s": 256 / wall,
                       "one_launch_per_class": {"what": "lym_wilson_solve_multi: the lattices of each (D, N) class "
@@ -1040,7 +1051,9 @@ def run_batch_lattices(args, local_rank):
                                                "kernel_launches": multi_launches},
                       "plain_fp64_one_at_a_time": {"ok": sum(r.status == serving.OK for r in plain),
                                                    "wall_s": plain_wall, "solves_per_s": 256 / plain_wall},
-                      "gauge_hmc_step_all_lattices_ms": e0.elapsed_time(e1),
+                      "gauge_hmc_step_all_lattices_ms": {"per_lattice_two_launches_each": per_lattice_ms,
+                                                         "all_lattices_two_launches":
+                                                         two_launch_ms},
                       "config": {"lattices": "22 x 2D SU(2) 8^2..64^2 + 21 x 3D SU(2) 8^3..16^3 + "
                                                  "21 x 4D SU(3) 8^4..12^3x24",
                                  "inner_precision": "f32", "outer_precision": "f64", "tol": 1e-10,
@@ -1241,7 +1254,7 @@ def run_hmc(args, rank, world, local_rank):
     """HMC on 4D SU(3) 16^4: beta = 5.6, Nf = 2 Wilson fermions at kappa = 0.13
     (pseudofermion phi = Q eta, Q = gamma_d D, antiperiodic time), links
     reunit(exp(i 0.25 H)) to start, Gaussian su(3) momenta, Omelyan nested
-    integrator with 10 outer (fermion) steps and ``--hmc-inner`` (default 2)
+    integrator with ``--hmc-outer`` (default 10) outer (fermion) steps and ``--hmc-inner`` (default 2)
     inner (gauge) steps per outer step, trajectory length 1, force and energy solves (Q^2)^-1 phi by two
     even-odd CG solves of Q at 1e-10 true relative residual.  One warm-up
     trajectory, then ``--trajectories`` timed with CUDA events; the value is
@@ -1272,7 +1285,7 @@ def run_hmc(args, rank, world, local_rank):
     gen = torch.Generator(device=dev)
     gen.manual_seed(2026 + rank)
     rng = np.random.default_rng(2026 + rank)
-    steps = [10, args.hmc_inner]
+    steps = [args.hmc_outer, args.hmc_inner]
     stream = torch.cuda.current_stream()
     records = []
     clocks = None

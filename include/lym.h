@@ -288,6 +288,18 @@ int lym_update_momenta(int64_t n, void* momenta, const void* force, double eps, 
 int lym_update_links(int nd, int nc, int64_t volume, void* gauge, const void* momenta,
                      double eps, int reunitarize, void* stream);
 
+/* The gauge part of an HMC step on nlat independent lattices (each its own lattice
+ * object, N, beta, links gauges[l] and momenta momenta[l], reference layout) in two
+ * launches whatever their sizes and (nd, N): momenta += eps_p * F_gauge(U) for every
+ * link of every lattice (gauge_action.py:13-24 + hmc.py:59-61), then U <- exp(eps_u P) U
+ * (hmc.py:40-43).  No reference counterpart (the reference runs one lattice per
+ * process); the same arithmetic as lym_gauge_force into the momenta followed by
+ * lym_update_links.  nlat <= 256; no buffer may belong to two lattices
+ * (LYM_ERR_BAD_ARG). */
+int lym_gauge_hmc_step_multi(int nlat, const lym_lattice* const* lats, const int* nc, const double* betas,
+                             void* const* gauges, void* const* momenta, double eps_p, double eps_u,
+                             void* stream);
+
 /* out = X (X^dag X)^{-1/2} / det^{1/N} per link (smearing.py:17-31). */
 int lym_unitary_projection(int nd, int nc, int64_t volume, const void* in, void* out, void* stream);
 

@@ -834,3 +834,56 @@ def test_random_momenta_kernel(cuda_device, nc):
     n = w.shape[-1]
     assert np.abs(w.mean(-1)).max() < 5 / np.sqrt(n)
     assert np.abs(w.var(-1) - 1.0).max() < 6 * np.sqrt(2.0 / n)
+
+
+def test_gauge_hmc_step_on_many_lattices_in_two_launches(cuda_device):
+    """lym_gauge_hmc_step_multi over a mix of 2D SU(2), 3D SU(2), 4D SU(2) and 4D SU(3)
+    lattices equals, lattice by lattice, the fused force-into-momenta kernel followed
+    by the link update (1e-13)."""
+    from tfleonardym_b200 import gauge_action, hmc
+    from tfleonardym_b200 import lattice as lt
+    specs = [((8, 6), 2, 2.3), ((4, 6, 4), 2, 2.0), ((4, 4, 2, 6), 2, 2.3), ((2, 4, 4, 6), 3, 5.6),
+             ((10, 12), 2, 3.0), ((4, 4, 4, 4), 3, 5.8)]
+    rng = np.random.default_rng(9)
+    cfgs, moms, ref_u, ref_p = [], [], [], []
+    for geom, nc, beta in specs:
+        nd, vol = len(geom), int(np.prod(geom))
+        u = O.unitary_sqrt_projection(rng.normal(size=(nd, nc, nc, vol)) + 1j * rng.normal(size=(nd, nc, nc, vol)))
+        p = np_(hmc.random_momenta(nc, nd, vol))
+        cfg = lt.Configuration(cu(u), geom, nc, nd)
+        pr = cu(p)
+        gauge_action.yang_mills(cfg, beta).force_into_momenta(pr, -0.07)
+        ref_p.append(np_(pr))
+        ref_u.append(np_(hmc.update_link_field(cu(u), pr, 0.05)))
+        cfgs.append(lt.Configuration(cu(u), geom, nc, nd))
+        moms.append(cu(p))
+    hmc.gauge_step_lattices(cfgs, moms, [b for _, _, b in specs], -0.07, 0.05)
+    for k in range(len(specs)):
+        assert relerr(np_(moms[k]), ref_p[k]) < 1e-13, k
+        assert relerr(np_(cfgs[k].gauge_field), ref_u[k]) < 1e-13, k
+
+
+def test_md_energy_violation_is_second_order(cuda_device):
+    """Nf = 2 Wilson + Wilson gauge action on 2x4x4x6 SU(3), Omelyan [n, 1], t = 1, the same
+    momenta and pseudofermions for every n: the energy violation of the second-order
+    integrator (hmc.py:104-162) falls by four when the step halves -- the molecular
+    dynamics integrates the Hamiltonian whose energy the Metropolis step measures."""
+    from tfleonardym_b200 import dirac, dirac_solver, fermion_action, gauge_action, hmc
+    dirac_solver.VERBOSE = False
+    g = load_golden("d4")
+    spec = GOLDEN_CASES["d4"]
+    q = make_op(g, spec)
+    solver = dirac_solver.multishift_solver(5000, 1e-24)
+    ra = dirac.RationalApproximation(dirac.SquareOperator(q), [1.0], [0.0], 0, solver)
+    nf = fermion_action.n_flavor([ra], [ra], [q], solver, q)
+    dhs = []
+    for n in (4, 8, 16):
+        cfg = make_cfg(g["gauge"], spec["geometry"])
+        nf.set_gauge_configuration(cfg)
+        nf.initialize_pseudofermions([cu(g["eta"])])
+        ym = gauge_action.yang_mills(cfg, spec["beta"])
+        _, minus_dh, _ = hmc.hybrid_mc(cfg, [nf, ym], [n, 1], 1.0, momenta=cu(g["momenta"]), uniform=1.0)
+        dhs.append(abs(minus_dh))
+    assert dhs[0] > dhs[1] > dhs[2] > 0, dhs
+    for a, b in zip(dhs, dhs[1:]):
+        assert 3.0 < a / b < 5.5, dhs

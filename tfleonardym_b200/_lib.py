@@ -80,6 +80,8 @@ SIGNATURES = {
     "lym_staples": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
     "lym_staple_terms": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
     "lym_momenta_from_normals": (c_int, [c_int, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
+    "lym_gauge_hmc_step_multi": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_double,
+                                         c_double, c_void_p]),
     "lym_plaquette_sum": (c_int, [c_void_p, c_int, c_void_p, P(c_double), c_void_p]),
     "lym_momenta_energy": (c_int, [c_int, c_int, c_int64, c_void_p, P(c_double), c_void_p]),
     "lym_update_momenta": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p]),

@@ -81,6 +81,25 @@ __global__ void __launch_bounds__(128) staple_terms_kernel(const int32_t* __rest
   }
 }
 
+// F = -beta/(4N) (W^dag - W) - trace/N, W = U S^dag at one link (gauge_action.py:42-53)
+template <int ND, int NC>
+LYM_D Mat<NC> gauge_force_link(const int32_t* __restrict__ tab, int64_t V, const double2* __restrict__ U,
+                               double beta, int mu, int64_t s) {
+  Mat<NC> S = staple_sum<ND, NC>(tab, V, U, mu, s, -1);
+  Mat<NC> W = mul_nd(load_link<NC>(U, mu, s, V), S);
+  const double c = -0.25 * beta / NC;
+  Mat<NC> F;
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) F.m[i][j] = c * (conj(W.m[j][i]) - W.m[i][j]);
+  cx<double> tr = trace(F);
+  tr = (1.0 / NC) * tr;
+#pragma unroll
+  for (int i = 0; i < NC; ++i) F.m[i][i] -= tr;
+  return F;
+}
+
 // F = -beta/(4N) (W^dag - W) - trace/N, W = U S^dag (gauge_action.py:42-53).
 // With mom != null: mom += eps F instead of storing F (hmc.py:59-61).
 template <int ND, int NC>
@@ -483,6 +502,82 @@ __global__ void __launch_bounds__(128) fermion_force_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// The gauge part of an HMC step on many lattices at once (builder-defined: the
+// reference runs one lattice per process, hmc.py:218-246): momenta P += eps_p F(U)
+// for every link of every lattice in one launch, then U <- exp(eps_u P) U in a
+// second (the force reads neighbouring links, so all forces come first).  The
+// lattices' descriptors travel as the kernel parameter; every lattice owns a
+// contiguous range of blocks (nd x its site blocks) and a block finds its lattice
+// by binary search over the range starts.  Any mix of (nd, N) in one launch.
+// ---------------------------------------------------------------------------
+struct HmcLat {
+  const int32_t* tab;
+  double2* U;
+  double2* P;
+  int64_t V;
+  double beta;
+  int nd, nc;
+  int b0;  // first block of this lattice
+};
+constexpr int kHmcMaxLat = 256;
+struct HmcTable {
+  int n;
+  double eps;
+  HmcLat l[kHmcMaxLat];
+};
+
+LYM_D int hmc_lat_of(const HmcTable& t, int b) {
+  int lo = 0, hi = t.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (t.l[mid].b0 <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int ND, int NC>
+LYM_D void hmc_kick_link(const HmcLat& L, double eps, int mu, int64_t s) {
+  const Mat<NC> F = gauge_force_link<ND, NC>(L.tab, L.V, L.U, L.beta, mu, s);
+  Mat<NC> P = load_link<NC>(L.P, mu, s, L.V);
+#pragma unroll
+  for (int i = 0; i < NC; ++i)
+#pragma unroll
+    for (int j = 0; j < NC; ++j) P.m[i][j] += eps * F.m[i][j];
+  store_link<NC>(L.P, mu, s, L.V, P);
+}
+
+template <int NC>
+LYM_D void hmc_drift_link(const HmcLat& L, double eps, int mu, int64_t s) {
+  const Mat<NC> e = expm(mscale(cx<double>{eps, 0.0}, load_link<NC>(L.P, mu, s, L.V)));
+  store_link<NC>(L.U, mu, s, L.V, mul(e, load_link<NC>(L.U, mu, s, L.V)));
+}
+
+// kick = 1: momenta from the force; 0: links from the momenta
+__global__ void __launch_bounds__(128) hmc_multi_kernel(const __grid_constant__ HmcTable t, int kick) {
+  const HmcLat& L = t.l[hmc_lat_of(t, blockIdx.x)];
+  const int64_t nb = (L.V + 127) / 128;
+  const int64_t lb = blockIdx.x - L.b0;
+  const int mu = (int)(lb / nb);
+  const int64_t s = (lb - mu * nb) * 128 + threadIdx.x;
+  if (s >= L.V) return;
+  if (kick) {
+    switch (L.nd * 10 + L.nc) {
+      case 22: hmc_kick_link<2, 2>(L, t.eps, mu, s); break;
+      case 23: hmc_kick_link<2, 3>(L, t.eps, mu, s); break;
+      case 32: hmc_kick_link<3, 2>(L, t.eps, mu, s); break;
+      case 33: hmc_kick_link<3, 3>(L, t.eps, mu, s); break;
+      case 42: hmc_kick_link<4, 2>(L, t.eps, mu, s); break;
+      default: hmc_kick_link<4, 3>(L, t.eps, mu, s); break;
+    }
+  } else if (L.nc == 2) {
+    hmc_drift_link<2>(L, t.eps, mu, s);
+  } else {
+    hmc_drift_link<3>(L, t.eps, mu, s);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
 #define LYM_DISPATCH_ND_NC(nd, nc, CALL)                                              \
@@ -603,6 +698,38 @@ int lym_update_momenta(int64_t n, void* momenta, const void* force, double eps, 
   if (n == 0) return LYM_OK;
   axpy_real_kernel<<<reduction_blocks(n, 256) * 4, 256, 0, (cudaStream_t)stream>>>(n, (double2*)momenta,
                                                                                      (const double2*)force, eps);
+  LYM_CHECK_LAUNCH();
+  return LYM_OK;
+}
+
+int lym_gauge_hmc_step_multi(int nlat, const lym_lattice* const* lats, const int* nc, const double* betas,
+                             void* const* gauges, void* const* momenta, double eps_p, double eps_u, void* stream) {
+  LYM_REQUIRE(nlat >= 1 && nlat <= kHmcMaxLat, LYM_ERR_BAD_ARG, "nlat must be in [1, %d]", kHmcMaxLat);
+  LYM_REQUIRE(lats && nc && betas && gauges && momenta, LYM_ERR_BAD_ARG, "null argument");
+  HmcTable t;
+  t.n = nlat;
+  int64_t blocks = 0;
+  for (int l = 0; l < nlat; ++l) {
+    LYM_REQUIRE(lats[l] && gauges[l] && momenta[l], LYM_ERR_BAD_ARG, "null argument (lattice %d)", l);
+    LYM_REQUIRE(nc[l] == 2 || nc[l] == 3, LYM_ERR_UNSUPPORTED, "N must be 2 or 3 (lattice %d)", l);
+    LYM_REQUIRE(lats[l]->nd >= 2 && lats[l]->nd <= 4, LYM_ERR_UNSUPPORTED, "nd must be 2, 3 or 4 (lattice %d)", l);
+    LYM_REQUIRE(lats[l]->V >= 1, LYM_ERR_BAD_ARG, "empty lattice %d", l);
+    LYM_REQUIRE(gauges[l] != momenta[l], LYM_ERR_BAD_ARG, "gauge and momenta alias (lattice %d)", l);
+    for (int k = 0; k < l; ++k)  // two lattices on one buffer would race in the same launch
+      LYM_REQUIRE(gauges[k] != gauges[l] && momenta[k] != momenta[l] && gauges[k] != momenta[l] &&
+                      momenta[k] != gauges[l],
+                  LYM_ERR_BAD_ARG, "lattices %d and %d share a buffer", k, l);
+    t.l[l] = HmcLat{lats[l]->d_tab, (double2*)gauges[l], (double2*)momenta[l], lats[l]->V, betas[l], lats[l]->nd,
+                    nc[l], (int)blocks};
+    blocks += (int64_t)lats[l]->nd * ((lats[l]->V + 127) / 128);
+  }
+  LYM_REQUIRE(blocks < (int64_t(1) << 31), LYM_ERR_UNSUPPORTED, "too many links for one launch");
+  cudaStream_t st = (cudaStream_t)stream;
+  t.eps = eps_p;
+  hmc_multi_kernel<<<(unsigned)blocks, 128, 0, st>>>(t, 1);
+  LYM_CHECK_LAUNCH();
+  t.eps = eps_u;
+  hmc_multi_kernel<<<(unsigned)blocks, 128, 0, st>>>(t, 0);
   LYM_CHECK_LAUNCH();
   return LYM_OK;
 }

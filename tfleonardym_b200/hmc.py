@@ -119,6 +119,26 @@ def generate_random_vector(nc=3, spinor_dimension=4, representation="fundamental
     return torch.complex(re, im)
 
 
+def gauge_step_lattices(configs, momenta, betas, eps_p, eps_u):
+    """The gauge part of one HMC step on many independent lattices at once (any mix of
+    dimension, N and size; builder-defined: the reference runs one lattice per process):
+    momenta[l] += eps_p * F_gauge(configs[l]) for every lattice, then every link
+    U <- exp(eps_u P) U, in two launches (lym_gauge_hmc_step_multi).  Updates the
+    momenta tensors and the configurations' gauge fields in place."""
+    n = len(configs)
+    if n != len(momenta) or n != len(betas):
+        raise ValueError("one momenta tensor and one beta per configuration")
+    us = [_dev.as_c128(c.gauge_field, "gauge_field") for c in configs]
+    ps = [_dev.as_c128(p, "momenta") for p in momenta]
+    lats = (ctypes.c_void_p * n)(*[lt.get_lattice(tuple(c.geometry)).handle.value for c in configs])
+    ncs = (ctypes.c_int * n)(*[int(u.shape[1]) for u in us])
+    bs = (ctypes.c_double * n)(*[float(b) for b in betas])
+    up = (ctypes.c_void_p * n)(*[u.data_ptr() for u in us])
+    pp = (ctypes.c_void_p * n)(*[p.data_ptr() for p in ps])
+    _lib.check(_lib.lib().lym_gauge_hmc_step_multi(n, lats, ncs, bs, up, pp, float(eps_p), float(eps_u),
+                                                   _dev.stream()), "lym_gauge_hmc_step_multi")
+
+
 # ---------------------------------------------------------------------------
 # Molecular dynamics as a flat schedule
 #
