@@ -106,6 +106,9 @@ def parse_args():
     ap.add_argument("--serve-rates", default="20,100,400", help="request rates (per second) of --serve-sweep")
     ap.add_argument("--serve-max-queue", type=int, default=2000,
                     help="solve server: requests that find this many queued are rejected (overload shedding)")
+    ap.add_argument("--serve-max-wait", type=float, default=1.0,
+                    help="solve server: requests whose expected wait exceeds this many seconds are rejected "
+                         "(overload shedding by latency; <= 0: no limit)")
     ap.add_argument("--serve-multi", type=int, default=1,
                     help="solve server: batches on up to this many different gauge fields of one class run as one "
                          "multi-lattice solve (<= 1: each batch on its own)")
@@ -833,12 +836,13 @@ def _request_specs(rng, n, max_bytes=2 << 30):
 
 
 def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=1,
-           max_queue=None):
+           max_queue=None, max_wait_s=None):
     import torch
 
     from tfleonardym_b200 import serving
     srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=dev.index,
-                              shifted_precision=shifted_precision, multi_lattice=multi_lattice, max_queue=max_queue)
+                              shifted_precision=shifted_precision, multi_lattice=multi_lattice, max_queue=max_queue,
+                              max_wait_s=max_wait_s)
     futs = []
     t0 = time.perf_counter()
     for sp, t in zip(specs, times):
@@ -905,10 +909,12 @@ def run_serve_sweep(args, local_rank):
         specs = _request_specs(rng, len(times))
         if first is None:
             first = (specs, times)
+        max_wait = args.serve_max_wait if args.serve_max_wait > 0 else None
         r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget, shifted, args.serve_multi,
-                   args.serve_max_queue)
+                   args.serve_max_queue, max_wait)
         print(json.dumps({"serve_sweep": "mixed", "rate_per_s": rate, "workers": args.workers,
                           "window_s": args.serve_seconds, "max_queue": args.serve_max_queue,
+                          "max_wait_s": max_wait,
                           "max_batch_rhs": args.nrhs, "shifted_solver": args.serve_shifted,
                           "multi_lattice": args.serve_multi, **r}), flush=True)
     specs, times = first

@@ -76,6 +76,26 @@ def test_overload_sheds_requests_beyond_the_queue_limit():
     assert all(r.latency < 1.0 for r in rejected)
 
 
+def test_overload_sheds_requests_whose_expected_wait_is_too_long():
+    """With max_wait_s, once the completion rate is known a request whose expected
+    wait (queued requests over that rate) exceeds the limit is rejected at once, so
+    the served requests' latency stays near the limit however fast requests arrive."""
+    srv = _FakeServer(hbm_budget_bytes=1 << 40, workers=1, max_wait_s=0.2)  # ~50 requests/s served
+    futs = []
+    for k in range(120):  # ~200 requests/s offered
+        futs.append(srv.submit(_req("g", kappa=0.1 + 0.001 * k)))
+        time.sleep(0.005)
+    res = [f.result(timeout=30) for f in futs]
+    rate = srv.drain_rate()
+    srv.close()
+    rejected = [r for r in res if r.status == serving.REJECTED]
+    served = [r for r in res if r.status == serving.OK]
+    assert len(rejected) > 40 and len(served) > 20
+    assert rate is None or rate > 10
+    assert all(r.latency < 0.05 for r in rejected)
+    assert max(r.latency for r in served) < 1.0
+
+
 def test_callable_source_is_made_when_the_request_runs():
     """A source given as a callable is produced by the worker (a backlog holds no
     source memory) and released after the batch."""

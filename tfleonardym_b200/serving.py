@@ -4,7 +4,10 @@ Requests of different geometry, N, kappa, tolerance, precision and shift count
 arrive at any time (``submit`` returns a future).  Each request is admitted by its HBM
 footprint against a byte budget: a request that could never fit is rejected
 (status REJECTED); one that fits but finds the budget in use waits in the
-queue and is admitted as earlier requests finish and free their bytes.
+queue and is admitted as earlier requests finish and free their bytes.  Under
+overload, a request is rejected at once when it finds ``max_queue`` requests
+queued, or when its expected wait (the queue over the measured completion rate)
+exceeds ``max_wait_s``.
 Gauge fields stay resident in an LRU cache keyed by the caller's gauge key,
 so repeated requests on the same configuration skip the upload.
 
@@ -195,7 +198,7 @@ class _Done:
 
 class SolveServer:
     def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
-                 shifted_precision="f64", multi_lattice=1, max_queue=None):
+                 shifted_precision="f64", multi_lattice=1, max_queue=None, max_wait_s=None):
         self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
         # shifted requests: a precision = the even-odd multishift (lym_multishift_solve_eo) with that inner
         # precision (FP64 by default: the fastest for the mixed request streams measured); None = the
@@ -212,6 +215,12 @@ class SolveServer:
         # overload: a request that finds this many requests queued (admitted and waiting)
         # is rejected at once instead of joining an ever longer queue (None: no limit)
         self.max_queue = None if max_queue is None else int(max_queue)
+        # overload, by latency: a request whose expected wait -- the requests queued ahead
+        # of it over the rate at which requests completed in the last RATE_WINDOW_S -- is
+        # above max_wait_s is rejected at once (None: no limit)
+        self.max_wait_s = None if max_wait_s is None else float(max_wait_s)
+        self._done = collections.deque()  # (time, requests) of recent completions
+        self._done_n = 0
         self.max_batch = int(max_batch)
         self.device = device  # CUDA device index; None: the caller's current device
         self.cache_size = int(gauge_cache)
@@ -241,7 +250,8 @@ class SolveServer:
         with self._lock:
             if self._closed:
                 raise RuntimeError("server closed")
-            if self.max_queue is not None and len(self._pending) + len(self._waiting) >= self.max_queue:
+            queued = len(self._pending) + len(self._waiting)
+            if (self.max_queue is not None and queued >= self.max_queue) or self._wait_too_long(queued):
                 req.t_end = time.perf_counter()
                 req.future.set_result(SolveResult(req, None, REJECTED, []))
                 return req.future
@@ -281,8 +291,31 @@ class SolveServer:
         req.t_admit = time.perf_counter()
         self._pending.append(req)
 
+    RATE_WINDOW_S = 2.0
+
+    def drain_rate(self):
+        """Requests completed per second over the last RATE_WINDOW_S (None before two
+        completions fall in the window)."""
+        with self._lock:
+            return self._drain_rate(time.perf_counter())
+
+    def _drain_rate(self, now):
+        while self._done and now - self._done[0][0] > self.RATE_WINDOW_S:
+            self._done_n -= self._done.popleft()[1]
+        if len(self._done) < 2 or now <= self._done[0][0]:
+            return None
+        return (self._done_n - self._done[0][1]) / (now - self._done[0][0])
+
+    def _wait_too_long(self, queued):
+        if self.max_wait_s is None or not queued:
+            return False
+        rate = self._drain_rate(time.perf_counter())
+        return rate is not None and (queued + 1) > rate * self.max_wait_s
+
     def _release(self, reqs):
         with self._lock:
+            self._done.append((time.perf_counter(), len(reqs)))
+            self._done_n += len(reqs)
             for r in reqs:
                 self._in_use -= r._bytes
             while self._waiting and self._in_use + self._waiting[0]._bytes <= self.budget:
