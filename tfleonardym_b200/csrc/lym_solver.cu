@@ -461,11 +461,11 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_t_kernel(EoGeom g,
   cg_t_body<ND, NC, SP, GP, COMP, R, MX>(g, hg, s, p, t, k2, st, partials, counters, nblk, blockIdx.x, blockIdx.y);
 }
 
-// Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr   (rhs tile of R)
-template <int ND, int NC, int SP, int GP, bool COMP, int XP, int R, int MX>
-LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s, const EoField& t, const EoField& p,
-                          const EoField& x, const EoField& r, double k2, CGState* st, double* partials,
-                          unsigned* counters, int nblk, int bx, int by) {
+// Ap = t - kappa^2 gamma_d H_eo s ; r -= alpha Ap ; beta = |r|^2 / rr   (rhs tile of R).
+// x += alpha p runs in cg_p, which reads p anyway.
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
+LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s, const EoField& t, const EoField& r,
+                          double k2, CGState* st, double* partials, unsigned* counters, int nblk, int bx, int by) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC;
   __shared__ double sh[R * 32];
   const int i = bx * blockDim.x + threadIdx.x;
@@ -479,7 +479,6 @@ LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s,
   }
   if (!any) return;  // uniform per block
   using RT = typename Prec<SP>::real;
-  using XR = typename Prec<XP>::real;
   double n[R];
 #pragma unroll
   for (int q = 0; q < R; ++q) n[q] = 0.0;
@@ -492,14 +491,10 @@ LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s,
     for (int q = 0; q < R; ++q) {
       const int m = q, cb = i;
       if (!act[q]) continue;
-      const double alpha = st[rhs0 + q].alpha;
-      cx<RT> tv[NCOMP], pv[NCOMP], rv[NCOMP];
-      cx<XR> xv[NCOMP];
+      cx<RT> tv[NCOMP], rv[NCOMP];
       load_sp<SP, NCOMP>(t, rhs0 + q, cb, tv);
-      load_sp<SP, NCOMP>(p, rhs0 + q, cb, pv);
       load_sp<SP, NCOMP>(r, rhs0 + q, cb, rv);
-      load_sp<XP, NCOMP>(x, rhs0 + q, cb, xv);
-      const RT a = (RT)alpha;
+      const RT a = (RT)st[rhs0 + q].alpha;
 #pragma unroll
       for (int sp = 0; sp < NS; ++sp)
 #pragma unroll
@@ -509,11 +504,9 @@ LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s,
           if (ND != 3 && sp >= NS / 2) h = -h;
           cx<RT> ap = tv[k] - (RT)k2 * h;
           rv[k] -= a * ap;
-          xv[k] += (XR)alpha * cx<XR>{(XR)pv[k].re, (XR)pv[k].im};
           n[q] += (double)rv[k].re * rv[k].re + (double)rv[k].im * rv[k].im;
         }
       store_sp<SP, NCOMP>(r, rhs0 + q, cb, rv);
-      store_sp<XP, NCOMP>(x, rhs0 + q, cb, xv);
     }
   }
   if (grid_sum_n<R>(n, partials + (int64_t)by * nblk * R, counters + by, sh, bx, nblk) && threadIdx.x == 0) {
@@ -530,12 +523,13 @@ LYM_D void cg_update_body(const EoGeom& g, const HopGauge& hg, const EoField& s,
   }
 }
 
-template <int ND, int NC, int SP, int GP, bool COMP, int XP, int R, int MX>
-__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_update_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
-                                                        EoField x, EoField r, double k2, CGState* st,
-                                                        double* partials, unsigned* counters, int nblk) {
-  cg_update_body<ND, NC, SP, GP, COMP, XP, R, MX>(g, hg, s, t, p, x, r, k2, st, partials, counters, nblk, blockIdx.x,
-                                                  blockIdx.y);
+template <int ND, int NC, int SP, int GP, bool COMP, int R, int MX>
+__global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cg_update_kernel(EoGeom g, HopGauge hg, EoField s, EoField t,
+                                                                           EoField r, double k2, CGState* st,
+                                                                           double* partials, unsigned* counters,
+                                                                           int nblk) {
+  cg_update_body<ND, NC, SP, GP, COMP, R, MX>(g, hg, s, t, r, k2, st, partials, counters, nblk, blockIdx.x,
+                                              blockIdx.y);
 }
 
 // Reliable-update residual in the sloppy precision: r = t - kappa^2 gamma_d H_eo s
@@ -609,23 +603,32 @@ __global__ void __launch_bounds__(128) copy_sp_kernel(int64_t Vh, EoField src, E
   store_sp<SP, NCOMP>(dst, rhs, cb, v);
 }
 
-// p = r + beta p; the last block of each rhs to finish then turns the "stop
-// after the p update" marker (active == 2) into a pause.  Every block of the rhs
-// read `active` before it counted itself, so the last one may change it.
-template <int SP, int NCOMP>
-LYM_D void cg_p_body(int64_t Vh, const EoField& r, const EoField& p, CGState* st, unsigned* counters, int bx, int rhs,
-                     int nblk) {
+// x += alpha p (x in the accumulator precision XP), then p = r + beta p; the
+// last block of each rhs to finish then turns the "stop after the p update"
+// marker (active == 2) into a pause.  Every block of the rhs read `active`
+// before it counted itself, so the last one may change it.
+template <int SP, int XP, int NCOMP>
+LYM_D void cg_p_body(int64_t Vh, const EoField& r, const EoField& p, const EoField& x, CGState* st,
+                     unsigned* counters, int bx, int rhs, int nblk) {
   const int64_t cb = bx * (int64_t)blockDim.x + threadIdx.x;
   const int act = st[rhs].active;
   if (!act) return;  // uniform per rhs
   if (cb < Vh) {
     using R = typename Prec<SP>::real;
+    using XR = typename Prec<XP>::real;
     const R b = (R)st[rhs].beta;
+    const XR alpha = (XR)st[rhs].alpha;
     cx<R> rv[NCOMP], pv[NCOMP];
+    cx<XR> xv[NCOMP];
     load_sp<SP, NCOMP>(r, rhs, cb, rv);
     load_sp<SP, NCOMP>(p, rhs, cb, pv);
+    load_sp<XP, NCOMP>(x, rhs, cb, xv);
 #pragma unroll
-    for (int k = 0; k < NCOMP; ++k) pv[k] = rv[k] + b * pv[k];
+    for (int k = 0; k < NCOMP; ++k) {
+      xv[k] += alpha * cx<XR>{(XR)pv[k].re, (XR)pv[k].im};
+      pv[k] = rv[k] + b * pv[k];
+    }
+    store_sp<XP, NCOMP>(x, rhs, cb, xv);
     store_sp<SP, NCOMP>(p, rhs, cb, pv);
   }
   __syncthreads();
@@ -638,10 +641,10 @@ LYM_D void cg_p_body(int64_t Vh, const EoField& r, const EoField& p, CGState* st
   }
 }
 
-template <int SP, int NCOMP>
-__global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoField p, CGState* st,
+template <int SP, int XP, int NCOMP>
+__global__ void __launch_bounds__(128) cg_p_kernel(int64_t Vh, EoField r, EoField p, EoField x, CGState* st,
                                                    unsigned* counters) {
-  cg_p_body<SP, NCOMP>(Vh, r, p, st, counters, blockIdx.x, blockIdx.y, gridDim.x);
+  cg_p_body<SP, XP, NCOMP>(Vh, r, p, x, st, counters, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -717,10 +720,10 @@ __global__ void __launch_bounds__(tc::kThreads) cg_t_tc_kernel(EoGeom g, HopGaug
   }
 }
 
-// Ap = t - kappa^2 gamma_d H_eo s ; x += alpha p ; r -= alpha Ap ; beta = |r|^2 / rr
-__global__ void __launch_bounds__(tc::kThreads) cg_update_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t, EoField p,
-                                                           EoField x, EoField r, double k2, CGState* st,
-                                                           double* partials, unsigned* counters, int nblk) {
+// Ap = t - kappa^2 gamma_d H_eo s ; r -= alpha Ap ; beta = |r|^2 / rr (x += alpha p in cg_p)
+__global__ void __launch_bounds__(tc::kThreads) cg_update_tc_kernel(EoGeom g, HopGauge hg, EoField s, EoField t,
+                                                                   EoField r, double k2, CGState* st,
+                                                                   double* partials, unsigned* counters, int nblk) {
   extern __shared__ __align__(16) char smem[];
   constexpr int S = tc::kS, RG = tc::kRG, NCOMP = 12;
   const int i = threadIdx.x % S, q = threadIdx.x / S, rhs = blockIdx.y * RG + q;
@@ -731,13 +734,10 @@ __global__ void __launch_bounds__(tc::kThreads) cg_update_tc_kernel(EoGeom g, Ho
   tc::hop_tc<false>(g, hg, s, 0, blockIdx.x * S, blockIdx.y * RG, i, q, act, smem, acc);
   double n = 0.0;
   if (act && cb < g.Vh) {
-    const double alpha = st[rhs].alpha;
-    cx<float> tv[NCOMP], pv[NCOMP], rv[NCOMP], xv[NCOMP];
+    cx<float> tv[NCOMP], rv[NCOMP];
     load_sp<SP16, NCOMP>(t, rhs, cb, tv);
-    load_sp<SP16, NCOMP>(p, rhs, cb, pv);
     load_sp<SP16, NCOMP>(r, rhs, cb, rv);
-    load_sp<SP32, NCOMP>(x, rhs, cb, xv);
-    const float a = (float)alpha;
+    const float a = (float)st[rhs].alpha;
 #pragma unroll
     for (int sp = 0; sp < 4; ++sp)
 #pragma unroll
@@ -747,11 +747,9 @@ __global__ void __launch_bounds__(tc::kThreads) cg_update_tc_kernel(EoGeom g, Ho
         if (sp >= 2) h = -h;
         const cx<float> ap = tv[k] - (float)k2 * h;
         rv[k] -= a * ap;
-        xv[k] += (float)alpha * pv[k];
         n += (double)rv[k].re * rv[k].re + (double)rv[k].im * rv[k].im;
       }
     store_sp<SP16, NCOMP>(r, rhs, cb, rv);
-    store_sp<SP32, NCOMP>(x, rhs, cb, xv);
   }
   double tot = 0.0;
   if (tc::grid_rhs_sum(n, tc_red(smem), partials, counters, nblk, tot) && threadIdx.x < RG) {
@@ -906,9 +904,9 @@ struct Impl {
            w.st, w.partials, w.counters, w.nblk);
     launch(w, st, cg_hop_kernel<ND, NC, SP, GP, COMP, true, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.t, w.s, 1,
            cst);
-    launch(w, st, cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.s, w.t,
-           w.p, w.xs, w.r, k2, w.st, w.partials, w.counters, w.nblk);
-    launch(w, st, cg_p_kernel<SP, NCOMP>, grid, dim3(128), w.Vh, w.r, w.p, w.st, w.counters);
+    launch(w, st, cg_update_kernel<ND, NC, SP, GP, COMP, R, MX>, tile, dim3(128), w.g->geom, w.hgs, w.s, w.t, w.r,
+           k2, w.st, w.partials, w.counters, w.nblk);
+    launch(w, st, cg_p_kernel<SP, XP, NCOMP>, grid, dim3(128), w.Vh, w.r, w.p, w.xs, w.st, w.counters);
   }
 
   static void hop64(Work& w, int par, const EoField& in, const EoField& out, const EoField& z0, const EoField& z1,
@@ -984,8 +982,8 @@ struct Impl {
     cudaFuncGetAttributes(&a, cg_hop_kernel<ND, NC, SP, GP, COMP, false, R, MX>);
     cudaFuncGetAttributes(&a, cg_hop_kernel<ND, NC, SP, GP, COMP, true, R, MX>);
     cudaFuncGetAttributes(&a, cg_t_kernel<ND, NC, SP, GP, COMP, R, MX>);
-    cudaFuncGetAttributes(&a, cg_update_kernel<ND, NC, SP, GP, COMP, XP, R, MX>);
-    cudaFuncGetAttributes(&a, cg_p_kernel<SP, NCOMP>);
+    cudaFuncGetAttributes(&a, cg_update_kernel<ND, NC, SP, GP, COMP, R, MX>);
+    cudaFuncGetAttributes(&a, cg_p_kernel<SP, XP, NCOMP>);
   }
 
   static CgOps table() {
@@ -1019,9 +1017,9 @@ struct ImplTC {
     launch_smem(w, st, cg_t_tc_kernel, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.s, w.p, w.t, k2, w.st,
                 w.partials_tc, w.counters, nb);
     launch_smem(w, st, cg_hop_tc_kernel<true>, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.t, w.s, 1, cst);
-    launch_smem(w, st, cg_update_tc_kernel, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.s, w.t, w.p, w.xs,
-                w.r, k2, w.st, w.partials_tc, w.counters, nb);
-    launch(w, st, cg_p_kernel<SP16, 12>, grid, dim3(128), w.Vh, w.r, w.p, w.st, w.counters);
+    launch_smem(w, st, cg_update_tc_kernel, tile, dim3(tc::kThreads), P::kBytes, w.g->geom, w.hgs, w.s, w.t, w.r, k2,
+                w.st, w.partials_tc, w.counters, nb);
+    launch(w, st, cg_p_kernel<SP16, SP32, 12>, grid, dim3(128), w.Vh, w.r, w.p, w.xs, w.st, w.counters);
   }
   static void dslash(Work& w, cudaStream_t st) {
     prepare();
@@ -1691,19 +1689,19 @@ __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cgm_t_kernel(const Cg
                                          by);
 }
 
-template <int ND, int NC, int SP, int GP, bool COMP, int XP, int MX>
+template <int ND, int NC, int SP, int GP, bool COMP, int MX>
 __global__ void __launch_bounds__(128, SP == SP64 ? 1 : 0) cgm_update_kernel(const CgLat* __restrict__ lats, int n) {
   const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
   const int local = blockIdx.x - D.b0, by = local / D.nblk, bx = local - by * D.nblk;
-  cg_update_body<ND, NC, SP, GP, COMP, XP, 1, MX>(D.g, D.hg, D.s, D.t, D.p, D.xs, D.r, D.k2, D.st, D.partials,
-                                                  D.counters, D.nblk, bx, by);
+  cg_update_body<ND, NC, SP, GP, COMP, 1, MX>(D.g, D.hg, D.s, D.t, D.r, D.k2, D.st, D.partials, D.counters, D.nblk,
+                                              bx, by);
 }
 
-template <int SP, int NCOMP>
+template <int SP, int XP, int NCOMP>
 __global__ void __launch_bounds__(128) cgm_p_kernel(const CgLat* __restrict__ lats, int n) {
   const CgLat& D = lats[cg_lat_of(lats, n, blockIdx.x)];
   const int local = blockIdx.x - D.b0, rhs = local / D.nblk, bx = local - rhs * D.nblk;
-  cg_p_body<SP, NCOMP>(D.Vh, D.r, D.p, D.st, D.counters, bx, rhs, D.nblk);
+  cg_p_body<SP, XP, NCOMP>(D.Vh, D.r, D.p, D.xs, D.st, D.counters, bx, rhs, D.nblk);
 }
 
 // The FP64 reliable update of every lattice (the rhs with upd set), as
@@ -1775,8 +1773,8 @@ struct MultiImpl {
     launch_rec(rec, st, cgm_hop_kernel<ND, NC, SP, GP, COMP, false, MX>, grid, blk, lats, n);
     launch_rec(rec, st, cgm_t_kernel<ND, NC, SP, GP, COMP, MX>, grid, blk, lats, n);
     launch_rec(rec, st, cgm_hop_kernel<ND, NC, SP, GP, COMP, true, MX>, grid, blk, lats, n);
-    launch_rec(rec, st, cgm_update_kernel<ND, NC, SP, GP, COMP, XP, MX>, grid, blk, lats, n);
-    launch_rec(rec, st, cgm_p_kernel<SP, NCOMP>, grid, blk, lats, n);
+    launch_rec(rec, st, cgm_update_kernel<ND, NC, SP, GP, COMP, MX>, grid, blk, lats, n);
+    launch_rec(rec, st, cgm_p_kernel<SP, XP, NCOMP>, grid, blk, lats, n);
   }
   static void q_part(cudaStream_t st, const CgLat* lats, int n, int blocks) {
     if constexpr (SP != SP64) cgm_accumulate_kernel<XP, NCOMP><<<blocks, 128, 0, st>>>(lats, n);
@@ -1793,8 +1791,8 @@ struct MultiImpl {
     cudaFuncGetAttributes(&a, cgm_hop_kernel<ND, NC, SP, GP, COMP, false, MX>);
     cudaFuncGetAttributes(&a, cgm_t_kernel<ND, NC, SP, GP, COMP, MX>);
     cudaFuncGetAttributes(&a, cgm_hop_kernel<ND, NC, SP, GP, COMP, true, MX>);
-    cudaFuncGetAttributes(&a, cgm_update_kernel<ND, NC, SP, GP, COMP, XP, MX>);
-    cudaFuncGetAttributes(&a, cgm_p_kernel<SP, NCOMP>);
+    cudaFuncGetAttributes(&a, cgm_update_kernel<ND, NC, SP, GP, COMP, MX>);
+    cudaFuncGetAttributes(&a, cgm_p_kernel<SP, XP, NCOMP>);
   }
   static MultiOps table() { return MultiOps{&iterate, &q_part, &r_part, &preload}; }
 };

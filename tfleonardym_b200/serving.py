@@ -216,11 +216,16 @@ class SolveServer:
         # is rejected at once instead of joining an ever longer queue (None: no limit)
         self.max_queue = None if max_queue is None else int(max_queue)
         # overload, by latency: a request whose expected wait -- the requests queued ahead
-        # of it over the rate at which requests completed in the last RATE_WINDOW_S -- is
-        # above max_wait_s is rejected at once (None: no limit)
+        # of it over the server's service rate -- is above max_wait_s is rejected at once
+        # (None: no limit).  The service rate is the requests completed in the last
+        # RATE_WINDOW_S per second of worker time spent on them (batch wall time over the
+        # worker count), so that a lightly loaded server is credited with the rate it
+        # could sustain, not with the arrival rate it happens to see.
         self.max_wait_s = None if max_wait_s is None else float(max_wait_s)
-        self._done = collections.deque()  # (time, requests) of recent completions
+        self._done = collections.deque()  # (time, requests, busy seconds) of recent batches
         self._done_n = 0
+        self._done_busy = 0.0
+        self._nworkers = max(1, int(workers))
         self.max_batch = int(max_batch)
         self.device = device  # CUDA device index; None: the caller's current device
         self.cache_size = int(gauge_cache)
@@ -294,17 +299,19 @@ class SolveServer:
     RATE_WINDOW_S = 2.0
 
     def drain_rate(self):
-        """Requests completed per second over the last RATE_WINDOW_S (None before two
-        completions fall in the window)."""
+        """Requests served per second of the workers' time, over the batches that
+        finished in the last RATE_WINDOW_S (None before two batches fall in the window)."""
         with self._lock:
             return self._drain_rate(time.perf_counter())
 
     def _drain_rate(self, now):
         while self._done and now - self._done[0][0] > self.RATE_WINDOW_S:
-            self._done_n -= self._done.popleft()[1]
-        if len(self._done) < 2 or now <= self._done[0][0]:
+            _, n, busy = self._done.popleft()
+            self._done_n -= n
+            self._done_busy -= busy
+        if len(self._done) < 2 or self._done_busy <= 0.0:
             return None
-        return (self._done_n - self._done[0][1]) / (now - self._done[0][0])
+        return self._done_n * self._nworkers / self._done_busy
 
     def _wait_too_long(self, queued):
         if self.max_wait_s is None or not queued:
@@ -312,10 +319,17 @@ class SolveServer:
         rate = self._drain_rate(time.perf_counter())
         return rate is not None and (queued + 1) > rate * self.max_wait_s
 
-    def _release(self, reqs):
+    def _release(self, reqs, busy_s=None):
+        """Frees the requests' bytes and admits waiting ones; busy_s: the worker time of
+        the batch (default: from the requests' start and end times)."""
+        if busy_s is None:
+            ends = [r.t_end for r in reqs if getattr(r, "t_end", None) is not None]
+            starts = [r.t_start for r in reqs if getattr(r, "t_start", None) is not None]
+            busy_s = max(ends) - min(starts) if ends and starts else 0.0
         with self._lock:
-            self._done.append((time.perf_counter(), len(reqs)))
+            self._done.append((time.perf_counter(), len(reqs), max(0.0, float(busy_s))))
             self._done_n += len(reqs)
+            self._done_busy += max(0.0, float(busy_s))
             for r in reqs:
                 self._in_use -= r._bytes
             while self._waiting and self._in_use + self._waiting[0]._bytes <= self.budget:
@@ -442,7 +456,7 @@ class SolveServer:
             finally:
                 for r in reqs:
                     r.release_source()
-                self._release(reqs)
+                self._release(reqs, time.perf_counter() - t0)
 
     def _solve_shifted(self, req, g, widx):
         """(Q^2 + sigma_k) x_k = b by multishift CG (the server's shifted_precision
