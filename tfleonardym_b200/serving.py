@@ -217,10 +217,12 @@ class SolveServer:
         self.max_queue = None if max_queue is None else int(max_queue)
         # overload, by latency: a request whose expected wait -- the requests queued ahead
         # of it over the server's service rate -- is above max_wait_s is rejected at once
-        # (None: no limit).  The service rate is the requests completed in the last
-        # RATE_WINDOW_S per second of worker time spent on them (batch wall time over the
-        # worker count), so that a lightly loaded server is credited with the rate it
-        # could sustain, not with the arrival rate it happens to see.
+        # (None: no limit).  The service rate is the larger of the requests completed per
+        # second over the last RATE_WINDOW_S and the requests completed per second of
+        # worker time spent on them (batch wall time over the worker count): a lightly
+        # loaded server is credited with the rate it could sustain, not with the arrival
+        # rate it happens to see.  Fewer than RATE_MIN_REQUESTS completions in the window
+        # give no estimate (and no rejection).
         self.max_wait_s = None if max_wait_s is None else float(max_wait_s)
         self._done = collections.deque()  # (time, requests, busy seconds) of recent batches
         self._done_n = 0
@@ -297,10 +299,11 @@ class SolveServer:
         self._pending.append(req)
 
     RATE_WINDOW_S = 2.0
+    RATE_MIN_REQUESTS = 8
 
     def drain_rate(self):
-        """Requests served per second of the workers' time, over the batches that
-        finished in the last RATE_WINDOW_S (None before two batches fall in the window)."""
+        """The service rate the expected wait is judged by (requests per second; None
+        while fewer than RATE_MIN_REQUESTS requests finished in the last RATE_WINDOW_S)."""
         with self._lock:
             return self._drain_rate(time.perf_counter())
 
@@ -309,9 +312,12 @@ class SolveServer:
             _, n, busy = self._done.popleft()
             self._done_n -= n
             self._done_busy -= busy
-        if len(self._done) < 2 or self._done_busy <= 0.0:
+        if self._done_n < self.RATE_MIN_REQUESTS or len(self._done) < 2:
             return None
-        return self._done_n * self._nworkers / self._done_busy
+        span = now - self._done[0][0]
+        by_time = (self._done_n - self._done[0][1]) / span if span > 0.0 else 0.0
+        by_work = self._done_n * self._nworkers / self._done_busy if self._done_busy > 0.0 else 0.0
+        return max(by_time, by_work) or None
 
     def _wait_too_long(self, queued):
         if self.max_wait_s is None or not queued:
