@@ -283,6 +283,12 @@ class DiracWilsonOperator(Operator):
             _lib.lib().lym_gauge_destroy(self._solver_gauge)
         self._solver_gauge = None
 
+    def release(self):
+        """Frees the solver's device objects (lym_gauge, workspaces, graphs) now, on the
+        calling thread; the next solve builds them again."""
+        self._free_solver_gauge()
+        self._solver_gauge_key = None
+
     def __del__(self):
         try:
             self._free_solver_gauge()

@@ -28,6 +28,7 @@ batch that served the request.
 import collections
 import concurrent.futures
 import itertools
+import queue
 import threading
 import time
 
@@ -188,6 +189,11 @@ class _Gauge:
         op.hermitian = hermitian
         return op
 
+    def release(self):
+        for op in self.ops.values():
+            op.release()
+        self.ops.clear()
+
 
 class _Done:
     __slots__ = ("latency", "status")
@@ -242,6 +248,12 @@ class SolveServer:
         self.completed = collections.deque(maxlen=1 << 18)
         if self.device is None and torch.cuda.is_available():
             self.device = torch.cuda.current_device()
+        # evicted gauge fields are destroyed on a thread of their own: releasing a
+        # lym_gauge synchronises the device, which would otherwise stall the worker that
+        # evicted it until every other worker's batch on the GPU had finished
+        self._reap_q = queue.SimpleQueue()
+        self._reaper = threading.Thread(target=self._reap, daemon=True)
+        self._reaper.start()
         self._workers = [threading.Thread(target=self._run, args=(i,), daemon=True) for i in range(workers)]
         for t in self._workers:
             t.start()
@@ -277,7 +289,20 @@ class SolveServer:
         if wait:
             for t in self._workers:
                 t.join()
+        self._reap_q.put(None)
+        if wait:
+            self._reaper.join()
         self._gauges.clear()
+
+    def _reap(self):
+        if self.device is not None and torch.cuda.is_available():
+            torch.cuda.set_device(self.device)
+        while True:
+            item = self._reap_q.get()
+            if item is None:
+                return
+            for g in item:
+                g.release()
 
     def stats(self):
         lat = [r.latency for r in self.completed if r.status != REJECTED]
@@ -428,10 +453,8 @@ class SolveServer:
                 if self._gauges[k].users:
                     break
                 evicted.append(self._gauges.pop(k))
-        # the evicted fields' operators release their lym_gauge objects here, outside the
-        # server lock: lym_gauge_destroy synchronises the device, which must not hold up
-        # the other workers' batch selection
-        evicted.clear()
+        if evicted:
+            self._reap_q.put(evicted)  # destroyed on the reaper thread, not on this worker
         return g
 
     def _run(self, widx):
