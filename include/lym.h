@@ -160,7 +160,9 @@ typedef struct lym_solver_params {
                         converted values; 1 = half spinor in FP16, U h through f16 x f16 + f32
                         FMAs; 2 = the tensor-core hop (4D SU(3), nrhs a multiple of 16, with
                         rhs_per_thread = 16): projected FP16 half spinors x FP16 links on
-                        mma.sync with FP32 accumulation, 8 sites x 16 rhs per CTA */
+                        mma.sync with FP32 accumulation, 8 sites x 16 rhs per CTA; 3 = the
+                        colour contraction of each direction in packed FP16 FMAs (half2),
+                        accumulated over directions in FP32 (rhs_per_thread = 1) */
   double switch_residual; /* lym_multishift_solve_eo with a reduced inner precision: the
                         iterations run in FP64 until the true relative residual of the
                         smallest shift is below this, then in the inner precision
@@ -176,7 +178,8 @@ typedef struct lym_solver_report {
   int rhs_per_thread;    /* right-hand sides per thread the autotuner picked for the hop kernels
                             (the tensor-core hop: right-hand sides per CTA, 16) */
   int compressed_links;  /* 1: the hop kernels read the N-1-row sloppy links, 0: full links */
-  int mixed_fma;         /* 1: the hop kernels ran the mixed-precision FP16 form; 2: the tensor-core form */
+  int mixed_fma;         /* 1: the hop kernels ran the mixed-precision FP16 form; 2: the tensor-core
+                            form; 3: the packed-half form */
 } lym_solver_report;
 
 /* Solve D x_i = b_i (or Q x_i = b_i) for nrhs right-hand sides stored back to

@@ -470,6 +470,76 @@ def test_eo_cg_tensor_core_hop(cuda_device, geometry, nrhs):
         assert abs(its - base) <= max(3, base // 10), (herm, its, base)
 
 
+@pytest.mark.parametrize("geometry,nc", [((8, 8, 8, 16), 3), ((4, 6, 4, 8), 2), ((16, 12), 3)])
+def test_eo_cg_packed_half_hop(cuda_device, geometry, nc):
+    """The packed-half FP16 hop (colour contraction of each direction in half2 FMAs,
+    FP32 over the directions; mixed_fma = 3) meets the oracle's true residual for every
+    rhs, with the iteration count of the mixed-precision hop within 10 %."""
+    from tfleonardym_b200 import boundary_conditions as bcs
+    from tfleonardym_b200 import dirac, dirac_solver
+    from tfleonardym_b200 import lattice as lt
+    u = _smooth_links(geometry, nc, seed=sum(geometry) + nc)
+    kappa = 0.12
+    tables = O.lookup_tables(geometry)
+    ub = O.apply_time_bc(u, O.antiperiodic_field(geometry))
+    cfg = lt.Configuration(cu(u), tuple(geometry), nc, len(geometry))
+    ns = 4 if len(geometry) == 4 else 2
+    nrhs = 8
+    rng = np.random.default_rng(nc)
+    b = rng.normal(size=(nrhs, ns, nc, u.shape[-1])) + 1j * rng.normal(size=(nrhs, ns, nc, u.shape[-1]))
+    for herm in (False, True):
+        op = dirac.DiracWilsonOperator(cfg, kappa, herm, representation="fundamental",
+                                       boundary_condition_provider=bcs.time_antiperiodic_provider(-1))
+        ref = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=1, mixed_fma=1)
+        ref.solve(op, cu(b))
+        assert ref.reports[0]["mixed_fma"] == 1
+        base = max(r["iterations"] for r in ref.reports)
+        h2 = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=1, mixed_fma=3)
+        x = np_(h2.solve(op, cu(b)))
+        rep = h2.reports[0]
+        assert rep["mixed_fma"] == 3 and rep["rhs_per_thread"] == 1 and rep["compressed_links"] == 0, rep
+        for i in range(nrhs):
+            res = np.linalg.norm(b[i] - O.wilson_apply(ub, x[i], kappa, herm, tables)) / np.linalg.norm(b[i])
+            assert res < 1e-10, (herm, i, res, h2.reports[i])
+        its = max(r["iterations"] for r in h2.reports)
+        assert abs(its - base) <= max(3, base // 10), (herm, its, base)
+
+
+def test_eo_cg_workspace_reused_across_batch_sizes(cuda_device):
+    """Batches of 5, then 3, then 8 and 1 right-hand sides share workspaces by capacity
+    (8, 8, 8, 1): every answer meets the oracle's true residual and equals the answer
+    of a solve of that right-hand side alone (the smaller batch's unused slots are
+    cleared, so nothing of the earlier sources leaks in)."""
+    from tfleonardym_b200 import boundary_conditions as bcs
+    from tfleonardym_b200 import dirac, dirac_solver
+    from tfleonardym_b200 import lattice as lt
+    geometry, nc, kappa = (4, 4, 4, 8), 3, 0.12
+    u = _smooth_links(geometry, nc, seed=77)
+    tables = O.lookup_tables(geometry)
+    ub = O.apply_time_bc(u, O.antiperiodic_field(geometry))
+    cfg = lt.Configuration(cu(u), tuple(geometry), nc, len(geometry))
+    op = dirac.DiracWilsonOperator(cfg, kappa, False, representation="fundamental",
+                                   boundary_condition_provider=bcs.time_antiperiodic_provider(-1))
+    rng = np.random.default_rng(5)
+    b = rng.normal(size=(17, 4, nc, u.shape[-1])) + 1j * rng.normal(size=(17, 4, nc, u.shape[-1]))
+    for precision in ("f64", "f16"):
+        solver = dirac_solver.conjugate_gradient(tol=1e-10, precision=precision, delta=0.01)
+        alone = dirac_solver.conjugate_gradient(tol=1e-10, precision=precision, delta=0.01)
+        start = 0
+        for n in (5, 3, 8, 1):
+            x = np_(solver.solve(op, cu(b[start:start + n])))
+            if x.ndim == 3:
+                x = x[None]
+            assert len(solver.reports) == n
+            for i in range(n):
+                bi = b[start + i]
+                res = np.linalg.norm(bi - O.wilson_apply(ub, x[i], kappa, False, tables)) / np.linalg.norm(bi)
+                assert res < 1e-10, (precision, n, i, res)
+                xa = np_(alone.solve(op, cu(bi)))
+                assert np.linalg.norm(x[i] - xa) / np.linalg.norm(xa) < 1e-9, (precision, n, i)
+            start += n
+
+
 def test_eo_cg_batch_equals_single(cuda_device):
     """A right-hand side gives the same answer alone and inside a batch."""
     from tfleonardym_b200 import dirac_solver

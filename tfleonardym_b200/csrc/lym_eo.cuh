@@ -631,16 +631,106 @@ LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, i
   }
 }
 
+// --- FP16 hop with packed half arithmetic ---------------------------------------
+// As hop_tile_mx, but the colour contraction t = U h of each direction runs on packed
+// FP16 pairs: t = sum_j (u_re, u_re) * (h_re, h_im) + (u_im, u_im) * hs_j with
+// hs = (-h_im, h_re) for U and (h_im, -h_re) for U^dag, two fused half FMAs per
+// complex term (__hfma2, one rounding each) and no value converted on its own.  Each
+// t (at most |U| |h| <= 6 in magnitude: links unitary, stored spinors scaled to
+// |component| <= 1) is converted to FP32 once and accumulated over the directions in
+// FP32 with the neighbour's norm, as in hop_tile_mx.  Against hop_tile_mx the added
+// rounding is that of the three-term sums (about 2^-11 relative each).
+template <int ND, int NC, bool G5IN, int R>
+LYM_D void hop_tile_h2(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
+                       const int (&act)[R], cx<float> (&acc)[R][Gamma<ND>::NS][NC]) {
+  constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC, NU = units_for(NCOMP, 4);
+  constexpr int NCX = NC * NC, NLU = units_for(NCX, 2);
+  const int vh = (int)g.Vh;
+  const int* nb = g.nbr + par * 2 * ND * vh + cb;
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int a = 0; a < NS; ++a)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[r][a][c] = czero<float>();
+  // hs = swap(h) * (-1, 1) for U, swap(h) * (1, -1) for U^dag
+  const __half2 sw_f = __halves2half2(__float2half_rn(-1.f), __float2half_rn(1.f));
+  const __half2 sw_b = __halves2half2(__float2half_rn(1.f), __float2half_rn(-1.f));
+#pragma unroll
+  for (int mu = 0; mu < ND; ++mu) {
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      const bool fwd = dir == 0;
+      const int code = __ldg(nb + (2 * mu + dir) * vh);
+      const int ncb = code & 0x7fffffff;
+      const uint2* lp = reinterpret_cast<const uint2*>(hg.data) +
+                        (size_t)((mu * 2 + (fwd ? par : 1 - par)) * hg.nunits) * vh + (fwd ? cb : ncb);
+      __half2 u[NCX];
+#pragma unroll
+      for (int k = 0; k < NLU; ++k) {
+        const uint2 t = __ldg(lp + k * vh);
+        u[2 * k] = as_h2(t.x);
+        if (2 * k + 1 < NCX) u[2 * k + 1] = as_h2(t.y);
+      }
+      const bool s2pos = fwd != G5IN;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!act[r]) continue;
+        uint4 raw[NU];
+        const float nrm = load_sp_units<SP16, NCOMP>(in, rhs0 + r, ncb, raw);
+        const float nnrm = -nrm;
+        __half2 psi[NCOMP];
+#pragma unroll
+        for (int k = 0; k < NU; ++k) {
+          const unsigned w[4] = {raw[k].x, raw[k].y, raw[k].z, raw[k].w};
+#pragma unroll
+          for (int m = 0; m < 4; ++m)
+            if (4 * k + m < NCOMP) psi[4 * k + m] = as_h2(w[m]);
+        }
+#pragma unroll
+        for (int a = 0; a < NS / 2; ++a) {
+          const int jb = Gamma<ND>::col(mu, a), ph = Gamma<ND>::phase(mu, a);
+          const int kph = s2pos ? phase_neg(ph) : ph;
+          __half2 h[NC], hs[NC];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            h[c] = proj_h2(psi[a * NC + c], psi[jb * NC + c], kph);
+            hs[c] = __hmul2(__lowhigh2highlow(h[c]), fwd ? sw_f : sw_b);
+          }
+          const int lph = fwd ? phase_neg(phase_conj(ph)) : phase_conj(ph);
+#pragma unroll
+          for (int i = 0; i < NC; ++i) {
+            __half2 t = __float2half2_rn(0.f);
+#pragma unroll
+            for (int j = 0; j < NC; ++j) {
+              const __half2 uu = fwd ? u[i * NC + j] : u[j * NC + i];
+              t = __hfma2(__low2half2(uu), h[j], t);
+              t = __hfma2(__high2half2(uu), hs[j], t);
+            }
+            const float2 tf = __half22float2(t);
+            acc_phase(acc[r][a][i], 0, nrm, nnrm, tf.x, tf.y);
+            acc_phase(acc[r][jb][i], lph, nrm, nnrm, tf.x, tf.y);
+          }
+        }
+      }
+    }
+  }
+}
+
 // The hop of the solver kernels for R right-hand sides at one site: FP32
 // arithmetic (MX = 0, hop_tile), or for FP16 spinors with full links the
-// mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx).
+// mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx) or the
+// packed-half form (MX = 3: half2 FMAs within a direction, hop_tile_h2).
 template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
 LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
                    const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
   if constexpr (MX != 0) {
     static_assert(SP == SP16 && GP == SP16 && !COMP, "the mixed-precision hop takes FP16 spinors and full links");
     static_assert(ND != 3, "the mixed-precision hop has no three-dimensional form");
-    hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+    if constexpr (MX == 3)
+      hop_tile_h2<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+    else
+      hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
   } else {
     hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
   }

@@ -820,13 +820,14 @@ struct CgOps {
 };
 // kernels one iterate() call launches
 constexpr int kLaunchesPerIteration = 5;
-// solver workspaces a gauge object keeps, keyed by (precision, nrhs)
-constexpr size_t kMaxWorkspaces = 4;
+// solver workspaces a gauge object keeps, keyed by (precision, capacity)
+constexpr size_t kMaxWorkspaces = 6;
 
 struct Work {
   lym_gauge* g = nullptr;
   int nrhs = 0, sp = 0, xp = 0;  // nrhs: padded count every field holds
-  int nreal = 0;                 // right-hand sides the caller passes
+  int nreal = 0;                 // right-hand sides the caller passes (this call)
+  int dirty = 0;                 // leading source slots that may hold an earlier call's sources
   int R = 1;                     // right-hand sides per thread in the hop kernels (autotuned)
   int mx = 0;                    // FP16 hop arithmetic: 0 FP32 (hop_tile), 1 mixed (hop_tile_mx)
   bool tuned = false;
@@ -1062,6 +1063,9 @@ static CgOps pick_sp(int sp, bool comp, int mx) {
     case SP32: return comp ? Impl<ND, NC, SP32, true, R, 0>::table() : Impl<ND, NC, SP32, false, R, 0>::table();
     case SP16:
       if constexpr (ND != 3) {
+        if constexpr (R == 1) {
+          if (mx == 3) return Impl<ND, NC, SP16, false, 1, 3>::table();
+        }
         if (mx) return Impl<ND, NC, SP16, false, R, 1>::table();
       }
       return comp ? Impl<ND, NC, SP16, true, R, 0>::table() : Impl<ND, NC, SP16, false, R, 0>::table();
@@ -1081,7 +1085,8 @@ static bool pick_ops_r(int nd, int nc, int sp, bool comp, int mx, CgOps* out) {
   return true;
 }
 
-// mx: the mixed-precision hop (FP16 spinors, full links; f16 x f16 + f32 FMAs)
+// mx: the mixed-precision hops (FP16 spinors, full links): 1 = f16 x f16 + f32 FMAs,
+// 3 = packed half FMAs within a direction (one rhs per thread)
 static bool pick_ops(int nd, int nc, int sp, bool comp, int R, int mx, CgOps* out) {
   if (R == 4) return pick_ops_r<4>(nd, nc, sp, comp, mx, out);
   if (R == 2) return pick_ops_r<2>(nd, nc, sp, comp, mx, out);
@@ -1127,10 +1132,36 @@ static void free_work(Work* w) {
   delete w;
 }
 
+// Workspace capacity for nrhs right-hand sides: 1, 2, then 4, 8, 16, then multiples of
+// 16, so that a handful of workspaces serve every batch size a server forms (the
+// padding rhs get zero sources and finish before the first iteration).
+static int work_capacity(int nrhs) {
+  if (nrhs <= 2) return nrhs;
+  if (nrhs <= 16) {
+    int c = 4;
+    while (c < nrhs) c *= 2;
+    return c;
+  }
+  return (nrhs + 15) / 16 * 16;
+}
+
+// Zero the source slots an earlier call with more right-hand sides left behind
+// (slots nreal .. dirty of the even and odd source fields), on the solve's stream.
+static int clear_stale_sources(Work& w, cudaStream_t st) {
+  if (w.dirty > w.nreal) {
+    const size_t per = (size_t)w.g->ncomp * sizeof(double2) * (size_t)w.Vh;  // one rhs of an FP64 field
+    const size_t off = per * (size_t)w.nreal, len = per * (size_t)(w.dirty - w.nreal);
+    LYM_CUDA(cudaMemsetAsync((char*)w.be.data + off, 0, len, st));
+    LYM_CUDA(cudaMemsetAsync((char*)w.bo.data + off, 0, len, st));
+  }
+  w.dirty = w.nreal;
+  return LYM_OK;
+}
+
 static Work* find_work(lym_gauge* g, int nrhs, int sp) {
   for (size_t i = 0; i < g->works.size(); ++i) {
     Work* w = g->works[i];
-    if (w->nreal == nrhs && w->sp == sp) {
+    if (w->nrhs == nrhs && w->sp == sp) {
       g->works.erase(g->works.begin() + i);  // most recently used first
       g->works.insert(g->works.begin(), w);
       return w;
@@ -1145,8 +1176,10 @@ static void free_all_work(lym_gauge* g) {
 }
 
 static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
-  Work* w = find_work(g, nrhs, sp);
+  const int cap = work_capacity(nrhs);
+  Work* w = find_work(g, cap, sp);
   if (w) {
+    w->nreal = nrhs;
     *out = w;
     return LYM_OK;
   }
@@ -1157,9 +1190,9 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   w = new Work();
   w->g = g;
   w->nreal = nrhs;
-  // pad to a multiple of 4 so the hop kernels can take 1, 2 or 4 rhs per
-  // thread; padding rhs have zero sources and finish before the first iteration
-  nrhs = (sp == SP64 || nrhs <= 2) ? nrhs : (nrhs + 3) / 4 * 4;
+  // the capacity is 1, 2 or a multiple of 4, so the hop kernels can take 1, 2 or 4
+  // rhs per thread; padding rhs have zero sources and finish before the first iteration
+  nrhs = cap;
   w->nrhs = nrhs;
   w->sp = sp;
   w->xp = (sp == SP16 || sp == SPB16) ? SP32 : sp;
@@ -1168,10 +1201,11 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   int nc_ = 0;
   for (int comp = 0; comp < 2; ++comp) {
     if (comp && !(g->comp && sp != SP64)) continue;  // compressed links need SU(N) links and a sloppy precision
-    for (int mx = 0; mx < 2; ++mx) {
-      if (mx && (sp != SP16 || comp || g->nd == 3)) continue;  // the mixed-precision hop: FP16 spinors, full links, 2 or 4 dimensions
+    for (int mx : {0, 1, 3}) {
+      if (mx && (sp != SP16 || comp || g->nd == 3)) continue;  // the mixed-precision hops: FP16 spinors, full links, 2 or 4 dimensions
       for (int R : {1, 2, 4}) {
         if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
+        if (mx == 3 && R != 1) continue;  // the packed-half hop: one rhs per thread
         if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, mx, &w->ops_r[nc_])) {
           delete w;
           set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
@@ -1486,6 +1520,8 @@ static int cg_solve_on(Work& w, lym_gauge* g, double kappa, int nrhs, const void
   EoField none;
 
   // source: b (or gamma_d b for Q x = b) in even-odd form, |b|^2, b' = b_e - kappa H_eo b_o
+  rc = clear_stale_sources(w, st);
+  if (rc) return rc;
   w.ops.to_eo(w, b, prm->hermitian ? 1 : 0, st);
   w.ops.norm64(w, w.be, 0, st);
   w.ops.norm64(w, w.bo, 1, st);
@@ -1976,6 +2012,8 @@ static int cg_solve_multi(int nlat, lym_gauge* const* gs, const double* kappas, 
     w.kappa = kappas[l];
     w.launches = 0;
     const double k = kappas[l];
+    int rz = clear_stale_sources(w, st);
+    if (rz) return rz;
     w.ops.to_eo(w, bs[l], prm->hermitian ? 1 : 0, st);
     w.ops.norm64(w, w.be, 0, st);
     w.ops.norm64(w, w.bo, 1, st);
