@@ -577,9 +577,16 @@ class SolveServer:
         dev = torch.device("cuda", self.device)
         host = not first.on_device
         try:
-            # host sources (the reference-facing path) cross here, on this worker's stream
-            b = torch.cat([(r.source() if r.batched else r.source()[None]).to(dev, non_blocking=True)
-                           for r in batch])
+            # host sources (the reference-facing path) cross here, on this worker's stream,
+            # straight into their slots of the batch's source tensor
+            srcs = [r.source() if r.batched else r.source()[None] for r in batch]
+            b = torch.empty((sum(t.shape[0] for t in srcs),) + tuple(srcs[0].shape[1:]), dtype=srcs[0].dtype,
+                            device=dev)
+            k = 0
+            for t in srcs:
+                b[k:k + t.shape[0]].copy_(t, non_blocking=True)
+                k += t.shape[0]
+            del srcs
             solver = dirac_solver.conjugate_gradient(max_steps=max(r.max_iter for r in batch), tol=first.tol,
                                                      precision=first.precision, **self.solver_options)
             op = g.op_for(widx, first.kappa, first.hermitian)
