@@ -77,6 +77,8 @@ def parse_args():
     ap.add_argument("--trajectories", type=int, default=5)
     ap.add_argument("--hmc-inner", type=int, default=2, help="gauge steps per fermion step of the integrator")
     ap.add_argument("--hmc-outer", type=int, default=10, help="fermion steps per trajectory of the integrator")
+    ap.add_argument("--batch-precision", default="f32", choices=["f32", "f16"],
+                    help="inner precision of --batch-lattices (FP64 reliable updates either way)")
     ap.add_argument("--hmc-precision", default="f64", choices=["f64", "f32", "f16", "bf16"],
                     help="inner precision of the HMC's CG solves (f64: the plain FP64 method)")
     ap.add_argument("--serve-sweep", action="store_true",
@@ -930,7 +932,8 @@ def run_batch_lattices(args, local_rank):
     to 16^3 and 4D SU(3) from 8^4 to 12^3 x 24, kappa in [0.10, 0.14], links
     reunit(exp(i eps H)) with eps in
     [0.1, 0.4] -- with 4 unit complex Gaussian rhs each (256 solves), submitted
-    together to the solve server (4 workers, one CUDA stream each) with FP32 inner
+    together to the solve server (4 workers, one CUDA stream each) with FP32 (or
+    --batch-precision) inner
     and FP64 outer iterations to true relative residual 1e-10; the same 256 solves
     with all lattices of one (D, N) class in the same launches
     (dirac_solver.solve_lattices, two calls).  Then the same 256
@@ -987,10 +990,11 @@ def run_batch_lattices(args, local_rank):
         srv.close()
         return res
 
-    solve_all("f32", 4, 16, args.serve_multi)  # warm-up: workspaces, autotuning, graphs
+    bp = args.batch_precision
+    solve_all(bp, 4, 16, args.serve_multi)  # warm-up: workspaces, autotuning, graphs
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res = solve_all("f32", 4, 16, args.serve_multi)
+    res = solve_all(bp, 4, 16, args.serve_multi)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     ok = sum(r.status == serving.OK for r in res)
@@ -1009,7 +1013,7 @@ def run_batch_lattices(args, local_rank):
         worst_m, launches = 0.0, 0
         for ks in classes.values():
             _, reps = dirac_solver.solve_lattices([ops[k] for k in ks], [sources[k] for k in ks], tol=1e-10,
-                                                  precision="f32", delta=0.01)
+                                                  precision=bp, delta=0.01)
             worst_m = max([worst_m] + [m["true_residual"] for r in reps for m in r])
             launches += reps[0][0]["kernel_launches"]
             ok_m = all(m["status"] == 0 for r in reps for m in r)
@@ -1064,7 +1068,7 @@ def run_batch_lattices(args, local_rank):
                                                          two_launch_ms},
                       "config": {"lattices": "22 x 2D SU(2) 8^2..64^2 + 21 x 3D SU(2) 8^3..16^3 + "
                                                  "21 x 4D SU(3) 8^4..12^3x24",
-                                 "inner_precision": "f32", "outer_precision": "f64", "tol": 1e-10,
+                                 "inner_precision": bp, "outer_precision": "f64", "tol": 1e-10,
                                  "server_workers": 4, "max_batch_rhs": 16,
                                  "server_multi_lattice": args.serve_multi}}), flush=True)
     return 0

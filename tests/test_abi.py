@@ -83,3 +83,19 @@ def test_solver_entry_points_validate_before_any_device_work():
     assert lib.lym_wilson_solve_multi(1, one, k, None, n, one, one, ctypes.byref(zero), reps, None) == \
         _lib.LYM_ERR_BAD_ARG
     assert b"tol" in lib.lym_last_error()
+
+
+def test_multi_lattice_hmc_step_validates_before_any_device_work():
+    """lym_gauge_hmc_step_multi refuses an empty or oversized lattice list and null
+    arrays or entries before reading a lattice or launching anything."""
+    import ctypes
+    lib = _lib.lib()
+    one = (ctypes.c_void_p * 1)(None)
+    nc = (ctypes.c_int * 1)(3)
+    beta = (ctypes.c_double * 1)(5.6)
+    f = lib.lym_gauge_hmc_step_multi
+    assert f(0, one, nc, beta, one, one, 0.1, 0.1, None) == _lib.LYM_ERR_BAD_ARG
+    assert f(257, one, nc, beta, one, one, 0.1, 0.1, None) == _lib.LYM_ERR_BAD_ARG
+    assert f(1, None, nc, beta, one, one, 0.1, 0.1, None) == _lib.LYM_ERR_BAD_ARG
+    assert f(1, one, nc, beta, one, one, 0.1, 0.1, None) == _lib.LYM_ERR_BAD_ARG
+    assert b"lattice 0" in lib.lym_last_error()

@@ -931,6 +931,9 @@ def test_gauge_hmc_step_on_many_lattices_in_two_launches(cuda_device):
     for k in range(len(specs)):
         assert relerr(np_(moms[k]), ref_p[k]) < 1e-13, k
         assert relerr(np_(cfgs[k].gauge_field), ref_u[k]) < 1e-13, k
+    # two lattices on one momenta buffer would race in the same launch: refused
+    with pytest.raises(RuntimeError, match="share a buffer"):
+        hmc.gauge_step_lattices(cfgs[:2], [moms[0], moms[0]], [2.3, 2.3], -0.07, 0.05)
 
 
 def test_md_energy_violation_is_second_order(cuda_device):
