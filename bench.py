@@ -112,6 +112,10 @@ def parse_args():
     ap.add_argument("--serve-max-wait", type=float, default=1.0,
                     help="solve server: requests whose expected wait exceeds this many seconds are rejected "
                          "(overload shedding by latency; <= 0: no limit)")
+    ap.add_argument("--serve-release", default="async", choices=["async", "inline"],
+                    help="solve server: evicted gauge fields released on a background thread or by the worker")
+    ap.add_argument("--serve-plain", type=int, default=1,
+                    help="--serve-sweep: 1 = end with the plain FP64 one-at-a-time pass at the lowest rate")
     ap.add_argument("--serve-multi", type=int, default=1,
                     help="solve server: batches on up to this many different gauge fields of one class run as one "
                          "multi-lattice solve (<= 1: each batch on its own)")
@@ -840,13 +844,13 @@ def _request_specs(rng, n, max_bytes=2 << 30):
 
 
 def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=1,
-           max_queue=None, max_wait_s=None):
+           max_queue=None, max_wait_s=None, release="async"):
     import torch
 
     from tfleonardym_b200 import serving
     srv = serving.SolveServer(budget, max_batch=max_batch, workers=workers, device=dev.index,
                               shifted_precision=shifted_precision, multi_lattice=multi_lattice, max_queue=max_queue,
-                              max_wait_s=max_wait_s)
+                              max_wait_s=max_wait_s, release=release)
     futs = []
     t0 = time.perf_counter()
     for sp, t in zip(specs, times):
@@ -915,12 +919,14 @@ def run_serve_sweep(args, local_rank):
             first = (specs, times)
         max_wait = args.serve_max_wait if args.serve_max_wait > 0 else None
         r = _serve(specs, times, "f16", args.workers, args.nrhs, dev, budget, shifted, args.serve_multi,
-                   args.serve_max_queue, max_wait)
+                   args.serve_max_queue, max_wait, args.serve_release)
         print(json.dumps({"serve_sweep": "mixed", "rate_per_s": rate, "workers": args.workers,
                           "window_s": args.serve_seconds, "max_queue": args.serve_max_queue,
-                          "max_wait_s": max_wait,
+                          "max_wait_s": max_wait, "release": args.serve_release,
                           "max_batch_rhs": args.nrhs, "shifted_solver": args.serve_shifted,
                           "multi_lattice": args.serve_multi, **r}), flush=True)
+    if not args.serve_plain:
+        return 0
     specs, times = first
     r = _serve(specs, times, "f64", 1, 1, dev, budget, None, 1)  # plain: one request at a time, full-lattice multishift
     print(json.dumps({"serve_sweep": "plain_fp64_one_at_a_time", "rate_per_s": rates[0], **r}), flush=True)

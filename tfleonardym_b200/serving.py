@@ -204,7 +204,7 @@ class _Done:
 
 class SolveServer:
     def __init__(self, hbm_budget_bytes, max_batch=16, workers=2, device=None, gauge_cache=8, solver_options=None,
-                 shifted_precision="f64", multi_lattice=1, max_queue=None, max_wait_s=None):
+                 shifted_precision="f64", multi_lattice=1, max_queue=None, max_wait_s=None, release="async"):
         self.solver_options = dict(solver_options or {})  # delta, chunk, rhs_per_thread of the CG
         # shifted requests: a precision = the even-odd multishift (lym_multishift_solve_eo) with that inner
         # precision (FP64 by default: the fastest for the mixed request streams measured); None = the
@@ -248,9 +248,13 @@ class SolveServer:
         self.completed = collections.deque(maxlen=1 << 18)
         if self.device is None and torch.cuda.is_available():
             self.device = torch.cuda.current_device()
-        # evicted gauge fields are destroyed on a thread of their own: releasing a
-        # lym_gauge synchronises the device, which would otherwise stall the worker that
-        # evicted it until every other worker's batch on the GPU had finished
+        # evicted gauge fields are destroyed on a thread of their own (release "async"):
+        # releasing a lym_gauge synchronises the device, which would otherwise stall the
+        # worker that evicted it until every other worker's batch on the GPU had finished;
+        # "inline": the evicting worker releases them itself
+        if release not in ("async", "inline"):
+            raise ValueError("release is 'async' or 'inline'")
+        self.release = release
         self._reap_q = queue.SimpleQueue()
         self._reaper = threading.Thread(target=self._reap, daemon=True)
         self._reaper.start()
@@ -454,7 +458,11 @@ class SolveServer:
                     break
                 evicted.append(self._gauges.pop(k))
         if evicted:
-            self._reap_q.put(evicted)  # destroyed on the reaper thread, not on this worker
+            if self.release == "async":
+                self._reap_q.put(evicted)  # destroyed on the reaper thread, not on this worker
+            else:
+                for e in evicted:
+                    e.release()
         return g
 
     def _run(self, widx):
