@@ -112,7 +112,7 @@ def parse_args():
     ap.add_argument("--serve-max-wait", type=float, default=1.0,
                     help="solve server: requests whose expected wait exceeds this many seconds are rejected "
                          "(overload shedding by latency; <= 0: no limit)")
-    ap.add_argument("--serve-release", default="async", choices=["async", "inline"],
+    ap.add_argument("--serve-release", default="inline", choices=["async", "inline"],
                     help="solve server: evicted gauge fields released on a background thread or by the worker")
     ap.add_argument("--serve-plain", type=int, default=1,
                     help="--serve-sweep: 1 = end with the plain FP64 one-at-a-time pass at the lowest rate")
@@ -844,7 +844,7 @@ def _request_specs(rng, n, max_bytes=2 << 30):
 
 
 def _serve(specs, times, precision, workers, max_batch, dev, budget, shifted_precision="f64", multi_lattice=1,
-           max_queue=None, max_wait_s=None, release="async"):
+           max_queue=None, max_wait_s=None, release="inline"):
     import torch
 
     from tfleonardym_b200 import serving

@@ -1132,17 +1132,15 @@ static void free_work(Work* w) {
   delete w;
 }
 
-// Workspace capacity for nrhs right-hand sides: 1, 2, then 4, 8, 16, then multiples of
-// 16, so that a handful of workspaces serve every batch size a server forms (the
-// padding rhs get zero sources and finish before the first iteration).
-static int work_capacity(int nrhs) {
-  if (nrhs <= 2) return nrhs;
-  if (nrhs <= 16) {
-    int c = 4;
-    while (c < nrhs) c *= 2;
-    return c;
-  }
-  return (nrhs + 15) / 16 * 16;
+// Workspace capacity for nrhs right-hand sides: FP64 exactly nrhs; the sloppy
+// precisions 1, 2, or nrhs rounded up to a multiple of 4 (so the hop kernels can take
+// 1, 2 or 4 rhs per thread).  Batches of 3 and 4 rhs share one workspace, and so on:
+// the padding never exceeds 3 slots (they get zero sources and finish before the first
+// iteration), while a server's varying batch sizes need at most six workspaces per
+// precision up to 16 rhs.
+static int work_capacity(int nrhs, int sp) {
+  if (sp == SP64 || nrhs <= 2) return nrhs;
+  return (nrhs + 3) / 4 * 4;
 }
 
 // Zero the source slots an earlier call with more right-hand sides left behind
@@ -1176,7 +1174,7 @@ static void free_all_work(lym_gauge* g) {
 }
 
 static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
-  const int cap = work_capacity(nrhs);
+  const int cap = work_capacity(nrhs, sp);
   Work* w = find_work(g, cap, sp);
   if (w) {
     w->nreal = nrhs;
