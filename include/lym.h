@@ -162,7 +162,8 @@ typedef struct lym_solver_params {
                         rhs_per_thread = 16): projected FP16 half spinors x FP16 links on
                         mma.sync with FP32 accumulation, 8 sites x 16 rhs per CTA; 3 = the
                         colour contraction of each direction in packed FP16 FMAs (half2),
-                        accumulated over directions in FP32 (rhs_per_thread = 1) */
+                        accumulated over directions in FP32 (rhs_per_thread = 1; only when
+                        asked for: the autotuner does not pick it) */
   double switch_residual; /* lym_multishift_solve_eo with a reduced inner precision: the
                         iterations run in FP64 until the true relative residual of the
                         smallest shift is below this, then in the inner precision
