@@ -98,7 +98,7 @@ def test_overload_sheds_requests_whose_expected_wait_is_too_long():
 
 
 def test_light_load_is_not_shed():
-    """Below the service rate nothing is rejected: the rate the wait is judged by is
+    """Below the service rate nothing is rejected: the rate the wait is measured against is
     requests per second of worker time, not the (low) arrival rate."""
     srv = _FakeServer(hbm_budget_bytes=1 << 40, workers=1, max_wait_s=0.1)  # ~50 requests/s served
     futs = []

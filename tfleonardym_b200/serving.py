@@ -331,7 +331,7 @@ class SolveServer:
     RATE_MIN_REQUESTS = 8
 
     def drain_rate(self):
-        """The service rate the expected wait is judged by (requests per second; None
+        """The service rate the expected wait is measured against (requests per second; None
         while fewer than RATE_MIN_REQUESTS requests finished in the last RATE_WINDOW_S)."""
         with self._lock:
             return self._drain_rate(time.perf_counter())
