@@ -68,7 +68,8 @@ def parse_args():
     ap.add_argument("--compressed-links", type=int, default=0, help="with a forced tile: 1 = N-1-row links")
     ap.add_argument("--mixed-fma", type=int, default=0,
                     help="with a forced tile and f16: 1 = the mixed-precision hop (f16 x f16 + f32 FMAs), "
-                         "2 = the tensor-core hop (--rhs-per-thread 16), 3 = the packed-half hop")
+                         "2 = the tensor-core hop (--rhs-per-thread 16), 3 = the packed-half hop, "
+                         "4 = form 1 with arithmetic neighbours")
     ap.add_argument("--dslash-sweep", action="store_true",
                     help="dslash throughput sweep at 16^4 and 32^4 (one JSON line per case), no solve timing")
     ap.add_argument("--hmc", action="store_true",
@@ -567,7 +568,8 @@ def run_lym(args, rank, world, local_rank):
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = algo_bytes / hop_s / 1e9
     kind = {0: "FP32-arithmetic", 1: "mixed-precision (f16 x f16 + f32 FMA)", 2: "tensor-core (mma.sync f16, f32 accum)",
-            3: "packed-half (half2 FMA per direction, f32 accum)"}
+            3: "packed-half (half2 FMA per direction, f32 accum)",
+            4: "mixed-precision (f16 x f16 + f32 FMA), arithmetic neighbours"}
     traffic = STORED_TRAFFIC.get((args.precision, B, rep0["mixed_fma"], rep0["rhs_per_thread"], comp))
 
     # ---- CPU baseline (rank 0, N = 1 only): the reference's solve path on the host ----
@@ -720,9 +722,10 @@ def run_dslash_sweep(args, local_rank):
                                   "gflops": nvec * vol * (flops_site + 4 * ns * NC) / t / 1e9}), flush=True)
             del x, y
         # (rhs per thread, compressed links, mixed-precision FP16 hop); None: the autotuner's pick
-        # (rhs per CTA, 0, 2): the tensor-core FP16 hop; (1, 0, 3): the packed-half FP16 hop
+        # (rhs per CTA, 0, 2): the tensor-core FP16 hop; (1, 0, 3): the packed-half FP16 hop;
+        # (R, 0, 4): the mixed-precision hop with arithmetic neighbours
         forced = [None, (1, 0, 0), (1, 1, 0), (2, 0, 0), (4, 0, 0), (1, 0, 1), (2, 0, 1), (4, 0, 1),
-                  (4, 0, 2), (8, 0, 2), (16, 0, 2), (1, 0, 3)]
+                  (4, 0, 2), (8, 0, 2), (16, 0, 2), (1, 0, 3), (1, 0, 4), (2, 0, 4), (4, 0, 4)]
         for prec, nrhs in (("f64", 1), ("f32", 1), ("f16", 1), ("f32", 16), ("f16", 16)):
             b = torch.randn((nrhs, ns, NC, vol), dtype=torch.complex128, device=dev)
             tiles = [None]

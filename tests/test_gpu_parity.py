@@ -404,8 +404,10 @@ def test_solve_lattices_together(cuda_device, precision, nd_nc):
                                          ((8, 6), 2), ((12, 4), 3)])
 def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
     """The mixed-precision FP16 hop (half spinor in FP16, U h through
-    f16 x f16 + f32 FMAs) at 1, 2 and 4 rhs per thread meets the true residual
-    in about the iterations of the FP32-arithmetic FP16 hop."""
+    f16 x f16 + f32 FMAs) at 1, 2 and 4 rhs per thread, with neighbour indices from
+    the table (mixed_fma 1) or from coordinate arithmetic (4), meets the true residual
+    in about the iterations of the FP32-arithmetic FP16 hop; both neighbour forms give
+    the same iterates (bit for bit: the same arithmetic on the same neighbours)."""
     from tfleonardym_b200 import boundary_conditions as bcs
     from tfleonardym_b200 import dirac, dirac_solver
     from tfleonardym_b200 import lattice as lt
@@ -423,9 +425,11 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
     ref.solve(op, cu(b))
     assert ref.reports[0]["mixed_fma"] == 0
     base = max(r["iterations"] for r in ref.reports)
-    for arith, tile in ((1, 1), (1, 2), (1, 4)):
+    xs = {}
+    for arith, tile in ((1, 1), (1, 2), (1, 4), (4, 1), (4, 2), (4, 4)):
         mx = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=tile, mixed_fma=arith)
         x = np_(mx.solve(op, cu(b)))
+        xs[(arith, tile)] = x
         rep = mx.reports[0]
         assert rep["mixed_fma"] == arith and rep["rhs_per_thread"] == tile and rep["compressed_links"] == 0, rep
         for i in range(4):
@@ -433,6 +437,8 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
             assert res < 1e-10, (tile, i, res)
         its = max(r["iterations"] for r in mx.reports)
         assert abs(its - base) <= max(3, base // 10), (arith, tile, its, base)
+    for tile in (1, 2, 4):
+        np.testing.assert_array_equal(xs[(1, tile)], xs[(4, tile)])
 
 
 @pytest.mark.parametrize("geometry,nrhs", [((4, 4, 4, 8), 16), ((2, 4, 4, 6), 16), ((6, 4, 2, 4), 32)])

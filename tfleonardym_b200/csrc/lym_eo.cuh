@@ -541,14 +541,19 @@ LYM_D void acc_phase(cx<float>& acc, int k, float s, float ns, float tr, float t
 }
 
 // Same result per site as hop_tile<ND, NC, SP16, SP16, false, G5IN, R> up to
-// the rounding of h; R right-hand sides share each link.
-template <int ND, int NC, bool G5IN, int R>
+// the rounding of h; R right-hand sides share each link.  ARITH: the neighbours'
+// checkerboard indices come from the site's coordinates instead of the neighbour
+// table (no dependent index load per direction; measured faster at 32^4, not at 16^4).
+template <int ND, int NC, bool G5IN, int R, bool ARITH = false>
 LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
                        const int (&act)[R], cx<float> (&acc)[R][Gamma<ND>::NS][NC]) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC, NU = units_for(NCOMP, 4);
   constexpr int NCX = NC * NC, NLU = units_for(NCX, 2);
   const int vh = (int)g.Vh;
   const int* nb = g.nbr + par * 2 * ND * vh + cb;
+  int xc[ND];
+  int lex = 0;
+  if constexpr (ARITH) lex = eo_coords<ND>(g, cb, par, xc);
 #pragma unroll
   for (int r = 0; r < R; ++r)
 #pragma unroll
@@ -562,8 +567,11 @@ LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, i
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
       const bool fwd = dir == 0;
-      const int code = __ldg(nb + (2 * mu + dir) * vh);
-      const int ncb = code & 0x7fffffff;
+      int ncb;
+      if constexpr (ARITH)
+        ncb = (fwd ? nb_fwd<ND>(g, lex, xc, mu) : nb_bwd<ND>(g, lex, xc, mu)) >> 1;
+      else
+        ncb = __ldg(nb + (2 * mu + dir) * vh) & 0x7fffffff;
       // full N x N link, boundary factor folded in; forward link on x (parity
       // par), backward link on x - mu (parity 1-par)
       const uint2* lp = reinterpret_cast<const uint2*>(hg.data) +
@@ -719,8 +727,9 @@ LYM_D void hop_tile_h2(const EoGeom& g, const HopGauge& hg, const EoField& in, i
 
 // The hop of the solver kernels for R right-hand sides at one site: FP32
 // arithmetic (MX = 0, hop_tile), or for FP16 spinors with full links the
-// mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx) or the
-// packed-half form (MX = 3: half2 FMAs within a direction, hop_tile_h2).
+// mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx; MX = 4: the same
+// with neighbour indices from coordinate arithmetic) or the packed-half form (MX = 3:
+// half2 FMAs within a direction, hop_tile_h2).
 template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
 LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
                    const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
@@ -730,7 +739,7 @@ LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int r
     if constexpr (MX == 3)
       hop_tile_h2<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
     else
-      hop_tile_mx<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
+      hop_tile_mx<ND, NC, G5IN, R, MX == 4>(g, hg, in, rhs0, cb, par, act, acc);
   } else {
     hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
   }

@@ -834,7 +834,7 @@ struct Work {
   int tuned_i = 0;
   // hop-kernel candidates: right-hand sides per thread x compressed / full links
   // (x FP32 / mixed-precision arithmetic for FP16)
-  static constexpr int kMaxCand = 13;
+  static constexpr int kMaxCand = 16;
   int ncand = 0, cur = 0;
   int rcand[kMaxCand] = {1};
   bool ccand[kMaxCand] = {};
@@ -1066,6 +1066,7 @@ static CgOps pick_sp(int sp, bool comp, int mx) {
         if constexpr (R == 1) {
           if (mx == 3) return Impl<ND, NC, SP16, false, 1, 3>::table();
         }
+        if (mx == 4) return Impl<ND, NC, SP16, false, R, 4>::table();
         if (mx) return Impl<ND, NC, SP16, false, R, 1>::table();
       }
       return comp ? Impl<ND, NC, SP16, true, R, 0>::table() : Impl<ND, NC, SP16, false, R, 0>::table();
@@ -1086,7 +1087,8 @@ static bool pick_ops_r(int nd, int nc, int sp, bool comp, int mx, CgOps* out) {
 }
 
 // mx: the mixed-precision hops (FP16 spinors, full links): 1 = f16 x f16 + f32 FMAs,
-// 3 = packed half FMAs within a direction (one rhs per thread)
+// 4 = the same with neighbour indices from coordinate arithmetic, 3 = packed half FMAs
+// within a direction (one rhs per thread)
 static bool pick_ops(int nd, int nc, int sp, bool comp, int R, int mx, CgOps* out) {
   if (R == 4) return pick_ops_r<4>(nd, nc, sp, comp, mx, out);
   if (R == 2) return pick_ops_r<2>(nd, nc, sp, comp, mx, out);
@@ -1199,7 +1201,7 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   int nc_ = 0;
   for (int comp = 0; comp < 2; ++comp) {
     if (comp && !(g->comp && sp != SP64)) continue;  // compressed links need SU(N) links and a sloppy precision
-    for (int mx : {0, 1, 3}) {
+    for (int mx : {0, 1, 3, 4}) {
       if (mx && (sp != SP16 || comp || g->nd == 3)) continue;  // the mixed-precision hops: FP16 spinors, full links, 2 or 4 dimensions
       for (int R : {1, 2, 4}) {
         if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
