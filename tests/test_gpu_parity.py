@@ -407,7 +407,8 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
     f16 x f16 + f32 FMAs) at 1, 2 and 4 rhs per thread, with neighbour indices from
     the table (mixed_fma 1) or from coordinate arithmetic (4), meets the true residual
     in about the iterations of the FP32-arithmetic FP16 hop; both neighbour forms give
-    the same iterates (bit for bit: the same arithmetic on the same neighbours)."""
+    the same solutions to the tolerance's scale (the same arithmetic on the same
+    neighbours; the compiler may fuse a multiply-add differently in the two kernels)."""
     from tfleonardym_b200 import boundary_conditions as bcs
     from tfleonardym_b200 import dirac, dirac_solver
     from tfleonardym_b200 import lattice as lt
@@ -438,7 +439,7 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
         its = max(r["iterations"] for r in mx.reports)
         assert abs(its - base) <= max(3, base // 10), (arith, tile, its, base)
     for tile in (1, 2, 4):
-        np.testing.assert_array_equal(xs[(1, tile)], xs[(4, tile)])
+        assert relerr(xs[(4, tile)], xs[(1, tile)]) < 1e-8, tile
 
 
 @pytest.mark.parametrize("geometry,nrhs", [((4, 4, 4, 8), 16), ((2, 4, 4, 6), 16), ((6, 4, 2, 4), 32)])
