@@ -1448,9 +1448,20 @@ static int autotune(Work& w, cudaStream_t st, int forced_rhs, int forced_comp, i
   constexpr int kRounds = 5;
   float times[Work::kMaxCand][kRounds];
   float tbest[Work::kMaxCand];
-  // the packed-half hop (mixed_fma 3) runs only when asked for: its FP16 colour sums
-  // cost iterations at tight tolerances that a dslash timing does not see
-  auto tunable = [&](int i) { return w.mcand[i] != 3; };
+  // Candidates timed: the packed-half hop (mixed_fma 3) and the tensor-core hop (2) run
+  // only when asked for (the first's FP16 colour sums cost iterations at tight
+  // tolerances that a dslash timing does not see; the second never won a measured
+  // workspace).  With FP16 spinors and a mixed-precision form available, the forms that
+  // never won in the tile sweeps at 16^4 and 32^4 (FP32 arithmetic, compressed links,
+  // 4 rhs per thread) are not timed either: every timed candidate costs each new
+  // (geometry, precision, capacity) of a solve server a few dozen dslash launches.
+  bool has_mx = false;
+  for (int i = 0; i < w.ncand; ++i) has_mx = has_mx || w.mcand[i] == 1;
+  auto tunable = [&](int i) {
+    if (w.mcand[i] == 2 || w.mcand[i] == 3) return false;
+    if (w.sp == SP16 && has_mx && (w.mcand[i] == 0 || w.rcand[i] == 4)) return false;
+    return true;
+  };
   for (int round = 0; round < kRounds; ++round) {
     for (int i = 0; i < w.ncand; ++i) {
       if (!tunable(i)) continue;
@@ -1470,9 +1481,10 @@ static int autotune(Work& w, cudaStream_t st, int forced_rhs, int forced_comp, i
     std::sort(times[i], times[i] + kRounds);
     tbest[i] = times[i][kRounds / 2];
   }
-  int bi = 0;
-  for (int i = 1; i < w.ncand; ++i)
-    if (tunable(i) && tbest[i] < tbest[bi]) bi = i;
+  int bi = -1;
+  for (int i = 0; i < w.ncand; ++i)
+    if (tunable(i) && (bi < 0 || tbest[i] < tbest[bi])) bi = i;
+  if (bi < 0) bi = 0;  // nothing timed (cannot happen: the one-rhs form of each precision is timed)
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   LYM_CHECK_LAUNCH();
