@@ -69,7 +69,7 @@ def parse_args():
     ap.add_argument("--mixed-fma", type=int, default=0,
                     help="with a forced tile and f16: 1 = the mixed-precision hop (f16 x f16 + f32 FMAs), "
                          "2 = the tensor-core hop (--rhs-per-thread 16), 3 = the packed-half hop, "
-                         "4 = form 1 with arithmetic neighbours")
+                         "4 = form 1 with arithmetic neighbours, 5 = form 4 with the t neighbours by warp shuffle")
     ap.add_argument("--dslash-sweep", action="store_true",
                     help="dslash throughput sweep at 16^4 and 32^4 (one JSON line per case), no solve timing")
     ap.add_argument("--hmc", action="store_true",
@@ -569,7 +569,8 @@ def run_lym(args, rank, world, local_rank):
     achieved = algo_bytes / hop_s / 1e9
     kind = {0: "FP32-arithmetic", 1: "mixed-precision (f16 x f16 + f32 FMA)", 2: "tensor-core (mma.sync f16, f32 accum)",
             3: "packed-half (half2 FMA per direction, f32 accum)",
-            4: "mixed-precision (f16 x f16 + f32 FMA), arithmetic neighbours"}
+            4: "mixed-precision (f16 x f16 + f32 FMA), arithmetic neighbours",
+            5: "mixed-precision (f16 x f16 + f32 FMA), arithmetic neighbours, t neighbours by warp shuffle"}
     traffic = STORED_TRAFFIC.get((args.precision, B, rep0["mixed_fma"], rep0["rhs_per_thread"], comp))
 
     # ---- CPU baseline (rank 0, N = 1 only): the reference's solve path on the host ----
@@ -725,7 +726,7 @@ def run_dslash_sweep(args, local_rank):
         # (rhs per CTA, 0, 2): the tensor-core FP16 hop; (1, 0, 3): the packed-half FP16 hop;
         # (R, 0, 4): the mixed-precision hop with arithmetic neighbours
         forced = [None, (1, 0, 0), (1, 1, 0), (2, 0, 0), (4, 0, 0), (1, 0, 1), (2, 0, 1), (4, 0, 1),
-                  (4, 0, 2), (8, 0, 2), (16, 0, 2), (1, 0, 3), (1, 0, 4), (2, 0, 4), (4, 0, 4)]
+                  (4, 0, 2), (8, 0, 2), (16, 0, 2), (1, 0, 3), (1, 0, 4), (2, 0, 4), (4, 0, 4), (1, 0, 5), (2, 0, 5)]
         for prec, nrhs in (("f64", 1), ("f32", 1), ("f16", 1), ("f32", 16), ("f16", 16)):
             b = torch.randn((nrhs, ns, NC, vol), dtype=torch.complex128, device=dev)
             tiles = [None]

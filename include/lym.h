@@ -165,7 +165,8 @@ typedef struct lym_solver_params {
                         accumulated over directions in FP32 (rhs_per_thread = 1; only when
                         asked for: the autotuner does not pick it); 4 = form 1 with the
                         neighbours' indices from coordinate arithmetic instead of the
-                        neighbour table */
+                        neighbour table; 5 = form 4 with the +-t neighbours' spinors by warp
+                        shuffle (when Lt/2 is a power of two <= 32 and V/2 a multiple of 32) */
   double switch_residual; /* lym_multishift_solve_eo with a reduced inner precision: the
                         iterations run in FP64 until the true relative residual of the
                         smallest shift is below this, then in the inner precision
@@ -182,7 +183,8 @@ typedef struct lym_solver_report {
                             (the tensor-core hop: right-hand sides per CTA, 16) */
   int compressed_links;  /* 1: the hop kernels read the N-1-row sloppy links, 0: full links */
   int mixed_fma;         /* 1: the hop kernels ran the mixed-precision FP16 form; 2: the tensor-core
-                            form; 3: the packed-half form; 4: form 1 with arithmetic neighbours */
+                            form; 3: the packed-half form; 4: form 1 with arithmetic neighbours;
+                            5: form 4 with the t neighbours by warp shuffle */
 } lym_solver_report;
 
 /* Solve D x_i = b_i (or Q x_i = b_i) for nrhs right-hand sides stored back to

@@ -401,11 +401,12 @@ def test_solve_lattices_together(cuda_device, precision, nd_nc):
 
 
 @pytest.mark.parametrize("geometry,nc", [((4, 4, 4, 8), 3), ((2, 4, 4, 6), 3), ((4, 4, 4, 4), 2),
-                                         ((8, 6), 2), ((12, 4), 3)])
+                                         ((8, 6), 2), ((12, 4), 3), ((4, 4, 2, 16), 3), ((8, 64), 2)])
 def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
     """The mixed-precision FP16 hop (half spinor in FP16, U h through
     f16 x f16 + f32 FMAs) at 1, 2 and 4 rhs per thread, with neighbour indices from
-    the table (mixed_fma 1) or from coordinate arithmetic (4), meets the true residual
+    the table (mixed_fma 1), from coordinate arithmetic (4) or with the t neighbours
+    by warp shuffle (5, where the t rows fill whole warps), meets the true residual
     in about the iterations of the FP32-arithmetic FP16 hop; both neighbour forms give
     the same solutions to the tolerance's scale (the same arithmetic on the same
     neighbours; the compiler may fuse a multiply-add differently in the two kernels)."""
@@ -427,7 +428,11 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
     assert ref.reports[0]["mixed_fma"] == 0
     base = max(r["iterations"] for r in ref.reports)
     xs = {}
-    for arith, tile in ((1, 1), (1, 2), (1, 4), (4, 1), (4, 2), (4, 4)):
+    forms = [(1, 1), (1, 2), (1, 4), (4, 1), (4, 2), (4, 4)]
+    lh, vh = geometry[-1] // 2, int(np.prod(geometry)) // 2
+    if lh <= 32 and lh & (lh - 1) == 0 and vh % 32 == 0:
+        forms += [(5, 1), (5, 2)]  # t neighbours by warp shuffle: full warps, t rows aligned to them
+    for arith, tile in forms:
         mx = dirac_solver.conjugate_gradient(tol=1e-10, precision="f16", rhs_per_thread=tile, mixed_fma=arith)
         x = np_(mx.solve(op, cu(b)))
         xs[(arith, tile)] = x
@@ -440,6 +445,8 @@ def test_eo_cg_mixed_fma_hop(cuda_device, geometry, nc):
         assert abs(its - base) <= max(3, base // 10), (arith, tile, its, base)
     for tile in (1, 2, 4):
         assert relerr(xs[(4, tile)], xs[(1, tile)]) < 1e-8, tile
+        if (5, tile) in xs:
+            assert relerr(xs[(5, tile)], xs[(1, tile)]) < 1e-8, tile
 
 
 @pytest.mark.parametrize("geometry,nrhs", [((4, 4, 4, 8), 16), ((2, 4, 4, 6), 16), ((6, 4, 2, 4), 32)])

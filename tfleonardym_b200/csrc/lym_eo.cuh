@@ -544,13 +544,21 @@ LYM_D void acc_phase(cx<float>& acc, int k, float s, float ns, float tr, float t
 // the rounding of h; R right-hand sides share each link.  ARITH: the neighbours'
 // checkerboard indices come from the site's coordinates instead of the neighbour
 // table (no dependent index load per direction; measured faster at 32^4, not at 16^4).
-template <int ND, int NC, bool G5IN, int R, bool ARITH = false>
+// TSH (with ARITH): the +t and -t neighbours' spinors come from the input field at the
+// site's own checkerboard index, loaded once, and from the neighbouring lane of the same
+// t row by a warp shuffle -- one coalesced load instead of two gathers.  The output site
+// at t = 2 th + o (o = its row's parity offset) has its -t (o = 1) or +t (o = 0)
+// neighbour at its own index th and the other one at th -+ 1 (periodic in the row).
+// Needs every warp full and the rows of Lh = Lt/2 sites aligned to warps: Lh a power of
+// two <= 32 and Vh a multiple of 32 (the host registers the form only then).
+template <int ND, int NC, bool G5IN, int R, bool ARITH = false, bool TSH = false>
 LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
                        const int (&act)[R], cx<float> (&acc)[R][Gamma<ND>::NS][NC]) {
   constexpr int NS = Gamma<ND>::NS, NCOMP = NS * NC, NU = units_for(NCOMP, 4);
   constexpr int NCX = NC * NC, NLU = units_for(NCX, 2);
   const int vh = (int)g.Vh;
   const int* nb = g.nbr + par * 2 * ND * vh + cb;
+  static_assert(!TSH || ARITH, "the t-shuffle form takes the coordinates of the arithmetic form");
   int xc[ND];
   int lex = 0;
   if constexpr (ARITH) lex = eo_coords<ND>(g, cb, par, xc);
@@ -562,16 +570,42 @@ LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, i
       for (int c = 0; c < NC; ++c) acc[r][a][c] = czero<float>();
   const __half2 conj_f = __halves2half2(__float2half_rn(1.f), __float2half_rn(-1.f));
   const __half2 negre_f = __halves2half2(__float2half_rn(-1.f), __float2half_rn(1.f));
+  // t direction by shuffle: the input spinors at the own index, the lanes holding the
+  // row neighbours, and this site's row parity offset
+  uint4 own[R][NU];
+  float own_n[R];
+  int srcf = 0, srcb = 0, lhm = 0;
+  bool odd = false;
+  if constexpr (TSH) {
 #pragma unroll
-  for (int mu = 0; mu < ND; ++mu) {
+    for (int r = 0; r < R; ++r)
+      if (act[r]) own_n[r] = load_sp_units<SP16, NCOMP>(in, rhs0 + r, cb, own[r]);
+    const int lane = (int)(threadIdx.x & 31u);
+    lhm = g.Lh - 1;
+    const int seg = lane & ~lhm;
+    srcf = seg | ((lane + 1) & lhm);
+    srcb = seg | ((lane - 1) & lhm);
+    odd = (xc[ND - 1] & 1) != 0;
+  }
+  // with TSH the t direction (mu = ND - 1) goes first, so the own-index loads die early
+#pragma unroll
+  for (int m = 0; m < ND; ++m) {
+    const int mu = TSH ? (m == 0 ? ND - 1 : m - 1) : m;
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
       const bool fwd = dir == 0;
+      const bool tsh = TSH && mu == ND - 1;
       int ncb;
-      if constexpr (ARITH)
+      if constexpr (TSH) {
+        if (tsh)  // the -t neighbour's index (its link is read there); +t: not needed
+          ncb = (cb & ~lhm) | ((cb - (odd ? 0 : 1)) & lhm);
+        else
+          ncb = (fwd ? nb_fwd<ND>(g, lex, xc, mu) : nb_bwd<ND>(g, lex, xc, mu)) >> 1;
+      } else if constexpr (ARITH) {
         ncb = (fwd ? nb_fwd<ND>(g, lex, xc, mu) : nb_bwd<ND>(g, lex, xc, mu)) >> 1;
-      else
+      } else {
         ncb = __ldg(nb + (2 * mu + dir) * vh) & 0x7fffffff;
+      }
       // full N x N link, boundary factor folded in; forward link on x (parity
       // par), backward link on x - mu (parity 1-par)
       const uint2* lp = reinterpret_cast<const uint2*>(hg.data) +
@@ -588,7 +622,25 @@ LYM_D void hop_tile_mx(const EoGeom& g, const HopGauge& hg, const EoField& in, i
       for (int r = 0; r < R; ++r) {
         if (!act[r]) continue;
         uint4 raw[NU];
-        const float nrm = load_sp_units<SP16, NCOMP>(in, rhs0 + r, ncb, raw);
+        float nrm;
+        if (tsh) {
+          // every lane of the warp takes part (act is uniform over the block)
+          const int src = fwd ? srcf : srcb;
+          const bool mine = fwd ? !odd : odd;
+#pragma unroll
+          for (int k = 0; k < NU; ++k) {
+            uint4 t;
+            t.x = __shfl_sync(0xffffffffu, own[r][k].x, src);
+            t.y = __shfl_sync(0xffffffffu, own[r][k].y, src);
+            t.z = __shfl_sync(0xffffffffu, own[r][k].z, src);
+            t.w = __shfl_sync(0xffffffffu, own[r][k].w, src);
+            raw[k] = mine ? own[r][k] : t;
+          }
+          const float tn = __shfl_sync(0xffffffffu, own_n[r], src);
+          nrm = mine ? own_n[r] : tn;
+        } else {
+          nrm = load_sp_units<SP16, NCOMP>(in, rhs0 + r, ncb, raw);
+        }
         const float nnrm = -nrm;
         __half2 psi[NCOMP];
 #pragma unroll
@@ -728,8 +780,9 @@ LYM_D void hop_tile_h2(const EoGeom& g, const HopGauge& hg, const EoField& in, i
 // The hop of the solver kernels for R right-hand sides at one site: FP32
 // arithmetic (MX = 0, hop_tile), or for FP16 spinors with full links the
 // mixed-precision form (MX = 1: f16 x f16 + f32 FMAs, hop_tile_mx; MX = 4: the same
-// with neighbour indices from coordinate arithmetic) or the packed-half form (MX = 3:
-// half2 FMAs within a direction, hop_tile_h2).
+// with neighbour indices from coordinate arithmetic; MX = 5: that with the t direction
+// by warp shuffle) or the packed-half form (MX = 3: half2 FMAs within a direction,
+// hop_tile_h2).
 template <int ND, int NC, int SP, int GP, bool COMP, bool G5IN, int R, int MX>
 LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int rhs0, int cb, int par,
                    const int (&act)[R], cx<typename Prec<SP>::real> (&acc)[R][Gamma<ND>::NS][NC]) {
@@ -739,7 +792,7 @@ LYM_D void hop_any(const EoGeom& g, const HopGauge& hg, const EoField& in, int r
     if constexpr (MX == 3)
       hop_tile_h2<ND, NC, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
     else
-      hop_tile_mx<ND, NC, G5IN, R, MX == 4>(g, hg, in, rhs0, cb, par, act, acc);
+      hop_tile_mx<ND, NC, G5IN, R, MX == 4 || MX == 5, MX == 5>(g, hg, in, rhs0, cb, par, act, acc);
   } else {
     hop_tile<ND, NC, SP, GP, COMP, G5IN, R>(g, hg, in, rhs0, cb, par, act, acc);
   }

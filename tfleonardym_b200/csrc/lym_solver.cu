@@ -1067,6 +1067,9 @@ static CgOps pick_sp(int sp, bool comp, int mx) {
           if (mx == 3) return Impl<ND, NC, SP16, false, 1, 3>::table();
         }
         if (mx == 4) return Impl<ND, NC, SP16, false, R, 4>::table();
+        if constexpr (R <= 2) {
+          if (mx == 5) return Impl<ND, NC, SP16, false, R, 5>::table();
+        }
         if (mx) return Impl<ND, NC, SP16, false, R, 1>::table();
       }
       return comp ? Impl<ND, NC, SP16, true, R, 0>::table() : Impl<ND, NC, SP16, false, R, 0>::table();
@@ -1087,8 +1090,9 @@ static bool pick_ops_r(int nd, int nc, int sp, bool comp, int mx, CgOps* out) {
 }
 
 // mx: the mixed-precision hops (FP16 spinors, full links): 1 = f16 x f16 + f32 FMAs,
-// 4 = the same with neighbour indices from coordinate arithmetic, 3 = packed half FMAs
-// within a direction (one rhs per thread)
+// 4 = the same with neighbour indices from coordinate arithmetic, 5 = that with the t
+// neighbours by warp shuffle (1 or 2 rhs per thread), 3 = packed half FMAs within a
+// direction (one rhs per thread)
 static bool pick_ops(int nd, int nc, int sp, bool comp, int R, int mx, CgOps* out) {
   if (R == 4) return pick_ops_r<4>(nd, nc, sp, comp, mx, out);
   if (R == 2) return pick_ops_r<2>(nd, nc, sp, comp, mx, out);
@@ -1201,11 +1205,16 @@ static int get_work(lym_gauge* g, int nrhs, int sp, Work** out) {
   int nc_ = 0;
   for (int comp = 0; comp < 2; ++comp) {
     if (comp && !(g->comp && sp != SP64)) continue;  // compressed links need SU(N) links and a sloppy precision
-    for (int mx : {0, 1, 3, 4}) {
+    // the t-shuffle form needs full warps and t rows aligned to them
+    const int lh = g->geom.Lh;
+    const bool tsh_ok = lh >= 1 && lh <= 32 && (lh & (lh - 1)) == 0 && g->Vh % 32 == 0;
+    for (int mx : {0, 1, 3, 4, 5}) {
       if (mx && (sp != SP16 || comp || g->nd == 3)) continue;  // the mixed-precision hops: FP16 spinors, full links, 2 or 4 dimensions
+      if (mx == 5 && !tsh_ok) continue;
       for (int R : {1, 2, 4}) {
         if (nrhs % R != 0 || (sp == SP64 && R > 1)) continue;
         if (mx == 3 && R != 1) continue;  // the packed-half hop: one rhs per thread
+        if (mx == 5 && R > 2) continue;
         if (!pick_ops(g->nd, g->nc, sp, comp != 0, R, mx, &w->ops_r[nc_])) {
           delete w;
           set_error("unsupported (nd=%d, N=%d) for the even-odd solver", g->nd, g->nc);
