@@ -160,7 +160,10 @@ def test_wilson_apply_and_fp16_cg_32x32x32x32_sampled(cuda_device):
     assert relerr(dx, b_host[:, :, sites]) < 1e-9
 
 
-def test_multishift_eo_24x24x24x48_vs_oracle(cuda_device):
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_multishift_eo_24x24x24x48_vs_oracle(cuda_device, precision):
+    """Every shift's oracle Q^2 residual <= 1e-10 (FP16: the mixed-precision hop with
+    arithmetic neighbours, which the multishift takes at this size)."""
     from tfleonardym_b200 import dirac, dirac_solver
     geom = (24, 24, 24, 48)
     u = exp_links(geom, 3, 0.3, 48)
@@ -169,7 +172,7 @@ def test_multishift_eo_24x24x24x48_vs_oracle(cuda_device):
     b = sources(geom, 3, 1, 3)[0]
     op = operator(u, geom, 0.13, True)
     shifts = [0.0001, 0.01, 0.5]
-    ms = dirac_solver.multishift_cg(8000, 1e-10, precision="f32", delta=0.01)
+    ms = dirac_solver.multishift_cg(8000, 1e-10, precision=precision, delta=0.01)
     xs = ms.solve(dirac.SquareOperator(op), cu(b), shifts)
     nb = np.linalg.norm(b)
     for s, xk in zip(shifts, xs):

@@ -816,25 +816,26 @@ struct MsImpl {
 };
 
 // FP64: one group per thread; FP32: R groups per thread, 12-real links when
-// the links allow; FP16: one group per thread, full links, mixed-precision hop;
+// the links allow; FP16: one group per thread, full links, mixed-precision hop
+// (with neighbour indices from coordinate arithmetic on large lattices, arith);
 // BF16: one group per thread, full links (the 16-bit choices are the fastest
 // tiles of the CG's hop sweep)
 template <int ND, int NC, int R>
-static MsOps ms_pick_sp(int sp, bool comp) {
+static MsOps ms_pick_sp(int sp, bool comp, bool arith) {
   switch (sp) {
     case SP64: return MsImpl<ND, NC, SP64, false, 1, 0>::table();
     case SP32: return comp ? MsImpl<ND, NC, SP32, true, R, 0>::table() : MsImpl<ND, NC, SP32, false, R, 0>::table();
-    case SP16: return MsImpl<ND, NC, SP16, false, 1, 1>::table();
+    case SP16: return arith ? MsImpl<ND, NC, SP16, false, 1, 4>::table() : MsImpl<ND, NC, SP16, false, 1, 1>::table();
     default: return MsImpl<ND, NC, SPB16, false, 1, 0>::table();
   }
 }
 
 template <int R>
-static bool ms_pick_r(int nd, int nc, int sp, bool comp, MsOps* out) {
-  if (nd == 2 && nc == 2) *out = ms_pick_sp<2, 2, R>(sp, comp);
-  else if (nd == 2 && nc == 3) *out = ms_pick_sp<2, 3, R>(sp, comp);
-  else if (nd == 4 && nc == 2) *out = ms_pick_sp<4, 2, R>(sp, comp);
-  else if (nd == 4 && nc == 3) *out = ms_pick_sp<4, 3, R>(sp, comp);
+static bool ms_pick_r(int nd, int nc, int sp, bool comp, bool arith, MsOps* out) {
+  if (nd == 2 && nc == 2) *out = ms_pick_sp<2, 2, R>(sp, comp, arith);
+  else if (nd == 2 && nc == 3) *out = ms_pick_sp<2, 3, R>(sp, comp, arith);
+  else if (nd == 4 && nc == 2) *out = ms_pick_sp<4, 2, R>(sp, comp, arith);
+  else if (nd == 4 && nc == 3) *out = ms_pick_sp<4, 3, R>(sp, comp, arith);
   else return false;
   return true;
 }
@@ -945,7 +946,11 @@ static int ms_get(lym_gauge* g, int cap, int S, int sp, int store_rhs, int want_
   w->Vh = g->Vh;
   w->nblk = (int)grid_for(g->Vh, 128);
   w->store_rhs = store_rhs;
-  const bool ok = R == 4 ? ms_pick_r<4>(g->nd, g->nc, sp, comp, &w->ops) : ms_pick_r<1>(g->nd, g->nc, sp, comp, &w->ops);
+  // the CG's tile sweeps: arithmetic neighbours win from 24^3 x 48 (V/2 = 331 776) up,
+  // the neighbour table at 16^4 (V/2 = 32 768)
+  const bool arith = g->Vh >= (int64_t(1) << 17);
+  const bool ok = R == 4 ? ms_pick_r<4>(g->nd, g->nc, sp, comp, arith, &w->ops)
+                         : ms_pick_r<1>(g->nd, g->nc, sp, comp, arith, &w->ops);
   if (!ok) {
     delete w;
     set_error("unsupported (nd=%d, N=%d) for the even-odd multishift", g->nd, g->nc);
